@@ -1,0 +1,39 @@
+"""Writes heat_equation_published.json from the reference's own benchmark report.
+
+The reference publishes, for its heat-equation benchmark, the relative L2 error
+after 10 steps for three ARS schemes at seven timesteps, as literal lists in
+etc/benchmarks/00_heat_equation/error_report.py:4-15.  This script reads that
+file as text (it does not execute it) and stores the numbers, so the tests can
+run where the reference tree is absent.  The analytic stress-free
+Rayleigh-Benard growth rate quoted by benchmark 01
+(etc/benchmarks/01_Rayleigh_Benard_stressFree/benchmark_01_stressfree_rayleigh_benard.ipynb:68)
+is stored beside them.
+
+usage: python tests/golden/extract_published.py <path-to-coral-tree>
+"""
+import ast
+import json
+import os
+import re
+import sys
+
+
+def main(root):
+    src = open(os.path.join(root, "etc/benchmarks/00_heat_equation/error_report.py")).read()
+    out = {"source": "etc/benchmarks/00_heat_equation/error_report.py:4-15"}
+    for name in ("err111", "err222", "err443", "dt"):
+        m = re.search(name + r"\s*=\s*(\[[^\]]*\])", src, re.S)
+        out[name] = ast.literal_eval(m.group(1))
+    nb = open(os.path.join(root, "etc/benchmarks/01_Rayleigh_Benard_stressFree/"
+                                 "benchmark_01_stressfree_rayleigh_benard.ipynb")).read()
+    m = re.search(r"maximum growthrate s = ([0-9.]+)", nb)
+    out["stressfree_rb_max_growthrate"] = float(m.group(1))
+    out["stressfree_rb_source"] = ("etc/benchmarks/01_Rayleigh_Benard_stressFree/"
+                                   "benchmark_01_stressfree_rayleigh_benard.ipynb:68")
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "heat_equation_published.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,110 @@
+"""CPU tests of the oracle against the reference's published numbers and
+analytic results (no GPU needed)."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+import scipy.linalg as sla
+
+from oracle import coral_oracle as co
+from tests.heat_problem import heat_equations, heat_params
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "heat_equation_published.json")))
+CFG = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "coral_b200", "configs")
+
+
+def _heat_error(scheme, dt):
+    """Benchmark 00 protocol: restart divides dt by 50 for the first step
+    (timeKeeping.f90:108), profiles are taken after 9 and 19 steps and the
+    10-step decay of uMean is compared with exp(-Pr*k^2*10*dt)."""
+    s = co.Solver(heat_equations(), heat_params(128, dt, scheme))
+    z = s.g.zgrid()
+    s.set_zero_var_from_phys(0, 0, 1.34e-4 * np.sin(9 * (z - 1) * np.pi / 2))
+    s.set_zero_var_from_phys(1, 0, -2.3e-2 * np.sin(7 * z * np.pi / 2))
+    s.set_zero_var_from_phys(2, 0, np.pi * 1e-3 * np.sin(5 * z * np.pi))
+    s.step(dt / 50)
+    for _ in range(8):
+        s.step(dt)
+    u1 = s.zero_var_profile(0, 0)
+    for _ in range(10):
+        s.step(dt)
+    u2 = s.zero_var_profile(0, 0)
+    rate = 0.33 * (9 * np.pi / 2) ** 2
+    return math.sqrt(np.sum((u2 - u1 * np.exp(-rate * 10 * dt)) ** 2) / np.sum(u1 ** 2))
+
+
+@pytest.mark.parametrize("scheme,key,idx", [
+    ("ARS_222", "err222", 3), ("ARS_222", "err222", 6), ("ARS_111", "err111", 5),
+    ("ARS_443", "err443", 4)])
+def test_heat_equation_published_errors(scheme, key, idx):
+    dt = GOLD["dt"][idx]
+    err = _heat_error(scheme, dt)
+    # the reference prints four significant digits
+    assert err == pytest.approx(GOLD[key][idx], rel=2e-3)
+
+
+def test_stressfree_growth_rate_matches_analytic():
+    eq = open(os.path.join(CFG, "rrbc_stressfree_ek1e-4_ra5e7.equations")).read()
+    eq = eq.replace("5.d7", "2.d3").replace("Prandtl := 1.d0", "Prandtl := 7.d0").replace("iEkman := 1.d4", "iEkman := 0.d0")
+    par = heat_params(24, 1e-3, "ARS_222", NX=12, NY=12).replace("1.0d0", "10.0d0")
+    s = co.Solver(eq, par)
+    Ra, Pr = 2000.0, 7.0
+    best = -1e9
+    for ix, iy in [(3, 0), (2, 3), (3, 1)]:
+        mass, stif = s.kxky_ops[0]
+        cm, cs = s.coef[0]
+        M = sum(c[ix, iy] * B.toarray() for (p, B), c in zip(mass, cm))
+        L = sum(c[ix, iy] * B.toarray() for (p, B), c in zip(stif, cs))
+        w = sla.eigvals(L, M)
+        w = w[np.isfinite(w)]
+        k = math.hypot(s.g.kx[ix], s.g.ky[iy])
+        D2 = k * k + math.pi ** 2
+        an = 0.5 * (-D2 * (Pr + 1) + math.sqrt((Pr + 1) ** 2 * D2 ** 2 - 4 * (Pr * D2 ** 2 - Ra * Pr * k * k / D2)))
+        assert w.real.max() == pytest.approx(an, rel=1e-9, abs=1e-9)
+        best = max(best, an)
+    # the reference's quoted maximum growth rate lies just above the modes probed here
+    assert best < GOLD["stressfree_rb_max_growthrate"] < best + 2.0
+
+
+def test_transform_round_trip_and_single_mode():
+    g = co.Geometry(16, 12, 10, 2.0, 3.0, 1.0, 0.5)
+    rng = np.random.default_rng(0)
+    spec = co.phys_to_spec(rng.standard_normal((g.NYAA, g.NXAA, g.NZAA)), g)
+    spec[:, g.deal_y, :] = 0
+    s2 = co.phys_to_spec(co.spec_to_phys(spec, g), g)
+    assert np.abs(s2 - spec).max() < 1e-14 * np.abs(spec).max()
+    s = np.zeros_like(spec)
+    s[2, 1, 1] = 0.3 + 0.4j
+    p = co.spec_to_phys(s, g)
+    x = np.arange(g.NXAA) * g.Lx / g.NXAA
+    y = np.arange(g.NYAA) * g.Ly / g.NYAA
+    z = np.cos(np.pi * (2 * np.arange(g.NZAA) + 1) / (2 * g.NZAA))
+    ref = 2 * np.real((0.3 + 0.4j) * np.exp(1j * (g.kx[2] * x[None, :, None] + g.ky[1] * y[:, None, None]))) * z
+    assert np.abs(p - ref).max() < 1e-14
+
+
+def test_band_lu_matches_dense_solve():
+    rng = np.random.default_rng(1)
+    n, kl, ku = 40, 3, 5
+    A = np.zeros((n, n), dtype=complex)
+    for d in range(-kl, ku + 1):
+        A += np.diag(rng.standard_normal(n - abs(d)) + 1j * rng.standard_normal(n - abs(d)), d)
+    dia = np.zeros((kl + ku + 1, n), dtype=complex)
+    for i in range(n):
+        for j in range(max(0, i - kl), min(n, i + ku + 1)):
+            dia[ku + i - j, j] = A[i, j]
+    lu, piv = co.zgbtrf_band(dia, kl, ku)
+    b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    x = co.zgbtrs_band(lu, piv, kl, ku, b)
+    assert np.abs(A @ x - b).max() < 1e-12 * np.abs(b).max()
+
+
+def test_rbc_system_band_structure():
+    """The interleaved RBC system is banded with nl=16, nu=27 (ldab=60)."""
+    eq = open(os.path.join(CFG, "rbc_noslip_ra1e5.equations")).read()
+    s = co.Solver(eq, heat_params(48, 1e-4, "ARS_222", NX=8, NY=8))
+    assert s.lay[0].T == 6 * 48 - 8
+    s.factorize(1e-4)
+    assert s.kl_ku[0] == (16, 27)
