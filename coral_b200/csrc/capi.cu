@@ -1,0 +1,962 @@
+// The C-ABI (include/coral_b200.h): a handle owns the parsed problem, the
+// device-resident state, operators, LU factors and transform buffers, one CUDA
+// stream and a CUDA graph of one timestep.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/coral_b200.h"
+#include "device.hpp"
+#include "host.hpp"
+
+using namespace coral;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+#define CK(call)                                                                                   \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      throw CoralError(e_ == cudaErrorMemoryAllocation ? CORAL_ENOMEM : CORAL_ECUDA,               \
+                       std::string(#call) + ": " + cudaGetErrorString(e_));                       \
+  } while (0)
+
+struct DevAlloc {
+  std::vector<void*> ptrs;
+  size_t bytes = 0;
+  template <typename T>
+  T* get(size_t n) {
+    if (n == 0) n = 1;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess)
+      throw CoralError(CORAL_ENOMEM, "device allocation of " + std::to_string(n * sizeof(T)) + " bytes failed: " +
+                                         cudaGetErrorString(e));
+    ptrs.push_back(p);
+    bytes += n * sizeof(T);
+    return static_cast<T*>(p);
+  }
+  template <typename T>
+  T* upload(const std::vector<T>& v) {
+    T* p = get<T>(v.size());
+    if (!v.empty()) CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return p;
+  }
+  void free_all() {
+    for (void* p : ptrs) cudaFree(p);
+    ptrs.clear();
+  }
+};
+
+bool smooth23(int n) {
+  if (n <= 0) return false;
+  while (n % 2 == 0) n /= 2;
+  while (n % 3 == 0) n /= 3;
+  return n == 1;
+}
+
+struct KSys {
+  SystemOps ops;
+  DevEll M, L, NL;
+  int T, kl, ku, ldab;
+  double2 *field, *aux;
+  double2* Kstd[kMaxStages];
+  double2* Khat[kMaxStages];
+  double2* ab;
+  unsigned char* dpiv;
+  int* info;
+  std::vector<std::vector<int>> tab_t;   // per var: [NZ][kTabW]
+  std::vector<std::vector<double>> tab_v;
+  std::vector<int*> d_tab_t;
+  std::vector<double*> d_tab_v;
+  std::vector<int*> d_var_pos;
+  std::vector<int*> d_sq_col;
+  std::vector<double*> d_sq_val;
+};
+
+struct ZSys {
+  SystemOps ops;
+  ZeroSysDev dev;
+  std::vector<std::vector<int>> tab_t;
+  std::vector<std::vector<double>> tab_v;
+  std::vector<int*> d_tab_t;
+  std::vector<double*> d_tab_v;
+};
+
+}  // namespace
+
+struct coral_handle {
+  std::string err;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  Parameters P;
+  Recipe R;
+  std::unique_ptr<Geometry> G;
+  Tableau TB;
+  Dims d;
+  DevAlloc mem;
+  std::vector<KSys> ks;
+  std::vector<ZSys> zs;
+  int nF = 0, nQ = 0, nact = 0;
+  int* d_act_index = nullptr;
+  int* d_act_list = nullptr;
+  double *d_kx = nullptr, *d_ky = nullptr, *d_wz = nullptr;
+  FftPlan py{}, px{}, pz{};
+  double2* dct_tw = nullptr;
+  FullVarDev* d_fv = nullptr;
+  QuadDesc quads{};
+  std::vector<int> zmean_quads;
+  double2 *Y1 = nullptr, *qspec = nullptr, *tmp_spec = nullptr;
+  double *Y2 = nullptr, *fphys = nullptr, *tmp_phys = nullptr;
+  double* ke_partial = nullptr;
+  size_t n_ke_partial = 0;
+  unsigned long long* cfl_bits = nullptr;
+  unsigned int* flags = nullptr;
+  int* zinfo = nullptr;
+  double dt_factored = -1.0;
+  cudaGraphExec_t graph = nullptr;
+  double graph_dt = -1.0;
+  long long launches = 0;
+  int launches_per_step = 0;
+};
+
+namespace {
+
+FftPlan make_plan(DevAlloc& mem, int N) {
+  FftPlan p{};
+  p.N = N;
+  int n = N, s = 0;
+  while (n % 4 == 0) { p.radix[s++] = 4; n /= 4; }
+  while (n % 3 == 0) { p.radix[s++] = 3; n /= 3; }
+  while (n % 2 == 0) { p.radix[s++] = 2; n /= 2; }
+  if (n != 1 || s > 16) throw CoralError(CORAL_EUNSUPPORTED, "transform length " + std::to_string(N) + " is not 2^a 3^b");
+  p.nst = s;
+  std::vector<double2> tw(N);
+  const long double pi = 3.141592653589793238462643383279502884L;
+  for (int k = 0; k < N; ++k) {
+    long double a = -2.0L * pi * (long double)k / (long double)N;
+    tw[k] = make_double2((double)cosl(a), (double)sinl(a));
+  }
+  p.tw = mem.upload(tw);
+  return p;
+}
+
+DevEll upload_ell(DevAlloc& mem, const EllOp& op) {
+  DevEll e{};
+  e.rows = op.rows;
+  e.width = op.width;
+  e.ngroups = (int)op.groups.size();
+  if (e.ngroups > kMaxGroups) throw CoralError(CORAL_EUNSUPPORTED, "too many (kx,ky) monomials in one operator");
+  for (int g = 0; g < e.ngroups; ++g) {
+    e.gkx[g] = op.groups[g].first;
+    e.gky[g] = op.groups[g].second;
+  }
+  e.col = mem.upload(op.col);
+  e.val = mem.upload(op.val);
+  e.grp = mem.upload(op.grp);
+  return e;
+}
+
+// Galerkin -> Chebyshev table of one variable: tab[n][k] = (state index, value)
+void stencil_tab(const SystemOps& o, int v, int NZ, std::vector<int>& tt, std::vector<double>& tv) {
+  tt.assign((size_t)NZ * kTabW, -1);
+  tv.assign((size_t)NZ * kTabW, 0.0);
+  for (int n = 0; n < NZ; ++n) {
+    const auto& row = o.stencil_rows[v][n];
+    if ((int)row.size() > kTabW) throw CoralError(CORAL_EUNSUPPORTED, "stencil row wider than the table");
+    for (size_t k = 0; k < row.size(); ++k) {
+      tt[(size_t)n * kTabW + k] = o.var_pos[v][row[k].first];
+      tv[(size_t)n * kTabW + k] = row[k].second;
+    }
+  }
+}
+
+void setup(coral_handle* h, const std::string& eqs, const std::string& pars, const char* scheme, int device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) throw CoralError(CORAL_ENODEV, "no CUDA device");
+  if (device < 0 || device >= ndev) throw CoralError(CORAL_EBADARG, "device index out of range");
+  h->device = device;
+  CK(cudaSetDevice(device));
+  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  h->P = parse_parameters(pars);
+  h->R = parse_equations(eqs);
+  h->TB = ars_tableau(scheme && *scheme ? std::string(scheme) : h->P.scheme);
+  if (h->TB.stages > kMaxStages) throw CoralError(CORAL_EUNSUPPORTED, "too many implicit stages");
+  const Parameters& P = h->P;
+  if (P.NX % 4 || P.NY % 4 || P.NZ % 4)
+    throw CoralError(CORAL_EUNSUPPORTED, "NX, NY and NZ must be multiples of 4");
+  h->G = std::make_unique<Geometry>(P);
+  const Geometry& g = *h->G;
+  if (!smooth23(g.NXAA) || !smooth23(g.NYAA) || !smooth23(g.NZAA))
+    throw CoralError(CORAL_EUNSUPPORTED, "grid sizes must be of the form 2^a 3^b");
+  h->d = Dims{g.NXH, g.NYAA, g.NXAA, g.NZ, g.NZAA};
+  const Recipe& R = h->R;
+  h->nF = (int)R.full.size();
+  h->nQ = (int)R.quad.size();
+  if (h->nF > kMaxFull || h->nQ > kMaxQuad || R.kxky.size() > (size_t)kMaxSets || R.zero.size() > (size_t)kMaxSets)
+    throw CoralError(CORAL_EUNSUPPORTED, "recipe exceeds the built-in table sizes");
+  DevAlloc& mem = h->mem;
+  const size_t nsys = (size_t)g.NXH * g.NYAA;
+
+  // geometry on the device
+  h->d_kx = mem.upload(g.kx);
+  h->d_ky = mem.upload(g.ky);
+  h->d_wz = mem.upload(g.zweights());
+  std::vector<int> act_index(nsys, -1), act_list;
+  for (int ix = 0; ix < g.NXH; ++ix)
+    for (int iy = 0; iy < g.NYAA; ++iy)
+      if (g.active(ix, iy)) {
+        act_index[(size_t)ix * g.NYAA + iy] = (int)act_list.size();
+        act_list.push_back(ix * g.NYAA + iy);
+      }
+  h->nact = (int)act_list.size();
+  h->d_act_index = mem.upload(act_index);
+  h->d_act_list = mem.upload(act_list);
+
+  // transforms
+  h->py = make_plan(mem, g.NYAA);
+  h->px = make_plan(mem, g.NXAA);
+  h->pz = make_plan(mem, g.NZAA);
+  {
+    std::vector<double2> t(g.NZAA);
+    const long double pi = 3.141592653589793238462643383279502884L;
+    for (int n = 0; n < g.NZAA; ++n) {
+      long double a = -pi * (long double)n / (2.0L * (long double)g.NZAA);
+      t[n] = make_double2((double)cosl(a), (double)sinl(a));
+    }
+    h->dct_tw = mem.upload(t);
+  }
+
+  // coupled kxky systems
+  h->ks.resize(R.kxky.size());
+  for (size_t s = 0; s < R.kxky.size(); ++s) {
+    KSys& k = h->ks[s];
+    k.ops = assemble_system(g, R, R.kxky[s]);
+    k.T = k.ops.T;
+    k.kl = k.ops.kl;
+    k.ku = k.ops.ku;
+    k.ldab = 2 * k.kl + k.ku + 1;
+    if (k.kl > 31 || k.kl + k.ku > 64)
+      throw CoralError(CORAL_EUNSUPPORTED, "band of the coupled system exceeds kl <= 31, kl+ku <= 64");
+    k.M = upload_ell(mem, k.ops.M);
+    k.L = upload_ell(mem, k.ops.L);
+    k.NL = upload_ell(mem, k.ops.NLop);
+    const size_t n = nsys * k.T;
+    k.field = mem.get<double2>(n);
+    k.aux = mem.get<double2>(n);
+    CK(cudaMemset(k.field, 0, n * sizeof(double2)));
+    CK(cudaMemset(k.aux, 0, n * sizeof(double2)));
+    for (int i = 0; i < kMaxStages; ++i) {
+      k.Kstd[i] = (i < h->TB.stages - 1) ? mem.get<double2>(n) : nullptr;
+      k.Khat[i] = (i < h->TB.stages) ? mem.get<double2>(n) : nullptr;
+    }
+    k.ab = mem.get<double2>((size_t)h->nact * k.T * k.ldab);
+    k.dpiv = mem.get<unsigned char>((size_t)h->nact * k.T);
+    k.info = mem.get<int>((size_t)std::max(h->nact, 1));
+    for (int v = 0; v < k.ops.nV; ++v) {
+      std::vector<int> tt;
+      std::vector<double> tv;
+      stencil_tab(k.ops, v, g.NZ, tt, tv);
+      k.tab_t.push_back(tt);
+      k.tab_v.push_back(tv);
+      k.d_tab_t.push_back(mem.upload(tt));
+      k.d_tab_v.push_back(mem.upload(tv));
+      k.d_var_pos.push_back(mem.upload(k.ops.var_pos[v]));
+      // square stencil rows (lower triangular)
+      int nc = k.ops.var_size[v];
+      std::vector<int> sc((size_t)nc * kTabW, -1);
+      std::vector<double> sv((size_t)nc * kTabW, 0.0);
+      for (int r = 0; r < nc; ++r) {
+        int q = 0;
+        for (auto& e : k.ops.stencil_rows[v][r])
+          if (e.first < nc) { sc[(size_t)r * kTabW + q] = e.first; sv[(size_t)r * kTabW + q] = e.second; ++q; }
+      }
+      k.d_sq_col.push_back(mem.upload(sc));
+      k.d_sq_val.push_back(mem.upload(sv));
+    }
+  }
+  // mean systems
+  h->zs.resize(R.zero.size());
+  for (size_t s = 0; s < R.zero.size(); ++s) {
+    ZSys& z = h->zs[s];
+    z.ops = assemble_system(g, R, R.zero[s]);
+    for (auto& gp : z.ops.M.groups)
+      if (gp.first || gp.second) throw CoralError(CORAL_EPARSE, "x/y-derivative in a mean-field recipe");
+    for (auto& gp : z.ops.L.groups)
+      if (gp.first || gp.second) throw CoralError(CORAL_EPARSE, "x/y-derivative in a mean-field recipe");
+    ZeroSysDev& dz = z.dev;
+    dz.T = z.ops.T;
+    dz.kl = z.ops.kl;
+    dz.ku = z.ops.ku;
+    dz.ldab = 2 * dz.kl + dz.ku + 1;
+    dz.M = upload_ell(mem, z.ops.M);
+    dz.L = upload_ell(mem, z.ops.L);
+    dz.NL = upload_ell(mem, z.ops.NLop);
+    dz.field = mem.get<double>(dz.T);
+    dz.aux = mem.get<double>(dz.T);
+    CK(cudaMemset(dz.field, 0, dz.T * sizeof(double)));
+    CK(cudaMemset(dz.aux, 0, dz.T * sizeof(double)));
+    for (int i = 0; i < kMaxStages; ++i) {
+      dz.Kstd[i] = (i < h->TB.stages - 1) ? mem.get<double>(dz.T) : nullptr;
+      dz.Khat[i] = (i < h->TB.stages) ? mem.get<double>(dz.T) : nullptr;
+    }
+    dz.ab = mem.get<double>((size_t)dz.T * dz.ldab);
+    dz.dpiv = mem.get<unsigned char>(dz.T);
+    for (int v = 0; v < z.ops.nV; ++v) {
+      std::vector<int> tt;
+      std::vector<double> tv;
+      stencil_tab(z.ops, v, g.NZ, tt, tv);
+      z.tab_t.push_back(tt);
+      z.tab_v.push_back(tv);
+      z.d_tab_t.push_back(mem.upload(tt));
+      z.d_tab_v.push_back(mem.upload(tv));
+    }
+  }
+  h->zinfo = mem.get<int>(kMaxSets);
+
+  // full variables
+  std::vector<FullVarDev> fv(h->nF);
+  for (int f = 0; f < h->nF; ++f) {
+    const FullVar& F = R.full[f];
+    if (F.terms.size() > (size_t)kMaxFullTerms) throw CoralError(CORAL_EUNSUPPORTED, "too many terms in a full variable");
+    fv[f].nterms = (int)F.terms.size();
+    for (size_t t = 0; t < F.terms.size(); ++t) {
+      const FullTerm& ft = F.terms[t];
+      if (ft.dz != 0 || ft.mz != 0)
+        throw CoralError(CORAL_EUNSUPPORTED, "dz/mz in a full-variable build is not supported by this build");
+      FullTermDev& o = fv[f].term[t];
+      o.zero_kind = ft.zero_kind ? 1 : 0;
+      o.dx = ft.dx;
+      o.dy = ft.dy;
+      o.dsca = ft.dsca;
+      if (ft.zero_kind) {
+        auto loc = R.zero_loc.at(R.zero_vars[ft.var]);
+        o.set = loc.first;
+        o.tab_t = h->zs[loc.first].d_tab_t[loc.second];
+        o.tab_v = h->zs[loc.first].d_tab_v[loc.second];
+      } else {
+        auto it = R.kxky_loc.find(R.kxky_vars[ft.var]);
+        if (it == R.kxky_loc.end()) throw CoralError(CORAL_EPARSE, "kxky variable in no coupled system");
+        o.set = it->second.first;
+        o.tab_t = h->ks[it->second.first].d_tab_t[it->second.second];
+        o.tab_v = h->ks[it->second.first].d_tab_v[it->second.second];
+      }
+    }
+  }
+  h->d_fv = mem.upload(fv);
+  // quadratic variables
+  h->quads.nq = h->nQ;
+  h->quads.ke_q[0] = h->quads.ke_q[1] = h->quads.ke_q[2] = -1;
+  for (int q = 0; q < h->nQ; ++q) {
+    h->quads.v1[q] = R.quad[q].v1;
+    h->quads.v2[q] = R.quad[q].v2;
+    if (R.quad[q].remove_mean) h->zmean_quads.push_back(q);
+    if (R.quad[q].name == "uu") h->quads.ke_q[0] = q;
+    if (R.quad[q].name == "vv") h->quads.ke_q[1] = q;
+    if (R.quad[q].name == "ww") h->quads.ke_q[2] = q;
+  }
+  // transform buffers
+  const int nmax = std::max(std::max(h->nF, h->nQ), 1);
+  h->Y1 = mem.get<double2>((size_t)nmax * g.NYAA * g.NXH * g.NZ);
+  h->Y2 = mem.get<double>((size_t)nmax * g.NYAA * g.NXAA * g.NZ);
+  h->fphys = mem.get<double>((size_t)std::max(h->nF, 1) * g.NYAA * g.NXAA * g.NZAA);
+  h->qspec = mem.get<double2>((size_t)std::max(h->nQ, 1) * nsys * g.NZ);
+  h->tmp_spec = mem.get<double2>(nsys * g.NZ);
+  h->tmp_phys = mem.get<double>((size_t)g.NYAA * g.NXAA * g.NZAA);
+  h->n_ke_partial = (size_t)((g.NXAA + 1) / 2) * g.NYAA * 3;
+  h->ke_partial = mem.get<double>(h->n_ke_partial);
+  CK(cudaMemset(h->ke_partial, 0, h->n_ke_partial * sizeof(double)));
+  h->cfl_bits = mem.get<unsigned long long>(3);
+  CK(cudaMemset(h->cfl_bits, 0, 3 * sizeof(unsigned long long)));
+  h->flags = mem.get<unsigned int>(1);
+  CK(cudaMemset(h->flags, 0, sizeof(unsigned int)));
+  CK(cudaDeviceSynchronize());
+}
+
+StateSet state_set(coral_handle* h, bool use_field) {
+  StateSet st{};
+  for (size_t s = 0; s < h->ks.size(); ++s) {
+    st.k[s] = use_field ? h->ks[s].field : h->ks[s].aux;
+    st.kT[s] = h->ks[s].T;
+  }
+  for (size_t s = 0; s < h->zs.size(); ++s) st.z[s] = use_field ? h->zs[s].dev.field : h->zs[s].dev.aux;
+  return st;
+}
+
+// inverse transforms of all full variables built from field (stage 0) or aux
+int full_vars_to_phys(coral_handle* h, bool use_field, bool cfl) {
+  const Dims& d = h->d;
+  launch_inv_y(d, h->nF, h->d_fv, state_set(h, use_field), nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream);
+  launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream);
+  if (cfl) CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
+  launch_inv_z(d, h->nF, h->Y2, h->fphys, h->pz, h->dct_tw, h->d_wz, cfl ? h->cfl_bits : nullptr, h->stream);
+  return 3;
+}
+
+int enqueue_step(coral_handle* h, double dt) {
+  const Dims& d = h->d;
+  const Geometry& g = *h->G;
+  int nl = 0;
+  const int S = h->TB.stages;
+  const double scale = 1.0 / ((double)g.NXAA * (double)g.NYAA * (double)g.NZAA);
+  for (int i = 0; i < S; ++i) {
+    const bool last = (i == S - 1);
+    nl += full_vars_to_phys(h, i == 0, true);
+    launch_fwd_z(d, h->nF, h->quads, h->fphys, h->Y2, h->pz, h->dct_tw, h->d_wz, i == 0 ? h->ke_partial : nullptr,
+                 h->stream);
+    launch_fwd_x(d, h->nQ, h->Y2, h->Y1, h->px, h->stream);
+    launch_fwd_y(d, h->nQ, h->Y1, h->qspec, scale, h->py, h->stream);
+    nl += 3;
+    for (int q : h->zmean_quads) {
+      launch_remove_zmean(d, h->qspec + (size_t)q * d.NXH * d.NYA * d.NZ, h->stream);
+      ++nl;
+    }
+    for (auto& k : h->ks) {
+      NLArgs na{};
+      na.d = d;
+      na.T = k.T;
+      na.NL = k.NL;
+      na.qspec = h->qspec;
+      na.kx = h->d_kx;
+      na.ky = h->d_ky;
+      na.act_index = h->d_act_index;
+      na.Khat = k.Khat[i];
+      launch_nl(na, h->stream);
+      SolveArgs sa{};
+      sa.d = d;
+      sa.T = k.T;
+      sa.kl = k.kl;
+      sa.ku = k.ku;
+      sa.ldab = k.ldab;
+      sa.M = k.M;
+      sa.L = k.L;
+      sa.field = k.field;
+      sa.out = last ? k.field : k.aux;
+      sa.Kstd_out = last ? nullptr : k.Kstd[i];
+      sa.nprev = i;
+      for (int j = 0; j <= i; ++j) {
+        sa.Kstd[j] = k.Kstd[j];
+        sa.Khat[j] = k.Khat[j];
+        sa.ca[j] = (j < i) ? dt * h->TB.a(i, j) : 0.0;
+        sa.ch[j] = dt * h->TB.ahat(i + 1, j);
+      }
+      sa.ab = k.ab;
+      sa.dpiv = k.dpiv;
+      sa.act_index = h->d_act_index;
+      sa.last_stage = last ? 1 : 0;
+      sa.kx = h->d_kx;
+      sa.ky = h->d_ky;
+      sa.flags = h->flags;
+      launch_solve(sa, h->stream);
+      nl += 2;
+    }
+    if (!h->zs.empty()) {
+      ZeroArgs za{};
+      za.nsys = (int)h->zs.size();
+      for (size_t s = 0; s < h->zs.size(); ++s) za.sys[s] = h->zs[s].dev;
+      za.qspec = h->qspec;
+      za.d = d;
+      za.stage = i;
+      for (int j = 0; j <= i; ++j) {
+        za.ca[j] = (j < i) ? dt * h->TB.a(i, j) : 0.0;
+        za.ch[j] = dt * h->TB.ahat(i + 1, j);
+      }
+      za.last_stage = last ? 1 : 0;
+      launch_zero_step(za, h->stream);
+      ++nl;
+    }
+  }
+  CK(cudaGetLastError());
+  return nl;
+}
+
+void factorize(coral_handle* h, double dt) {
+  const Dims& d = h->d;
+  const double zsca = -dt * h->TB.a(0, 0);
+  for (auto& k : h->ks) {
+    FactorArgs fa{};
+    fa.d = d;
+    fa.T = k.T;
+    fa.kl = k.kl;
+    fa.ku = k.ku;
+    fa.ldab = k.ldab;
+    fa.nact = h->nact;
+    fa.M = k.M;
+    fa.L = k.L;
+    fa.zsca = zsca;
+    fa.act_list = h->d_act_list;
+    fa.ab = k.ab;
+    fa.dpiv = k.dpiv;
+    fa.kx = h->d_kx;
+    fa.ky = h->d_ky;
+    fa.info = k.info;
+    launch_factor(fa, h->stream);
+    ++h->launches;
+  }
+  if (!h->zs.empty()) {
+    ZeroArgs za{};
+    za.nsys = (int)h->zs.size();
+    for (size_t s = 0; s < h->zs.size(); ++s) za.sys[s] = h->zs[s].dev;
+    za.zsca = zsca;
+    za.info = h->zinfo;
+    launch_zero_factor(za, h->stream);
+    ++h->launches;
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(h->stream));
+  for (auto& k : h->ks) {
+    std::vector<int> info(std::max(h->nact, 1));
+    CK(cudaMemcpy(info.data(), k.info, info.size() * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < h->nact; ++i)
+      if (info[i]) throw CoralError(CORAL_ESINGULAR, "zero pivot in the factorisation of a (kx,ky) system");
+  }
+  if (!h->zs.empty()) {
+    std::vector<int> info(kMaxSets);
+    CK(cudaMemcpy(info.data(), h->zinfo, kMaxSets * sizeof(int), cudaMemcpyDeviceToHost));
+    for (size_t s = 0; s < h->zs.size(); ++s)
+      if (info[s]) throw CoralError(CORAL_ESINGULAR, "zero pivot in the factorisation of a mean system");
+  }
+  h->dt_factored = dt;
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+}
+
+void march(coral_handle* h, double dt, int nsteps) {
+  if (!(dt > 0.0) || nsteps < 0) throw CoralError(CORAL_EBADARG, "march: dt must be > 0 and nsteps >= 0");
+  CK(cudaSetDevice(h->device));
+  if (h->dt_factored != dt) factorize(h, dt);
+  int done = 0;
+  if (!h->graph || h->graph_dt != dt) {
+    // one eager step (sets kernel attributes), then capture one step as a graph
+    if (nsteps == 0) return;
+    h->launches_per_step = enqueue_step(h, dt);
+    h->launches += h->launches_per_step;
+    done = 1;
+    if (h->graph) {
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
+    cudaGraph_t gr;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      enqueue_step(h, dt);
+    } catch (...) {
+      cudaStreamEndCapture(h->stream, &gr);
+      throw;
+    }
+    CK(cudaStreamEndCapture(h->stream, &gr));
+    CK(cudaGraphInstantiate(&h->graph, gr, 0));
+    cudaGraphDestroy(gr);
+    h->graph_dt = dt;
+  }
+  for (int s = done; s < nsteps; ++s) {
+    CK(cudaGraphLaunch(h->graph, h->stream));
+    h->launches += h->launches_per_step;
+  }
+}
+
+void check_sys(coral_handle* h, int isys, bool zero) {
+  if (isys < 0 || isys >= (int)(zero ? h->zs.size() : h->ks.size()))
+    throw CoralError(CORAL_EBADARG, "system index out of range");
+}
+
+void spec_to_phys_dev(coral_handle* h, const double2* d_spec, double* d_phys_out) {
+  const Dims& d = h->d;
+  launch_inv_y(d, 1, h->d_fv, StateSet{}, d_spec, h->d_kx, h->d_ky, h->Y1, h->py, h->stream);
+  launch_inv_x(d, 1, h->Y1, h->Y2, h->px, h->stream);
+  launch_inv_z(d, 1, h->Y2, d_phys_out, h->pz, h->dct_tw, h->d_wz, nullptr, h->stream);
+  h->launches += 3;
+}
+
+void phys_to_spec_dev(coral_handle* h, const double* d_phys, double2* d_spec_out) {
+  const Dims& d = h->d;
+  const Geometry& g = *h->G;
+  QuadDesc q{};
+  q.nq = 1;
+  q.v1[0] = 0;
+  q.v2[0] = -1;
+  q.ke_q[0] = q.ke_q[1] = q.ke_q[2] = -1;
+  launch_fwd_z(d, 1, q, d_phys, h->Y2, h->pz, h->dct_tw, h->d_wz, nullptr, h->stream);
+  launch_fwd_x(d, 1, h->Y2, h->Y1, h->px, h->stream);
+  launch_fwd_y(d, 1, h->Y1, d_spec_out, 1.0 / ((double)g.NXAA * g.NYAA * g.NZAA), h->py, h->stream);
+  h->launches += 3;
+}
+
+std::vector<double> read_file(const std::string& fn, size_t n) {
+  std::vector<double> v(n);
+  FILE* f = std::fopen(fn.c_str(), "rb");
+  if (!f) throw CoralError(CORAL_EIO, "cannot open " + fn);
+  size_t r = std::fread(v.data(), sizeof(double), n, f);
+  std::fclose(f);
+  if (r != n) throw CoralError(CORAL_EIO, "short read in " + fn);
+  return v;
+}
+
+void write_file(const std::string& fn, const std::vector<double>& v) {
+  FILE* f = std::fopen(fn.c_str(), "wb");
+  if (!f) throw CoralError(CORAL_EIO, "cannot create " + fn);
+  size_t w = std::fwrite(v.data(), sizeof(double), v.size(), f);
+  std::fclose(f);
+  if (w != v.size()) throw CoralError(CORAL_EIO, "short write in " + fn);
+}
+
+std::string qs_name(const char* dir, const char* kind, int sys, int var, int rolling) {
+  char b[96];
+  std::snprintf(b, sizeof(b), "/QuickSave.%s.sys%03d.var%03d.rolling%d", kind, sys, var, rolling);
+  return std::string(dir) + b;
+}
+
+// mean-profile (NZAA values) <-> Galerkin coefficients of one mean variable, via
+// the (0,0) column of the 3-D transforms
+void import_zero_var(coral_handle* h, ZSys& z, int v, const std::vector<double>& prof) {
+  const Geometry& g = *h->G;
+  std::vector<double> phys((size_t)g.NYAA * g.NXAA * g.NZAA);
+  for (size_t c = 0; c < (size_t)g.NYAA * g.NXAA; ++c)
+    std::memcpy(&phys[c * g.NZAA], prof.data(), g.NZAA * sizeof(double));
+  CK(cudaMemcpyAsync(h->tmp_phys, phys.data(), phys.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  phys_to_spec_dev(h, h->tmp_phys, h->tmp_spec);
+  std::vector<double2> cheb(g.NZ);
+  CK(cudaMemcpyAsync(cheb.data(), h->tmp_spec, g.NZ * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  // forward substitution with the (lower-triangular) square stencil
+  const SystemOps& o = z.ops;
+  const int nc = o.var_size[v];
+  std::vector<double> gal(nc, 0.0);
+  for (int r = 0; r < nc; ++r) {
+    double acc = cheb[r].x, diag = 1.0;
+    for (auto& e : o.stencil_rows[v][r]) {
+      if (e.first == r) diag = e.second;
+      else if (e.first < r) acc -= e.second * gal[e.first];
+    }
+    gal[r] = acc / diag;
+  }
+  std::vector<double> field(o.T);
+  CK(cudaMemcpy(field.data(), z.dev.field, o.T * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int c = 0; c < nc; ++c) field[o.var_pos[v][c]] += gal[c];
+  CK(cudaMemcpy(z.dev.field, field.data(), o.T * sizeof(double), cudaMemcpyHostToDevice));
+}
+
+std::vector<double> export_zero_var(coral_handle* h, ZSys& z, int v) {
+  const Geometry& g = *h->G;
+  const size_t nsys = (size_t)g.NXH * g.NYAA;
+  std::vector<double> field(z.ops.T);
+  CK(cudaMemcpy(field.data(), z.dev.field, z.ops.T * sizeof(double), cudaMemcpyDeviceToHost));
+  std::vector<double2> spec(nsys * g.NZ, make_double2(0.0, 0.0));
+  for (int n = 0; n < g.NZ; ++n) {
+    double s = 0.0;
+    for (int k = 0; k < kTabW; ++k) {
+      int tt = z.tab_t[v][(size_t)n * kTabW + k];
+      if (tt >= 0) s += z.tab_v[v][(size_t)n * kTabW + k] * field[tt];
+    }
+    spec[n] = make_double2(s, 0.0);
+  }
+  CK(cudaMemcpyAsync(h->tmp_spec, spec.data(), spec.size() * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+  spec_to_phys_dev(h, h->tmp_spec, h->tmp_phys);
+  std::vector<double> prof(g.NZAA);
+  CK(cudaMemcpyAsync(prof.data(), h->tmp_phys, g.NZAA * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return prof;
+}
+
+template <typename F>
+int guarded(coral_handle* h, F&& f) {
+  if (!h) return CORAL_EBADARG;
+  try {
+    CK(cudaSetDevice(h->device));
+    f();
+    return CORAL_OK;
+  } catch (const CoralError& e) {
+    h->err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    h->err = e.what();
+    return CORAL_EBADARG;
+  }
+}
+
+std::string slurp(const char* path) {
+  std::ifstream f(path, std::ios::binary);
+  if (!f) throw CoralError(CORAL_EIO, std::string("cannot open ") + path);
+  std::stringstream ss;
+  ss << f.rdbuf();
+  return ss.str();
+}
+
+}  // namespace
+
+extern "C" {
+
+int coral_create(const char* equations_text, const char* parameters_text, const char* scheme, int device,
+                 coral_handle** out) {
+  if (!out || !equations_text || !parameters_text) {
+    g_create_error = "coral_create: null argument";
+    return CORAL_EBADARG;
+  }
+  *out = nullptr;
+  auto* h = new coral_handle();
+  try {
+    setup(h, equations_text, parameters_text, scheme, device);
+  } catch (const CoralError& e) {
+    g_create_error = e.what();
+    h->mem.free_all();
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return e.code;
+  } catch (const std::exception& e) {
+    g_create_error = e.what();
+    h->mem.free_all();
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return CORAL_EBADARG;
+  }
+  *out = h;
+  return CORAL_OK;
+}
+
+int coral_create_from_files(const char* equations_path, const char* parameters_path, const char* scheme, int device,
+                            coral_handle** out) {
+  if (!equations_path || !parameters_path) {
+    g_create_error = "coral_create_from_files: null path";
+    return CORAL_EBADARG;
+  }
+  std::string e, p;
+  try {
+    e = slurp(equations_path);
+    p = slurp(parameters_path);
+  } catch (const CoralError& err) {
+    g_create_error = err.what();
+    return err.code;
+  }
+  return coral_create(e.c_str(), p.c_str(), scheme, device, out);
+}
+
+void coral_destroy(coral_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  h->mem.free_all();
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+const char* coral_last_error(const coral_handle* h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int coral_query(const coral_handle* hc, int what, long long* value) {
+  if (!hc || !value) return CORAL_EBADARG;
+  const coral_handle* h = hc;
+  const Geometry& g = *h->G;
+  switch (what) {
+    case CORAL_Q_NX: *value = g.NX; return 0;
+    case CORAL_Q_NY: *value = g.NY; return 0;
+    case CORAL_Q_NZ: *value = g.NZ; return 0;
+    case CORAL_Q_NXAA: *value = g.NXAA; return 0;
+    case CORAL_Q_NYAA: *value = g.NYAA; return 0;
+    case CORAL_Q_NZAA: *value = g.NZAA; return 0;
+    case CORAL_Q_N_KXKY_SYSTEMS: *value = (long long)h->ks.size(); return 0;
+    case CORAL_Q_N_ZERO_SYSTEMS: *value = (long long)h->zs.size(); return 0;
+    case CORAL_Q_N_FULL_VARS: *value = h->nF; return 0;
+    case CORAL_Q_N_QUAD_VARS: *value = h->nQ; return 0;
+    case CORAL_Q_STAGES: *value = h->TB.stages; return 0;
+    case CORAL_Q_DEVICE_BYTES: *value = (long long)h->mem.bytes; return 0;
+    case CORAL_Q_KERNEL_LAUNCHES: *value = h->launches; return 0;
+    default: break;
+  }
+  int base = (what / 100) * 100, i = what % 100;
+  if (base == CORAL_Q_SYS_T && i < (int)h->ks.size()) { *value = h->ks[i].T; return 0; }
+  if (base == CORAL_Q_ZSYS_T && i < (int)h->zs.size()) { *value = h->zs[i].dev.T; return 0; }
+  if (base == CORAL_Q_SYS_NVARS && i < (int)h->ks.size()) { *value = h->ks[i].ops.nV; return 0; }
+  if (base == CORAL_Q_ZSYS_NVARS && i < (int)h->zs.size()) { *value = h->zs[i].ops.nV; return 0; }
+  if (base == CORAL_Q_SYS_KL && i < (int)h->ks.size()) { *value = h->ks[i].kl; return 0; }
+  if (base == CORAL_Q_SYS_KU && i < (int)h->ks.size()) { *value = h->ks[i].ku; return 0; }
+  return CORAL_EBADARG;
+}
+
+int coral_factorize(coral_handle* h, double dt) {
+  return guarded(h, [&] {
+    if (!(dt > 0.0)) throw CoralError(CORAL_EBADARG, "dt must be > 0");
+    factorize(h, dt);
+  });
+}
+
+int coral_march(coral_handle* h, double dt, int nsteps) { return guarded(h, [&] { march(h, dt, nsteps); }); }
+
+int coral_synchronize(coral_handle* h) {
+  return guarded(h, [&] {
+    CK(cudaStreamSynchronize(h->stream));
+    unsigned int f = 0;
+    CK(cudaMemcpy(&f, h->flags, sizeof(f), cudaMemcpyDeviceToHost));
+    if (f & 1u) throw CoralError(CORAL_ENONFINITE, "non-finite value in the state");
+  });
+}
+
+int coral_get_field(coral_handle* h, int isys, double* field) {
+  return guarded(h, [&] {
+    check_sys(h, isys, false);
+    if (!field) throw CoralError(CORAL_EBADARG, "null buffer");
+    const KSys& k = h->ks[isys];
+    size_t n = (size_t)h->d.NXH * h->d.NYA * k.T;
+    CK(cudaMemcpyAsync(field, k.field, n * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int coral_set_field(coral_handle* h, int isys, const double* field) {
+  return guarded(h, [&] {
+    check_sys(h, isys, false);
+    if (!field) throw CoralError(CORAL_EBADARG, "null buffer");
+    const KSys& k = h->ks[isys];
+    size_t n = (size_t)h->d.NXH * h->d.NYA * k.T;
+    CK(cudaMemcpyAsync(k.field, field, n * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int coral_get_mean_field(coral_handle* h, int isys, double* field) {
+  return guarded(h, [&] {
+    check_sys(h, isys, true);
+    if (!field) throw CoralError(CORAL_EBADARG, "null buffer");
+    const ZSys& z = h->zs[isys];
+    CK(cudaMemcpyAsync(field, z.dev.field, z.dev.T * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int coral_set_mean_field(coral_handle* h, int isys, const double* field) {
+  return guarded(h, [&] {
+    check_sys(h, isys, true);
+    if (!field) throw CoralError(CORAL_EBADARG, "null buffer");
+    const ZSys& z = h->zs[isys];
+    CK(cudaMemcpyAsync(z.dev.field, field, z.dev.T * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int coral_spec_to_phys(coral_handle* h, const double* spec, double* phys) {
+  return guarded(h, [&] {
+    if (!spec || !phys) throw CoralError(CORAL_EBADARG, "null buffer");
+    const Dims& d = h->d;
+    size_t ns = (size_t)d.NXH * d.NYA * d.NZ, np = (size_t)d.NYA * d.NXA * d.NZA;
+    CK(cudaMemcpyAsync(h->tmp_spec, spec, ns * sizeof(double2), cudaMemcpyHostToDevice, h->stream));
+    spec_to_phys_dev(h, h->tmp_spec, h->tmp_phys);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(phys, h->tmp_phys, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int coral_phys_to_spec(coral_handle* h, const double* phys, double* spec) {
+  return guarded(h, [&] {
+    if (!spec || !phys) throw CoralError(CORAL_EBADARG, "null buffer");
+    const Dims& d = h->d;
+    size_t ns = (size_t)d.NXH * d.NYA * d.NZ, np = (size_t)d.NYA * d.NXA * d.NZA;
+    CK(cudaMemcpyAsync(h->tmp_phys, phys, np * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    phys_to_spec_dev(h, h->tmp_phys, h->tmp_spec);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(spec, h->tmp_spec, ns * sizeof(double2), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int coral_get_full_phys(coral_handle* h, int ivar, double* phys) {
+  return guarded(h, [&] {
+    if (ivar < 0 || ivar >= h->nF || !phys) throw CoralError(CORAL_EBADARG, "bad full-variable index or buffer");
+    const Dims& d = h->d;
+    h->launches += full_vars_to_phys(h, true, false);
+    CK(cudaGetLastError());
+    size_t np = (size_t)d.NYA * d.NXA * d.NZA;
+    CK(cudaMemcpyAsync(phys, h->fphys + (size_t)ivar * np, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int coral_import_quicksave(coral_handle* h, const char* directory, int rolling) {
+  return guarded(h, [&] {
+    if (!directory) throw CoralError(CORAL_EBADARG, "null directory");
+    const Dims& d = h->d;
+    const size_t np = (size_t)d.NYA * d.NXA * d.NZA;
+    for (size_t s = 0; s < h->ks.size(); ++s) {
+      KSys& k = h->ks[s];
+      CK(cudaMemsetAsync(k.field, 0, (size_t)d.NXH * d.NYA * k.T * sizeof(double2), h->stream));
+      for (int v = 0; v < k.ops.nV; ++v) {
+        std::vector<double> buf = read_file(qs_name(directory, "kxky", (int)s + 1, v + 1, rolling), np);
+        CK(cudaMemcpyAsync(h->tmp_phys, buf.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+        // file order is z fastest, then y, then x: transpose to (z, x, y)
+        launch_transpose_xy(d, h->tmp_phys, h->fphys, 0, h->stream);
+        phys_to_spec_dev(h, h->fphys, h->tmp_spec);
+        launch_galerkin_insert(d, h->tmp_spec, k.T, k.d_var_pos[v], k.ops.var_size[v], k.d_sq_val[v], k.d_sq_col[v],
+                               k.field, h->stream);
+        h->launches += 2;
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(h->stream));
+      }
+    }
+    for (size_t s = 0; s < h->zs.size(); ++s) {
+      ZSys& z = h->zs[s];
+      CK(cudaMemset(z.dev.field, 0, z.dev.T * sizeof(double)));
+      for (int v = 0; v < z.ops.nV; ++v)
+        import_zero_var(h, z, v, read_file(qs_name(directory, "zero", (int)s + 1, v + 1, rolling), d.NZA));
+    }
+  });
+}
+
+int coral_export_checkpoint(coral_handle* h, const char* directory, int rolling) {
+  return guarded(h, [&] {
+    if (!directory) throw CoralError(CORAL_EBADARG, "null directory");
+    const Dims& d = h->d;
+    const size_t np = (size_t)d.NYA * d.NXA * d.NZA;
+    std::vector<double> buf(np);
+    for (size_t s = 0; s < h->ks.size(); ++s) {
+      KSys& k = h->ks[s];
+      for (int v = 0; v < k.ops.nV; ++v) {
+        launch_cheb_extract(d, k.field, k.T, k.d_tab_t[v], k.d_tab_v[v], h->tmp_spec, h->stream);
+        spec_to_phys_dev(h, h->tmp_spec, h->tmp_phys);
+        launch_transpose_xy(d, h->tmp_phys, h->fphys, 1, h->stream);
+        h->launches += 2;
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(buf.data(), h->fphys, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        write_file(qs_name(directory, "kxky", (int)s + 1, v + 1, rolling), buf);
+      }
+    }
+    for (size_t s = 0; s < h->zs.size(); ++s)
+      for (int v = 0; v < h->zs[s].ops.nV; ++v)
+        write_file(qs_name(directory, "zero", (int)s + 1, v + 1, rolling), export_zero_var(h, h->zs[s], v));
+  });
+}
+
+int coral_diagnostics(coral_handle* h, double* out3) {
+  return guarded(h, [&] {
+    if (!out3) throw CoralError(CORAL_EBADARG, "null buffer");
+    const Geometry& g = *h->G;
+    CK(cudaStreamSynchronize(h->stream));
+    unsigned long long bits[3];
+    CK(cudaMemcpy(bits, h->cfl_bits, sizeof(bits), cudaMemcpyDeviceToHost));
+    double mx[3];
+    for (int i = 0; i < 3; ++i) std::memcpy(&mx[i], &bits[i], sizeof(double));
+    // compute_cfl_based_timestep (marching.f90:219-238), cflFactor_along_z = 1
+    double u = mx[0] * g.NXAA / g.Lx, v = mx[1] * g.NYAA / g.Ly;
+    double w = std::max(v, mx[2]);
+    double m = std::max(u, std::max(v, w));
+    out3[0] = (h->nF >= 3 && m > 0.0) ? 1.0 / m : (h->nF >= 3 ? INFINITY : 1.0);
+    std::vector<double> part(h->n_ke_partial);
+    CK(cudaMemcpy(part.data(), h->ke_partial, part.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    double ke = 0.0;
+    for (size_t i = 0; i < part.size(); ++i) ke += part[i];
+    out3[1] = ke / g.NXAA / g.NYAA;
+    unsigned int f = 0;
+    CK(cudaMemcpy(&f, h->flags, sizeof(f), cudaMemcpyDeviceToHost));
+    out3[2] = (f & 1u) ? 1.0 : 0.0;
+  });
+}
+
+}  // extern "C"

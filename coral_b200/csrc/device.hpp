@@ -1,0 +1,157 @@
+// Device-side descriptions (plain structs passed by value to kernels) and the
+// launchers of the kernels in kernels.cu.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "fft.cuh"
+
+namespace coral {
+
+constexpr int kMaxGroups = 8;   // monomial groups (i kx)^a (i ky)^b per operator
+constexpr int kMaxStages = 4;   // ARS_443 has 4 implicit stages
+constexpr int kMaxSets = 8;     // coupled systems of one kind
+constexpr int kMaxQuad = 16;    // quadratic variables
+constexpr int kMaxFull = 8;     // full variables
+constexpr int kMaxFullTerms = 8;
+constexpr int kTabW = 5;        // Galerkin -> Chebyshev entries per Chebyshev row
+
+// Row-list operator: y[r] = sum_k coef[grp[r,k]] * val[r,k] * x[col[r,k]]
+struct DevEll {
+  int rows, width, ngroups;
+  int gkx[kMaxGroups], gky[kMaxGroups];
+  const int* col;
+  const double* val;
+  const int* grp;
+};
+
+// one term of a full variable build: dsca * (i kx)^dx (i ky)^dy * S_var g
+struct FullTermDev {
+  int zero_kind;  // 1: mean variable (adds to the (0,0) mode only)
+  int set;        // coupled system index
+  int dx, dy;
+  double dsca;
+  const int* tab_t;      // [NZ][kTabW] state index or -1
+  const double* tab_v;   // [NZ][kTabW] stencil value
+};
+struct FullVarDev {
+  int nterms;
+  FullTermDev term[kMaxFullTerms];
+};
+
+struct StateSet {  // pointers of the coupled kxky systems for the full-variable build
+  const double2* k[kMaxSets];
+  int kT[kMaxSets];
+  const double* z[kMaxSets];
+};
+
+struct QuadDesc {
+  int nq;
+  int v1[kMaxQuad], v2[kMaxQuad];
+  int ke_q[3];  // quadratic variables whose volume averages form KE (uu, vv, ww), -1 if absent
+};
+
+struct Dims {
+  int NXH, NYA, NXA, NZ, NZA;
+};
+
+// ---- launchers (kernels.cu) -------------------------------------------------
+// inverse transform of nf scalars: spectral build (or a plain spec input) + y-FFT
+void launch_inv_y(const Dims& d, int nf, const FullVarDev* fv, StateSet st, const double2* plain_spec,
+                  const double* kx, const double* ky, double2* Y1, const FftPlan& py, cudaStream_t s);
+void launch_inv_x(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s);
+// z DCT-III; cfl: maxima of |u|, |v|, |w|/wz written (as uint64 bit patterns) to cfl_bits when non-null
+void launch_inv_z(const Dims& d, int nf, const double* Y2, double* phys, const FftPlan& pz,
+                  const double2* dct_tw, const double* wz, unsigned long long* cfl_bits, cudaStream_t s);
+void launch_fwd_z(const Dims& d, int nf, const QuadDesc& q, const double* phys, double* Q2, const FftPlan& pz,
+                  const double2* dct_tw, const double* wz, double* ke_partial, cudaStream_t s);
+void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s);
+void launch_fwd_y(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
+                  cudaStream_t s);
+void launch_remove_zmean(const Dims& d, double2* qspec_q, cudaStream_t s);
+
+struct NLArgs {
+  Dims d;
+  int T;
+  DevEll NL;
+  const double2* qspec;
+  const double* kx;
+  const double* ky;
+  const int* act_index;  // [kx*NYA+ky] -> factor slot, -1 for dealiased modes and (0,0)
+  double2* Khat;
+};
+void launch_nl(const NLArgs& a, cudaStream_t s);
+
+struct SolveArgs {
+  Dims d;
+  int T, kl, ku, ldab;
+  DevEll M, L;
+  const double2* field;
+  double2* out;          // aux (or field itself in the last stage)
+  double2* Kstd_out;     // null in the last stage
+  int nprev;             // stage index i (0-based): Kstd[0..i-1], Khat[0..i]
+  const double2* Kstd[kMaxStages];
+  const double2* Khat[kMaxStages];
+  double ca[kMaxStages];  // dt * a(i, j)
+  double ch[kMaxStages];  // dt * ahat(i+1, j)
+  const double2* ab;
+  const unsigned char* dpiv;
+  const int* act_index;
+  int last_stage;
+  const double* kx;
+  const double* ky;
+  unsigned int* flags;   // bit 0: non-finite value produced
+};
+void launch_solve(const SolveArgs& a, cudaStream_t s);
+
+struct FactorArgs {
+  Dims d;
+  int T, kl, ku, ldab, nact;
+  DevEll M, L;
+  double zsca;           // -dt * a(0,0)
+  const int* act_list;   // [nact] kx*NYA+ky
+  double2* ab;
+  unsigned char* dpiv;
+  const double* kx;
+  const double* ky;
+  int* info;             // first zero pivot (1-based column) per system, 0 if none
+};
+void launch_factor(const FactorArgs& a, cudaStream_t s);
+
+// mean (kx = ky = 0) systems, real arithmetic
+struct ZeroSysDev {
+  int T, kl, ku, ldab;
+  DevEll M, L, NL;
+  double* field;
+  double* aux;
+  double* Kstd[kMaxStages];
+  double* Khat[kMaxStages];
+  double* ab;
+  unsigned char* dpiv;
+};
+struct ZeroArgs {
+  int nsys;
+  ZeroSysDev sys[kMaxSets];
+  const double2* qspec;  // [q][kx][ky][n]; the (0,0) column is read
+  Dims d;
+  int stage;
+  double ca[kMaxStages], ch[kMaxStages];
+  int last_stage;
+  double zsca;
+  int* info;
+};
+void launch_zero_step(const ZeroArgs& a, cudaStream_t s);
+void launch_zero_factor(const ZeroArgs& a, cudaStream_t s);
+
+// QuickSave helpers
+void launch_transpose_xy(const Dims& d, const double* in, double* out, int to_file_order, cudaStream_t s);
+// project Chebyshev coefficients spec[kx][ky][n] onto the Galerkin basis of one
+// variable (lower-triangular square stencil) and add them into the state
+void launch_galerkin_insert(const Dims& d, const double2* spec, int T, const int* var_pos, int nc,
+                            const double* sq /*nc x kTabW band, row-major*/, const int* sq_off,
+                            double2* field, cudaStream_t s);
+void launch_cheb_extract(const Dims& d, const double2* field, int T, const int* tab_t, const double* tab_v,
+                         double2* spec, cudaStream_t s);
+void launch_check_finite(const double2* x, size_t n, unsigned int* flags, cudaStream_t s);
+
+}  // namespace coral

@@ -1,0 +1,920 @@
+// CUDA kernels (sm_100a, FP64) of the plane-layer IMEX timestep.
+//
+// Layouts (first index slowest, C order), identical in memory to the
+// reference's Fortran arrays:
+//   state       field[kx][ky][t]          (Fortran field(T, NYAA, NX/2))
+//   spectral    spec [kx][ky][n]          (Fortran spec(NZ, NYAA, NX/2))
+//   physical    phys [y][x][z]            (Fortran phys(NZAA, NXAA, NYAA))
+// Transform intermediates (this build's own choice):
+//   Y1 / Q1     [var][y][kx][n]  complex  (after the y transform / before it)
+//   Y2 / Q2     [var][y][x][n]   real     (after the x transform / before it)
+// The x<->y exchange of the reference's slab decomposition
+// (src/slabs.fftw3mpi/domain_decomposition.f90:152-183) is the change of
+// layout between the y pass and the x pass, done in shared memory.
+#include <cstdio>
+
+#include "device.hpp"
+
+namespace coral {
+
+namespace {
+
+constexpr int kNB1 = 4;  // n lines per CTA, inverse / forward y pass
+constexpr int kNB2 = 8;  // n lines per CTA, x passes (packed in pairs)
+constexpr int kXB3 = 8;  // x columns per CTA, inverse z pass (packed in pairs)
+constexpr int kThreads = 256;
+constexpr int kWPB = 8;  // warps (systems) per CTA in the per-system kernels
+
+__device__ __forceinline__ double2 zero2() { return make_double2(0.0, 0.0); }
+
+__device__ __forceinline__ double2 ipow(double k, int e) {
+  // (i k)^e by repeated multiplication, as Fortran's complex**integer
+  double2 r = make_double2(1.0, 0.0);
+  double2 z = make_double2(0.0, k);
+  for (int q = 0; q < e; ++q) r = cmul(r, z);
+  return r;
+}
+
+// ------------------------------------------------------------------------------
+// inverse transform, pass 1: spectral build of the full variables + y c2c (e^{+i})
+// (compute_full_variables_in_physical_space, marching.f90:436-503, then
+//  c2r_transform steps 1-2 and the 0.5 of the x padding, transforms.f90:172-198)
+// ------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_inv_y(Dims d, const FullVarDev* fv, StateSet st,
+                                                     const double2* plain_spec, const double* kxv,
+                                                     const double* kyv, double2* Y1, FftPlan py) {
+  extern __shared__ double2 sm[];
+  const int f = blockIdx.x, n0 = blockIdx.y * kNB1, kx = blockIdx.z;
+  const int NYA = d.NYA;
+  double2* A = sm;
+  double2* B = sm + kNB1 * NYA;
+  for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
+    const int ln = idx % kNB1, iy = idx / kNB1, n = n0 + ln;
+    double2 c = zero2();
+    if (n < d.NZ) {
+      if (plain_spec) {
+        c = plain_spec[((size_t)kx * NYA + iy) * d.NZ + n];
+      } else {
+        const FullVarDev& v = fv[f];
+        for (int t = 0; t < v.nterms; ++t) {
+          const FullTermDev& ft = v.term[t];
+          if (ft.zero_kind) {
+            if (kx == 0 && iy == 0) {
+              const double* zs = st.z[ft.set];
+              double s = 0.0;
+              for (int k = 0; k < kTabW; ++k) {
+                int tt = ft.tab_t[n * kTabW + k];
+                if (tt >= 0) s += ft.tab_v[n * kTabW + k] * zs[tt];
+              }
+              c.x += s * ft.dsca;
+            }
+          } else {
+            const double2* sv = st.k[ft.set] + ((size_t)kx * NYA + iy) * st.kT[ft.set];
+            double2 s = zero2();
+            for (int k = 0; k < kTabW; ++k) {
+              int tt = ft.tab_t[n * kTabW + k];
+              if (tt >= 0) {
+                double w = ft.tab_v[n * kTabW + k];
+                double2 x = sv[tt];
+                s.x += w * x.x;
+                s.y += w * x.y;
+              }
+            }
+            s = cscale(s, ft.dsca);
+            if (ft.dx || ft.dy) s = cmul(cmul(s, ipow(kxv[kx], ft.dx)), ipow(kyv[iy], ft.dy));
+            c = cadd(c, s);
+          }
+        }
+      }
+    }
+    A[ln * NYA + iy] = c;
+  }
+  __syncthreads();
+  const double2* R = fft_lines<true>(A, B, kNB1, py);
+  for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
+    const int ln = idx % kNB1, y = idx / kNB1, n = n0 + ln;
+    if (n < d.NZ) {
+      const double s = (n == 0) ? 1.0 : 0.5;  // (x2 on Chebyshev index 0) * (0.5 of the x padding)
+      Y1[(((size_t)f * NYA + y) * d.NXH + kx) * d.NZ + n] = cscale(R[ln * NYA + y], s);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------
+// inverse transform, pass 2: x c2r with zero padding NX/2 -> NXAA (transforms.f90:197-210)
+// two real output lines per complex FFT
+// ------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_inv_x(Dims d, const double2* Y1, double* Y2, FftPlan px) {
+  extern __shared__ double2 sm[];
+  const int f = blockIdx.x, n0 = blockIdx.y * kNB2, y = blockIdx.z;
+  const int NXA = d.NXA, NP = kNB2 / 2;
+  double2* A = sm;
+  double2* B = sm + NP * NXA;
+  for (int idx = threadIdx.x; idx < NP * NXA; idx += blockDim.x) A[idx] = zero2();
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < NP * d.NXH; idx += blockDim.x) {
+    const int m = idx % NP, kx = idx / NP, na = n0 + 2 * m;
+    const double2* src = Y1 + (((size_t)f * d.NYA + y) * d.NXH + kx) * d.NZ;
+    double2 a = (na < d.NZ) ? src[na] : zero2();
+    double2 b = (na + 1 < d.NZ) ? src[na + 1] : zero2();
+    if (kx == 0) {
+      A[m * NXA] = make_double2(a.x, b.x);  // c2r reads only the real part of the DC term
+    } else {
+      A[m * NXA + kx] = make_double2(a.x - b.y, a.y + b.x);        // a + i b
+      A[m * NXA + NXA - kx] = make_double2(a.x + b.y, b.x - a.y);  // conj(a) + i conj(b)
+    }
+  }
+  __syncthreads();
+  const double2* R = fft_lines<true>(A, B, NP, px);
+  for (int idx = threadIdx.x; idx < NP * NXA; idx += blockDim.x) {
+    const int m = idx % NP, x = idx / NP, na = n0 + 2 * m;
+    double2 z = R[m * NXA + x];
+    double* dst = Y2 + (((size_t)f * d.NYA + y) * NXA + x) * d.NZ;
+    if (na < d.NZ) dst[na] = z.x;
+    if (na + 1 < d.NZ) dst[na + 1] = z.y;
+  }
+}
+
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {
+  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+// ------------------------------------------------------------------------------
+// inverse transform, pass 3: z REDFT01 with zero padding NZ -> NZAA (transforms.f90:216-223)
+// via an NZAA-point complex FFT (two columns per FFT); also the CFL maxima of
+// compute_cfl_based_timestep (marching.f90:219-238) for the first three full variables
+// ------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_inv_z(Dims d, const double* Y2, double* phys, FftPlan pz,
+                                                     const double2* dct_tw, const double* wz,
+                                                     unsigned long long* cfl_bits) {
+  extern __shared__ double2 sm[];
+  __shared__ double red[kThreads / 32];
+  const int f = blockIdx.x, x0 = blockIdx.y * kXB3, y = blockIdx.z;
+  const int N = d.NZA, NP = kXB3 / 2;
+  double2* A = sm;
+  double2* B = sm + NP * N;
+  for (int idx = threadIdx.x; idx < NP * N; idx += blockDim.x) {
+    const int m = idx / N, n = idx - m * N;
+    const int xa = x0 + 2 * m, xb = xa + 1;
+    const double* sa = Y2 + (((size_t)f * d.NYA + y) * d.NXA + xa) * d.NZ;
+    const double* sb = sa + d.NZ;
+    double a0 = 0, a1 = 0, b0 = 0, b1 = 0;  // X_n, X_{N-n}
+    if (xa < d.NXA) {
+      if (n < d.NZ) a0 = sa[n];
+      if (n > 0 && N - n < d.NZ) a1 = sa[N - n];
+    }
+    if (xb < d.NXA) {
+      if (n < d.NZ) b0 = sb[n];
+      if (n > 0 && N - n < d.NZ) b1 = sb[N - n];
+    }
+    const double2 w = cconj(dct_tw[n]);  // exp(+i pi n / 2N)
+    double2 va = cmul(w, make_double2(a0, -a1));
+    double2 vb = cmul(w, make_double2(b0, -b1));
+    A[m * N + n] = make_double2(va.x - vb.y, va.y + vb.x);  // va + i vb
+  }
+  __syncthreads();
+  const double2* R = fft_lines<true>(A, B, NP, pz);
+  double mx = 0.0;
+  const int which = (f < 3) ? f : -1;
+  for (int idx = threadIdx.x; idx < NP * N; idx += blockDim.x) {
+    const int m = idx / N, k = idx - m * N;
+    const int xa = x0 + 2 * m, xb = xa + 1;
+    const int zi = (k & 1) ? (N - 1 - (k >> 1)) : (k >> 1);
+    const double2 z = R[m * N + zi];
+    double* dst = phys + (((size_t)f * d.NYA + y) * d.NXA + xa) * N;
+    if (xa < d.NXA) dst[k] = z.x;
+    if (xb < d.NXA) dst[N + k] = z.y;
+    if (which >= 0) {
+      double s = (which == 2) ? 1.0 / wz[k] : 1.0;
+      if (xa < d.NXA) mx = fmax(mx, fabs(z.x) * s);
+      if (xb < d.NXA) mx = fmax(mx, fabs(z.y) * s);
+    }
+  }
+  if (cfl_bits && which >= 0) {
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m2 = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m2 = fmax(m2, red[w]);
+      atomic_max_nonneg(cfl_bits + which, m2);
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------
+// forward transform, pass 1: pointwise products (marching.f90:279-291) + z REDFT10
+// truncated to NZ (transforms.f90:243-249), for all quadratic variables of one
+// pair of x columns; also partial volume averages for KE (output.f90:84-102)
+// ------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_fwd_z(Dims d, int nf, QuadDesc q, const double* phys, double* Q2,
+                                                     FftPlan pz, const double2* dct_tw, const double* wz,
+                                                     double* ke_partial) {
+  extern __shared__ double2 sm[];
+  __shared__ double red[3][kThreads / 32];
+  const int x0 = blockIdx.x * 2, y = blockIdx.y;
+  const int N = d.NZA, nq = q.nq;
+  double* P = reinterpret_cast<double*>(sm);  // [nf][2][N]
+  double2* A = sm + nf * N;                    // nq lines
+  double2* B = A + nq * N;
+  for (int idx = threadIdx.x; idx < nf * 2 * N; idx += blockDim.x) {
+    const int fv = idx / (2 * N), r = idx - fv * 2 * N;
+    const int xc = x0 + r / N, z = r % N;
+    P[idx] = (xc < d.NXA) ? phys[(((size_t)fv * d.NYA + y) * d.NXA + xc) * N + z] : 0.0;
+  }
+  __syncthreads();
+  double ke[3] = {0.0, 0.0, 0.0};
+  for (int idx = threadIdx.x; idx < nq * N; idx += blockDim.x) {
+    const int qi = idx / N, m = idx - qi * N;
+    const int z = (m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1;  // Makhoul reordering
+    const int v1 = q.v1[qi], v2 = q.v2[qi];
+    double pa, pb;
+    if (v1 < 0) { pa = P[(v2 * 2) * N + z]; pb = P[(v2 * 2 + 1) * N + z]; }
+    else if (v2 < 0) { pa = P[(v1 * 2) * N + z]; pb = P[(v1 * 2 + 1) * N + z]; }
+    else {
+      pa = P[(v1 * 2) * N + z] * P[(v2 * 2) * N + z];
+      pb = P[(v1 * 2 + 1) * N + z] * P[(v2 * 2 + 1) * N + z];
+    }
+    A[qi * N + m] = make_double2(pa, pb);
+    if (ke_partial) {
+      for (int j = 0; j < 3; ++j)
+        if (q.ke_q[j] == qi) ke[j] += wz[z] * (pa + ((x0 + 1 < d.NXA) ? pb : 0.0));
+    }
+  }
+  __syncthreads();
+  const double2* R = fft_lines<false>(A, B, nq, pz);
+  for (int idx = threadIdx.x; idx < nq * d.NZ; idx += blockDim.x) {
+    const int qi = idx / d.NZ, n = idx - qi * d.NZ;
+    const double2 Z = R[qi * N + n];
+    const double2 Zc = cconj(R[qi * N + ((N - n) % N)]);
+    const double2 va = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
+    const double2 dd = csub(Z, Zc);
+    const double2 vb = make_double2(0.5 * dd.y, -0.5 * dd.x);  // (Z - Zc) / 2i
+    const double2 w = dct_tw[n];                                // exp(-i pi n / 2N)
+    const double xa = 2.0 * (w.x * va.x - w.y * va.y);
+    const double xb = 2.0 * (w.x * vb.x - w.y * vb.y);
+    double* dst = Q2 + (((size_t)qi * d.NYA + y) * d.NXA + x0) * d.NZ;
+    dst[n] = xa;
+    if (x0 + 1 < d.NXA) dst[d.NZ + n] = xb;
+  }
+  if (ke_partial) {
+    for (int j = 0; j < 3; ++j) {
+      double v = ke[j];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if ((threadIdx.x & 31) == 0) red[j][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+      double s = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
+      ke_partial[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 3 + threadIdx.x] = s;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------
+// forward transform, pass 2: x r2c, keep kx < NX/2 (transforms.f90:255-267)
+// ------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_fwd_x(Dims d, const double* Q2, double2* Q1, FftPlan px) {
+  extern __shared__ double2 sm[];
+  const int qi = blockIdx.x, n0 = blockIdx.y * kNB2, y = blockIdx.z;
+  const int NXA = d.NXA, NP = kNB2 / 2;
+  double2* A = sm;
+  double2* B = sm + NP * NXA;
+  for (int idx = threadIdx.x; idx < NP * NXA; idx += blockDim.x) {
+    const int m = idx % NP, x = idx / NP, na = n0 + 2 * m;
+    const double* src = Q2 + (((size_t)qi * d.NYA + y) * NXA + x) * d.NZ;
+    A[m * NXA + x] = make_double2(na < d.NZ ? src[na] : 0.0, na + 1 < d.NZ ? src[na + 1] : 0.0);
+  }
+  __syncthreads();
+  const double2* R = fft_lines<false>(A, B, NP, px);
+  for (int idx = threadIdx.x; idx < NP * d.NXH; idx += blockDim.x) {
+    const int m = idx % NP, kx = idx / NP, na = n0 + 2 * m;
+    const double2 Z = R[m * NXA + kx];
+    const double2 Zc = cconj(R[m * NXA + ((NXA - kx) % NXA)]);
+    const double2 a = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
+    const double2 dd = csub(Z, Zc);
+    const double2 b = make_double2(0.5 * dd.y, -0.5 * dd.x);
+    double2* dst = Q1 + (((size_t)qi * d.NYA + y) * d.NXH + kx) * d.NZ;
+    if (na < d.NZ) dst[na] = a;
+    if (na + 1 < d.NZ) dst[na + 1] = b;
+  }
+}
+
+// ------------------------------------------------------------------------------
+// forward transform, pass 3: y c2c (e^{-i}), x0.5 on Chebyshev index 0 and the
+// 1/(NXAA NYAA NZAA) normalisation (transforms.f90:280-296)
+// ------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kThreads) k_fwd_y(Dims d, const double2* Q1, double2* qspec, double scale,
+                                                     FftPlan py) {
+  extern __shared__ double2 sm[];
+  const int qi = blockIdx.x, n0 = blockIdx.y * kNB1, kx = blockIdx.z;
+  const int NYA = d.NYA;
+  double2* A = sm;
+  double2* B = sm + kNB1 * NYA;
+  for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
+    const int ln = idx % kNB1, y = idx / kNB1, n = n0 + ln;
+    double2 v = zero2();
+    if (n < d.NZ) {
+      v = Q1[(((size_t)qi * NYA + y) * d.NXH + kx) * d.NZ + n];
+      if (n == 0) v = cscale(v, 0.5);
+    }
+    A[ln * NYA + y] = v;
+  }
+  __syncthreads();
+  const double2* R = fft_lines<false>(A, B, kNB1, py);
+  for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
+    const int ln = idx % kNB1, ky = idx / kNB1, n = n0 + ln;
+    if (n < d.NZ) qspec[(((size_t)qi * d.NXH + kx) * NYA + ky) * d.NZ + n] = cscale(R[ln * NYA + ky], scale);
+  }
+}
+
+// remove_vertical_mean_of_quadratic_var (PL_IMEX_timestepping.f90:223-235)
+__global__ void k_remove_zmean(Dims d, double2* qs) {
+  const size_t col = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= (size_t)d.NXH * d.NYA) return;
+  double2* s = qs + col * d.NZ;
+  double2 acc = zero2();
+  for (int q = 1; q <= d.NZ / 2 - 1; ++q) {
+    const double c = 0.5 / (2.0 * q + 1.0) - 0.5 / (2.0 * q - 1.0);
+    acc = csub(acc, cscale(s[2 * q], c));
+  }
+  s[0] = acc;
+}
+
+// ------------------------------------------------------------------------------
+// NL assembly K_hat = sum_terms (i kx)^a (i ky)^b dsca trunc(I^Iz M^mz) qhat,
+// inserted in the interleaved ordering (marching.f90:319-367); zero for dealiased
+// modes and (0,0).  One warp per (kx,ky) system.
+// ------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kWPB * 32) k_nl(NLArgs a) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sid = blockIdx.x * kWPB + warp;
+  const int nsys = a.d.NXH * a.d.NYA;
+  if (sid >= nsys) return;
+  const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
+  const bool act = a.act_index[sid] >= 0;
+  double2 coef[kMaxGroups];
+#pragma unroll
+  for (int g = 0; g < kMaxGroups; ++g)
+    coef[g] = (g < a.NL.ngroups) ? cmul(ipow(a.kx[kx], a.NL.gkx[g]), ipow(a.ky[ky], a.NL.gky[g])) : zero2();
+  double2* out = a.Khat + (size_t)sid * a.T;
+  const int NZ = a.d.NZ;
+  for (int t = lane; t < a.T; t += 32) {
+    double2 acc = zero2();
+    for (int k = 0; act && k < a.NL.width; ++k) {
+      const int c = a.NL.col[(size_t)t * a.NL.width + k];
+      if (c < 0) break;
+      const int qv = c / NZ, n = c - qv * NZ;
+      const double2 qh = a.qspec[(((size_t)qv * a.d.NXH + kx) * a.d.NYA + ky) * NZ + n];
+      const double v = a.NL.val[(size_t)t * a.NL.width + k];
+      double2 cv = coef[0];
+      const int g = a.NL.grp[(size_t)t * a.NL.width + k];
+#pragma unroll
+      for (int gg = 1; gg < kMaxGroups; ++gg)
+        if (g == gg) cv = coef[gg];
+      acc = cadd(acc, cmul(cv, make_double2(v * qh.x, v * qh.y)));
+    }
+    out[t] = acc;
+  }
+}
+
+// ------------------------------------------------------------------------------
+// stage update and banded solve, one warp per (kx,ky) system
+//   rhs = M field + sum_{j<i} dt a(i,j) Kstd_j + dt ahat(i+1,j) Khat_j + dt ahat(i+1,i) Khat_i
+//   aux = E^{-1} rhs  (E = identity for dealiased modes; (0,0): M is empty)
+//   Kstd_i = L aux    (zero for dealiased modes and (0,0))
+// (marching.f90:16-29, 53-171; PL_algebra_z_3D.f90:218-243 zgbtrs semantics)
+// ------------------------------------------------------------------------------
+constexpr int kPF = 8;  // factor columns prefetched ahead
+
+__device__ __forceinline__ double2 ell_row(const DevEll& op, int t, const double2* coef, const double2* x) {
+  double2 acc = zero2();
+  for (int k = 0; k < op.width; ++k) {
+    const size_t e = (size_t)t * op.width + k;
+    const int c = op.col[e];
+    if (c < 0) break;
+    const double v = op.val[e];
+    const double2 xv = x[c];
+    acc = cadd(acc, cmul(coef[op.grp[e]], make_double2(v * xv.x, v * xv.y)));
+  }
+  return acc;
+}
+
+__global__ void __launch_bounds__(kWPB * 32) k_solve(SolveArgs a) {
+  extern __shared__ double2 sm[];
+  __shared__ double2 coefs[kWPB][2][kMaxGroups];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sid = blockIdx.x * kWPB + warp;
+  const int nsys = a.d.NXH * a.d.NYA;
+  if (sid >= nsys) return;
+  const int T = a.T;
+  double2* b = sm + (size_t)warp * T;
+  const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
+  const int act = a.act_index[sid];
+  const bool origin = (kx == 0 && ky == 0);
+  if (lane < kMaxGroups) {
+    coefs[warp][0][lane] = (lane < a.M.ngroups) ? cmul(ipow(a.kx[kx], a.M.gkx[lane]), ipow(a.ky[ky], a.M.gky[lane])) : zero2();
+    coefs[warp][1][lane] = (lane < a.L.ngroups) ? cmul(ipow(a.kx[kx], a.L.gkx[lane]), ipow(a.ky[ky], a.L.gky[lane])) : zero2();
+  }
+  __syncwarp();
+  const double2* field = a.field + (size_t)sid * T;
+  // ---- right-hand side
+  for (int t = lane; t < T; t += 32) {
+    double2 r = origin ? zero2() : ell_row(a.M, t, coefs[warp][0], field);
+    for (int j = 0; j < a.nprev; ++j) {
+      const double2 ks = a.Kstd[j][(size_t)sid * T + t];
+      r = cadd(r, cscale(ks, a.ca[j]));
+      const double2 kh = a.Khat[j][(size_t)sid * T + t];
+      r = cadd(r, cscale(kh, a.ch[j]));
+    }
+    const double2 kh = a.Khat[a.nprev][(size_t)sid * T + t];
+    r = cadd(r, cscale(kh, a.ch[a.nprev]));
+    b[t] = r;
+  }
+  __syncwarp();
+  if (act >= 0) {
+    const int kl = a.kl, kv = a.kl + a.ku, ldab = a.ldab;
+    const double2* ab = a.ab + (size_t)act * T * ldab;
+    const unsigned char* dp = a.dpiv + (size_t)act * T;
+    // ---- forward: apply row interchanges and L (zgbtrs, 'N', kl > 0)
+    {
+      double2 lr[kPF];
+#pragma unroll
+      for (int q = 0; q < kPF; ++q)
+        lr[q] = (q < T - 1 && lane < kl) ? ab[(size_t)q * ldab + kv + 1 + lane] : zero2();
+      for (int j0 = 0; j0 < T - 1; j0 += kPF) {
+#pragma unroll
+        for (int q = 0; q < kPF; ++q) {
+          const int j = j0 + q;
+          if (j < T - 1) {
+            const double2 l = lr[q];
+            const int jn = j + kPF;
+            lr[q] = (jn < T - 1 && lane < kl) ? ab[(size_t)jn * ldab + kv + 1 + lane] : zero2();
+            const int p = j + dp[j];
+            if (p != j) {
+              if (lane == 0) {
+                double2 tmp = b[p];
+                b[p] = b[j];
+                b[j] = tmp;
+              }
+              __syncwarp();
+            }
+            const double2 bj = b[j];
+            const int lm = min(kl, T - 1 - j);
+            if (lane < lm) b[j + 1 + lane] = csub(b[j + 1 + lane], cmul(l, bj));
+            __syncwarp();
+          }
+        }
+      }
+    }
+    // ---- backward: U x = y, U with kl+ku super-diagonals, diagonal stored as its reciprocal
+    {
+      double2 u1[kPF], u2[kPF], dg[kPF];
+#pragma unroll
+      for (int q = 0; q < kPF; ++q) {
+        const int j = T - 1 - q;
+        if (j >= 0) {
+          const double2* col = ab + (size_t)j * ldab;
+          dg[q] = col[kv];
+          u1[q] = (lane + 1 <= kv) ? col[kv - 1 - lane] : zero2();
+          u2[q] = (lane + 33 <= kv) ? col[kv - 33 - lane] : zero2();
+        }
+      }
+      for (int j0 = T - 1; j0 >= 0; j0 -= kPF) {
+#pragma unroll
+        for (int q = 0; q < kPF; ++q) {
+          const int j = j0 - q;
+          if (j >= 0) {
+            const double2 d = dg[q], c1 = u1[q], c2 = u2[q];
+            const int jn = j - kPF;
+            if (jn >= 0) {
+              const double2* col = ab + (size_t)jn * ldab;
+              dg[q] = col[kv];
+              u1[q] = (lane + 1 <= kv) ? col[kv - 1 - lane] : zero2();
+              u2[q] = (lane + 33 <= kv) ? col[kv - 33 - lane] : zero2();
+            }
+            const double2 bj = cmul(b[j], d);
+            __syncwarp();
+            if (lane == 0) b[j] = bj;
+            if (lane + 1 <= kv && j - lane - 1 >= 0) b[j - lane - 1] = csub(b[j - lane - 1], cmul(c1, bj));
+            if (lane + 33 <= kv && j - lane - 33 >= 0) b[j - lane - 33] = csub(b[j - lane - 33], cmul(c2, bj));
+            __syncwarp();
+          }
+        }
+      }
+    }
+  }
+  // ---- outputs
+  double2* out = a.out + (size_t)sid * T;
+  bool bad = false;
+  const bool zero_out = a.last_stage && (act < 0);
+  for (int t = lane; t < T; t += 32) {
+    const double2 v = zero_out ? zero2() : b[t];
+    bad |= !(isfinite(v.x) && isfinite(v.y));
+    out[t] = v;
+  }
+  if (a.Kstd_out) {
+    double2* ko = a.Kstd_out + (size_t)sid * T;
+    for (int t = lane; t < T; t += 32) ko[t] = (act >= 0) ? ell_row(a.L, t, coefs[warp][1], b) : zero2();
+  }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.flags, 1u);
+}
+
+// ------------------------------------------------------------------------------
+// factorisation of E = M + zsca L (zsca = -dt a11) with partial pivoting, one warp
+// per active system, in place in LAPACK band storage (PL_IMEX_timestepping.f90:382-410;
+// PL_algebra_z_3D.f90:245-276; the unblocked ZGBTF2 algorithm that ZGBTRF runs for
+// kl < 32).  Pivot offsets are kept as bytes; U's diagonal is replaced by its reciprocal.
+// ------------------------------------------------------------------------------
+__device__ __forceinline__ double2 crecip(double2 p) {
+  if (fabs(p.x) >= fabs(p.y)) {
+    const double t = p.y / p.x, den = p.x + p.y * t;
+    return make_double2(1.0 / den, -t / den);
+  } else {
+    const double t = p.x / p.y, den = p.y + p.x * t;
+    return make_double2(t / den, -1.0 / den);
+  }
+}
+
+__global__ void __launch_bounds__(kWPB * 32) k_factor(FactorArgs a) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sys = blockIdx.x * kWPB + warp;
+  if (sys >= a.nact) return;
+  const int T = a.T, kl = a.kl, ku = a.ku, kv = kl + ku, ldab = a.ldab;
+  const int sid = a.act_list[sys];
+  const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
+  double2 cm[kMaxGroups], cl[kMaxGroups];
+#pragma unroll
+  for (int g = 0; g < kMaxGroups; ++g) {
+    cm[g] = (g < a.M.ngroups) ? cmul(ipow(a.kx[kx], a.M.gkx[g]), ipow(a.ky[ky], a.M.gky[g])) : zero2();
+    cl[g] = (g < a.L.ngroups) ? cmul(ipow(a.kx[kx], a.L.gkx[g]), ipow(a.ky[ky], a.L.gky[g])) : zero2();
+  }
+  double2* ab = a.ab + (size_t)sys * T * ldab;
+  for (size_t e = lane; e < (size_t)T * ldab; e += 32) ab[e] = zero2();
+  __syncwarp();
+  // E(t,c) = M(t,c) + zsca * L(t,c); lane owns rows t = lane mod 32 (no write conflicts)
+  for (int t = lane; t < T; t += 32) {
+    for (int k = 0; k < a.M.width; ++k) {
+      const size_t e = (size_t)t * a.M.width + k;
+      const int c = a.M.col[e];
+      if (c < 0) break;
+      double2 cv = zero2();
+      const int g = a.M.grp[e];
+#pragma unroll
+      for (int gg = 0; gg < kMaxGroups; ++gg)
+        if (g == gg) cv = cm[gg];
+      double2& dst = ab[(size_t)c * ldab + kv + t - c];
+      dst = cadd(dst, cscale(cv, a.M.val[e]));
+    }
+    for (int k = 0; k < a.L.width; ++k) {
+      const size_t e = (size_t)t * a.L.width + k;
+      const int c = a.L.col[e];
+      if (c < 0) break;
+      double2 cv = zero2();
+      const int g = a.L.grp[e];
+#pragma unroll
+      for (int gg = 0; gg < kMaxGroups; ++gg)
+        if (g == gg) cv = cl[gg];
+      double2& dst = ab[(size_t)c * ldab + kv + t - c];
+      dst = cadd(dst, cscale(cscale(cv, a.L.val[e]), a.zsca));
+    }
+  }
+  __syncwarp();
+  int ju = 0, info = 0;
+  for (int j = 0; j < T; ++j) {
+    const int km = min(kl, T - 1 - j);
+    // pivot: first index of the largest |re|+|im| among rows j..j+km
+    double mag = -1.0;
+    int idx = 1 << 30;
+    if (lane <= km) {
+      const double2 v = ab[(size_t)j * ldab + kv + lane];
+      mag = fabs(v.x) + fabs(v.y);
+      idx = lane;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double m2 = __shfl_xor_sync(0xffffffffu, mag, o);
+      const int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
+      if (m2 > mag || (m2 == mag && i2 < idx)) { mag = m2; idx = i2; }
+    }
+    const int jp = idx;
+    if (lane == 0) a.dpiv[(size_t)sys * T + j] = (unsigned char)jp;
+    const double2 piv = ab[(size_t)j * ldab + kv + jp];
+    if (piv.x == 0.0 && piv.y == 0.0) {
+      if (info == 0) info = j + 1;
+      continue;
+    }
+    ju = max(ju, min(j + ku + jp, T - 1));
+    if (jp != 0) {
+      for (int c = j + lane; c <= ju; c += 32) {
+        double2* p1 = ab + (size_t)c * ldab + kv + j + jp - c;
+        double2* p0 = ab + (size_t)c * ldab + kv + j - c;
+        const double2 t0 = *p0;
+        *p0 = *p1;
+        *p1 = t0;
+      }
+      __syncwarp();
+    }
+    const double2 r = crecip(ab[(size_t)j * ldab + kv]);
+    __syncwarp();
+    if (km > 0) {
+      if (lane >= 1 && lane <= km) {
+        double2* m = ab + (size_t)j * ldab + kv + lane;
+        *m = cmul(*m, r);
+      }
+      __syncwarp();
+      const int nc = ju - j;
+      for (int e = lane; e < nc * km; e += 32) {
+        const int c = j + 1 + e / km, i = 1 + e % km;
+        const double2 mult = ab[(size_t)j * ldab + kv + i];
+        const double2 rowv = ab[(size_t)c * ldab + kv + j - c];
+        double2* dst = ab + (size_t)c * ldab + kv + j + i - c;
+        *dst = csub(*dst, cmul(mult, rowv));
+      }
+    }
+    __syncwarp();
+    if (lane == 0) ab[(size_t)j * ldab + kv] = r;
+    __syncwarp();
+  }
+  if (lane == 0) a.info[sys] = info;
+}
+
+// ------------------------------------------------------------------------------
+// mean (kx = ky = 0) systems: real arithmetic, one warp per system
+// ------------------------------------------------------------------------------
+__device__ double ell_row_real(const DevEll& op, int t, const double* x) {
+  double acc = 0.0;
+  for (int k = 0; k < op.width; ++k) {
+    const size_t e = (size_t)t * op.width + k;
+    const int c = op.col[e];
+    if (c < 0) break;
+    acc += op.val[e] * x[c];
+  }
+  return acc;
+}
+
+__global__ void k_zero_step(ZeroArgs a) {
+  extern __shared__ double smd[];
+  const int lane = threadIdx.x;
+  const int s = blockIdx.x;
+  if (s >= a.nsys) return;
+  const ZeroSysDev& z = a.sys[s];
+  const int T = z.T, i = a.stage;
+  double* b = smd;
+  double* kh = a.sys[s].Khat[i];
+  // NL: K_hat_i from the real part of the (0,0) Chebyshev coefficients (marching.f90:372-397)
+  for (int t = lane; t < T; t += 32) {
+    double acc = 0.0;
+    for (int k = 0; k < z.NL.width; ++k) {
+      const size_t e = (size_t)t * z.NL.width + k;
+      const int c = z.NL.col[e];
+      if (c < 0) break;
+      const int qv = c / a.d.NZ, n = c - qv * a.d.NZ;
+      acc += z.NL.val[e] * a.qspec[(size_t)qv * a.d.NXH * a.d.NYA * a.d.NZ + n].x;
+    }
+    kh[t] = acc;
+  }
+  __syncwarp();
+  for (int t = lane; t < T; t += 32) {
+    double r = ell_row_real(z.M, t, z.field);
+    for (int j = 0; j < i; ++j) {
+      r = r + a.ca[j] * z.Kstd[j][t];
+      r = r + a.ch[j] * z.Khat[j][t];
+    }
+    r = r + a.ch[i] * kh[t];
+    b[t] = r;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    const int kl = z.kl, kv = z.kl + z.ku, ldab = z.ldab;
+    for (int j = 0; j < T - 1; ++j) {
+      const int p = j + z.dpiv[j];
+      if (p != j) { double tmp = b[p]; b[p] = b[j]; b[j] = tmp; }
+      const int lm = min(kl, T - 1 - j);
+      for (int q = 1; q <= lm; ++q) b[j + q] -= z.ab[(size_t)j * ldab + kv + q] * b[j];
+    }
+    for (int j = T - 1; j >= 0; --j) {
+      const double bj = b[j] * z.ab[(size_t)j * ldab + kv];
+      b[j] = bj;
+      for (int q = 1; q <= kv && j - q >= 0; ++q) b[j - q] -= z.ab[(size_t)j * ldab + kv - q] * bj;
+    }
+  }
+  __syncwarp();
+  double* out = a.last_stage ? z.field : z.aux;
+  if (!a.last_stage)
+    for (int t = lane; t < T; t += 32) z.Kstd[i][t] = ell_row_real(z.L, t, b);
+  __syncwarp();
+  for (int t = lane; t < T; t += 32) out[t] = b[t];
+}
+
+__global__ void k_zero_factor(ZeroArgs a) {
+  const int s = blockIdx.x;
+  if (s >= a.nsys || threadIdx.x != 0) return;
+  const ZeroSysDev& z = a.sys[s];
+  const int T = z.T, kl = z.kl, ku = z.ku, kv = kl + ku, ldab = z.ldab;
+  double* ab = z.ab;
+  for (size_t e = 0; e < (size_t)T * ldab; ++e) ab[e] = 0.0;
+  for (int t = 0; t < T; ++t) {
+    for (int k = 0; k < z.M.width; ++k) {
+      const size_t e = (size_t)t * z.M.width + k;
+      const int c = z.M.col[e];
+      if (c < 0) break;
+      ab[(size_t)c * ldab + kv + t - c] += z.M.val[e];
+    }
+    for (int k = 0; k < z.L.width; ++k) {
+      const size_t e = (size_t)t * z.L.width + k;
+      const int c = z.L.col[e];
+      if (c < 0) break;
+      ab[(size_t)c * ldab + kv + t - c] += a.zsca * z.L.val[e];
+    }
+  }
+  int ju = 0, info = 0;
+  for (int j = 0; j < T; ++j) {
+    const int km = min(kl, T - 1 - j);
+    int jp = 0;
+    double best = -1.0;
+    for (int q = 0; q <= km; ++q) {
+      const double v = fabs(ab[(size_t)j * ldab + kv + q]);
+      if (v > best) { best = v; jp = q; }
+    }
+    z.dpiv[j] = (unsigned char)jp;
+    if (ab[(size_t)j * ldab + kv + jp] == 0.0) { if (!info) info = j + 1; continue; }
+    ju = max(ju, min(j + ku + jp, T - 1));
+    if (jp != 0)
+      for (int c = j; c <= ju; ++c) {
+        double* p1 = ab + (size_t)c * ldab + kv + j + jp - c;
+        double* p0 = ab + (size_t)c * ldab + kv + j - c;
+        double t0 = *p0; *p0 = *p1; *p1 = t0;
+      }
+    const double r = 1.0 / ab[(size_t)j * ldab + kv];
+    for (int q = 1; q <= km; ++q) ab[(size_t)j * ldab + kv + q] *= r;
+    for (int c = j + 1; c <= ju; ++c) {
+      const double rowv = ab[(size_t)c * ldab + kv + j - c];
+      for (int q = 1; q <= km; ++q) ab[(size_t)c * ldab + kv + j + q - c] -= ab[(size_t)j * ldab + kv + q] * rowv;
+    }
+    ab[(size_t)j * ldab + kv] = r;
+  }
+  a.info[s] = info;
+}
+
+// ------------------------------------------------------------------------------
+// QuickSave / checkpoint helpers
+// ------------------------------------------------------------------------------
+__global__ void k_transpose_xy(Dims d, const double* in, double* out, int to_file) {
+  const size_t n = (size_t)d.NXA * d.NYA * d.NZA;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const int z = (int)(e % d.NZA);
+    const size_t r = e / d.NZA;
+    // e indexes the output array
+    if (to_file) {  // out[x][y][z] <- in[y][x][z]
+      const int y = (int)(r % d.NYA), x = (int)(r / d.NYA);
+      out[e] = in[((size_t)y * d.NXA + x) * d.NZA + z];
+    } else {        // out[y][x][z] <- in[x][y][z]
+      const int x = (int)(r % d.NXA), y = (int)(r / d.NXA);
+      out[e] = in[((size_t)x * d.NYA + y) * d.NZA + z];
+    }
+  }
+}
+
+// Projection of Chebyshev coefficients onto one variable's Galerkin basis
+// (square-stencil solve of import_quicksave, PL_IMEX_timestepping_output.f90:343-355).
+// The square stencil is lower triangular, so a forward substitution solves it;
+// the caller has zeroed the state, so the result is written into the slots.
+__global__ void k_galerkin_insert(Dims d, const double2* spec, int T, const int* var_pos, int nc,
+                                  const double* sq, const int* sq_col, double2* field) {
+  const size_t col = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= (size_t)d.NXH * d.NYA) return;
+  const double2* c = spec + col * d.NZ;
+  double2* f = field + col * T;
+  for (int r = 0; r < nc; ++r) {
+    double2 acc = c[r];
+    double diag = 1.0;
+    for (int k = 0; k < kTabW; ++k) {
+      const int cc = sq_col[r * kTabW + k];
+      if (cc < 0) continue;
+      const double v = sq[r * kTabW + k];
+      if (cc == r) diag = v;
+      else if (cc < r) acc = csub(acc, cscale(f[var_pos[cc]], v));
+    }
+    f[var_pos[r]] = make_double2(acc.x / diag, acc.y / diag);
+  }
+}
+
+__global__ void k_cheb_extract(Dims d, const double2* field, int T, const int* tab_t, const double* tab_v,
+                               double2* spec) {
+  const size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t n_all = (size_t)d.NXH * d.NYA * d.NZ;
+  if (e >= n_all) return;
+  const int n = (int)(e % d.NZ);
+  const size_t col = e / d.NZ;
+  const double2* f = field + col * T;
+  double2 s = zero2();
+  for (int k = 0; k < kTabW; ++k) {
+    const int tt = tab_t[n * kTabW + k];
+    if (tt >= 0) s = cadd(s, cscale(f[tt], tab_v[n * kTabW + k]));
+  }
+  spec[e] = s;
+}
+
+__global__ void k_check_finite(const double2* x, size_t n, unsigned int* flags) {
+  bool bad = false;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    bad |= !(isfinite(x[e].x) && isfinite(x[e].y));
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flags, 1u);
+}
+
+int grid1d(size_t n, int bs) { return (int)((n + bs - 1) / bs); }
+
+template <typename K>
+void set_smem(K kernel, size_t bytes) {
+  static size_t done = 0;
+  (void)done;
+  if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+}  // namespace
+
+// ---- launchers ----------------------------------------------------------------
+void launch_inv_y(const Dims& d, int nf, const FullVarDev* fv, StateSet st, const double2* plain_spec,
+                  const double* kx, const double* ky, double2* Y1, const FftPlan& py, cudaStream_t s) {
+  size_t sm = 2 * kNB1 * (size_t)d.NYA * sizeof(double2);
+  set_smem(k_inv_y, sm);
+  dim3 g(nf, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
+  k_inv_y<<<g, kThreads, sm, s>>>(d, fv, st, plain_spec, kx, ky, Y1, py);
+}
+void launch_inv_x(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s) {
+  size_t sm = 2 * (kNB2 / 2) * (size_t)d.NXA * sizeof(double2);
+  set_smem(k_inv_x, sm);
+  dim3 g(nf, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
+  k_inv_x<<<g, kThreads, sm, s>>>(d, Y1, Y2, px);
+}
+void launch_inv_z(const Dims& d, int nf, const double* Y2, double* phys, const FftPlan& pz,
+                  const double2* dct_tw, const double* wz, unsigned long long* cfl_bits, cudaStream_t s) {
+  size_t sm = 2 * (kXB3 / 2) * (size_t)d.NZA * sizeof(double2);
+  set_smem(k_inv_z, sm);
+  dim3 g(nf, (d.NXA + kXB3 - 1) / kXB3, d.NYA);
+  k_inv_z<<<g, kThreads, sm, s>>>(d, Y2, phys, pz, dct_tw, wz, cfl_bits);
+}
+void launch_fwd_z(const Dims& d, int nf, const QuadDesc& q, const double* phys, double* Q2, const FftPlan& pz,
+                  const double2* dct_tw, const double* wz, double* ke_partial, cudaStream_t s) {
+  size_t sm = (size_t)nf * d.NZA * sizeof(double2) + 2 * (size_t)q.nq * d.NZA * sizeof(double2);
+  set_smem(k_fwd_z, sm);
+  dim3 g((d.NXA + 1) / 2, d.NYA);
+  k_fwd_z<<<g, kThreads, sm, s>>>(d, nf, q, phys, Q2, pz, dct_tw, wz, ke_partial);
+}
+void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s) {
+  size_t sm = 2 * (kNB2 / 2) * (size_t)d.NXA * sizeof(double2);
+  set_smem(k_fwd_x, sm);
+  dim3 g(nq, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
+  k_fwd_x<<<g, kThreads, sm, s>>>(d, Q2, Q1, px);
+}
+void launch_fwd_y(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
+                  cudaStream_t s) {
+  size_t sm = 2 * kNB1 * (size_t)d.NYA * sizeof(double2);
+  set_smem(k_fwd_y, sm);
+  dim3 g(nq, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
+  k_fwd_y<<<g, kThreads, sm, s>>>(d, Q1, qspec, scale, py);
+}
+void launch_remove_zmean(const Dims& d, double2* qspec_q, cudaStream_t s) {
+  k_remove_zmean<<<grid1d((size_t)d.NXH * d.NYA, 128), 128, 0, s>>>(d, qspec_q);
+}
+void launch_nl(const NLArgs& a, cudaStream_t s) {
+  const int nsys = a.d.NXH * a.d.NYA;
+  k_nl<<<(nsys + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
+}
+void launch_solve(const SolveArgs& a, cudaStream_t s) {
+  const int nsys = a.d.NXH * a.d.NYA;
+  size_t sm = (size_t)kWPB * a.T * sizeof(double2);
+  set_smem(k_solve, sm);
+  k_solve<<<(nsys + kWPB - 1) / kWPB, kWPB * 32, sm, s>>>(a);
+}
+void launch_factor(const FactorArgs& a, cudaStream_t s) {
+  if (a.nact <= 0) return;
+  k_factor<<<(a.nact + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
+}
+void launch_zero_step(const ZeroArgs& a, cudaStream_t s) {
+  if (a.nsys <= 0) return;
+  int Tmax = 1;
+  for (int i = 0; i < a.nsys; ++i) Tmax = a.sys[i].T > Tmax ? a.sys[i].T : Tmax;
+  k_zero_step<<<a.nsys, 32, (size_t)Tmax * sizeof(double), s>>>(a);
+}
+void launch_zero_factor(const ZeroArgs& a, cudaStream_t s) {
+  if (a.nsys <= 0) return;
+  k_zero_factor<<<a.nsys, 32, 0, s>>>(a);
+}
+void launch_transpose_xy(const Dims& d, const double* in, double* out, int to_file, cudaStream_t s) {
+  k_transpose_xy<<<1024, 256, 0, s>>>(d, in, out, to_file);
+}
+void launch_galerkin_insert(const Dims& d, const double2* spec, int T, const int* var_pos, int nc, const double* sq,
+                            const int* sq_col, double2* field, cudaStream_t s) {
+  k_galerkin_insert<<<grid1d((size_t)d.NXH * d.NYA, 128), 128, 0, s>>>(d, spec, T, var_pos, nc, sq, sq_col, field);
+}
+void launch_cheb_extract(const Dims& d, const double2* field, int T, const int* tab_t, const double* tab_v,
+                         double2* spec, cudaStream_t s) {
+  k_cheb_extract<<<grid1d((size_t)d.NXH * d.NYA * d.NZ, 256), 256, 0, s>>>(d, field, T, tab_t, tab_v, spec);
+}
+void launch_check_finite(const double2* x, size_t n, unsigned int* flags, cudaStream_t s) {
+  k_check_finite<<<1024, 256, 0, s>>>(x, n, flags);
+}
+
+}  // namespace coral

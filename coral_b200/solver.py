@@ -1,0 +1,159 @@
+"""Python mirror of the reference's plane-layer data structure
+(full_problem_data_structure_T, src/plane_layer/PL_IMEX_timestepping.f90:143-219)
+on top of the C-ABI.  Same procedure names and argument meaning:
+
+    init                  -> PlaneLayer(...)            (PL_IMEX_timestepping.f90:510)
+    factorize_operators   -> factorize_operators(dt)    (:351-422)
+    march_forward         -> march_forward(dt)          (PL_IMEX_timestepping_marching.f90:3)
+    import_quickSave      -> import_quicksave(dir)      (PL_IMEX_timestepping_output.f90:309)
+    export_checkpoints    -> export_checkpoints(dir)    (PL_IMEX_timestepping_output.f90:385)
+    PS_fields_T%spec_to_phys / phys_to_spec             (slabs.fftw3mpi/transforms.f90:155-301)
+
+Errors raise CoralError (the reference prints and stops).
+Arrays use C order with the reference's Fortran shapes reversed:
+    field (NX/2, NYAA, T) complex128, spec (NX/2, NYAA, NZ) complex128,
+    phys (NYAA, NXAA, NZAA) float64.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib
+
+
+class CoralError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (_lib.ERRORS.get(code, "?"), code, msg))
+        self.code = code
+
+
+Q = dict(NX=0, NY=1, NZ=2, NXAA=3, NYAA=4, NZAA=5, N_KXKY=6, N_ZERO=7, N_FULL=8, N_QUAD=9, STAGES=10,
+         DEVICE_BYTES=11, LAUNCHES=12)
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class PlaneLayer:
+    def __init__(self, equations_text, parameters_text, scheme=None, device=0):
+        self._lib = _lib.load()
+        h = ctypes.c_void_p()
+        rc = self._lib.coral_create(equations_text.encode(), parameters_text.encode(),
+                                    scheme.encode() if scheme else None, int(device), ctypes.byref(h))
+        if rc != 0:
+            raise CoralError(rc, self._lib.coral_last_error(None).decode())
+        self._h = h
+        q = self.query
+        self.NX, self.NY, self.NZ = q(Q["NX"]), q(Q["NY"]), q(Q["NZ"])
+        self.NXAA, self.NYAA, self.NZAA = q(Q["NXAA"]), q(Q["NYAA"]), q(Q["NZAA"])
+        self.NXH = self.NX // 2
+        self.n_kxky = q(Q["N_KXKY"])
+        self.n_zero = q(Q["N_ZERO"])
+        self.n_full = q(Q["N_FULL"])
+        self.n_quad = q(Q["N_QUAD"])
+        self.stages = q(Q["STAGES"])
+        self.T = [q(100 + i) for i in range(self.n_kxky)]
+        self.Tz = [q(200 + i) for i in range(self.n_zero)]
+
+    @classmethod
+    def from_files(cls, equations_path, parameters_path, scheme=None, device=0):
+        with open(equations_path) as f:
+            e = f.read()
+        with open(parameters_path) as f:
+            p = f.read()
+        return cls(e, p, scheme, device)
+
+    # --- plumbing
+    def _check(self, rc):
+        if rc != 0:
+            raise CoralError(rc, self._lib.coral_last_error(self._h).decode())
+
+    def query(self, what):
+        v = ctypes.c_longlong()
+        self._check(self._lib.coral_query(self._h, int(what), ctypes.byref(v)))
+        return v.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.coral_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def device_bytes(self):
+        return self.query(Q["DEVICE_BYTES"])
+
+    @property
+    def kernel_launches(self):
+        return self.query(Q["LAUNCHES"])
+
+    # --- reference procedures
+    def factorize_operators(self, dt):
+        self._check(self._lib.coral_factorize(self._h, float(dt)))
+
+    def march_forward(self, dt, nsteps=1):
+        self._check(self._lib.coral_march(self._h, float(dt), int(nsteps)))
+
+    def synchronize(self):
+        self._check(self._lib.coral_synchronize(self._h))
+
+    def get_field(self, isys=0):
+        a = np.empty((self.NXH, self.NYAA, self.T[isys]), dtype=np.complex128)
+        self._check(self._lib.coral_get_field(self._h, isys, _dptr(a)))
+        return a
+
+    def set_field(self, isys, field):
+        a = np.ascontiguousarray(field, dtype=np.complex128)
+        if a.shape != (self.NXH, self.NYAA, self.T[isys]):
+            raise ValueError("field shape %s != %s" % (a.shape, (self.NXH, self.NYAA, self.T[isys])))
+        self._check(self._lib.coral_set_field(self._h, isys, _dptr(a)))
+
+    def get_mean_field(self, isys=0):
+        a = np.empty(self.Tz[isys], dtype=np.float64)
+        self._check(self._lib.coral_get_mean_field(self._h, isys, _dptr(a)))
+        return a
+
+    def set_mean_field(self, isys, field):
+        a = np.ascontiguousarray(field, dtype=np.float64)
+        if a.shape != (self.Tz[isys],):
+            raise ValueError("mean field shape")
+        self._check(self._lib.coral_set_mean_field(self._h, isys, _dptr(a)))
+
+    def spec_to_phys(self, spec):
+        s = np.ascontiguousarray(spec, dtype=np.complex128)
+        if s.shape != (self.NXH, self.NYAA, self.NZ):
+            raise ValueError("spec shape")
+        p = np.empty((self.NYAA, self.NXAA, self.NZAA))
+        self._check(self._lib.coral_spec_to_phys(self._h, _dptr(s), _dptr(p)))
+        return p
+
+    def phys_to_spec(self, phys):
+        p = np.ascontiguousarray(phys, dtype=np.float64)
+        if p.shape != (self.NYAA, self.NXAA, self.NZAA):
+            raise ValueError("phys shape")
+        s = np.empty((self.NXH, self.NYAA, self.NZ), dtype=np.complex128)
+        self._check(self._lib.coral_phys_to_spec(self._h, _dptr(p), _dptr(s)))
+        return s
+
+    def full_phys(self, ivar):
+        p = np.empty((self.NYAA, self.NXAA, self.NZAA))
+        self._check(self._lib.coral_get_full_phys(self._h, int(ivar), _dptr(p)))
+        return p
+
+    def import_quicksave(self, directory, rolling=1):
+        self._check(self._lib.coral_import_quicksave(self._h, os.fsencode(directory), int(rolling)))
+
+    def export_checkpoints(self, directory, rolling=1):
+        self._check(self._lib.coral_export_checkpoint(self._h, os.fsencode(directory), int(rolling)))
+
+    def diagnostics(self):
+        out = np.zeros(3)
+        self._check(self._lib.coral_diagnostics(self._h, _dptr(out)))
+        return dict(cfl_dt=float(out[0]), KE=float(out[1]), nonfinite=bool(out[2]))

@@ -1,0 +1,151 @@
+/*
+ * coral_b200.h -- C-ABI of the B200 plane-layer IMEX timestep.
+ *
+ * This is the drop-in boundary for Coral's plane-layer hot path: the Fortran
+ * driver (src/plane_layer/plane_layer_main.f90) binds these functions with
+ * ISO_C_BINDING exactly like it already binds the C text readers of
+ * src/text_parsing/cwraps.f90:1-23.  All arguments are plain pointers, sizes
+ * and doubles; no C++ or torch types cross the boundary.
+ *
+ * Conventions
+ *  - Complex arrays are interleaved (re, im) doubles: the memory layout of
+ *    Fortran complex(kind=8).
+ *  - Multi-dimensional arrays use the reference's Fortran (column-major)
+ *    shapes, named here with the first index fastest:
+ *      coupled-system state  field(T, NYAA, NX/2)       complex
+ *      spectral scalar       spec (NZ, NYAA, NX/2)      complex
+ *      physical scalar       phys (NZAA, NXAA, NYAA)    real
+ *      mean-system state     field(T)                   real
+ *    (src/plane_layer/PL_IMEX_timestepping.f90:90-112,
+ *     src/slabs.fftw3mpi/transforms.f90:107-131).
+ *  - Every function returns 0 on success or a negative CORAL_E* code; the
+ *    text of the last error is returned by coral_last_error().  The reference
+ *    prints and stops instead (e.g. src/plane_layer/PL_algebra_z_3D.f90:238-240);
+ *    a Fortran shim maps a non-zero code to `error stop`.
+ *  - One host thread per handle; a handle owns one CUDA stream and all of its
+ *    device memory.  Host buffers are only read or written during the call.
+ */
+#ifndef CORAL_B200_H
+#define CORAL_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CORAL_OK 0
+#define CORAL_EBADARG -1      /* invalid argument or size                       */
+#define CORAL_ENOMEM -2       /* device allocation failed                       */
+#define CORAL_ECUDA -3        /* a CUDA call or kernel launch failed            */
+#define CORAL_ESINGULAR -4    /* zero pivot in a band LU factorisation          */
+#define CORAL_ENONFINITE -5   /* NaN/Inf detected in the state                  */
+#define CORAL_EPARSE -6       /* equation or parameter file could not be read   */
+#define CORAL_EIO -7          /* file input/output failed                       */
+#define CORAL_EUNSUPPORTED -8 /* recipe feature outside this build              */
+#define CORAL_ENODEV -9       /* no usable CUDA device                          */
+
+typedef struct coral_handle coral_handle;
+
+/* Quantities for coral_query(). */
+#define CORAL_Q_NX 0
+#define CORAL_Q_NY 1
+#define CORAL_Q_NZ 2
+#define CORAL_Q_NXAA 3
+#define CORAL_Q_NYAA 4
+#define CORAL_Q_NZAA 5
+#define CORAL_Q_N_KXKY_SYSTEMS 6
+#define CORAL_Q_N_ZERO_SYSTEMS 7
+#define CORAL_Q_N_FULL_VARS 8
+#define CORAL_Q_N_QUAD_VARS 9
+#define CORAL_Q_STAGES 10
+#define CORAL_Q_DEVICE_BYTES 11
+#define CORAL_Q_KERNEL_LAUNCHES 12   /* kernels launched by this handle so far */
+#define CORAL_Q_SYS_T 100            /* + isys: size T of kxky system isys      */
+#define CORAL_Q_ZSYS_T 200           /* + isys: size of mean system isys        */
+#define CORAL_Q_SYS_NVARS 300        /* + isys: coupled vars of kxky system     */
+#define CORAL_Q_ZSYS_NVARS 400       /* + isys: coupled vars of mean system     */
+#define CORAL_Q_SYS_KL 500           /* + isys: sub-diagonals of the evolution band   */
+#define CORAL_Q_SYS_KU 600           /* + isys: super-diagonals of the evolution band */
+
+/*
+ * Create a solver from the text of coral.equations and coral.parameters.in.
+ * Replaces, for one rank: main%recipe%build (src/plane_layer/PL_equations.f90:435),
+ * main%geometry%init (src/plane_layer/PL_geometry.f90:80), main%init
+ * (src/plane_layer/PL_IMEX_timestepping.f90:510) and dct_planner
+ * (src/slabs.fftw3mpi/transforms.f90:304).  scheme may be NULL (use the one in
+ * the parameter text, e.g. 'ARS_222').  The state starts at zero.
+ */
+int coral_create(const char* equations_text, const char* parameters_text, const char* scheme,
+                 int device, coral_handle** out);
+/* Same, reading the two files. */
+int coral_create_from_files(const char* equations_path, const char* parameters_path,
+                            const char* scheme, int device, coral_handle** out);
+void coral_destroy(coral_handle* h);
+/* Text of the last error of h (or of the last failed create when h is NULL). */
+const char* coral_last_error(const coral_handle* h);
+int coral_query(const coral_handle* h, int what, long long* value);
+
+/*
+ * Build E = M - dt*a11*L for every (kx,ky) system and LU-factorise it with
+ * partial pivoting on the GPU.  Replaces main%factorize_operators
+ * (src/plane_layer/PL_IMEX_timestepping.f90:351-422 with
+ * src/plane_layer/PL_algebra_z_3D.f90:245-276).
+ */
+int coral_factorize(coral_handle* h, double dt);
+
+/*
+ * Advance nsteps timesteps of size dt (refactorising first if dt differs from
+ * the factorised one).  Replaces main%march_forward = one_step_beyond
+ * (src/plane_layer/PL_IMEX_timestepping_marching.f90:3-48).  The work is
+ * queued on the handle's stream; the call returns after the launches.
+ */
+int coral_march(coral_handle* h, double dt, int nsteps);
+
+/* Wait for the handle's stream; reports device-side errors. */
+int coral_synchronize(coral_handle* h);
+
+/* State of kxky system isys in the layout field(T, NYAA, NX/2) (complex). */
+int coral_get_field(coral_handle* h, int isys, double* field);
+int coral_set_field(coral_handle* h, int isys, const double* field);
+/* State of mean system isys, field(T) (real). */
+int coral_get_mean_field(coral_handle* h, int isys, double* field);
+int coral_set_mean_field(coral_handle* h, int isys, const double* field);
+
+/*
+ * Transforms of one scalar.  Replace PS_fields_T%spec_to_phys = c2r_transform
+ * and PS_fields_T%phys_to_spec = r2c_transform
+ * (src/slabs.fftw3mpi/transforms.f90:155-301) with the slab transposes done
+ * on the device.
+ */
+int coral_spec_to_phys(coral_handle* h, const double* spec, double* phys);
+int coral_phys_to_spec(coral_handle* h, const double* phys, double* spec);
+
+/*
+ * Full variable ivar (uFull, vFull, ...) in physical space, phys(NZAA, NXAA, NYAA),
+ * as computed from the current state (compute_full_variables_in_physical_space,
+ * src/plane_layer/PL_IMEX_timestepping_marching.f90:420-588).
+ */
+int coral_get_full_phys(coral_handle* h, int ivar, double* phys);
+
+/*
+ * Read / write the QuickSave files of a directory (…/QuickSave.kxky.sysSSS.varVVV.rollingR,
+ * …/QuickSave.zero.sysSSS.varVVV.rollingR; physical fields in z-fastest, y, x order).
+ * Replace main%import_quickSave and main%export_checkpoints
+ * (src/plane_layer/PL_IMEX_timestepping_output.f90:309-456).
+ */
+int coral_import_quicksave(coral_handle* h, const char* directory, int rolling);
+int coral_export_checkpoint(coral_handle* h, const char* directory, int rolling);
+
+/*
+ * Diagnostics of the first stage of the last step: out[0] = cargo%cfl_based_DT
+ * (marching.f90:200-254), out[1] = cargo%KE_display = sum of the volume
+ * averages of uu, vv and ww (PL_IMEX_timestepping_output.f90:84-102; 0 when
+ * those quadratic variables are absent), out[2] = 1 if any state entry is
+ * non-finite.
+ */
+int coral_diagnostics(coral_handle* h, double* out3);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CORAL_B200_H */

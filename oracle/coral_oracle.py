@@ -891,7 +891,8 @@ class Solver:
         u = np.abs(fphys[0]).max() * g.NXAA / g.Lx
         v = np.abs(fphys[1]).max() * g.NYAA / g.Ly
         wz = max(v, (np.abs(fphys[2]) / w[None, None, :]).max())
-        self.cfl_dt = 1.0 / max(u, v, wz)
+        m = max(u, v, wz)
+        self.cfl_dt = 1.0 / m if m > 0 else float('inf')
 
     def volume_average(self, phys: np.ndarray) -> float:
         """output_global_quantities 'volume' object (PL_IMEX_timestepping_output.f90:38-52)."""

@@ -1,0 +1,133 @@
+"""Parity of the CUDA path (through the C-ABI) with the CPU oracle.
+
+Tolerances: FP64 everywhere; transforms agree to 1e-13 of the field's maximum;
+timesteps to a relative L2 error of 1e-10 per coupled variable (the bound the
+plain FP64 path must hold against the reference after 100 steps)."""
+import math
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle import coral_oracle as co
+from tests.problems import equations, params
+
+pytestmark = pytest.mark.gpu
+
+
+def _pl(eq, par, scheme=None):
+    from coral_b200.solver import PlaneLayer
+    return PlaneLayer(eq, par, scheme=scheme)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.mark.parametrize("N", [(16, 16, 16), (24, 32, 12), (64, 64, 48)])
+def test_transforms_match_oracle(N):
+    NX, NY, NZ = N
+    eq, par = equations(), params(NX, NY, NZ, Lx=2.0, Ly=3.0)
+    pl = _pl(eq, par)
+    g = co.Geometry(NX, NY, NZ, 2.0, 3.0, 1.0, 0.5)
+    rng = np.random.default_rng(1)
+    spec = rng.standard_normal((g.NXH, g.NYAA, NZ)) + 1j * rng.standard_normal((g.NXH, g.NYAA, NZ))
+    p_gpu = pl.spec_to_phys(spec)
+    p_ref = co.spec_to_phys(spec, g)
+    assert np.abs(p_gpu - p_ref).max() <= 1e-13 * np.abs(p_ref).max()
+    phys = rng.standard_normal((g.NYAA, g.NXAA, g.NZAA))
+    s_gpu = pl.phys_to_spec(phys)
+    s_ref = co.phys_to_spec(phys, g)
+    assert np.abs(s_gpu - s_ref).max() <= 1e-13 * np.abs(s_ref).max()
+    pl.close()
+
+
+def _random_state(solver, pl, seed, amp=1e-3):
+    rng = np.random.default_rng(seed)
+    for s, lay in enumerate(solver.lay):
+        f = amp * (rng.standard_normal((pl.NXH, pl.NYAA, lay.T)) + 1j * rng.standard_normal((pl.NXH, pl.NYAA, lay.T)))
+        solver.field[s] = f.copy()
+        pl.set_field(s, f)
+    for s, lay in enumerate(solver.zlay):
+        z = amp * rng.standard_normal(lay.T)
+        solver.zfield[s] = z.copy()
+        pl.set_mean_field(s, z)
+
+
+@pytest.mark.parametrize("scheme", ["ARS_222", "ARS_443", "ARS_111"])
+def test_steps_match_oracle_small(scheme):
+    eq = equations("rrbc_stressfree_ek1e-4_ra5e7", **{"5.d7": "2.d4", "1.d4": "1.d2"})
+    par = params(16, 12, 16, dt=2e-4, scheme=scheme)
+    ref = co.Solver(eq, par)
+    pl = _pl(eq, par)
+    assert pl.T == [l.T for l in ref.lay]
+    _random_state(ref, pl, 3, amp=1e-2)
+    for _ in range(4):
+        ref.step(2e-4)
+    pl.march_forward(2e-4, 4)
+    pl.synchronize()
+    for s in range(len(ref.lay)):
+        assert _rel(pl.get_field(s), ref.field[s]) < 1e-11
+    for s in range(len(ref.zlay)):
+        assert _rel(pl.get_mean_field(s), ref.zfield[s]) < 1e-11
+    d = pl.diagnostics()
+    assert d["nonfinite"] is False
+    pl.close()
+
+
+def test_quicksave_import_export_roundtrip():
+    from coral_b200 import initial_conditions as ic
+    NX, NY, NZ = 16, 16, 16
+    eq, par = equations(), params(NX, NY, NZ)
+    with tempfile.TemporaryDirectory() as d:
+        ic.white_noise_temperature(d, NX, NY, NZ, seed=5)
+        ref = co.Solver(eq, par)
+        ref.import_quicksave(d)
+        pl = _pl(eq, par)
+        pl.import_quicksave(d)
+        assert _rel(pl.get_field(0), ref.field[0]) < 1e-12
+        for s in range(len(ref.zlay)):
+            assert np.abs(pl.get_mean_field(s) - ref.zfield[s]).max() <= 1e-12 * max(np.abs(ref.zfield[s]).max(), 1e-30) + 1e-18
+        out = os.path.join(d, "out")
+        os.makedirs(out)
+        pl.export_checkpoints(out)
+        pl2 = _pl(eq, par)
+        pl2.import_quicksave(out)
+        # the state is a fixed point of export -> import except for the modes the
+        # dealiased transforms cannot represent (zero after a step)
+        f1, f2 = pl.get_field(0), pl2.get_field(0)
+        g = co.Geometry(NX, NY, NZ, 2 * math.pi, 2 * math.pi, 1.0, 0.5)
+        act = g.active
+        assert _rel(f2[act], f1[act]) < 1e-12
+        pl.close()
+        pl2.close()
+
+
+def test_cfg0_100_steps_within_1e10():
+    """64x64x48 no-slip Rayleigh-Benard, Ra=1e5, Pr=1, dt=1e-4, seeded white-noise
+    temperature IC through the QuickSave path, 100 ARS_222 steps: every coupled
+    variable and mean field within 1e-10 relative L2 of the oracle."""
+    from coral_b200 import initial_conditions as ic
+    from coral_b200 import CONFIG_DIR
+    eq = open(os.path.join(CONFIG_DIR, "rbc_noslip_ra1e5.equations")).read()
+    par = open(os.path.join(CONFIG_DIR, "rbc_noslip_ra1e5_64x64x48.parameters.in")).read()
+    with tempfile.TemporaryDirectory() as d:
+        ic.white_noise_temperature(d, 64, 64, 48, seed=0)
+        ref = co.Solver(eq, par)
+        ref.import_quicksave(d)
+        pl = _pl(eq, par)
+        pl.import_quicksave(d)
+    nsteps = 100
+    for _ in range(nsteps):
+        ref.step(1e-4)
+    pl.march_forward(1e-4, nsteps)
+    pl.synchronize()
+    f_gpu, f_ref = pl.get_field(0), ref.field[0]
+    lay = ref.lay[0]
+    for v in range(lay.nV):
+        idx = lay.var_pos[v]
+        assert _rel(f_gpu[..., idx], f_ref[..., idx]) < 1e-10, ref.recipe.kxky[0].vars[v]
+    for s in range(len(ref.zlay)):
+        assert _rel(pl.get_mean_field(s), ref.zfield[s]) < 1e-10
+    pl.close()
