@@ -1,0 +1,422 @@
+"""Benchmark of the plane-layer IMEX timestep on B200.
+
+Workload (the headline configuration): Rayleigh-Benard convection, no-slip,
+Ra = 1e8, Pr = 1, NX = NY = 384 Fourier x NZ = 192 Chebyshev modes (grid
+576 x 576 x 288), ARS_222, dt = 1e-6, FP64 path; seeded white-noise temperature
+initial condition (amplitude 1e-3, PCG64 seed 2) injected through the QuickSave
+projection.  A "step" is one full IMEX timestep of the whole domain.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config NAME]
+
+N > 1 runs N independent replicas (one process per GPU under torchrun): the
+timestep does not shard across GPUs at this size (replicas only).
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "rbc_384x384x192": dict(eq="rbc_noslip_ra1e8.equations", par="rbc_noslip_ra1e8_384x384x192.parameters.in",
+                            NX=384, NY=384, NZ=192, dt=1e-6, seed=2, Ra=1e8),
+    "rbc_64x64x48": dict(eq="rbc_noslip_ra1e5.equations", par="rbc_noslip_ra1e5_64x64x48.parameters.in",
+                         NX=64, NY=64, NZ=48, dt=1e-4, seed=0, Ra=1e5),
+    "rbc_32x32x192": dict(eq="rbc_noslip_ra1e8.equations", par="rbc_noslip_ra1e8_32x32x192.parameters.in",
+                          NX=32, NY=32, NZ=192, dt=1e-6, seed=2, Ra=1e8),
+    "rrbc_192x192x96": dict(eq="rrbc_stressfree_ek1e-4_ra5e7.equations", par="rrbc_stressfree_192x192x96.parameters.in",
+                            NX=192, NY=192, NZ=96, dt=5e-6, seed=1, Ra=5e7),
+}
+METRIC = "timesteps/s at 384^2x192 (FP64 path)"
+PHASES = ("inv_y", "inv_x", "inv_z", "fwd_z_products", "fwd_x", "fwd_y", "nl_assembly", "solve", "mean_systems")
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def read_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            p = [x.strip() for x in l.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_ic(cfg, pl):
+    """Seeded white-noise temperature (coral_b200.initial_conditions) projected
+    into the state: fluctuation into the kxky variable t, horizontal mean into tMean."""
+    from coral_b200.initial_conditions import gauss_chebyshev_z
+    NXAA, NYAA, NZAA = pl.NXAA, pl.NYAA, pl.NZAA
+    rng = np.random.Generator(np.random.PCG64(cfg["seed"]))
+    zp = gauss_chebyshev_z(NZAA, 0.5, 1.0)
+    theta = rng.uniform(-1e-3, 1e-3, size=(NXAA, NYAA, NZAA))  # file order: x, y, z
+    theta *= np.sin(math.pi * zp)[None, None, :]
+    mean = theta.mean(axis=(0, 1))
+    theta -= mean[None, None, :]
+    phys = np.ascontiguousarray(theta.transpose(1, 0, 2))  # (y, x, z)
+    del theta
+    pl.set_var_phys(0, 4, phys)  # t is the 5th coupled variable (u, v, w, p, t, chi)
+    pl.set_mean_var_profile(1, 0, mean)
+
+
+def solve_bytes_per_stage(pl, nact, nsys, T, ldab, stages):
+    """Algorithmic bytes of one launch of the stage-update + banded-solve kernel,
+    averaged over the stages: LU factors + pivot bytes of the active systems,
+    and for every system the state read, the K arrays read, and the outputs."""
+    tot = 0
+    for i in range(stages):
+        last = (i == stages - 1)
+        per_sys = 16 * T * (1 + (2 * i + 1) + 1 + (0 if last else 1))
+        tot += nsys * per_sys + nact * (16 * ldab * T + T)
+    return tot / stages
+
+
+def run_ours(args, cfg):
+    import torch
+    import torch.distributed as dist
+    from coral_b200 import CONFIG_DIR
+    from coral_b200.solver import PlaneLayer
+
+    rank, world, local = dist_env()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    dev = local
+    torch.cuda.set_device(dev)
+    eq = open(os.path.join(CONFIG_DIR, cfg["eq"])).read()
+    par = open(os.path.join(CONFIG_DIR, cfg["par"])).read()
+    pl = PlaneLayer(eq, par, device=dev)
+    make_ic(cfg, pl)
+    dt = cfg["dt"]
+    t0 = time.perf_counter()
+    pl.factorize_operators(dt)
+    pl.synchronize()
+    t_factor = time.perf_counter() - t0
+    stream = torch.cuda.ExternalStream(pl.stream, device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # warm-up (also captures the CUDA graph of one step)
+    pl.march_forward(dt, args.warmup)
+    pl.synchronize()
+    launches0 = pl.kernel_launches
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        e0.record(stream)
+        pl.march_forward(dt, args.steps)
+        e1.record(stream)
+        pl.synchronize()
+        torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1)
+    barrier()
+    gpu_launches = pl.kernel_launches - launches0
+    if world > 1:
+        t = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * args.steps / (ms / 1e3)
+    diag = pl.diagnostics()
+
+    # per-kernel times with events on the launching stream (eager steps)
+    prof = {k: 0.0 for k in PHASES}
+    nprof = 2
+    for _ in range(nprof):
+        p = pl.profile_step(dt)
+        for k in PHASES:
+            prof[k] += p[k] / nprof
+    pl.synchronize()
+
+    # end to end through the C-ABI with host buffers: the state goes host -> device,
+    # every step the driver reads back its diagnostics (CFL dt, KE), and the final
+    # state comes back to the host
+    field = pl.get_field(0)
+    zf = [pl.get_mean_field(s) for s in range(pl.n_zero)]
+    pin = torch.empty(field.size * 2, dtype=torch.float64, pin_memory=True).numpy().view(np.complex128).reshape(field.shape)
+    pin[...] = field
+    barrier()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    pl.set_field(0, pin)
+    for s in range(pl.n_zero):
+        pl.set_mean_field(s, zf[s])
+    for _ in range(args.steps):
+        pl.march_forward(dt, 1)
+        pl.diagnostics()
+    out = pl.get_field(0)
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=f"cuda:{dev}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    del out
+    state_bytes = field.nbytes + sum(z.nbytes for z in zf)
+    diag_bytes = 3 * 8 + 3 * 8 + 8 * ((pl.NXAA + 1) // 2) * pl.NYAA * 3
+    e2e = {"value": world * args.steps / e2e_s, "unit": "timesteps/s",
+           "h2d_bytes_per_step": state_bytes / args.steps,
+           "d2h_bytes_per_step": state_bytes / args.steps + diag_bytes}
+
+    # roofline of the dominant kernel (stage update + banded solve)
+    T = pl.T[0]
+    kl, ku = pl.query(500), pl.query(600)
+    ldab = 2 * kl + ku + 1
+    nsys = pl.NXH * pl.NYAA
+    nact = sum(1 for ix in range(pl.NXH) for iy in range(pl.NYAA)
+               if not (iy_dealiased(iy, pl.NY, pl.NYAA)) and not (ix == 0 and iy == 0))
+    algo = solve_bytes_per_stage(pl, nact, nsys, T, ldab, pl.stages)
+    launch_ms = prof["solve"] / pl.stages
+    achieved = algo / (launch_ms / 1e3) / 1e9
+    peak, src = read_peaks()
+    traffic = read_traffic(nact)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(cfg, eq, par, max_seconds=args.cpu_seconds)
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": "timesteps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded white-noise temperature IC, PCG64 seed %d)" % cfg["seed"],
+        "config": {"workload": "%s: RBC no-slip Ra=%g Pr=1, %dx%dx%d modes, grid %dx%dx%d, ARS_222, dt=%g, FP64"
+                               % (args.config, cfg["Ra"], pl.NX, pl.NY, pl.NZ, pl.NXAA, pl.NYAA, pl.NZAA, dt),
+                   "grid_points": pl.NXAA * pl.NYAA * pl.NZAA, "systems": nsys, "active_systems": nact, "T": T,
+                   "band": [kl, ku], "l2": "inputs larger than L2 (state %.2f GB, LU factors %.1f GB)"
+                   % (field.nbytes / 1e9, nact * ldab * T * 16 / 1e9),
+                   "parallelism": "replicas x%d" % world},
+        "grid_point_steps_per_s": value * pl.NXAA * pl.NYAA * pl.NZAA,
+        "e2e": e2e,
+        "gpu_launches": gpu_launches,
+        "phase_ms_per_step": {k: round(v, 4) for k, v in prof.items()},
+        "factorize_s": t_factor,
+        "roofline": {"kernel": "k_solve (stage update + banded LU solve)", "bound": "hbm", "achieved": achieved,
+                     "peak": peak, "peak_source": src, "unit": "GB/s", "frac": achieved / peak,
+                     "algorithmic_bytes_per_launch": algo, "launch_ms": launch_ms,
+                     "traffic": traffic},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "state_ok": not diag["nonfinite"],
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    pl.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def iy_dealiased(iy, NY, NYAA):
+    """ky of FFT index iy is dealiased when |ky| >= NY/2 (PL_geometry.f90:181-198)."""
+    k = -(NYAA - iy) if iy + 1 >= NYAA // 2 + 1 else iy
+    return abs(k) >= NY / 2
+
+
+def read_traffic(nact):
+    """DRAM traffic per launch of the solve kernel, scaled from the ncu capture
+    summarised in profiles/ (bytes per active system), or None."""
+    p = os.path.join(ROOT, "profiles", "k_solve_rbc_384x384x192.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_active_system"):
+            return float(line.split("=")[1]) * nact
+    return None
+
+
+def cpu_baseline(cfg, eq, par, max_seconds=20.0, processes=1):
+    """The oracle (CPU restatement, FP64) timed on a bounded sample of the same
+    workload: one inverse and one forward 3-D transform at full size, the band
+    LU solves of a sample of (kx,ky) systems and the operator applications of a
+    sample of kx slabs; the step time is extrapolated to the full step."""
+    from oracle import coral_oracle as co
+    import scipy.linalg.lapack as lapack
+    t_start = time.perf_counter()
+    s = co.Solver.__new__(co.Solver)
+    s.recipe = co.parse_equations(eq)
+    p = co.read_parameters_text(par)
+    s.params = p
+    g = co.Geometry(p["NX"], p["NY"], p["NZ"], p["Lx"], p["Ly"], p["gap"], p["center"])
+    s.g = g
+    s.scheme = p["scheme"]
+    s.nstages, s.A, s.Ah = co.ars_tableau(s.scheme)
+    # operators of the kxky system (reduced to a few kx slabs for the timing sample)
+    rec = s.recipe.kxky[0]
+    lay = co.SystemLayout(g.NZ, rec)
+    cache = {}
+    mass = [(pc, co.build_piece_matrix(g.NZ, g.center, g.gap, lay, rec, pc, cache)) for pc in rec.mass]
+    stif = [(pc, co.build_piece_matrix(g.NZ, g.center, g.gap, lay, rec, pc, cache)) for pc in rec.stif]
+    T = lay.T
+    nF, nQ = len(s.recipe.full_vars), len(s.recipe.quad_vars)
+    rng = np.random.default_rng(0)
+    # (a) transforms at full size
+    spec = rng.standard_normal((g.NXH, g.NYAA, g.NZ)) + 1j * rng.standard_normal((g.NXH, g.NYAA, g.NZ))
+    t0 = time.perf_counter()
+    ph = co.spec_to_phys(spec, g)
+    t_inv = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    co.phys_to_spec(ph * ph, g)
+    t_fwd = time.perf_counter() - t0
+    del ph, spec
+    # (b) band LU solve per system: factor a handful, time zgbtrs on them
+    kl = ku = 0
+    for _, B in mass + stif:
+        c = B.tocoo()
+        kl = max(kl, int((c.row - c.col).max()))
+        ku = max(ku, int((c.col - c.row).max()))
+    nsample = 16
+    facs = []
+    for k in range(nsample):
+        ix, iy = 1 + (k % max(g.NXH - 1, 1)), 1 + 7 * k % (g.NY // 2)
+        M = sum((pc.dsca * co.complex_pow(complex(g.py[iy]), pc.ky) * co.complex_pow(complex(g.px[ix]), pc.kx)) * B
+                for pc, B in mass)
+        L = sum((pc.dsca * co.complex_pow(complex(g.py[iy]), pc.ky) * co.complex_pow(complex(g.px[ix]), pc.kx)) * B
+                for pc, B in stif)
+        E = (M - cfg["dt"] * s.A[0, 0] * L).tocoo()
+        ab = np.zeros((2 * kl + ku + 1, T), dtype=np.complex128)
+        ab[kl + ku + E.row - E.col, E.col] = E.data
+        lu, piv, info = lapack.zgbtrf(ab, kl, ku)
+        facs.append((lu, piv))
+    b = rng.standard_normal(T) + 1j * rng.standard_normal(T)
+    reps = 0
+    t0 = time.perf_counter()
+    while True:
+        for lu, piv in facs:
+            lapack.zgbtrs(lu, kl, ku, b, piv)
+        reps += 1
+        if time.perf_counter() - t0 > 1.0:
+            break
+    t_solve = (time.perf_counter() - t0) / (reps * nsample)
+    # (c) mass / stiffness applications on one kx slab
+    X = (rng.standard_normal((g.NYAA, T)) + 1j * rng.standard_normal((g.NYAA, T)))
+    t0 = time.perf_counter()
+    for _, B in mass + stif:
+        (B @ X.T)
+    t_mv = (time.perf_counter() - t0) / g.NYAA
+    nsys = g.NXH * g.NYAA
+    nact = int(g.active.sum())
+    step = s.nstages * (nF * t_inv + nQ * t_fwd + nact * t_solve + nsys * t_mv)
+    return {"value": 1.0 / step, "unit": "timesteps/s", "cores": processes, "kind": "port",
+            "sample": ("oracle (numpy/scipy FP64, %d thread) timed on: 1 inverse + 1 forward 3-D transform at "
+                       "%dx%dx%d, zgbtrs on %d of the %d (kx,ky) systems (T=%d, kl=%d, ku=%d), M/L applications "
+                       "on one kx slab; extrapolated to %d stages x (%d inverse + %d forward transforms + %d solves "
+                       "+ %d operator applications); sample took %.1f s"
+                       % (processes, g.NXAA, g.NYAA, g.NZAA, nsample, nact, T, kl, ku, s.nstages, nF, nQ, nact,
+                          nsys, time.perf_counter() - t_start)),
+            "seconds_per_step_extrapolated": step}
+
+
+def run_reference(args, cfg):
+    """The reference arm: the reference itself cannot be built here (Fortran
+    2003 + MPI + FFTW3 + MKL, none installed), so its CPU restatement (the
+    oracle) is timed on the host cores, one bounded sample per step."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from coral_b200 import CONFIG_DIR
+    eq = open(os.path.join(CONFIG_DIR, cfg["eq"])).read()
+    par = open(os.path.join(CONFIG_DIR, cfg["par"])).read()
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(cfg, eq, par)
+        if i >= args.warmup:
+            vals.append(r["value"])
+    v = statistics.median(vals)
+    r["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "timesteps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.config}, "cpu_baseline": r,
+            "e2e": {"value": v, "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="rbc_384x384x192", choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    cfg = CONFIGS[args.config]
+    if args.impl == "reference":
+        run_reference(args, cfg)
+    else:
+        run_ours(args, cfg)
+
+
+if __name__ == "__main__":
+    main()

@@ -38,6 +38,10 @@ SIGNATURES = {
     "coral_import_quicksave": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_int]),
     "coral_export_checkpoint": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_int]),
     "coral_diagnostics": (ctypes.c_int, [_P, _D]),
+    "coral_set_var_phys": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _D]),
+    "coral_set_mean_var_profile": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _D]),
+    "coral_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
+    "coral_profile_step": (ctypes.c_int, [_P, ctypes.c_double, _D, ctypes.c_int]),
 }
 
 _lib = None

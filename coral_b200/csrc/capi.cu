@@ -400,7 +400,22 @@ int full_vars_to_phys(coral_handle* h, bool use_field, bool cfl) {
   return 3;
 }
 
-int enqueue_step(coral_handle* h, double dt) {
+struct PhaseTimer {
+  cudaStream_t s;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev;
+  void begin(int k) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaEventRecord(a, s);
+    ev.push_back({k, {a, b}});
+  }
+  void end() { cudaEventRecord(ev.back().second.second, s); }
+};
+
+int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
+  auto B = [&](int k) { if (pt) pt->begin(k); };
+  auto E = [&]() { if (pt) pt->end(); };
   const Dims& d = h->d;
   const Geometry& g = *h->G;
   int nl = 0;
@@ -408,11 +423,20 @@ int enqueue_step(coral_handle* h, double dt) {
   const double scale = 1.0 / ((double)g.NXAA * (double)g.NYAA * (double)g.NZAA);
   for (int i = 0; i < S; ++i) {
     const bool last = (i == S - 1);
-    nl += full_vars_to_phys(h, i == 0, true);
+    {
+      StateSet st = state_set(h, i == 0);
+      B(0); launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream); E();
+      B(1); launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream); E();
+      CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
+      B(2); launch_inv_z(d, h->nF, h->Y2, h->fphys, h->pz, h->dct_tw, h->d_wz, h->cfl_bits, h->stream); E();
+      nl += 3;
+    }
+    B(3);
     launch_fwd_z(d, h->nF, h->quads, h->fphys, h->Y2, h->pz, h->dct_tw, h->d_wz, i == 0 ? h->ke_partial : nullptr,
                  h->stream);
-    launch_fwd_x(d, h->nQ, h->Y2, h->Y1, h->px, h->stream);
-    launch_fwd_y(d, h->nQ, h->Y1, h->qspec, scale, h->py, h->stream);
+    E();
+    B(4); launch_fwd_x(d, h->nQ, h->Y2, h->Y1, h->px, h->stream); E();
+    B(5); launch_fwd_y(d, h->nQ, h->Y1, h->qspec, scale, h->py, h->stream); E();
     nl += 3;
     for (int q : h->zmean_quads) {
       launch_remove_zmean(d, h->qspec + (size_t)q * d.NXH * d.NYA * d.NZ, h->stream);
@@ -428,7 +452,7 @@ int enqueue_step(coral_handle* h, double dt) {
       na.ky = h->d_ky;
       na.act_index = h->d_act_index;
       na.Khat = k.Khat[i];
-      launch_nl(na, h->stream);
+      B(6); launch_nl(na, h->stream); E();
       SolveArgs sa{};
       sa.d = d;
       sa.T = k.T;
@@ -454,7 +478,7 @@ int enqueue_step(coral_handle* h, double dt) {
       sa.kx = h->d_kx;
       sa.ky = h->d_ky;
       sa.flags = h->flags;
-      launch_solve(sa, h->stream);
+      B(7); launch_solve(sa, h->stream); E();
       nl += 2;
     }
     if (!h->zs.empty()) {
@@ -469,7 +493,7 @@ int enqueue_step(coral_handle* h, double dt) {
         za.ch[j] = dt * h->TB.ahat(i + 1, j);
       }
       za.last_stage = last ? 1 : 0;
-      launch_zero_step(za, h->stream);
+      B(8); launch_zero_step(za, h->stream); E();
       ++nl;
     }
   }
@@ -615,6 +639,20 @@ std::string qs_name(const char* dir, const char* kind, int sys, int var, int rol
   return std::string(dir) + b;
 }
 
+// one coupled variable from a physical field already on the device ([y][x][z])
+void set_var_phys_dev(coral_handle* h, int s, int v, const double* d_phys) {
+  KSys& k = h->ks[s];
+  const Dims& d = h->d;
+  phys_to_spec_dev(h, d_phys, h->tmp_spec);
+  // clear the variable's slots, then insert its projection
+  std::vector<int> zero_slots = k.ops.var_pos[v];
+  (void)zero_slots;
+  launch_galerkin_insert(d, h->tmp_spec, k.T, k.d_var_pos[v], k.ops.var_size[v], k.d_sq_val[v], k.d_sq_col[v],
+                         k.field, h->stream);
+  h->launches += 1;
+  CK(cudaGetLastError());
+}
+
 // mean-profile (NZAA values) <-> Galerkin coefficients of one mean variable, via
 // the (0,0) column of the 3-D transforms
 void import_zero_var(coral_handle* h, ZSys& z, int v, const std::vector<double>& prof) {
@@ -641,7 +679,7 @@ void import_zero_var(coral_handle* h, ZSys& z, int v, const std::vector<double>&
   }
   std::vector<double> field(o.T);
   CK(cudaMemcpy(field.data(), z.dev.field, o.T * sizeof(double), cudaMemcpyDeviceToHost));
-  for (int c = 0; c < nc; ++c) field[o.var_pos[v][c]] += gal[c];
+  for (int c = 0; c < nc; ++c) field[o.var_pos[v][c]] = gal[c];
   CK(cudaMemcpy(z.dev.field, field.data(), o.T * sizeof(double), cudaMemcpyHostToDevice));
 }
 
@@ -892,11 +930,8 @@ int coral_import_quicksave(coral_handle* h, const char* directory, int rolling) 
         CK(cudaMemcpyAsync(h->tmp_phys, buf.data(), np * sizeof(double), cudaMemcpyHostToDevice, h->stream));
         // file order is z fastest, then y, then x: transpose to (z, x, y)
         launch_transpose_xy(d, h->tmp_phys, h->fphys, 0, h->stream);
-        phys_to_spec_dev(h, h->fphys, h->tmp_spec);
-        launch_galerkin_insert(d, h->tmp_spec, k.T, k.d_var_pos[v], k.ops.var_size[v], k.d_sq_val[v], k.d_sq_col[v],
-                               k.field, h->stream);
-        h->launches += 2;
-        CK(cudaGetLastError());
+        h->launches += 1;
+        set_var_phys_dev(h, (int)s, v, h->fphys);
         CK(cudaStreamSynchronize(h->stream));
       }
     }
@@ -931,6 +966,53 @@ int coral_export_checkpoint(coral_handle* h, const char* directory, int rolling)
     for (size_t s = 0; s < h->zs.size(); ++s)
       for (int v = 0; v < h->zs[s].ops.nV; ++v)
         write_file(qs_name(directory, "zero", (int)s + 1, v + 1, rolling), export_zero_var(h, h->zs[s], v));
+  });
+}
+
+int coral_set_var_phys(coral_handle* h, int isys, int ivar, const double* phys) {
+  return guarded(h, [&] {
+    check_sys(h, isys, false);
+    if (ivar < 0 || ivar >= h->ks[isys].ops.nV || !phys) throw CoralError(CORAL_EBADARG, "bad variable or buffer");
+    const Dims& d = h->d;
+    const size_t np = (size_t)d.NYA * d.NXA * d.NZA;
+    CK(cudaMemcpyAsync(h->tmp_phys, phys, np * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    set_var_phys_dev(h, isys, ivar, h->tmp_phys);
+    CK(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int coral_set_mean_var_profile(coral_handle* h, int isys, int ivar, const double* prof) {
+  return guarded(h, [&] {
+    check_sys(h, isys, true);
+    if (ivar < 0 || ivar >= h->zs[isys].ops.nV || !prof) throw CoralError(CORAL_EBADARG, "bad variable or buffer");
+    std::vector<double> p(prof, prof + h->d.NZA);
+    import_zero_var(h, h->zs[isys], ivar, p);
+  });
+}
+
+int coral_stream(coral_handle* h, void** stream) {
+  return guarded(h, [&] {
+    if (!stream) throw CoralError(CORAL_EBADARG, "null pointer");
+    *stream = (void*)h->stream;
+  });
+}
+
+int coral_profile_step(coral_handle* h, double dt, double* ms, int n) {
+  return guarded(h, [&] {
+    if (!ms || n < 9) throw CoralError(CORAL_EBADARG, "need 9 timing slots");
+    if (!(dt > 0.0)) throw CoralError(CORAL_EBADARG, "dt must be > 0");
+    if (h->dt_factored != dt) factorize(h, dt);
+    PhaseTimer pt{h->stream, {}};
+    h->launches += enqueue_step(h, dt, &pt);
+    CK(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < n; ++k) ms[k] = 0.0;
+    for (auto& e : pt.ev) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e.second.first, e.second.second);
+      ms[e.first] += t;
+      cudaEventDestroy(e.second.first);
+      cudaEventDestroy(e.second.second);
+    }
   });
 }
 

@@ -153,6 +153,33 @@ class PlaneLayer:
     def export_checkpoints(self, directory, rolling=1):
         self._check(self._lib.coral_export_checkpoint(self._h, os.fsencode(directory), int(rolling)))
 
+    def set_var_phys(self, isys, ivar, phys):
+        p = np.ascontiguousarray(phys, dtype=np.float64)
+        if p.shape != (self.NYAA, self.NXAA, self.NZAA):
+            raise ValueError("phys shape")
+        self._check(self._lib.coral_set_var_phys(self._h, int(isys), int(ivar), _dptr(p)))
+
+    def set_mean_var_profile(self, isys, ivar, prof):
+        p = np.ascontiguousarray(prof, dtype=np.float64)
+        if p.shape != (self.NZAA,):
+            raise ValueError("profile shape")
+        self._check(self._lib.coral_set_mean_var_profile(self._h, int(isys), int(ivar), _dptr(p)))
+
+    @property
+    def stream(self):
+        """The cudaStream_t of the handle, as an integer."""
+        v = ctypes.c_void_p()
+        self._check(self._lib.coral_stream(self._h, ctypes.byref(v)))
+        return v.value or 0
+
+    PHASES = ("inv_y", "inv_x", "inv_z", "fwd_z_products", "fwd_x", "fwd_y", "nl_assembly", "solve", "mean_systems")
+
+    def profile_step(self, dt):
+        """One eager step with CUDA events per kernel class; returns {phase: ms}."""
+        ms = np.zeros(len(self.PHASES))
+        self._check(self._lib.coral_profile_step(self._h, float(dt), _dptr(ms), len(ms)))
+        return dict(zip(self.PHASES, ms.tolist()))
+
     def diagnostics(self):
         out = np.zeros(3)
         self._check(self._lib.coral_diagnostics(self._h, _dptr(out)))

@@ -136,6 +136,34 @@ int coral_import_quicksave(coral_handle* h, const char* directory, int rolling);
 int coral_export_checkpoint(coral_handle* h, const char* directory, int rolling);
 
 /*
+ * Set one coupled variable (ivar of kxky system isys) from a physical field
+ * phys(NZAA, NXAA, NYAA), or one mean variable from a profile prof(NZAA): the
+ * per-variable step of import_quickSave (transform, square-stencil projection
+ * onto the Galerkin basis, insertion; PL_IMEX_timestepping_output.f90:338-381).
+ * The projection replaces that variable's coefficients.
+ */
+int coral_set_var_phys(coral_handle* h, int isys, int ivar, const double* phys);
+int coral_set_mean_var_profile(coral_handle* h, int isys, int ivar, const double* prof);
+
+/*
+ * The CUDA stream (a cudaStream_t, returned as void*) on which the handle
+ * queues all its work, so that callers can order their own work or record
+ * CUDA events around coral_march.
+ */
+int coral_stream(coral_handle* h, void** stream);
+
+/*
+ * Run one timestep of size dt with eager launches and CUDA events around each
+ * kernel class; ms[k] receives the device time of class k summed over the
+ * stages (k = 0 inverse y pass, 1 inverse x pass, 2 inverse z pass,
+ * 3 forward z pass with the products, 4 forward x pass, 5 forward y pass,
+ * 6 NL assembly, 7 stage update + banded solve, 8 mean systems).  n >= 9.
+ * The step advances the state exactly like coral_march(h, dt, 1).
+ * (The reference has wall-clock prints only, plane_layer_main.f90:166-171.)
+ */
+int coral_profile_step(coral_handle* h, double dt, double* ms, int n);
+
+/*
  * Diagnostics of the first stage of the last step: out[0] = cargo%cfl_based_DT
  * (marching.f90:200-254), out[1] = cargo%KE_display = sum of the volume
  * averages of uu, vv and ww (PL_IMEX_timestepping_output.f90:84-102; 0 when
