@@ -127,15 +127,16 @@ def make_ic(cfg, pl):
     pl.set_mean_var_profile(1, 0, mean)
 
 
-def solve_bytes_per_stage(pl, nact, nsys, T, ldab, stages):
+def solve_bytes_per_stage(nact, nsys, T, ldab, stages, factor_bytes):
     """Algorithmic bytes of one launch of the stage-update + banded-solve kernel,
-    averaged over the stages: LU factors + pivot bytes of the active systems,
-    and for every system the state read, the K arrays read, and the outputs."""
+    averaged over the stages: the LU factors (factor_bytes per entry: 8 when
+    stored real-scaled, 16 complex) and pivot bytes of the active systems, and
+    for every system the state read, the K arrays read and the outputs."""
     tot = 0
     for i in range(stages):
         last = (i == stages - 1)
         per_sys = 16 * T * (1 + (2 * i + 1) + 1 + (0 if last else 1))
-        tot += nsys * per_sys + nact * (16 * ldab * T + T)
+        tot += nsys * per_sys + nact * (factor_bytes * ldab * T + T)
     return tot / stages
 
 
@@ -235,7 +236,8 @@ def run_ours(args, cfg):
     nsys = pl.NXH * pl.NYAA
     nact = sum(1 for ix in range(pl.NXH) for iy in range(pl.NYAA)
                if not (iy_dealiased(iy, pl.NY, pl.NYAA)) and not (ix == 0 and iy == 0))
-    algo = solve_bytes_per_stage(pl, nact, nsys, T, ldab, pl.stages)
+    fbytes = 8 if pl.query(700) else 16
+    algo = solve_bytes_per_stage(nact, nsys, T, ldab, pl.stages, fbytes)
     launch_ms = prof["solve"] / pl.stages
     achieved = algo / (launch_ms / 1e3) / 1e9
     peak, src = read_peaks()
@@ -252,7 +254,8 @@ def run_ours(args, cfg):
                                % (args.config, cfg["Ra"], pl.NX, pl.NY, pl.NZ, pl.NXAA, pl.NYAA, pl.NZAA, dt),
                    "grid_points": pl.NXAA * pl.NYAA * pl.NZAA, "systems": nsys, "active_systems": nact, "T": T,
                    "band": [kl, ku], "l2": "inputs larger than L2 (state %.2f GB, LU factors %.1f GB)"
-                   % (field.nbytes / 1e9, nact * ldab * T * 16 / 1e9),
+                   % (field.nbytes / 1e9, nact * ldab * T * fbytes / 1e9),
+                   "lu_factors": "real-scaled" if fbytes == 8 else "complex",
                    "parallelism": "replicas x%d" % world},
         "grid_point_steps_per_s": value * pl.NXAA * pl.NYAA * pl.NZAA,
         "e2e": e2e,

@@ -3,6 +3,7 @@
 // stream and a CUDA graph of one timestep.
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <memory>
@@ -69,7 +70,10 @@ struct KSys {
   double2 *field, *aux;
   double2* Kstd[kMaxStages];
   double2* Khat[kMaxStages];
-  double2* ab;
+  double2* ab;           // complex LAPACK-band factors (general recipes)
+  double* abr;           // real-scaled factors (recipes that admit the +-i scaling)
+  bool real = false;
+  unsigned char *rowflip = nullptr, *colflip = nullptr;
   unsigned char* dpiv;
   int* info;
   std::vector<std::vector<int>> tab_t;   // per var: [NZ][kTabW]
@@ -158,9 +162,18 @@ DevEll upload_ell(DevAlloc& mem, const EllOp& op) {
     e.gkx[g] = op.groups[g].first;
     e.gky[g] = op.groups[g].second;
   }
-  e.col = mem.upload(op.col);
-  e.val = mem.upload(op.val);
-  e.grp = mem.upload(op.grp);
+  std::vector<int> cg((size_t)op.rows * op.width, 0);
+  std::vector<double> val((size_t)op.rows * op.width, 0.0);
+  for (int r = 0; r < op.rows; ++r)
+    for (int k = 0; k < op.width; ++k) {
+      const size_t src = (size_t)r * op.width + k, dst = (size_t)k * op.rows + r;
+      if (op.col[src] < 0) continue;
+      if (op.col[src] >= (1 << 24)) throw CoralError(CORAL_EUNSUPPORTED, "operator column index too large");
+      cg[dst] = op.col[src] | (op.grp[src] << 24);
+      val[dst] = op.val[src];
+    }
+  e.cg = mem.upload(cg);
+  e.val = mem.upload(val);
   return e;
 }
 
@@ -243,6 +256,7 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
     k.kl = k.ops.kl;
     k.ku = k.ops.ku;
     k.ldab = 2 * k.kl + k.ku + 1;
+    k.ldab += k.ldab & 1;  // even column stride: every column starts on a 16-byte boundary
     if (k.kl > 31 || k.kl + k.ku > 64)
       throw CoralError(CORAL_EUNSUPPORTED, "band of the coupled system exceeds kl <= 31, kl+ku <= 64");
     k.M = upload_ell(mem, k.ops.M);
@@ -257,7 +271,13 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
       k.Kstd[i] = (i < h->TB.stages - 1) ? mem.get<double2>(n) : nullptr;
       k.Khat[i] = (i < h->TB.stages) ? mem.get<double2>(n) : nullptr;
     }
-    k.ab = mem.get<double2>((size_t)h->nact * k.T * k.ldab);
+    k.real = k.ops.real_scalable && k.kl <= 16 && k.kl + k.ku <= 63 && std::getenv("CORAL_COMPLEX_FACTORS") == nullptr;
+    k.ab = nullptr;
+    k.abr = nullptr;
+    if (k.real) k.abr = mem.get<double>((size_t)h->nact * k.T * k.ldab);
+    else k.ab = mem.get<double2>((size_t)h->nact * k.T * k.ldab);
+    k.rowflip = mem.upload(k.ops.row_flip);
+    k.colflip = mem.upload(k.ops.col_flip);
     k.dpiv = mem.get<unsigned char>((size_t)h->nact * k.T);
     k.info = mem.get<int>((size_t)std::max(h->nact, 1));
     for (int v = 0; v < k.ops.nV; ++v) {
@@ -463,6 +483,7 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       sa.L = k.L;
       sa.field = k.field;
       sa.out = last ? k.field : k.aux;
+      sa.work = k.aux;
       sa.Kstd_out = last ? nullptr : k.Kstd[i];
       sa.nprev = i;
       for (int j = 0; j <= i; ++j) {
@@ -478,7 +499,18 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       sa.kx = h->d_kx;
       sa.ky = h->d_ky;
       sa.flags = h->flags;
-      B(7); launch_solve(sa, h->stream); E();
+      sa.abr = k.abr;
+      sa.rowflip = k.rowflip;
+      sa.colflip = k.colflip;
+      {
+        const int kv = k.kl + k.ku;
+        const int u_rows = (kv + 2) & ~1, l_rows = ((kv + 1 + k.kl + 1) & ~1) - ((kv + 1) & ~1);
+        sa.ring_cols = std::max(u_rows, l_rows);
+      }
+      B(7);
+      if (k.real) launch_solve_real(sa, h->stream);
+      else launch_solve(sa, h->stream);
+      E();
       nl += 2;
     }
     if (!h->zs.empty()) {
@@ -521,7 +553,11 @@ void factorize(coral_handle* h, double dt) {
     fa.kx = h->d_kx;
     fa.ky = h->d_ky;
     fa.info = k.info;
-    launch_factor(fa, h->stream);
+    fa.abr = k.abr;
+    fa.rowflip = k.rowflip;
+    fa.colflip = k.colflip;
+    if (k.real) launch_factor_real(fa, h->stream);
+    else launch_factor(fa, h->stream);
     ++h->launches;
   }
   if (!h->zs.empty()) {
@@ -816,6 +852,7 @@ int coral_query(const coral_handle* hc, int what, long long* value) {
   if (base == CORAL_Q_ZSYS_NVARS && i < (int)h->zs.size()) { *value = h->zs[i].ops.nV; return 0; }
   if (base == CORAL_Q_SYS_KL && i < (int)h->ks.size()) { *value = h->ks[i].kl; return 0; }
   if (base == CORAL_Q_SYS_KU && i < (int)h->ks.size()) { *value = h->ks[i].ku; return 0; }
+  if (base == CORAL_Q_SYS_REAL && i < (int)h->ks.size()) { *value = h->ks[i].real ? 1 : 0; return 0; }
   return CORAL_EBADARG;
 }
 

@@ -16,13 +16,18 @@ constexpr int kMaxFull = 8;     // full variables
 constexpr int kMaxFullTerms = 8;
 constexpr int kTabW = 5;        // Galerkin -> Chebyshev entries per Chebyshev row
 
-// Row-list operator: y[r] = sum_k coef[grp[r,k]] * val[r,k] * x[col[r,k]]
+// Row-list operator: y[r] = sum_k coef[grp(r,k)] * val(r,k) * x[col(r,k)].
+// Stored slot-major ([k][r]) so that a warp reading rows r..r+31 of one slot
+// touches consecutive words; the group index sits in the top byte of the
+// column word; empty slots hold column 0 and value 0.
 struct DevEll {
   int rows, width, ngroups;
   int gkx[kMaxGroups], gky[kMaxGroups];
-  const int* col;
+  const int* cg;
   const double* val;
-  const int* grp;
+  __device__ __forceinline__ int col(int r, int k) const { return cg[(size_t)k * rows + r] & 0xFFFFFF; }
+  __device__ __forceinline__ int grp(int r, int k) const { return cg[(size_t)k * rows + r] >> 24; }
+  __device__ __forceinline__ double v(int r, int k) const { return val[(size_t)k * rows + r]; }
 };
 
 // one term of a full variable build: dsca * (i kx)^dx (i ky)^dy * S_var g
@@ -88,6 +93,7 @@ struct SolveArgs {
   DevEll M, L;
   const double2* field;
   double2* out;          // aux (or field itself in the last stage)
+  double2* work;         // scratch vectors of the register-window solve (aux)
   double2* Kstd_out;     // null in the last stage
   int nprev;             // stage index i (0-based): Kstd[0..i-1], Khat[0..i]
   const double2* Kstd[kMaxStages];
@@ -101,8 +107,16 @@ struct SolveArgs {
   const double* kx;
   const double* ky;
   unsigned int* flags;   // bit 0: non-finite value produced
+  // real-scaled factors (see SystemOps::real_scalable): rows flagged in rowflip
+  // are multiplied by -i before the solve, columns flagged in colflip by +i after
+  const double* abr;
+  const unsigned char* rowflip;
+  const unsigned char* colflip;
+  int ring_cols;         // doubles per column slot of the solve's shared-memory ring
 };
 void launch_solve(const SolveArgs& a, cudaStream_t s);
+// register-window variant for real-scaled factors with kl <= 16, kl+ku <= 63
+void launch_solve_real(const SolveArgs& a, cudaStream_t s);
 
 struct FactorArgs {
   Dims d;
@@ -115,8 +129,12 @@ struct FactorArgs {
   const double* kx;
   const double* ky;
   int* info;             // first zero pivot (1-based column) per system, 0 if none
+  double* abr;           // real-scaled factors (when rowflip/colflip are set)
+  const unsigned char* rowflip;
+  const unsigned char* colflip;
 };
 void launch_factor(const FactorArgs& a, cudaStream_t s);
+void launch_factor_real(const FactorArgs& a, cudaStream_t s);
 
 // mean (kx = ky = 0) systems, real arithmetic
 struct ZeroSysDev {

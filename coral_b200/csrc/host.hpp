@@ -135,6 +135,12 @@ struct SystemOps {
   EllOp NLop;                                     // col = quad*NZ + n
   // Galerkin -> Chebyshev: for var v, row n: entries (galerkin coef c, value)
   std::vector<std::vector<std::vector<std::pair<int, double>>>> stencil_rows;
+  // Real scaling: when every entry of E = M - dt a L is real or imaginary in a
+  // pattern that multiplying some variables by i and some equations by -i turns
+  // real, row_flip[t] / col_flip[t] mark the rows (equations) and columns
+  // (variables) of that diagonal scaling and real_scalable is true.
+  bool real_scalable = false;
+  std::vector<unsigned char> row_flip, col_flip;
   // square stencil (var_size x var_size, lower-banded) for projections of
   // Chebyshev coefficients onto the Galerkin basis (QuickSave import)
   std::vector<Dense> sq_stencil;

@@ -2,6 +2,7 @@
 // Chebyshev matrices, Galerkin stencils and the assembly of the coupled
 // systems' operators in the interleaved polynomial ordering.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -567,6 +568,42 @@ SystemOps assemble_system(const Geometry& g, const Recipe& r, const CoupledSet& 
     }
     finish_ell(o.NLop, o.T, tr);
     if (o.NLop.groups.empty()) o.NLop.groups.emplace_back(0, 0);
+  }
+  // real scaling: parity of (i kx)^a (i ky)^b is a+b; an entry of equation e and
+  // variable v becomes real under the scaling iff r_e = (a+b+s_v) mod 2
+  {
+    const int nV = o.nV;
+    std::vector<int> r_e(nV, -1), s_v(nV, -1);
+    std::vector<std::array<int, 3>> edges;  // (e, v, parity)
+    for (const auto* pieces : {&s.mass, &s.stif})
+      for (const Piece& p : *pieces) edges.push_back({p.iEqn, p.jVar, (p.kx + p.ky) & 1});
+    bool ok = true;
+    // propagate from each unlabelled equation
+    for (int start = 0; start < nV && ok; ++start) {
+      if (r_e[start] >= 0) continue;
+      r_e[start] = 0;
+      bool changed = true;
+      while (changed && ok) {
+        changed = false;
+        for (auto& ed : edges) {
+          int e = ed[0], v = ed[1], par = ed[2];
+          if (r_e[e] >= 0 && s_v[v] < 0) { s_v[v] = (r_e[e] + par) & 1; changed = true; }
+          else if (s_v[v] >= 0 && r_e[e] < 0) { r_e[e] = (s_v[v] + par) & 1; changed = true; }
+          else if (s_v[v] >= 0 && r_e[e] >= 0 && r_e[e] != ((s_v[v] + par) & 1)) ok = false;
+        }
+      }
+    }
+    for (int v = 0; v < nV; ++v)
+      if (s_v[v] < 0) s_v[v] = 0;
+    o.real_scalable = ok;
+    o.row_flip.assign(o.T, 0);
+    o.col_flip.assign(o.T, 0);
+    if (ok) {
+      for (int e = 0; e < nV; ++e)
+        for (int rr : o.eq_pos[e]) o.row_flip[rr] = (unsigned char)r_e[e];
+      for (int v = 0; v < nV; ++v)
+        for (int c : o.var_pos[v]) o.col_flip[c] = (unsigned char)s_v[v];
+    }
   }
   // stencil rows and square stencils
   o.stencil_rows.resize(o.nV);

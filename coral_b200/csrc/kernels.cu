@@ -363,13 +363,13 @@ __global__ void __launch_bounds__(kWPB * 32) k_nl(NLArgs a) {
   for (int t = lane; t < a.T; t += 32) {
     double2 acc = zero2();
     for (int k = 0; act && k < a.NL.width; ++k) {
-      const int c = a.NL.col[(size_t)t * a.NL.width + k];
-      if (c < 0) break;
+      const double v = a.NL.v(t, k);
+      if (v == 0.0) break;  // slots are filled in order; exact zeros are not stored
+      const int c = a.NL.col(t, k);
       const int qv = c / NZ, n = c - qv * NZ;
       const double2 qh = a.qspec[(((size_t)qv * a.d.NXH + kx) * a.d.NYA + ky) * NZ + n];
-      const double v = a.NL.val[(size_t)t * a.NL.width + k];
       double2 cv = coef[0];
-      const int g = a.NL.grp[(size_t)t * a.NL.width + k];
+      const int g = a.NL.grp(t, k);
 #pragma unroll
       for (int gg = 1; gg < kMaxGroups; ++gg)
         if (g == gg) cv = coef[gg];
@@ -390,13 +390,12 @@ constexpr int kPF = 8;  // factor columns prefetched ahead
 
 __device__ __forceinline__ double2 ell_row(const DevEll& op, int t, const double2* coef, const double2* x) {
   double2 acc = zero2();
+#pragma unroll 4
   for (int k = 0; k < op.width; ++k) {
-    const size_t e = (size_t)t * op.width + k;
-    const int c = op.col[e];
-    if (c < 0) break;
-    const double v = op.val[e];
-    const double2 xv = x[c];
-    acc = cadd(acc, cmul(coef[op.grp[e]], make_double2(v * xv.x, v * xv.y)));
+    const int cg = op.cg[(size_t)k * op.rows + t];
+    const double v = op.val[(size_t)k * op.rows + t];
+    const double2 xv = x[cg & 0xFFFFFF];
+    acc = cadd(acc, cmul(coef[cg >> 24], make_double2(v * xv.x, v * xv.y)));
   }
   return acc;
 }
@@ -556,28 +555,26 @@ __global__ void __launch_bounds__(kWPB * 32) k_factor(FactorArgs a) {
   // E(t,c) = M(t,c) + zsca * L(t,c); lane owns rows t = lane mod 32 (no write conflicts)
   for (int t = lane; t < T; t += 32) {
     for (int k = 0; k < a.M.width; ++k) {
-      const size_t e = (size_t)t * a.M.width + k;
-      const int c = a.M.col[e];
-      if (c < 0) break;
+      const double v = a.M.v(t, k);
+      if (v == 0.0) continue;  // empty slot
+      const int c = a.M.col(t, k), g = a.M.grp(t, k);
       double2 cv = zero2();
-      const int g = a.M.grp[e];
 #pragma unroll
       for (int gg = 0; gg < kMaxGroups; ++gg)
         if (g == gg) cv = cm[gg];
       double2& dst = ab[(size_t)c * ldab + kv + t - c];
-      dst = cadd(dst, cscale(cv, a.M.val[e]));
+      dst = cadd(dst, cscale(cv, v));
     }
     for (int k = 0; k < a.L.width; ++k) {
-      const size_t e = (size_t)t * a.L.width + k;
-      const int c = a.L.col[e];
-      if (c < 0) break;
+      const double v = a.L.v(t, k);
+      if (v == 0.0) continue;
+      const int c = a.L.col(t, k), g = a.L.grp(t, k);
       double2 cv = zero2();
-      const int g = a.L.grp[e];
 #pragma unroll
       for (int gg = 0; gg < kMaxGroups; ++gg)
         if (g == gg) cv = cl[gg];
       double2& dst = ab[(size_t)c * ldab + kv + t - c];
-      dst = cadd(dst, cscale(cscale(cv, a.L.val[e]), a.zsca));
+      dst = cadd(dst, cscale(cscale(cv, v), a.zsca));
     }
   }
   __syncwarp();
@@ -639,17 +636,353 @@ __global__ void __launch_bounds__(kWPB * 32) k_factor(FactorArgs a) {
   if (lane == 0) a.info[sys] = info;
 }
 
+
+// ------------------------------------------------------------------------------
+// Real-scaled factorisation: E' = S_r E S_c with S_r = diag(-i on flagged
+// equation rows), S_c = diag(+i on flagged variable columns) is real; the
+// partial-pivoting choices equal those on E because |re|+|im| is unchanged by
+// the +-i factors.  Real ZGBTF2-equivalent (DGBTF2), one warp per system, in place
+// in LAPACK band storage; pivot offsets as bytes; U's diagonal as its reciprocal.
+// ------------------------------------------------------------------------------
+__device__ __forceinline__ double2 flip_row(double2 z, int f) { return f ? make_double2(z.y, -z.x) : z; }  // * (-i)
+__device__ __forceinline__ double2 flip_col(double2 z, int f) { return f ? make_double2(-z.y, z.x) : z; }  // * (+i)
+
+__global__ void __launch_bounds__(kWPB * 32) k_factor_real(FactorArgs a) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sys = blockIdx.x * kWPB + warp;
+  if (sys >= a.nact) return;
+  const int T = a.T, kl = a.kl, ku = a.ku, kv = kl + ku, ldab = a.ldab;
+  const int sid = a.act_list[sys];
+  const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
+  double2 cm[kMaxGroups], cl[kMaxGroups];
+#pragma unroll
+  for (int g = 0; g < kMaxGroups; ++g) {
+    cm[g] = (g < a.M.ngroups) ? cmul(ipow(a.kx[kx], a.M.gkx[g]), ipow(a.ky[ky], a.M.gky[g])) : zero2();
+    cl[g] = (g < a.L.ngroups) ? cmul(ipow(a.kx[kx], a.L.gkx[g]), ipow(a.ky[ky], a.L.gky[g])) : zero2();
+  }
+  double* ab = a.abr + (size_t)sys * T * ldab;
+  for (size_t e = lane; e < (size_t)T * ldab; e += 32) ab[e] = 0.0;
+  __syncwarp();
+  for (int t = lane; t < T; t += 32) {
+    const int rf = a.rowflip[t];
+    for (int pass = 0; pass < 2; ++pass) {
+      const DevEll& op = pass ? a.L : a.M;
+      for (int k = 0; k < op.width; ++k) {
+        const double v = op.v(t, k);
+        if (v == 0.0) continue;  // empty slot
+        const int c = op.col(t, k), g = op.grp(t, k);
+        double2 cv = zero2();
+#pragma unroll
+        for (int gg = 0; gg < kMaxGroups; ++gg)
+          if (g == gg) cv = pass ? cl[gg] : cm[gg];
+        double2 z = cscale(cv, v);
+        if (pass) z = cscale(z, a.zsca);
+        z = flip_col(flip_row(z, rf), a.colflip[c]);
+        ab[(size_t)c * ldab + kv + t - c] += z.x;
+      }
+    }
+  }
+  __syncwarp();
+  int ju = 0, info = 0;
+  for (int j = 0; j < T; ++j) {
+    const int km = min(kl, T - 1 - j);
+    double mag = -1.0;
+    int idx = 1 << 30;
+    if (lane <= km) {
+      mag = fabs(ab[(size_t)j * ldab + kv + lane]);
+      idx = lane;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double m2 = __shfl_xor_sync(0xffffffffu, mag, o);
+      const int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
+      if (m2 > mag || (m2 == mag && i2 < idx)) { mag = m2; idx = i2; }
+    }
+    const int jp = idx;
+    if (lane == 0) a.dpiv[(size_t)sys * T + j] = (unsigned char)jp;
+    const double piv = ab[(size_t)j * ldab + kv + jp];
+    if (piv == 0.0) {
+      if (info == 0) info = j + 1;
+      continue;
+    }
+    ju = max(ju, min(j + ku + jp, T - 1));
+    if (jp != 0) {
+      for (int c = j + lane; c <= ju; c += 32) {
+        double* p1 = ab + (size_t)c * ldab + kv + j + jp - c;
+        double* p0 = ab + (size_t)c * ldab + kv + j - c;
+        const double t0 = *p0;
+        *p0 = *p1;
+        *p1 = t0;
+      }
+      __syncwarp();
+    }
+    const double r = 1.0 / ab[(size_t)j * ldab + kv];
+    __syncwarp();
+    if (km > 0) {
+      if (lane >= 1 && lane <= km) ab[(size_t)j * ldab + kv + lane] *= r;
+      __syncwarp();
+      const int nc = ju - j;
+      for (int e = lane; e < nc * km; e += 32) {
+        const int c = j + 1 + e / km, i = 1 + e % km;
+        ab[(size_t)c * ldab + kv + j + i - c] -= ab[(size_t)j * ldab + kv + i] * ab[(size_t)c * ldab + kv + j - c];
+      }
+    }
+    __syncwarp();
+    if (lane == 0) ab[(size_t)j * ldab + kv] = r;
+    __syncwarp();
+  }
+  if (lane == 0) a.info[sys] = info;
+}
+
+// ------------------------------------------------------------------------------
+// Stage update + banded solve with real-scaled factors, one warp per system,
+// no shared-memory vectors: the right-hand side and the intermediate solutions
+// pass through the work array (L2-resident), while the active part of the
+// band lives in registers, each lane owning the positions p = lane (mod 32):
+//   forward  window [j, j+kl] (kl <= 31), one register per lane
+//   backward window [j-kv, j] (kv <= 63), two registers per lane
+// so a column step moves only the pivot value between lanes.  Factor entries
+// are loaded straight into the owning lane and prefetched in register rings
+// (16 columns of L, 8 columns of U).
+// ------------------------------------------------------------------------------
+constexpr int kWPBr = 4;   // warps per CTA
+constexpr int kCW = 8;     // factor columns per ring chunk (divides 32)
+constexpr int kNBUF = 4;   // ring chunks per warp
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ double2 shfl2(double2 v, int src) {
+  return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
+__global__ void __launch_bounds__(kWPBr * 32) k_solve_real(SolveArgs a) {
+  extern __shared__ double smr[];
+  __shared__ double2 coefs[kWPBr][2][kMaxGroups];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sid = blockIdx.x * kWPBr + warp;
+  const int nsys = a.d.NXH * a.d.NYA;
+  if (sid >= nsys) return;
+  const int T = a.T;
+  const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
+  const int act = a.act_index[sid];
+  const bool origin = (kx == 0 && ky == 0);
+  if (lane < kMaxGroups) {
+    coefs[warp][0][lane] = (lane < a.M.ngroups) ? cmul(ipow(a.kx[kx], a.M.gkx[lane]), ipow(a.ky[ky], a.M.gky[lane])) : zero2();
+    coefs[warp][1][lane] = (lane < a.L.ngroups) ? cmul(ipow(a.kx[kx], a.L.gkx[lane]), ipow(a.ky[ky], a.L.gky[lane])) : zero2();
+  }
+  __syncwarp();
+  const double2* field = a.field + (size_t)sid * T;
+  double2* x = a.work + (size_t)sid * T;  // never aliases field: M field is read while x is written
+  // ---- right-hand side (rows scaled by -i where flagged)
+  for (int t = lane; t < T; t += 32) {
+    double2 r = origin ? zero2() : ell_row(a.M, t, coefs[warp][0], field);
+    for (int j = 0; j < a.nprev; ++j) {
+      r = cadd(r, cscale(a.Kstd[j][(size_t)sid * T + t], a.ca[j]));
+      r = cadd(r, cscale(a.Khat[j][(size_t)sid * T + t], a.ch[j]));
+    }
+    r = cadd(r, cscale(a.Khat[a.nprev][(size_t)sid * T + t], a.ch[a.nprev]));
+    if (act >= 0) r = flip_row(r, a.rowflip[t]);
+    x[t] = r;
+  }
+  __syncwarp();
+  if (act >= 0) {
+    const int kl = a.kl, kv = a.kl + a.ku, ldab = a.ldab;
+    const double* ab = a.abr + (size_t)act * T * ldab;
+    const unsigned char* dp = a.dpiv + (size_t)act * T;
+    // Factor columns stream through a per-warp shared-memory ring (kNBUF chunks
+    // of kCW columns) with cp.async, kNBUF-1 chunks ahead of the sweep; the
+    // forward sweep copies only the L rows of each column, the backward sweep
+    // only the U rows.  (ldab is even, so both row ranges are 16-byte aligned.)
+    double* ring = smr + (size_t)warp * kNBUF * kCW * a.ring_cols;
+    const int u_rows = (kv + 2) & ~1;                 // rows [0, u_rows) hold U (+ maybe one L row)
+    const int l_row0 = (kv + 1) & ~1;                 // rows [l_row0, l_row1) hold L
+    const int l_rows = ((kv + 1 + kl + 1) & ~1) - l_row0;
+    // ================= forward: P and L =================
+    // lane l owns the positions p = l (mod 32); the active window is [j, j+kl].
+    // Vector traffic moves in blocks of 32 columns: the owner of column j takes
+    // the new position j+32 (loaded one block ahead) and parks y_j until the
+    // block's coalesced store.
+    {
+      const int nchunks = (T - 1 + kCW - 1) / kCW;
+      auto issue = [&](int c) {  // columns [c*kCW, min(T-1, c*kCW+kCW)) of L
+        if (c < nchunks) {
+          const int j0 = c * kCW, nc = min(kCW, T - 1 - j0);
+          double* dst = ring + (size_t)(c % kNBUF) * kCW * a.ring_cols;
+          const int per = l_rows / 2;  // 16-byte pieces per column
+          for (int e = lane; e < nc * per; e += 32) {
+            const int q = e / per, r = e - q * per;
+            cp_async16(dst + q * a.ring_cols + 2 * r, ab + (size_t)(j0 + q) * ldab + l_row0 + 2 * r);
+          }
+        }
+        cp_async_commit();
+      };
+#pragma unroll
+      for (int c = 0; c < kNBUF - 1; ++c) issue(c);
+      double2 w = (lane < T) ? x[lane] : zero2();
+      double2 incCur = (32 + lane < T) ? x[32 + lane] : zero2();
+      double2 incNext = zero2(), ysave = zero2();
+      int pv = 0, pvNext = (lane < T) ? dp[lane] : 0;
+      for (int c = 0; c < nchunks; ++c) {
+        const int j0 = c * kCW;
+        if ((j0 & 31) == 0) {  // new block of 32 columns: its pivots, prefetches for the next block
+          pv = pvNext;
+          pvNext = (j0 + 32 + lane < T) ? dp[j0 + 32 + lane] : 0;
+          incNext = (j0 + 64 + lane < T) ? x[j0 + 64 + lane] : zero2();
+        }
+        __syncwarp();
+        issue(c + kNBUF - 1);
+        cp_async_wait<kNBUF - 1>();
+        __syncwarp();
+        const double* cb = ring + (size_t)(c % kNBUF) * kCW * a.ring_cols;
+#pragma unroll
+        for (int q = 0; q < kCW; ++q) {
+          const int j = j0 + q;
+          if (j < T - 1) {
+            const int src = j & 31;
+            const int i = (lane - j) & 31;
+            const int lm = min(kl, T - 1 - j);
+            const double lv = (i >= 1 && i <= lm) ? cb[q * a.ring_cols + (kv + i - l_row0)] : 0.0;
+            const int jp = __shfl_sync(0xffffffffu, pv, j & 31);
+            if (jp != 0) {
+              const int r2 = (j + jp) & 31;
+              const double2 a0 = shfl2(w, r2), aj = shfl2(w, src);
+              if (lane == src) w = a0;
+              else if (lane == r2) w = aj;
+            }
+            const double2 bj = shfl2(w, src);
+            w.x -= lv * bj.x;
+            w.y -= lv * bj.y;
+            if (lane == src) {
+              ysave = w;
+              w = incCur;
+            }
+            if ((j & 31) == 31) {  // end of a block of 32 columns
+              x[j - 31 + lane] = ysave;
+              incCur = incNext;
+            }
+          }
+        }
+      }
+      cp_async_wait<0>();
+      // the last (partial) block of y values and y[T-1]
+      const int base = ((T - 1) >> 5) << 5;
+      if ((T - 1) & 31) {
+        if (base + lane <= T - 2) x[base + lane] = ysave;
+      }
+      if (lane == ((T - 1) & 31)) x[T - 1] = w;
+    }
+    __syncwarp();
+    // ================= backward: U (kl+ku super-diagonals, reciprocal diagonal) =================
+    // lane l owns p = l (mod 32) in two registers: w0 for (p>>5) even, w1 for odd.
+    // Blocks of 32 columns j = T-1-32b-s; the owner of j takes position j-64.
+    {
+      double2 w0 = zero2(), w1 = zero2();
+      {
+        const int ih = (T - 1 - lane) & 31, ph = T - 1 - ih, pl = ph - 32;
+        if (ph >= 0) { if ((ph >> 5) & 1) w1 = x[ph]; else w0 = x[ph]; }
+        if (pl >= 0) { if ((pl >> 5) & 1) w1 = x[pl]; else w0 = x[pl]; }
+      }
+      const int nchunks = (T + kCW - 1) / kCW;  // chunk c: columns T-1-c*kCW-q, q < kCW
+      auto issue = [&](int c) {
+        if (c < nchunks) {
+          const int jhi = T - 1 - c * kCW, jlo = max(0, jhi - kCW + 1), nc = jhi - jlo + 1;
+          double* dst = ring + (size_t)(c % kNBUF) * kCW * a.ring_cols;
+          const int per = u_rows / 2;
+          for (int e = lane; e < nc * per; e += 32) {
+            const int q = e / per, r = e - q * per;  // q counts down from jhi
+            cp_async16(dst + q * a.ring_cols + 2 * r, ab + (size_t)(jhi - q) * ldab + 2 * r);
+          }
+        }
+        cp_async_commit();
+      };
+      __syncwarp();
+#pragma unroll
+      for (int c = 0; c < kNBUF - 1; ++c) issue(c);
+      auto own_col = [&](int b) {  // column of block b finished by this lane (may be < 0)
+        const int top = T - 1 - 32 * b;
+        return top - ((top - lane) & 31);
+      };
+      int jl = own_col(0);
+      double2 incCur = (jl - 64 >= 0) ? x[jl - 64] : zero2();
+      int cfCur = (jl >= 0) ? a.colflip[jl] : 0;
+      double2 incNext = zero2(), xsave = zero2();
+      int cfNext = 0, jn = jl;
+      for (int c = 0; c < nchunks; ++c) {
+        const int k0 = c * kCW;  // steps taken before this chunk
+        if ((k0 & 31) == 0) {
+          jn = own_col((k0 >> 5) + 1);
+          incNext = (jn - 64 >= 0) ? x[jn - 64] : zero2();
+          cfNext = (jn >= 0) ? a.colflip[jn] : 0;
+        }
+        __syncwarp();
+        issue(c + kNBUF - 1);
+        cp_async_wait<kNBUF - 1>();
+        __syncwarp();
+        const double* cb = ring + (size_t)(c % kNBUF) * kCW * a.ring_cols;
+#pragma unroll
+        for (int q = 0; q < kCW; ++q) {
+          const int k = k0 + q;
+          const int j = T - 1 - k;
+          if (j >= 0) {
+            const int src = j & 31, sel = (j >> 5) & 1;
+            const double* col = cb + q * a.ring_cols;
+            const int ih = (j - lane) & 31, il = ih + 32;
+            const double h = (ih >= 1 && ih <= kv) ? col[kv - ih] : 0.0;
+            const double l_ = (il <= kv) ? col[kv - il] : 0.0;
+            const double d = col[kv];
+            const double2 yj = shfl2(sel ? w1 : w0, src);
+            const double2 xj = make_double2(yj.x * d, yj.y * d);
+            const int hreg = ((j - ih) >> 5) & 1;
+            if (hreg) { w1.x -= h * xj.x; w1.y -= h * xj.y; w0.x -= l_ * xj.x; w0.y -= l_ * xj.y; }
+            else      { w0.x -= h * xj.x; w0.y -= h * xj.y; w1.x -= l_ * xj.x; w1.y -= l_ * xj.y; }
+            if (lane == src) {
+              xsave = flip_col(xj, cfCur);
+              if (sel) w1 = incCur; else w0 = incCur;
+            }
+            if ((k & 31) == 31) {  // end of a block of 32 columns
+              if (jl >= 0) x[jl] = xsave;
+              jl = jn;
+              incCur = incNext;
+              cfCur = cfNext;
+            }
+          }
+        }
+      }
+      cp_async_wait<0>();
+      if ((T & 31) != 0 && jl >= 0) x[jl] = xsave;  // the last (partial) block
+    }
+  }
+  __syncwarp();
+  // ---- outputs (the last stage writes the new state into field)
+  bool bad = false;
+  const bool zero_out = a.last_stage && (act < 0);
+  double2* out = a.out + (size_t)sid * T;
+  for (int t = lane; t < T; t += 32) {
+    const double2 v = zero_out ? zero2() : x[t];
+    bad |= !(isfinite(v.x) && isfinite(v.y));
+    if (out != x || zero_out) out[t] = v;
+  }
+  __syncwarp();
+  if (a.Kstd_out) {
+    double2* ko = a.Kstd_out + (size_t)sid * T;
+    for (int t = lane; t < T; t += 32) ko[t] = (act >= 0) ? ell_row(a.L, t, coefs[warp][1], x) : zero2();
+  }
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.flags, 1u);
+}
+
 // ------------------------------------------------------------------------------
 // mean (kx = ky = 0) systems: real arithmetic, one warp per system
 // ------------------------------------------------------------------------------
 __device__ double ell_row_real(const DevEll& op, int t, const double* x) {
   double acc = 0.0;
-  for (int k = 0; k < op.width; ++k) {
-    const size_t e = (size_t)t * op.width + k;
-    const int c = op.col[e];
-    if (c < 0) break;
-    acc += op.val[e] * x[c];
-  }
+  for (int k = 0; k < op.width; ++k) acc += op.v(t, k) * x[op.col(t, k)];
   return acc;
 }
 
@@ -666,11 +999,9 @@ __global__ void k_zero_step(ZeroArgs a) {
   for (int t = lane; t < T; t += 32) {
     double acc = 0.0;
     for (int k = 0; k < z.NL.width; ++k) {
-      const size_t e = (size_t)t * z.NL.width + k;
-      const int c = z.NL.col[e];
-      if (c < 0) break;
+      const int c = z.NL.col(t, k);
       const int qv = c / a.d.NZ, n = c - qv * a.d.NZ;
-      acc += z.NL.val[e] * a.qspec[(size_t)qv * a.d.NXH * a.d.NYA * a.d.NZ + n].x;
+      acc += z.NL.v(t, k) * a.qspec[(size_t)qv * a.d.NXH * a.d.NYA * a.d.NZ + n].x;
     }
     kh[t] = acc;
   }
@@ -716,16 +1047,16 @@ __global__ void k_zero_factor(ZeroArgs a) {
   for (size_t e = 0; e < (size_t)T * ldab; ++e) ab[e] = 0.0;
   for (int t = 0; t < T; ++t) {
     for (int k = 0; k < z.M.width; ++k) {
-      const size_t e = (size_t)t * z.M.width + k;
-      const int c = z.M.col[e];
-      if (c < 0) break;
-      ab[(size_t)c * ldab + kv + t - c] += z.M.val[e];
+      const double v = z.M.v(t, k);
+      if (v == 0.0) continue;
+      const int c = z.M.col(t, k);
+      ab[(size_t)c * ldab + kv + t - c] += v;
     }
     for (int k = 0; k < z.L.width; ++k) {
-      const size_t e = (size_t)t * z.L.width + k;
-      const int c = z.L.col[e];
-      if (c < 0) break;
-      ab[(size_t)c * ldab + kv + t - c] += a.zsca * z.L.val[e];
+      const double v = z.L.v(t, k);
+      if (v == 0.0) continue;
+      const int c = z.L.col(t, k);
+      ab[(size_t)c * ldab + kv + t - c] += a.zsca * v;
     }
   }
   int ju = 0, info = 0;
@@ -891,6 +1222,16 @@ void launch_solve(const SolveArgs& a, cudaStream_t s) {
 void launch_factor(const FactorArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;
   k_factor<<<(a.nact + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
+}
+void launch_solve_real(const SolveArgs& a, cudaStream_t s) {
+  const int nsys = a.d.NXH * a.d.NYA;
+  const size_t sm = (size_t)kWPBr * kNBUF * kCW * a.ring_cols * sizeof(double);
+  set_smem(k_solve_real, sm);
+  k_solve_real<<<(nsys + kWPBr - 1) / kWPBr, kWPBr * 32, sm, s>>>(a);
+}
+void launch_factor_real(const FactorArgs& a, cudaStream_t s) {
+  if (a.nact <= 0) return;
+  k_factor_real<<<(a.nact + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
 }
 void launch_zero_step(const ZeroArgs& a, cudaStream_t s) {
   if (a.nsys <= 0) return;

@@ -65,6 +65,8 @@ typedef struct coral_handle coral_handle;
 #define CORAL_Q_ZSYS_NVARS 400       /* + isys: coupled vars of mean system     */
 #define CORAL_Q_SYS_KL 500           /* + isys: sub-diagonals of the evolution band   */
 #define CORAL_Q_SYS_KU 600           /* + isys: super-diagonals of the evolution band */
+#define CORAL_Q_SYS_REAL 700         /* + isys: 1 if its LU factors are stored real-scaled (8-byte entries),
+                                        0 if complex (16-byte entries) */
 
 /*
  * Create a solver from the text of coral.equations and coral.parameters.in.

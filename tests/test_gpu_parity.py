@@ -131,3 +131,25 @@ def test_cfg0_100_steps_within_1e10():
     for s in range(len(ref.zlay)):
         assert _rel(pl.get_mean_field(s), ref.zfield[s]) < 1e-10
     pl.close()
+
+
+@pytest.mark.parametrize("complex_factors", [False, True])
+def test_both_factor_paths_match_oracle(complex_factors, monkeypatch):
+    """The real-scaled factors (recipes whose variables/equations admit the +-i
+    scaling, like Rayleigh-Benard) and the general complex factors give the
+    same steps."""
+    if complex_factors:
+        monkeypatch.setenv("CORAL_COMPLEX_FACTORS", "1")
+    else:
+        monkeypatch.delenv("CORAL_COMPLEX_FACTORS", raising=False)
+    eq = equations("rrbc_stressfree_ek1e-4_ra5e7", **{"5.d7": "3.d4", "1.d4": "3.d2"})
+    par = params(12, 16, 24, dt=1e-4)
+    ref = co.Solver(eq, par)
+    pl = _pl(eq, par)
+    _random_state(ref, pl, 11, amp=1e-2)
+    for _ in range(3):
+        ref.step(1e-4)
+    pl.march_forward(1e-4, 3)
+    pl.synchronize()
+    assert _rel(pl.get_field(0), ref.field[0]) < 1e-11
+    pl.close()
