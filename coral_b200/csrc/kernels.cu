@@ -40,12 +40,13 @@ __device__ __forceinline__ double2 ipow(double k, int e) {
 // (compute_full_variables_in_physical_space, marching.f90:436-503, then
 //  c2r_transform steps 1-2 and the 0.5 of the x padding, transforms.f90:172-198)
 // ------------------------------------------------------------------------------
+template <int NF>
 __global__ void __launch_bounds__(kThreads) k_inv_y(Dims d, const FullVarDev* fv, StateSet st,
                                                      const double2* plain_spec, const double* kxv,
                                                      const double* kyv, double2* Y1, FftPlan py) {
   extern __shared__ double2 sm[];
   const int f = blockIdx.x, n0 = blockIdx.y * kNB1, kx = blockIdx.z;
-  const int NYA = d.NYA;
+  const int NYA = NF ? NF : d.NYA;
   double2* A = sm;
   double2* B = sm + kNB1 * NYA;
   for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
@@ -90,7 +91,7 @@ __global__ void __launch_bounds__(kThreads) k_inv_y(Dims d, const FullVarDev* fv
     A[ln * NYA + iy] = c;
   }
   __syncthreads();
-  const double2* R = fft_lines<true>(A, B, kNB1, py);
+  const double2* R = fft_lines_n<NF, true>(A, B, kNB1, py);
   for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
     const int ln = idx % kNB1, y = idx / kNB1, n = n0 + ln;
     if (n < d.NZ) {
@@ -104,10 +105,11 @@ __global__ void __launch_bounds__(kThreads) k_inv_y(Dims d, const FullVarDev* fv
 // inverse transform, pass 2: x c2r with zero padding NX/2 -> NXAA (transforms.f90:197-210)
 // two real output lines per complex FFT
 // ------------------------------------------------------------------------------
+template <int NF>
 __global__ void __launch_bounds__(kThreads) k_inv_x(Dims d, const double2* Y1, double* Y2, FftPlan px) {
   extern __shared__ double2 sm[];
   const int f = blockIdx.x, n0 = blockIdx.y * kNB2, y = blockIdx.z;
-  const int NXA = d.NXA, NP = kNB2 / 2;
+  const int NXA = NF ? NF : d.NXA, NP = kNB2 / 2;
   double2* A = sm;
   double2* B = sm + NP * NXA;
   for (int idx = threadIdx.x; idx < NP * NXA; idx += blockDim.x) A[idx] = zero2();
@@ -125,7 +127,7 @@ __global__ void __launch_bounds__(kThreads) k_inv_x(Dims d, const double2* Y1, d
     }
   }
   __syncthreads();
-  const double2* R = fft_lines<true>(A, B, NP, px);
+  const double2* R = fft_lines_n<NF, true>(A, B, NP, px);
   for (int idx = threadIdx.x; idx < NP * NXA; idx += blockDim.x) {
     const int m = idx % NP, x = idx / NP, na = n0 + 2 * m;
     double2 z = R[m * NXA + x];
@@ -144,13 +146,14 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, doub
 // via an NZAA-point complex FFT (two columns per FFT); also the CFL maxima of
 // compute_cfl_based_timestep (marching.f90:219-238) for the first three full variables
 // ------------------------------------------------------------------------------
+template <int NF>
 __global__ void __launch_bounds__(kThreads) k_inv_z(Dims d, const double* Y2, double* phys, FftPlan pz,
                                                      const double2* dct_tw, const double* wz,
                                                      unsigned long long* cfl_bits) {
   extern __shared__ double2 sm[];
   __shared__ double red[kThreads / 32];
   const int f = blockIdx.x, x0 = blockIdx.y * kXB3, y = blockIdx.z;
-  const int N = d.NZA, NP = kXB3 / 2;
+  const int N = NF ? NF : d.NZA, NP = kXB3 / 2;
   double2* A = sm;
   double2* B = sm + NP * N;
   for (int idx = threadIdx.x; idx < NP * N; idx += blockDim.x) {
@@ -173,7 +176,7 @@ __global__ void __launch_bounds__(kThreads) k_inv_z(Dims d, const double* Y2, do
     A[m * N + n] = make_double2(va.x - vb.y, va.y + vb.x);  // va + i vb
   }
   __syncthreads();
-  const double2* R = fft_lines<true>(A, B, NP, pz);
+  const double2* R = fft_lines_n<NF, true>(A, B, NP, pz);
   double mx = 0.0;
   const int which = (f < 3) ? f : -1;
   for (int idx = threadIdx.x; idx < NP * N; idx += blockDim.x) {
@@ -207,13 +210,14 @@ __global__ void __launch_bounds__(kThreads) k_inv_z(Dims d, const double* Y2, do
 // truncated to NZ (transforms.f90:243-249), for all quadratic variables of one
 // pair of x columns; also partial volume averages for KE (output.f90:84-102)
 // ------------------------------------------------------------------------------
+template <int NF>
 __global__ void __launch_bounds__(kThreads) k_fwd_z(Dims d, int nf, QuadDesc q, const double* phys, double* Q2,
                                                      FftPlan pz, const double2* dct_tw, const double* wz,
                                                      double* ke_partial) {
   extern __shared__ double2 sm[];
   __shared__ double red[3][kThreads / 32];
   const int x0 = blockIdx.x * 2, y = blockIdx.y;
-  const int N = d.NZA, nq = q.nq;
+  const int N = NF ? NF : d.NZA, nq = q.nq;
   double* P = reinterpret_cast<double*>(sm);  // [nf][2][N]
   double2* A = sm + nf * N;                    // nq lines
   double2* B = A + nq * N;
@@ -242,7 +246,7 @@ __global__ void __launch_bounds__(kThreads) k_fwd_z(Dims d, int nf, QuadDesc q, 
     }
   }
   __syncthreads();
-  const double2* R = fft_lines<false>(A, B, nq, pz);
+  const double2* R = fft_lines_n<NF, false>(A, B, nq, pz);
   for (int idx = threadIdx.x; idx < nq * d.NZ; idx += blockDim.x) {
     const int qi = idx / d.NZ, n = idx - qi * d.NZ;
     const double2 Z = R[qi * N + n];
@@ -275,10 +279,11 @@ __global__ void __launch_bounds__(kThreads) k_fwd_z(Dims d, int nf, QuadDesc q, 
 // ------------------------------------------------------------------------------
 // forward transform, pass 2: x r2c, keep kx < NX/2 (transforms.f90:255-267)
 // ------------------------------------------------------------------------------
+template <int NF>
 __global__ void __launch_bounds__(kThreads) k_fwd_x(Dims d, const double* Q2, double2* Q1, FftPlan px) {
   extern __shared__ double2 sm[];
   const int qi = blockIdx.x, n0 = blockIdx.y * kNB2, y = blockIdx.z;
-  const int NXA = d.NXA, NP = kNB2 / 2;
+  const int NXA = NF ? NF : d.NXA, NP = kNB2 / 2;
   double2* A = sm;
   double2* B = sm + NP * NXA;
   for (int idx = threadIdx.x; idx < NP * NXA; idx += blockDim.x) {
@@ -287,7 +292,7 @@ __global__ void __launch_bounds__(kThreads) k_fwd_x(Dims d, const double* Q2, do
     A[m * NXA + x] = make_double2(na < d.NZ ? src[na] : 0.0, na + 1 < d.NZ ? src[na + 1] : 0.0);
   }
   __syncthreads();
-  const double2* R = fft_lines<false>(A, B, NP, px);
+  const double2* R = fft_lines_n<NF, false>(A, B, NP, px);
   for (int idx = threadIdx.x; idx < NP * d.NXH; idx += blockDim.x) {
     const int m = idx % NP, kx = idx / NP, na = n0 + 2 * m;
     const double2 Z = R[m * NXA + kx];
@@ -305,11 +310,12 @@ __global__ void __launch_bounds__(kThreads) k_fwd_x(Dims d, const double* Q2, do
 // forward transform, pass 3: y c2c (e^{-i}), x0.5 on Chebyshev index 0 and the
 // 1/(NXAA NYAA NZAA) normalisation (transforms.f90:280-296)
 // ------------------------------------------------------------------------------
+template <int NF>
 __global__ void __launch_bounds__(kThreads) k_fwd_y(Dims d, const double2* Q1, double2* qspec, double scale,
                                                      FftPlan py) {
   extern __shared__ double2 sm[];
   const int qi = blockIdx.x, n0 = blockIdx.y * kNB1, kx = blockIdx.z;
-  const int NYA = d.NYA;
+  const int NYA = NF ? NF : d.NYA;
   double2* A = sm;
   double2* B = sm + kNB1 * NYA;
   for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
@@ -322,7 +328,7 @@ __global__ void __launch_bounds__(kThreads) k_fwd_y(Dims d, const double2* Q1, d
     A[ln * NYA + y] = v;
   }
   __syncthreads();
-  const double2* R = fft_lines<false>(A, B, kNB1, py);
+  const double2* R = fft_lines_n<NF, false>(A, B, kNB1, py);
   for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
     const int ln = idx % kNB1, ky = idx / kNB1, n = n0 + ln;
     if (n < d.NZ) qspec[(((size_t)qi * d.NXH + kx) * NYA + ky) * d.NZ + n] = cscale(R[ln * NYA + ky], scale);
@@ -1166,45 +1172,104 @@ void set_smem(K kernel, size_t bytes) {
 }  // namespace
 
 // ---- launchers ----------------------------------------------------------------
+// Each transform kernel is instantiated for the lengths of the usual grids
+// (compile-time FFT plans); other lengths use the runtime plan.
+#define CORAL_FFT_LENGTHS(X) X(24) X(36) X(48) X(72) X(96) X(144) X(192) X(288) X(384) X(576)
+
+template <template <int> class L, typename... Args>
+void dispatch_len(int n, Args&&... args) {
+  switch (n) {
+#define CORAL_CASE(v) \
+  case v:             \
+    L<v>::run(args...); \
+    return;
+    CORAL_FFT_LENGTHS(CORAL_CASE)
+#undef CORAL_CASE
+    default:
+      L<0>::run(args...);
+  }
+}
+
+template <int NF>
+struct InvY {
+  static void run(const Dims& d, int nf, const FullVarDev* fv, StateSet st, const double2* plain_spec,
+                  const double* kx, const double* ky, double2* Y1, const FftPlan& py, cudaStream_t s) {
+    size_t sm = 2 * kNB1 * (size_t)d.NYA * sizeof(double2);
+    set_smem(k_inv_y<NF>, sm);
+    dim3 g(nf, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
+    k_inv_y<NF><<<g, kThreads, sm, s>>>(d, fv, st, plain_spec, kx, ky, Y1, py);
+  }
+};
+template <int NF>
+struct InvX {
+  static void run(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s) {
+    size_t sm = 2 * (kNB2 / 2) * (size_t)d.NXA * sizeof(double2);
+    set_smem(k_inv_x<NF>, sm);
+    dim3 g(nf, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
+    k_inv_x<NF><<<g, kThreads, sm, s>>>(d, Y1, Y2, px);
+  }
+};
+template <int NF>
+struct InvZ {
+  static void run(const Dims& d, int nf, const double* Y2, double* phys, const FftPlan& pz, const double2* dct_tw,
+                  const double* wz, unsigned long long* cfl_bits, cudaStream_t s) {
+    size_t sm = 2 * (kXB3 / 2) * (size_t)d.NZA * sizeof(double2);
+    set_smem(k_inv_z<NF>, sm);
+    dim3 g(nf, (d.NXA + kXB3 - 1) / kXB3, d.NYA);
+    k_inv_z<NF><<<g, kThreads, sm, s>>>(d, Y2, phys, pz, dct_tw, wz, cfl_bits);
+  }
+};
+template <int NF>
+struct FwdZ {
+  static void run(const Dims& d, int nf, const QuadDesc& q, const double* phys, double* Q2, const FftPlan& pz,
+                  const double2* dct_tw, const double* wz, double* ke_partial, cudaStream_t s) {
+    size_t sm = (size_t)nf * d.NZA * sizeof(double2) + 2 * (size_t)q.nq * d.NZA * sizeof(double2);
+    set_smem(k_fwd_z<NF>, sm);
+    dim3 g((d.NXA + 1) / 2, d.NYA);
+    k_fwd_z<NF><<<g, kThreads, sm, s>>>(d, nf, q, phys, Q2, pz, dct_tw, wz, ke_partial);
+  }
+};
+template <int NF>
+struct FwdX {
+  static void run(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s) {
+    size_t sm = 2 * (kNB2 / 2) * (size_t)d.NXA * sizeof(double2);
+    set_smem(k_fwd_x<NF>, sm);
+    dim3 g(nq, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
+    k_fwd_x<NF><<<g, kThreads, sm, s>>>(d, Q2, Q1, px);
+  }
+};
+template <int NF>
+struct FwdY {
+  static void run(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
+                  cudaStream_t s) {
+    size_t sm = 2 * kNB1 * (size_t)d.NYA * sizeof(double2);
+    set_smem(k_fwd_y<NF>, sm);
+    dim3 g(nq, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
+    k_fwd_y<NF><<<g, kThreads, sm, s>>>(d, Q1, qspec, scale, py);
+  }
+};
+
 void launch_inv_y(const Dims& d, int nf, const FullVarDev* fv, StateSet st, const double2* plain_spec,
                   const double* kx, const double* ky, double2* Y1, const FftPlan& py, cudaStream_t s) {
-  size_t sm = 2 * kNB1 * (size_t)d.NYA * sizeof(double2);
-  set_smem(k_inv_y, sm);
-  dim3 g(nf, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
-  k_inv_y<<<g, kThreads, sm, s>>>(d, fv, st, plain_spec, kx, ky, Y1, py);
+  dispatch_len<InvY>(d.NYA, d, nf, fv, st, plain_spec, kx, ky, Y1, py, s);
 }
 void launch_inv_x(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s) {
-  size_t sm = 2 * (kNB2 / 2) * (size_t)d.NXA * sizeof(double2);
-  set_smem(k_inv_x, sm);
-  dim3 g(nf, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
-  k_inv_x<<<g, kThreads, sm, s>>>(d, Y1, Y2, px);
+  dispatch_len<InvX>(d.NXA, d, nf, Y1, Y2, px, s);
 }
 void launch_inv_z(const Dims& d, int nf, const double* Y2, double* phys, const FftPlan& pz,
                   const double2* dct_tw, const double* wz, unsigned long long* cfl_bits, cudaStream_t s) {
-  size_t sm = 2 * (kXB3 / 2) * (size_t)d.NZA * sizeof(double2);
-  set_smem(k_inv_z, sm);
-  dim3 g(nf, (d.NXA + kXB3 - 1) / kXB3, d.NYA);
-  k_inv_z<<<g, kThreads, sm, s>>>(d, Y2, phys, pz, dct_tw, wz, cfl_bits);
+  dispatch_len<InvZ>(d.NZA, d, nf, Y2, phys, pz, dct_tw, wz, cfl_bits, s);
 }
 void launch_fwd_z(const Dims& d, int nf, const QuadDesc& q, const double* phys, double* Q2, const FftPlan& pz,
                   const double2* dct_tw, const double* wz, double* ke_partial, cudaStream_t s) {
-  size_t sm = (size_t)nf * d.NZA * sizeof(double2) + 2 * (size_t)q.nq * d.NZA * sizeof(double2);
-  set_smem(k_fwd_z, sm);
-  dim3 g((d.NXA + 1) / 2, d.NYA);
-  k_fwd_z<<<g, kThreads, sm, s>>>(d, nf, q, phys, Q2, pz, dct_tw, wz, ke_partial);
+  dispatch_len<FwdZ>(d.NZA, d, nf, q, phys, Q2, pz, dct_tw, wz, ke_partial, s);
 }
 void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s) {
-  size_t sm = 2 * (kNB2 / 2) * (size_t)d.NXA * sizeof(double2);
-  set_smem(k_fwd_x, sm);
-  dim3 g(nq, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
-  k_fwd_x<<<g, kThreads, sm, s>>>(d, Q2, Q1, px);
+  dispatch_len<FwdX>(d.NXA, d, nq, Q2, Q1, px, s);
 }
 void launch_fwd_y(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
                   cudaStream_t s) {
-  size_t sm = 2 * kNB1 * (size_t)d.NYA * sizeof(double2);
-  set_smem(k_fwd_y, sm);
-  dim3 g(nq, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
-  k_fwd_y<<<g, kThreads, sm, s>>>(d, Q1, qspec, scale, py);
+  dispatch_len<FwdY>(d.NYA, d, nq, Q1, qspec, scale, py, s);
 }
 void launch_remove_zmean(const Dims& d, double2* qspec_q, cudaStream_t s) {
   k_remove_zmean<<<grid1d((size_t)d.NXH * d.NYA, 128), 128, 0, s>>>(d, qspec_q);
