@@ -42,6 +42,7 @@ SIGNATURES = {
     "coral_set_mean_var_profile": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _D]),
     "coral_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
     "coral_profile_step": (ctypes.c_int, [_P, ctypes.c_double, _D, ctypes.c_int]),
+    "coral_spec_to_phys_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D, _P]),
 }
 
 _lib = None

@@ -9,7 +9,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libcoral_b200.so")
-SOURCES = ["kernels.cu", "capi.cu", "host_setup.cpp"]
+SOURCES = ["kernels.cu", "capi.cu", "noalloc.cu", "host_setup.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

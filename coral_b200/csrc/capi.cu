@@ -96,6 +96,10 @@ struct ZSys {
 
 }  // namespace
 
+namespace coral {
+void set_global_error(const std::string& msg) { g_create_error = msg; }
+}  // namespace coral
+
 struct coral_handle {
   std::string err;
   int device = 0;

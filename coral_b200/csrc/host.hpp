@@ -22,6 +22,9 @@ struct CoralError : std::runtime_error {
   CoralError(int c, const std::string& m) : std::runtime_error(m), code(c) {}
 };
 
+// text returned by coral_last_error(NULL) (calls that have no handle)
+void set_global_error(const std::string& msg);
+
 // ---------------------------------------------------------------------------
 // coral.parameters.in  (src/plane_layer/PL_geometry.f90:269-305)
 // ---------------------------------------------------------------------------

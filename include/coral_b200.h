@@ -166,6 +166,25 @@ int coral_stream(coral_handle* h, void** stream);
 int coral_profile_step(coral_handle* h, double dt, double* ms, int n);
 
 /*
+ * coral_spec_to_phys_noalloc -- no counterpart in the reference.
+ *
+ * The inverse transform of coral_spec_to_phys for one scalar, for callers that
+ * cannot allocate device memory (their memory belongs to another allocator or
+ * runtime, or allocation is forbidden after start-up).  No handle is needed and
+ * nothing is allocated: spec (NZ, NYAA, NX/2 complex) and phys (NZAA, NXAA, NYAA
+ * real) are the caller's device buffers, and the transform's intermediate
+ * arrays live in a 64 MiB __device__ array that every GPU loading this library
+ * holds until exit.  Grids whose intermediates need more than 64 MiB (about
+ * 128 x 128 x 96 modes) are rejected with CORAL_EBADARG.  The work is queued on
+ * stream (a cudaStream_t; NULL = the legacy default stream) and the call returns
+ * after the launches.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) and sets kernel attributes: make it before any
+ * stream capture.  All calls on a device share the array, so calls that can
+ * overlap on the GPU (different streams, no ordering) race.
+ */
+int coral_spec_to_phys_noalloc(int NX, int NY, int NZ, const double* spec, double* phys, void* stream);
+
+/*
  * Diagnostics of the first stage of the last step: out[0] = cargo%cfl_based_DT
  * (marching.f90:200-254), out[1] = cargo%KE_display = sum of the volume
  * averages of uu, vv and ww (PL_IMEX_timestepping_output.f90:84-102; 0 when
