@@ -282,7 +282,7 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
     else k.ab = mem.get<double2>((size_t)h->nact * k.T * k.ldab);
     k.rowflip = mem.upload(k.ops.row_flip);
     k.colflip = mem.upload(k.ops.col_flip);
-    k.dpiv = mem.get<unsigned char>((size_t)h->nact * k.T);
+    k.dpiv = mem.get<unsigned char>((size_t)h->nact * ((k.T + 7) & ~7));  // rows padded to 8 bytes
     k.info = mem.get<int>((size_t)std::max(h->nact, 1));
     for (int v = 0; v < k.ops.nV; ++v) {
       std::vector<int> tt;
@@ -476,7 +476,6 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       na.ky = h->d_ky;
       na.act_index = h->d_act_index;
       na.Khat = k.Khat[i];
-      B(6); launch_nl(na, h->stream); E();
       SolveArgs sa{};
       sa.d = d;
       sa.T = k.T;
@@ -499,6 +498,8 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       sa.ab = k.ab;
       sa.dpiv = k.dpiv;
       sa.act_index = h->d_act_index;
+      sa.act_list = h->d_act_list;
+      sa.nact = h->nact;
       sa.last_stage = last ? 1 : 0;
       sa.kx = h->d_kx;
       sa.ky = h->d_ky;
@@ -511,11 +512,14 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
         const int u_rows = (kv + 2) & ~1, l_rows = ((kv + 1 + k.kl + 1) & ~1) - ((kv + 1) & ~1);
         sa.ring_cols = std::max(u_rows, l_rows);
       }
-      B(7);
-      if (k.real) launch_solve_real(sa, h->stream);
-      else launch_solve(sa, h->stream);
-      E();
-      nl += 2;
+      if (k.real) {
+        B(7); launch_solve_real(sa, na, h->stream); E();
+        nl += 3;
+      } else {
+        B(6); launch_nl(na, h->stream); E();
+        B(7); launch_solve(sa, h->stream); E();
+        nl += 2;
+      }
     }
     if (!h->zs.empty()) {
       ZeroArgs za{};

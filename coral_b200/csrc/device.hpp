@@ -113,10 +113,13 @@ struct SolveArgs {
   const unsigned char* rowflip;
   const unsigned char* colflip;
   int ring_cols;         // doubles per column slot of the solve's shared-memory ring
+  int nact;              // active systems (factor slots)
+  const int* act_list;   // [nact] kx*NYA+ky of each factor slot
 };
 void launch_solve(const SolveArgs& a, cudaStream_t s);
-// register-window variant for real-scaled factors with kl <= 16, kl+ku <= 63
-void launch_solve_real(const SolveArgs& a, cudaStream_t s);
+// real-scaled factors (kl <= 31, kl+ku <= 63): right-hand side with the NL
+// assembly fused in, substitutions, then K_std and outputs (three kernels)
+void launch_solve_real(const SolveArgs& a, const NLArgs& n, cudaStream_t s);
 
 struct FactorArgs {
   Dims d;

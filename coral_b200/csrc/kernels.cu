@@ -441,7 +441,7 @@ __global__ void __launch_bounds__(kWPB * 32) k_solve(SolveArgs a) {
   if (act >= 0) {
     const int kl = a.kl, kv = a.kl + a.ku, ldab = a.ldab;
     const double2* ab = a.ab + (size_t)act * T * ldab;
-    const unsigned char* dp = a.dpiv + (size_t)act * T;
+    const unsigned char* dp = a.dpiv + (size_t)act * ((T + 7) & ~7);
     // ---- forward: apply row interchanges and L (zgbtrs, 'N', kl > 0)
     {
       double2 lr[kPF];
@@ -601,7 +601,7 @@ __global__ void __launch_bounds__(kWPB * 32) k_factor(FactorArgs a) {
       if (m2 > mag || (m2 == mag && i2 < idx)) { mag = m2; idx = i2; }
     }
     const int jp = idx;
-    if (lane == 0) a.dpiv[(size_t)sys * T + j] = (unsigned char)jp;
+    if (lane == 0) a.dpiv[(size_t)sys * ((T + 7) & ~7) + j] = (unsigned char)jp;
     const double2 piv = ab[(size_t)j * ldab + kv + jp];
     if (piv.x == 0.0 && piv.y == 0.0) {
       if (info == 0) info = j + 1;
@@ -704,7 +704,7 @@ __global__ void __launch_bounds__(kWPB * 32) k_factor_real(FactorArgs a) {
       if (m2 > mag || (m2 == mag && i2 < idx)) { mag = m2; idx = i2; }
     }
     const int jp = idx;
-    if (lane == 0) a.dpiv[(size_t)sys * T + j] = (unsigned char)jp;
+    if (lane == 0) a.dpiv[(size_t)sys * ((T + 7) & ~7) + j] = (unsigned char)jp;
     const double piv = ab[(size_t)j * ldab + kv + jp];
     if (piv == 0.0) {
       if (info == 0) info = j + 1;
@@ -768,40 +768,18 @@ __device__ __forceinline__ double2 shfl2(double2 v, int src) {
   return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
 }
 
-__global__ void __launch_bounds__(kWPBr * 32) k_solve_real(SolveArgs a) {
+__global__ void __launch_bounds__(kWPBr * 32) k_subst_real(SolveArgs a) {
   extern __shared__ double smr[];
-  __shared__ double2 coefs[kWPBr][2][kMaxGroups];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int sid = blockIdx.x * kWPBr + warp;
-  const int nsys = a.d.NXH * a.d.NYA;
-  if (sid >= nsys) return;
+  const int act = blockIdx.x * kWPBr + warp;  // active systems only
+  if (act >= a.nact) return;
   const int T = a.T;
-  const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
-  const int act = a.act_index[sid];
-  const bool origin = (kx == 0 && ky == 0);
-  if (lane < kMaxGroups) {
-    coefs[warp][0][lane] = (lane < a.M.ngroups) ? cmul(ipow(a.kx[kx], a.M.gkx[lane]), ipow(a.ky[ky], a.M.gky[lane])) : zero2();
-    coefs[warp][1][lane] = (lane < a.L.ngroups) ? cmul(ipow(a.kx[kx], a.L.gkx[lane]), ipow(a.ky[ky], a.L.gky[lane])) : zero2();
-  }
-  __syncwarp();
-  const double2* field = a.field + (size_t)sid * T;
-  double2* x = a.work + (size_t)sid * T;  // never aliases field: M field is read while x is written
-  // ---- right-hand side (rows scaled by -i where flagged)
-  for (int t = lane; t < T; t += 32) {
-    double2 r = origin ? zero2() : ell_row(a.M, t, coefs[warp][0], field);
-    for (int j = 0; j < a.nprev; ++j) {
-      r = cadd(r, cscale(a.Kstd[j][(size_t)sid * T + t], a.ca[j]));
-      r = cadd(r, cscale(a.Khat[j][(size_t)sid * T + t], a.ch[j]));
-    }
-    r = cadd(r, cscale(a.Khat[a.nprev][(size_t)sid * T + t], a.ch[a.nprev]));
-    if (act >= 0) r = flip_row(r, a.rowflip[t]);
-    x[t] = r;
-  }
-  __syncwarp();
-  if (act >= 0) {
+  const int sid = a.act_list[act];
+  double2* x = a.work + (size_t)sid * T;  // right-hand side in, solution out
+  {
     const int kl = a.kl, kv = a.kl + a.ku, ldab = a.ldab;
     const double* ab = a.abr + (size_t)act * T * ldab;
-    const unsigned char* dp = a.dpiv + (size_t)act * T;
+    const unsigned char* dp = a.dpiv + (size_t)act * ((T + 7) & ~7);
     // Factor columns stream through a per-warp shared-memory ring (kNBUF chunks
     // of kCW columns) with cp.async, kNBUF-1 chunks ahead of the sweep; the
     // forward sweep copies only the L rows of each column, the backward sweep
@@ -834,14 +812,14 @@ __global__ void __launch_bounds__(kWPBr * 32) k_solve_real(SolveArgs a) {
       double2 w = (lane < T) ? x[lane] : zero2();
       double2 incCur = (32 + lane < T) ? x[32 + lane] : zero2();
       double2 incNext = zero2(), ysave = zero2();
-      int pv = 0, pvNext = (lane < T) ? dp[lane] : 0;
+      // pivot offsets of a chunk as two uniform 32-bit words (rows padded to 8 bytes)
+      uint2 pw = *reinterpret_cast<const uint2*>(dp);
       for (int c = 0; c < nchunks; ++c) {
         const int j0 = c * kCW;
-        if ((j0 & 31) == 0) {  // new block of 32 columns: its pivots, prefetches for the next block
-          pv = pvNext;
-          pvNext = (j0 + 32 + lane < T) ? dp[j0 + 32 + lane] : 0;
+        if ((j0 & 31) == 0)  // new block of 32 columns: next block's incoming values
           incNext = (j0 + 64 + lane < T) ? x[j0 + 64 + lane] : zero2();
-        }
+        const uint2 pwc = pw;
+        if (c + 1 < nchunks) pw = *reinterpret_cast<const uint2*>(dp + j0 + kCW);
         __syncwarp();
         issue(c + kNBUF - 1);
         cp_async_wait<kNBUF - 1>();
@@ -855,15 +833,16 @@ __global__ void __launch_bounds__(kWPBr * 32) k_solve_real(SolveArgs a) {
             const int i = (lane - j) & 31;
             const int lm = min(kl, T - 1 - j);
             const double lv = (i >= 1 && i <= lm) ? cb[q * a.ring_cols + (kv + i - l_row0)] : 0.0;
-            const int jp = __shfl_sync(0xffffffffu, pv, j & 31);
-            if (jp != 0) {
-              const int r2 = (j + jp) & 31;
-              const double2 a0 = shfl2(w, r2), aj = shfl2(w, src);
-              if (lane == src) w = a0;
-              else if (lane == r2) w = aj;
-            }
-            const double2 bj = shfl2(w, src);
-            w.x -= lv * bj.x;
+            const int jp = ((q < 4 ? pwc.x : pwc.y) >> (8 * (q & 3))) & 0xFF;
+            // Row interchange j <-> j+jp and broadcast of the pivot row in one shuffle:
+            // the owner of row j+jp fetches row j (its new content), every other lane
+            // fetches the pivot row; the owner of j+jp already holds the pivot value.
+            const int r2 = (j + jp) & 31;
+            const int from = (jp != 0 && lane == r2) ? src : r2;
+            const double2 got = shfl2(w, from);
+            const double2 bj = (jp != 0 && lane == r2) ? w : got;
+            if (lane == src || (jp != 0 && lane == r2)) w = got;
+            w.x -= lv * bj.x;  // zero multiplier outside rows j+1..j+lm
             w.y -= lv * bj.y;
             if (lane == src) {
               ysave = w;
@@ -966,19 +945,86 @@ __global__ void __launch_bounds__(kWPBr * 32) k_solve_real(SolveArgs a) {
     }
   }
   __syncwarp();
-  // ---- outputs (the last stage writes the new state into field)
+}
+
+
+// ------------------------------------------------------------------------------
+// Stage right-hand side with the NL assembly fused in, one warp per (kx,ky) system
+// (marching.f90:16-21, 93-125, 319-367):
+//   Khat_i = sum_terms (i kx)^a (i ky)^b dsca trunc(I^Iz M^mz) qhat    (0 for inactive)
+//   rhs    = M field + sum_{j<i} (dt a(i,j) Kstd_j + dt ahat(i+1,j) Khat_j) + dt ahat(i+1,i) Khat_i
+// rows flagged in rowflip are multiplied by -i for the real-scaled solve.
+// ------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kWPB * 32) k_rhs_nl(SolveArgs a, NLArgs n) {
+  __shared__ double2 cms[kWPB][kMaxGroups], cns[kWPB][kMaxGroups];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sid = blockIdx.x * kWPB + warp;
+  const int nsys = a.d.NXH * a.d.NYA;
+  if (sid >= nsys) return;
+  const int T = a.T, NZ = a.d.NZ;
+  const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
+  const bool act = a.act_index[sid] >= 0;
+  const bool origin = (kx == 0 && ky == 0);
+  if (lane < kMaxGroups) {
+    cms[warp][lane] = (lane < a.M.ngroups) ? cmul(ipow(a.kx[kx], a.M.gkx[lane]), ipow(a.ky[ky], a.M.gky[lane])) : zero2();
+    cns[warp][lane] = (lane < n.NL.ngroups) ? cmul(ipow(a.kx[kx], n.NL.gkx[lane]), ipow(a.ky[ky], n.NL.gky[lane])) : zero2();
+  }
+  __syncwarp();
+  const double2* field = a.field + (size_t)sid * T;
+  const size_t qcol = ((size_t)kx * a.d.NYA + ky) * NZ;            // (kx,ky) column of quad var 0
+  const size_t qstride = (size_t)a.d.NXH * a.d.NYA * NZ;           // between quad vars
+  const size_t base = (size_t)sid * T;
+  for (int t = lane; t < T; t += 32) {
+    double2 kh = zero2();
+    if (act) {
+      for (int k = 0; k < n.NL.width; ++k) {
+        const double v = n.NL.v(t, k);
+        if (v == 0.0) break;  // slots are filled in order; exact zeros are not stored
+        const int cg = n.NL.cg[(size_t)k * n.NL.rows + t];
+        const int c = cg & 0xFFFFFF;
+        const int qv = c / NZ, nn = c - qv * NZ;
+        const double2 qh = n.qspec[qv * qstride + qcol + nn];
+        kh = cadd(kh, cmul(cns[warp][cg >> 24], make_double2(v * qh.x, v * qh.y)));
+      }
+    }
+    n.Khat[base + t] = kh;
+    double2 r = origin ? zero2() : ell_row(a.M, t, cms[warp], field);
+    for (int j = 0; j < a.nprev; ++j) {
+      r = cadd(r, cscale(a.Kstd[j][base + t], a.ca[j]));
+      r = cadd(r, cscale(a.Khat[j][base + t], a.ch[j]));
+    }
+    r = cadd(r, cscale(kh, a.ch[a.nprev]));
+    if (act && a.rowflip) r = flip_row(r, a.rowflip[t]);
+    a.work[base + t] = r;
+  }
+}
+
+// ------------------------------------------------------------------------------
+// After the substitutions: K_std_i = L aux (0 for inactive systems), the stage
+// output (the new state in the last stage, zero on inactive systems), and the
+// non-finite check.  One warp per (kx,ky) system.
+// ------------------------------------------------------------------------------
+__global__ void __launch_bounds__(kWPB * 32) k_kstd_out(SolveArgs a) {
+  __shared__ double2 cls[kWPB][kMaxGroups];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sid = blockIdx.x * kWPB + warp;
+  const int nsys = a.d.NXH * a.d.NYA;
+  if (sid >= nsys) return;
+  const int T = a.T;
+  const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
+  const bool act = a.act_index[sid] >= 0;
+  if (lane < kMaxGroups)
+    cls[warp][lane] = (lane < a.L.ngroups) ? cmul(ipow(a.kx[kx], a.L.gkx[lane]), ipow(a.ky[ky], a.L.gky[lane])) : zero2();
+  __syncwarp();
+  const size_t base = (size_t)sid * T;
+  const double2* x = a.work + base;
+  const bool zero_out = a.last_stage && !act;
   bool bad = false;
-  const bool zero_out = a.last_stage && (act < 0);
-  double2* out = a.out + (size_t)sid * T;
   for (int t = lane; t < T; t += 32) {
     const double2 v = zero_out ? zero2() : x[t];
     bad |= !(isfinite(v.x) && isfinite(v.y));
-    if (out != x || zero_out) out[t] = v;
-  }
-  __syncwarp();
-  if (a.Kstd_out) {
-    double2* ko = a.Kstd_out + (size_t)sid * T;
-    for (int t = lane; t < T; t += 32) ko[t] = (act >= 0) ? ell_row(a.L, t, coefs[warp][1], x) : zero2();
+    if (a.out != a.work || zero_out) a.out[base + t] = v;
+    if (a.Kstd_out) a.Kstd_out[base + t] = act ? ell_row(a.L, t, cls[warp], x) : zero2();
   }
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.flags, 1u);
 }
@@ -1288,11 +1334,15 @@ void launch_factor(const FactorArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;
   k_factor<<<(a.nact + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
 }
-void launch_solve_real(const SolveArgs& a, cudaStream_t s) {
+void launch_solve_real(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
   const int nsys = a.d.NXH * a.d.NYA;
-  const size_t sm = (size_t)kWPBr * kNBUF * kCW * a.ring_cols * sizeof(double);
-  set_smem(k_solve_real, sm);
-  k_solve_real<<<(nsys + kWPBr - 1) / kWPBr, kWPBr * 32, sm, s>>>(a);
+  k_rhs_nl<<<(nsys + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a, n);
+  if (a.nact > 0) {
+    const size_t sm = (size_t)kWPBr * kNBUF * kCW * a.ring_cols * sizeof(double);
+    set_smem(k_subst_real, sm);
+    k_subst_real<<<(a.nact + kWPBr - 1) / kWPBr, kWPBr * 32, sm, s>>>(a);
+  }
+  k_kstd_out<<<(nsys + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
 }
 void launch_factor_real(const FactorArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;
