@@ -129,17 +129,44 @@ def make_ic(cfg, pl):
     pl.set_mean_var_profile(1, 0, mean)
 
 
-def solve_bytes_per_stage(nact, nsys, T, ldab, stages, factor_bytes):
-    """Algorithmic bytes of one launch of the stage-update + banded-solve kernel,
-    averaged over the stages: the LU factors (factor_bytes per entry: 8 when
-    stored real-scaled, 16 complex) and pivot bytes of the active systems, and
-    for every system the state read, the K arrays read and the outputs."""
+# kernels of each timed phase (names as ncu lists them)
+PHASE_KERNELS = {
+    "inv_y": "k_inv_y", "inv_x": "k_inv_x", "inv_z": "k_inv_z", "fwd_z_products": "k_fwd_z",
+    "fwd_x": "k_fwd_x", "fwd_y": "k_fwd_y", "nl_assembly": "k_nl",
+    "solve": "k_rhs_nl + k_subst_real + k_kstd_out", "mean_systems": "k_zero_step",
+}
+
+
+def phase_bytes(g, nsys, nact, T, ncls, Tc, kl, ku, stages, factor_bytes):
+    """Algorithmic HBM bytes of one launch of each phase (averaged over the
+    stages): every array a phase must read from or write to HBM once.
+    g: dict with NXH, NYA, NXA, NZ, NZA, nF (full variables), nQ (quadratic
+    variables).  Transform intermediates are 16-byte complex where the data are
+    complex (after an x r2c / before an x c2r) and 8-byte real otherwise."""
+    NXH, NYA, NXA, NZ, NZA, nF, nQ = (g[k] for k in ("NXH", "NYA", "NXA", "NZ", "NZA", "nF", "nQ"))
+    y1 = lambda nv: nv * NYA * NXH * NZ * 16   # [var][y][kx][n] complex
+    y2 = lambda nv: nv * NYA * NXA * NZ * 8    # [var][y][x][n] real
+    ph = lambda nv: nv * NYA * NXA * NZA * 8   # [var][y][x][z] real
+    out = {
+        # the Chebyshev coefficients of each full variable from the state, Y1 out
+        "inv_y": nsys * nF * NZ * 16 + y1(nF),
+        "inv_x": y1(nF) + y2(nF),
+        "inv_z": y2(nF) + ph(nF),
+        "fwd_z_products": ph(nF) + y2(nQ),
+        "fwd_x": y2(nQ) + y1(nQ),
+        "fwd_y": y1(nQ) + y1(nQ),
+    }
+    # solve: LU factors (2 kl + ku + 1 band entries per column of each block,
+    # plus one pivot byte) and quadratic-variable coefficients of the active
+    # systems; for every system the state read, the K arrays read and written
+    # and the outputs
     tot = 0
     for i in range(stages):
         last = (i == stages - 1)
-        per_sys = 16 * T * (1 + (2 * i + 1) + 1 + (0 if last else 1))
-        tot += nsys * per_sys + nact * (factor_bytes * ldab * T + T)
-    return tot / stages
+        per_sys = 16 * T * (1 + 2 * i + 1 + 1 + (0 if last else 1))
+        tot += nsys * per_sys + nact * (ncls * Tc * (factor_bytes * (2 * kl + ku + 1) + 1) + 16 * nQ * NZ)
+    out["solve"] = tot / stages
+    return out
 
 
 def run_ours(args, cfg):
@@ -231,19 +258,28 @@ def run_ours(args, cfg):
            "h2d_bytes_per_step": state_bytes / args.steps,
            "d2h_bytes_per_step": state_bytes / args.steps + diag_bytes}
 
-    # roofline of the dominant kernel (stage update + banded solve)
+    # roofline of every phase; the headline one is the phase with the largest time
     T = pl.T[0]
-    kl, ku = pl.query(500), pl.query(600)
-    ldab = 2 * kl + ku + 1
     nsys = pl.NXH * pl.NYAA
     nact = sum(1 for ix in range(pl.NXH) for iy in range(pl.NYAA)
                if not (iy_dealiased(iy, pl.NY, pl.NYAA)) and not (ix == 0 and iy == 0))
     fbytes = 8 if pl.query(700) else 16
-    algo = solve_bytes_per_stage(nact, nsys, T, ldab, pl.stages, fbytes)
-    launch_ms = prof["solve"] / pl.stages
-    achieved = algo / (launch_ms / 1e3) / 1e9
+    ncls, Tc, kl_c, ku_c = pl.query(800), pl.query(900), pl.query(1000), pl.query(1100)
+    geo = {"NXH": pl.NXH, "NYA": pl.NYAA, "NXA": pl.NXAA, "NZ": pl.NZ, "NZA": pl.NZAA,
+           "nF": pl.query(8), "nQ": pl.query(9)}
+    pbytes = phase_bytes(geo, nsys, nact, T, ncls, Tc, kl_c, ku_c, pl.stages, fbytes)
     peak, src = read_peaks()
-    traffic = read_traffic(nact)
+    phases = {}
+    for k, b in pbytes.items():
+        launch_ms = prof[k] / pl.stages
+        gbs = b / (launch_ms / 1e3) / 1e9 if launch_ms > 0 else None
+        phases[k] = {"kernels": PHASE_KERNELS[k], "ms_per_launch": round(launch_ms, 4),
+                     "algorithmic_bytes": b, "achieved_gbs": round(gbs, 1) if gbs else None,
+                     "frac": round(gbs / peak, 4) if gbs else None}
+    top = max(pbytes, key=lambda k: prof[k])
+    launch_ms = prof[top] / pl.stages
+    achieved = pbytes[top] / (launch_ms / 1e3) / 1e9
+    traffic = read_traffic(PHASE_KERNELS[top])
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(cfg, eq, par, max_seconds=args.cpu_seconds)
@@ -255,19 +291,21 @@ def run_ours(args, cfg):
         "config": {"workload": "%s: RBC no-slip Ra=%g Pr=1, %dx%dx%d modes, grid %dx%dx%d, ARS_222, dt=%g, FP64"
                                % (args.config, cfg["Ra"], pl.NX, pl.NY, pl.NZ, pl.NXAA, pl.NYAA, pl.NZAA, dt),
                    "grid_points": pl.NXAA * pl.NYAA * pl.NZAA, "systems": nsys, "active_systems": nact, "T": T,
-                   "band": [kl, ku], "l2": "inputs larger than L2 (state %.2f GB, LU factors %.1f GB)"
-                   % (field.nbytes / 1e9, nact * ldab * T * fbytes / 1e9),
-                   "lu_factors": "real-scaled" if fbytes == 8 else "complex",
+                   "band": [pl.query(500), pl.query(600)], "blocks": ncls, "block_T": Tc, "block_band": [kl_c, ku_c],
+                   "l2": "inputs larger than L2 (state %.2f GB, LU factors %.1f GB)"
+                   % (field.nbytes / 1e9, nact * ncls * Tc * (2 * kl_c + ku_c + 1) * fbytes / 1e9),
+                   "lu_factors": ("real-scaled" if fbytes == 8 else "complex")
+                                 + (", split into %d independent blocks per system" % ncls if ncls > 1 else ""),
                    "parallelism": "replicas x%d" % world},
         "grid_point_steps_per_s": value * pl.NXAA * pl.NYAA * pl.NZAA,
         "e2e": e2e,
         "gpu_launches": gpu_launches,
         "phase_ms_per_step": {k: round(v, 4) for k, v in prof.items()},
         "factorize_s": t_factor,
-        "roofline": {"kernel": "k_solve (stage update + banded LU solve)", "bound": "hbm", "achieved": achieved,
+        "roofline": {"kernel": PHASE_KERNELS[top], "phase": top, "bound": "hbm", "achieved": achieved,
                      "peak": peak, "peak_source": src, "unit": "GB/s", "frac": achieved / peak,
-                     "algorithmic_bytes_per_launch": algo, "launch_ms": launch_ms,
-                     "traffic": traffic},
+                     "algorithmic_bytes_per_launch": pbytes[top], "launch_ms": launch_ms,
+                     "traffic": traffic, "phases": phases},
         "cpu_baseline": cpu,
         "clocks": clocks,
         "state_ok": not diag["nonfinite"],
@@ -285,15 +323,15 @@ def iy_dealiased(iy, NY, NYAA):
     return abs(k) >= NY / 2
 
 
-def read_traffic(nact):
-    """DRAM traffic per launch of the solve kernel, scaled from the ncu capture
-    summarised in profiles/ (bytes per active system), or None."""
-    p = os.path.join(ROOT, "profiles", "k_solve_rbc_384x384x192.txt")
+def read_traffic(kernels):
+    """DRAM bytes (read + write) per launch of the phase's kernels at 384^2 x 192,
+    from the ncu launch list summarised in profiles/, or None."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic_rbc_384x384x192.txt")
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.startswith("dram_bytes_per_active_system"):
-            return float(line.split("=")[1]) * nact
+        if "=" in line and line.split("=")[0].strip() == kernels:
+            return float(line.split("=")[1])
     return None
 
 

@@ -76,6 +76,13 @@ struct KSys {
   unsigned char *rowflip = nullptr, *colflip = nullptr;
   unsigned char* dpiv;
   int* info;
+  // class split of the real-scaled solve (SystemOps::ncls == 2); when unsplit:
+  // ncls = 1, Tc = T, the band (kl_s, ku_s, ldab_s) of the whole system, work = aux
+  int ncls = 1, Tc = 0, kl_s = 0, ku_s = 0, ldab_s = 0, wst = 0;
+  int *row_pos = nullptr, *col_pos = nullptr, *cls_row = nullptr;
+  unsigned char* colflip_cls = nullptr;
+  DevEll Lp;
+  double2* work = nullptr;
   std::vector<std::vector<int>> tab_t;   // per var: [NZ][kTabW]
   std::vector<std::vector<double>> tab_v;
   std::vector<int*> d_tab_t;
@@ -278,11 +285,43 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
     k.real = k.ops.real_scalable && k.kl <= 16 && k.kl + k.ku <= 63 && std::getenv("CORAL_COMPLEX_FACTORS") == nullptr;
     k.ab = nullptr;
     k.abr = nullptr;
-    if (k.real) k.abr = mem.get<double>((size_t)h->nact * k.T * k.ldab);
-    else k.ab = mem.get<double2>((size_t)h->nact * k.T * k.ldab);
     k.rowflip = mem.upload(k.ops.row_flip);
     k.colflip = mem.upload(k.ops.col_flip);
-    k.dpiv = mem.get<unsigned char>((size_t)h->nact * ((k.T + 7) & ~7));  // rows padded to 8 bytes
+    k.ncls = 1;
+    k.Tc = k.T;
+    k.kl_s = k.kl;
+    k.ku_s = k.ku;
+    k.ldab_s = k.ldab;
+    k.wst = k.T;
+    k.work = k.aux;
+    k.Lp = k.L;
+    k.colflip_cls = k.colflip;
+    if (k.real && k.ops.ncls == 2 && k.ops.kl_cls <= 15 && k.ops.kl_cls + k.ops.ku_cls <= 31 &&
+        std::getenv("CORAL_NO_CLASS_SPLIT") == nullptr) {
+      k.ncls = 2;
+      k.Tc = k.ops.Tc;
+      k.kl_s = k.ops.kl_cls;
+      k.ku_s = k.ops.ku_cls;
+      k.ldab_s = 2 * k.kl_s + k.ku_s + 1;
+      k.ldab_s += k.ldab_s & 1;
+      k.wst = std::max(k.T, 2 * k.Tc);
+      k.work = mem.get<double2>(nsys * k.wst);  // never aliases aux: k_kstd_out gathers from it into aux
+      CK(cudaMemset(k.work, 0, nsys * k.wst * sizeof(double2)));
+      k.row_pos = mem.upload(k.ops.row_cls_pos);
+      k.col_pos = mem.upload(k.ops.col_cls_pos);
+      k.cls_row = mem.upload(k.ops.cls_row);
+      std::vector<unsigned char> cf(2 * (size_t)k.Tc, 0);
+      for (int t = 0; t < k.T; ++t) cf[k.ops.col_cls_pos[t]] = k.ops.col_flip[t];
+      k.colflip_cls = mem.upload(cf);
+      EllOp lp = k.ops.L;
+      for (int& c : lp.col)
+        if (c >= 0) c = k.ops.col_cls_pos[c];
+      k.Lp = upload_ell(mem, lp);
+    }
+    if (k.real) k.abr = mem.get<double>((size_t)h->nact * k.Tc * k.ncls * k.ldab_s);
+    else k.ab = mem.get<double2>((size_t)h->nact * k.T * k.ldab);
+    // pivot rows padded to 8 bytes, one row per system and class
+    k.dpiv = mem.get<unsigned char>((size_t)h->nact * k.ncls * ((k.Tc + 7) & ~7));
     k.info = mem.get<int>((size_t)std::max(h->nact, 1));
     for (int v = 0; v < k.ops.nV; ++v) {
       std::vector<int> tt;
@@ -479,14 +518,14 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       SolveArgs sa{};
       sa.d = d;
       sa.T = k.T;
-      sa.kl = k.kl;
-      sa.ku = k.ku;
-      sa.ldab = k.ldab;
+      sa.kl = k.real ? k.kl_s : k.kl;
+      sa.ku = k.real ? k.ku_s : k.ku;
+      sa.ldab = k.real ? k.ldab_s : k.ldab;
       sa.M = k.M;
       sa.L = k.L;
       sa.field = k.field;
       sa.out = last ? k.field : k.aux;
-      sa.work = k.aux;
+      sa.work = k.work;
       sa.Kstd_out = last ? nullptr : k.Kstd[i];
       sa.nprev = i;
       for (int j = 0; j <= i; ++j) {
@@ -507,10 +546,17 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       sa.abr = k.abr;
       sa.rowflip = k.rowflip;
       sa.colflip = k.colflip;
+      sa.ncls = k.ncls;
+      sa.Tc = k.Tc;
+      sa.wst = k.wst;
+      sa.row_pos = k.row_pos;
+      sa.col_pos = k.col_pos;
+      sa.colflip_cls = k.colflip_cls;
+      sa.Lp = k.Lp;
       {
-        const int kv = k.kl + k.ku;
-        const int u_rows = (kv + 2) & ~1, l_rows = ((kv + 1 + k.kl + 1) & ~1) - ((kv + 1) & ~1);
-        sa.ring_cols = std::max(u_rows, l_rows);
+        const int kv = sa.kl + sa.ku;
+        const int u_rows = (kv + 2) & ~1, l_rows = ((kv + 1 + sa.kl + 1) & ~1) - ((kv + 1) & ~1);
+        sa.ring_cols = k.ncls * std::max(u_rows, l_rows);
       }
       if (k.real) {
         B(7); launch_solve_real(sa, na, h->stream); E();
@@ -548,9 +594,13 @@ void factorize(coral_handle* h, double dt) {
     FactorArgs fa{};
     fa.d = d;
     fa.T = k.T;
-    fa.kl = k.kl;
-    fa.ku = k.ku;
-    fa.ldab = k.ldab;
+    fa.kl = k.real ? k.kl_s : k.kl;
+    fa.ku = k.real ? k.ku_s : k.ku;
+    fa.ldab = k.real ? k.ldab_s : k.ldab;
+    fa.ncls = k.ncls;
+    fa.Tc = k.Tc;
+    fa.cls_row = k.cls_row;
+    fa.col_pos = k.col_pos;
     fa.nact = h->nact;
     fa.M = k.M;
     fa.L = k.L;
@@ -564,6 +614,7 @@ void factorize(coral_handle* h, double dt) {
     fa.abr = k.abr;
     fa.rowflip = k.rowflip;
     fa.colflip = k.colflip;
+    CK(cudaMemsetAsync(k.info, 0, (size_t)std::max(h->nact, 1) * sizeof(int), h->stream));
     if (k.real) launch_factor_real(fa, h->stream);
     else launch_factor(fa, h->stream);
     ++h->launches;
@@ -861,6 +912,10 @@ int coral_query(const coral_handle* hc, int what, long long* value) {
   if (base == CORAL_Q_SYS_KL && i < (int)h->ks.size()) { *value = h->ks[i].kl; return 0; }
   if (base == CORAL_Q_SYS_KU && i < (int)h->ks.size()) { *value = h->ks[i].ku; return 0; }
   if (base == CORAL_Q_SYS_REAL && i < (int)h->ks.size()) { *value = h->ks[i].real ? 1 : 0; return 0; }
+  if (base == CORAL_Q_SYS_CLASSES && i < (int)h->ks.size()) { *value = h->ks[i].ncls; return 0; }
+  if (base == CORAL_Q_SYS_CLASS_T && i < (int)h->ks.size()) { *value = h->ks[i].Tc; return 0; }
+  if (base == CORAL_Q_SYS_CLASS_KL && i < (int)h->ks.size()) { *value = h->ks[i].kl_s; return 0; }
+  if (base == CORAL_Q_SYS_CLASS_KU && i < (int)h->ks.size()) { *value = h->ks[i].ku_s; return 0; }
   return CORAL_EBADARG;
 }
 

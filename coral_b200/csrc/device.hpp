@@ -115,10 +115,20 @@ struct SolveArgs {
   int ring_cols;         // doubles per column slot of the solve's shared-memory ring
   int nact;              // active systems (factor slots)
   const int* act_list;   // [nact] kx*NYA+ky of each factor slot
+  // class split (SystemOps::ncls == 2): factors of both classes interleaved per
+  // column (column stride ncls*ldab), kl/ku/ldab those of one class; the
+  // right-hand sides and solutions in work are stored class by class
+  // (work stride wst >= ncls*Tc) and mapped back through col_pos.
+  int ncls, Tc, wst;
+  const int* row_pos;    // [T] class position of an equation row (null: unsplit)
+  const int* col_pos;    // [T] class position of a variable column (null: unsplit)
+  const unsigned char* colflip_cls;  // [ncls*Tc] colflip in class order
+  DevEll Lp;             // L with its columns in class positions (= L when unsplit)
 };
 void launch_solve(const SolveArgs& a, cudaStream_t s);
-// real-scaled factors (kl <= 31, kl+ku <= 63): right-hand side with the NL
-// assembly fused in, substitutions, then K_std and outputs (three kernels)
+// real-scaled factors (unsplit: kl <= 31, kl+ku <= 63; class split: kl <= 15,
+// kl+ku <= 31 per class): right-hand side with the NL assembly fused in,
+// substitutions, then K_std and outputs (three kernels)
 void launch_solve_real(const SolveArgs& a, const NLArgs& n, cudaStream_t s);
 
 struct FactorArgs {
@@ -135,6 +145,10 @@ struct FactorArgs {
   double* abr;           // real-scaled factors (when rowflip/colflip are set)
   const unsigned char* rowflip;
   const unsigned char* colflip;
+  // class split of the real-scaled factors (see SolveArgs); ncls = 1: unsplit
+  int ncls, Tc;
+  const int* cls_row;    // [ncls*Tc] equation row of a class position, -1 = identity padding
+  const int* col_pos;    // [T] class position of a variable column
 };
 void launch_factor(const FactorArgs& a, cudaStream_t s);
 void launch_factor_real(const FactorArgs& a, cudaStream_t s);

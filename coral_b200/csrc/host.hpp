@@ -144,6 +144,18 @@ struct SystemOps {
   // (variables) of that diagonal scaling and real_scalable is true.
   bool real_scalable = false;
   std::vector<unsigned char> row_flip, col_flip;
+  // Independent blocks: when the pattern of M and L (equation rows x variable
+  // columns) falls apart into blocks that touch only themselves (Chebyshev
+  // parity does this for the plane-layer recipes), the components are gathered
+  // into ncls = 2 classes of equal size Tc (the smaller padded with identity
+  // rows).  Each class is its own band system of band (kl_cls, ku_cls) in the
+  // original relative order, and LU with partial pivoting of E factors class by
+  // class: the entries of the other class are exact zeros in every pivot
+  // column, so pivots and multipliers are those of the whole matrix.
+  int ncls = 1, Tc = 0, kl_cls = 0, ku_cls = 0;
+  std::vector<int> row_cls_pos;  // [T] class * Tc + index within the class (equation rows)
+  std::vector<int> col_cls_pos;  // [T] the same for variable columns
+  std::vector<int> cls_row;      // [ncls * Tc] equation row of a class position, -1 = identity padding
   // square stencil (var_size x var_size, lower-banded) for projections of
   // Chebyshev coefficients onto the Galerkin basis (QuickSave import)
   std::vector<Dense> sq_stencil;

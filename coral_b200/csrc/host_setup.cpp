@@ -488,6 +488,73 @@ static int group_of(EllOp& op, int a, int b) {
   return int(op.groups.size()) - 1;
 }
 
+// Connected components of the bipartite graph (equation rows, variable columns)
+// of every stored entry of M and L, gathered into two classes of equal size.
+// Leaves ncls = 1 when the pattern is one block or a block is not square.
+static void split_classes(SystemOps& o) {
+  const int T = o.T;
+  std::vector<int> par(2 * T);
+  for (int u = 0; u < 2 * T; ++u) par[u] = u;
+  auto find = [&](int u) {
+    while (par[u] != u) u = par[u] = par[par[u]];
+    return u;
+  };
+  for (const EllOp* op : {&o.M, &o.L})
+    for (int rr = 0; rr < op->rows; ++rr)
+      for (int k = 0; k < op->width; ++k) {
+        const int c = op->col[size_t(rr) * op->width + k];
+        if (c < 0) continue;
+        const int a = find(rr), b = find(T + c);
+        if (a != b) par[a] = b;
+      }
+  std::map<int, std::pair<int, int>> count;  // root -> (rows, columns)
+  for (int t = 0; t < T; ++t) {
+    ++count[find(t)].first;
+    ++count[find(T + t)].second;
+  }
+  if (count.size() < 2) return;
+  for (const auto& kv : count)
+    if (kv.second.first != kv.second.second) return;
+  // largest components first, each into the smaller class
+  std::vector<std::pair<int, int>> comps;  // (size, root)
+  for (const auto& kv : count) comps.emplace_back(kv.second.first, kv.first);
+  std::stable_sort(comps.begin(), comps.end(), [](const std::pair<int, int>& a, const std::pair<int, int>& b) {
+    return a.first > b.first;
+  });
+  std::map<int, int> cls_of_root;
+  int size[2] = {0, 0};
+  for (const auto& cp : comps) {
+    const int cl = (size[0] <= size[1]) ? 0 : 1;
+    cls_of_root[cp.second] = cl;
+    size[cl] += cp.first;
+  }
+  const int Tc = std::max(size[0], size[1]);
+  o.ncls = 2;
+  o.Tc = Tc;
+  o.row_cls_pos.assign(T, -1);
+  o.col_cls_pos.assign(T, -1);
+  o.cls_row.assign(2 * (size_t)Tc, -1);
+  int nr[2] = {0, 0}, nc[2] = {0, 0};
+  for (int t = 0; t < T; ++t) {
+    const int cr = cls_of_root[find(t)];
+    o.row_cls_pos[t] = cr * Tc + nr[cr];
+    o.cls_row[cr * Tc + nr[cr]] = t;
+    ++nr[cr];
+    const int cc = cls_of_root[find(T + t)];
+    o.col_cls_pos[t] = cc * Tc + nc[cc]++;
+  }
+  o.kl_cls = o.ku_cls = 0;
+  for (const EllOp* op : {&o.M, &o.L})
+    for (int rr = 0; rr < op->rows; ++rr)
+      for (int k = 0; k < op->width; ++k) {
+        const int c = op->col[size_t(rr) * op->width + k];
+        if (c < 0) continue;
+        const int i = o.row_cls_pos[rr] % Tc, j = o.col_cls_pos[c] % Tc;
+        o.kl_cls = std::max(o.kl_cls, i - j);
+        o.ku_cls = std::max(o.ku_cls, j - i);
+      }
+}
+
 SystemOps assemble_system(const Geometry& g, const Recipe& r, const CoupledSet& s) {
   (void)r;
   SystemOps o;
@@ -619,6 +686,7 @@ SystemOps assemble_system(const Geometry& g, const Recipe& r, const CoupledSet& 
       for (int j = 0; j < nc; ++j) sq[i][j] = S[v][i][j];
     o.sq_stencil[v] = sq;
   }
+  split_classes(o);
   return o;
 }
 

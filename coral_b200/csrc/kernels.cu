@@ -653,11 +653,17 @@ __global__ void __launch_bounds__(kWPB * 32) k_factor(FactorArgs a) {
 __device__ __forceinline__ double2 flip_row(double2 z, int f) { return f ? make_double2(z.y, -z.x) : z; }  // * (-i)
 __device__ __forceinline__ double2 flip_col(double2 z, int f) { return f ? make_double2(-z.y, z.x) : z; }  // * (+i)
 
+// With a class split (FactorArgs::ncls == 2) one warp factors one class of one
+// system (blockIdx.y = class): the class's rows and columns in their original
+// relative order, identity rows on padding positions, stored in the class's
+// ldab rows of each column (column stride ncls * ldab).
 __global__ void __launch_bounds__(kWPB * 32) k_factor_real(FactorArgs a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int sys = blockIdx.x * kWPB + warp;
   if (sys >= a.nact) return;
-  const int T = a.T, kl = a.kl, ku = a.ku, kv = kl + ku, ldab = a.ldab;
+  const int cls = blockIdx.y;
+  const int T = a.Tc, kl = a.kl, ku = a.ku, kv = kl + ku, ldab = a.ldab;
+  const size_t cstr = (size_t)a.ncls * ldab;  // column stride
   const int sid = a.act_list[sys];
   const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
   double2 cm[kMaxGroups], cl[kMaxGroups];
@@ -666,10 +672,15 @@ __global__ void __launch_bounds__(kWPB * 32) k_factor_real(FactorArgs a) {
     cm[g] = (g < a.M.ngroups) ? cmul(ipow(a.kx[kx], a.M.gkx[g]), ipow(a.ky[ky], a.M.gky[g])) : zero2();
     cl[g] = (g < a.L.ngroups) ? cmul(ipow(a.kx[kx], a.L.gkx[g]), ipow(a.ky[ky], a.L.gky[g])) : zero2();
   }
-  double* ab = a.abr + (size_t)sys * T * ldab;
-  for (size_t e = lane; e < (size_t)T * ldab; e += 32) ab[e] = 0.0;
+  double* ab = a.abr + (size_t)sys * T * cstr + (size_t)cls * ldab;
+  for (size_t e = lane; e < (size_t)T * ldab; e += 32) ab[(e / ldab) * cstr + e % ldab] = 0.0;
   __syncwarp();
-  for (int t = lane; t < T; t += 32) {
+  for (int i = lane; i < T; i += 32) {
+    const int t = a.cls_row ? a.cls_row[cls * T + i] : i;  // equation row of class position i
+    if (t < 0) {
+      ab[(size_t)i * cstr + kv] = 1.0;  // identity padding
+      continue;
+    }
     const int rf = a.rowflip[t];
     for (int pass = 0; pass < 2; ++pass) {
       const DevEll& op = pass ? a.L : a.M;
@@ -677,6 +688,7 @@ __global__ void __launch_bounds__(kWPB * 32) k_factor_real(FactorArgs a) {
         const double v = op.v(t, k);
         if (v == 0.0) continue;  // empty slot
         const int c = op.col(t, k), g = op.grp(t, k);
+        const int jc = a.col_pos ? a.col_pos[c] - cls * T : c;  // column in the class
         double2 cv = zero2();
 #pragma unroll
         for (int gg = 0; gg < kMaxGroups; ++gg)
@@ -684,18 +696,19 @@ __global__ void __launch_bounds__(kWPB * 32) k_factor_real(FactorArgs a) {
         double2 z = cscale(cv, v);
         if (pass) z = cscale(z, a.zsca);
         z = flip_col(flip_row(z, rf), a.colflip[c]);
-        ab[(size_t)c * ldab + kv + t - c] += z.x;
+        ab[(size_t)jc * cstr + kv + i - jc] += z.x;
       }
     }
   }
   __syncwarp();
+  unsigned char* dpiv = a.dpiv + ((size_t)sys * a.ncls + cls) * ((T + 7) & ~7);  // rows padded to 8 bytes
   int ju = 0, info = 0;
   for (int j = 0; j < T; ++j) {
     const int km = min(kl, T - 1 - j);
     double mag = -1.0;
     int idx = 1 << 30;
     if (lane <= km) {
-      mag = fabs(ab[(size_t)j * ldab + kv + lane]);
+      mag = fabs(ab[(size_t)j * cstr + kv + lane]);
       idx = lane;
     }
     for (int o = 16; o > 0; o >>= 1) {
@@ -704,8 +717,8 @@ __global__ void __launch_bounds__(kWPB * 32) k_factor_real(FactorArgs a) {
       if (m2 > mag || (m2 == mag && i2 < idx)) { mag = m2; idx = i2; }
     }
     const int jp = idx;
-    if (lane == 0) a.dpiv[(size_t)sys * ((T + 7) & ~7) + j] = (unsigned char)jp;
-    const double piv = ab[(size_t)j * ldab + kv + jp];
+    if (lane == 0) dpiv[j] = (unsigned char)jp;
+    const double piv = ab[(size_t)j * cstr + kv + jp];
     if (piv == 0.0) {
       if (info == 0) info = j + 1;
       continue;
@@ -713,30 +726,30 @@ __global__ void __launch_bounds__(kWPB * 32) k_factor_real(FactorArgs a) {
     ju = max(ju, min(j + ku + jp, T - 1));
     if (jp != 0) {
       for (int c = j + lane; c <= ju; c += 32) {
-        double* p1 = ab + (size_t)c * ldab + kv + j + jp - c;
-        double* p0 = ab + (size_t)c * ldab + kv + j - c;
+        double* p1 = ab + (size_t)c * cstr + kv + j + jp - c;
+        double* p0 = ab + (size_t)c * cstr + kv + j - c;
         const double t0 = *p0;
         *p0 = *p1;
         *p1 = t0;
       }
       __syncwarp();
     }
-    const double r = 1.0 / ab[(size_t)j * ldab + kv];
+    const double r = 1.0 / ab[(size_t)j * cstr + kv];
     __syncwarp();
     if (km > 0) {
-      if (lane >= 1 && lane <= km) ab[(size_t)j * ldab + kv + lane] *= r;
+      if (lane >= 1 && lane <= km) ab[(size_t)j * cstr + kv + lane] *= r;
       __syncwarp();
       const int nc = ju - j;
       for (int e = lane; e < nc * km; e += 32) {
         const int c = j + 1 + e / km, i = 1 + e % km;
-        ab[(size_t)c * ldab + kv + j + i - c] -= ab[(size_t)j * ldab + kv + i] * ab[(size_t)c * ldab + kv + j - c];
+        ab[(size_t)c * cstr + kv + j + i - c] -= ab[(size_t)j * cstr + kv + i] * ab[(size_t)c * cstr + kv + j - c];
       }
     }
     __syncwarp();
-    if (lane == 0) ab[(size_t)j * ldab + kv] = r;
+    if (lane == 0) ab[(size_t)j * cstr + kv] = r;
     __syncwarp();
   }
-  if (lane == 0) a.info[sys] = info;
+  if (lane == 0 && info) atomicMax(a.info + sys, info);
 }
 
 // ------------------------------------------------------------------------------
@@ -746,9 +759,8 @@ __global__ void __launch_bounds__(kWPB * 32) k_factor_real(FactorArgs a) {
 // band lives in registers, each lane owning the positions p = lane (mod 32):
 //   forward  window [j, j+kl] (kl <= 31), one register per lane
 //   backward window [j-kv, j] (kv <= 63), two registers per lane
-// so a column step moves only the pivot value between lanes.  Factor entries
-// are loaded straight into the owning lane and prefetched in register rings
-// (16 columns of L, 8 columns of U).
+// so a column step moves only the pivot value between lanes.  Factor columns
+// reach the lanes through a per-warp shared-memory ring filled by cp.async.
 // ------------------------------------------------------------------------------
 constexpr int kWPBr = 4;   // warps per CTA
 constexpr int kCW = 8;     // factor columns per ring chunk (divides 32)
@@ -768,30 +780,43 @@ __device__ __forceinline__ double2 shfl2(double2 v, int src) {
   return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
 }
 
+// H = lanes per system class: H = 32 for an unsplit system, H = 16 for a class
+// split, the two classes of one system side by side in the two half-warps, in
+// lockstep over their Tc columns (positions p = lane (mod H) of the half; the
+// window bounds become kl <= H-1 and kl+ku <= 2H-1).
+template <int H>
 __global__ void __launch_bounds__(kWPBr * 32) k_subst_real(SolveArgs a) {
+  constexpr int NC = 32 / H;            // classes per warp
+  constexpr int LH = (H == 32) ? 5 : 4;  // log2(H)
   extern __shared__ double smr[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int hl = lane & (H - 1);         // lane within the class's half
+  const int cls = lane >> LH;
+  const int hb = lane - hl;              // first lane of the half
   const int act = blockIdx.x * kWPBr + warp;  // active systems only
   if (act >= a.nact) return;
-  const int T = a.T;
+  const int T = a.Tc;
   const int sid = a.act_list[act];
-  double2* x = a.work + (size_t)sid * T;  // right-hand side in, solution out
+  double2* x = a.work + (size_t)sid * a.wst + (size_t)cls * T;  // right-hand side in, solution out
   {
     const int kl = a.kl, kv = a.kl + a.ku, ldab = a.ldab;
-    const double* ab = a.abr + (size_t)act * T * ldab;
-    const unsigned char* dp = a.dpiv + (size_t)act * ((T + 7) & ~7);
+    const size_t cstr = (size_t)NC * ldab;  // factor column stride (both classes)
+    const double* ab = a.abr + (size_t)act * T * cstr;
+    const unsigned char* dp = a.dpiv + ((size_t)act * NC + cls) * ((T + 7) & ~7);
+    const unsigned char* cflip = a.colflip_cls + (size_t)cls * T;
     // Factor columns stream through a per-warp shared-memory ring (kNBUF chunks
     // of kCW columns) with cp.async, kNBUF-1 chunks ahead of the sweep; the
     // forward sweep copies only the L rows of each column, the backward sweep
     // only the U rows.  (ldab is even, so both row ranges are 16-byte aligned.)
     double* ring = smr + (size_t)warp * kNBUF * kCW * a.ring_cols;
+    const int rc = a.ring_cols / NC;                  // ring doubles per class and column
     const int u_rows = (kv + 2) & ~1;                 // rows [0, u_rows) hold U (+ maybe one L row)
     const int l_row0 = (kv + 1) & ~1;                 // rows [l_row0, l_row1) hold L
     const int l_rows = ((kv + 1 + kl + 1) & ~1) - l_row0;
     // ================= forward: P and L =================
-    // lane l owns the positions p = l (mod 32); the active window is [j, j+kl].
-    // Vector traffic moves in blocks of 32 columns: the owner of column j takes
-    // the new position j+32 (loaded one block ahead) and parks y_j until the
+    // lane l owns the positions p = l (mod H); the active window is [j, j+kl].
+    // Vector traffic moves in blocks of H columns: the owner of column j takes
+    // the new position j+H (loaded one block ahead) and parks y_j until the
     // block's coalesced store.
     {
       const int nchunks = (T - 1 + kCW - 1) / kCW;
@@ -799,57 +824,57 @@ __global__ void __launch_bounds__(kWPBr * 32) k_subst_real(SolveArgs a) {
         if (c < nchunks) {
           const int j0 = c * kCW, nc = min(kCW, T - 1 - j0);
           double* dst = ring + (size_t)(c % kNBUF) * kCW * a.ring_cols;
-          const int per = l_rows / 2;  // 16-byte pieces per column
-          for (int e = lane; e < nc * per; e += 32) {
-            const int q = e / per, r = e - q * per;
-            cp_async16(dst + q * a.ring_cols + 2 * r, ab + (size_t)(j0 + q) * ldab + l_row0 + 2 * r);
+          const int per = l_rows / 2;  // 16-byte pieces per column and class
+          for (int e = lane; e < nc * NC * per; e += 32) {
+            const int q = e / (NC * per), rem = e - q * (NC * per), cc = rem / per, r = rem - cc * per;
+            cp_async16(dst + q * a.ring_cols + cc * rc + 2 * r, ab + (size_t)(j0 + q) * cstr + cc * ldab + l_row0 + 2 * r);
           }
         }
         cp_async_commit();
       };
 #pragma unroll
       for (int c = 0; c < kNBUF - 1; ++c) issue(c);
-      double2 w = (lane < T) ? x[lane] : zero2();
-      double2 incCur = (32 + lane < T) ? x[32 + lane] : zero2();
+      double2 w = (hl < T) ? x[hl] : zero2();
+      double2 incCur = (H + hl < T) ? x[H + hl] : zero2();
       double2 incNext = zero2(), ysave = zero2();
-      // pivot offsets of a chunk as two uniform 32-bit words (rows padded to 8 bytes)
+      // pivot offsets of a chunk as two 32-bit words, uniform over the half (rows padded to 8 bytes)
       uint2 pw = *reinterpret_cast<const uint2*>(dp);
       for (int c = 0; c < nchunks; ++c) {
         const int j0 = c * kCW;
-        if ((j0 & 31) == 0)  // new block of 32 columns: next block's incoming values
-          incNext = (j0 + 64 + lane < T) ? x[j0 + 64 + lane] : zero2();
+        if ((j0 & (H - 1)) == 0)  // new block of H columns: next block's incoming values
+          incNext = (j0 + 2 * H + hl < T) ? x[j0 + 2 * H + hl] : zero2();
         const uint2 pwc = pw;
         if (c + 1 < nchunks) pw = *reinterpret_cast<const uint2*>(dp + j0 + kCW);
         __syncwarp();
         issue(c + kNBUF - 1);
         cp_async_wait<kNBUF - 1>();
         __syncwarp();
-        const double* cb = ring + (size_t)(c % kNBUF) * kCW * a.ring_cols;
+        const double* cb = ring + (size_t)(c % kNBUF) * kCW * a.ring_cols + cls * rc;
 #pragma unroll
         for (int q = 0; q < kCW; ++q) {
           const int j = j0 + q;
           if (j < T - 1) {
-            const int src = j & 31;
-            const int i = (lane - j) & 31;
+            const int src = hb + (j & (H - 1));
+            const int i = (hl - j) & (H - 1);
             const int lm = min(kl, T - 1 - j);
             const double lv = (i >= 1 && i <= lm) ? cb[q * a.ring_cols + (kv + i - l_row0)] : 0.0;
             const int jp = ((q < 4 ? pwc.x : pwc.y) >> (8 * (q & 3))) & 0xFF;
             // Row interchange j <-> j+jp and broadcast of the pivot row in one shuffle:
             // the owner of row j+jp fetches row j (its new content), every other lane
             // fetches the pivot row; the owner of j+jp already holds the pivot value.
-            const int r2 = (j + jp) & 31;
-            const int from = (jp != 0 && lane == r2) ? src : r2;
-            const double2 got = shfl2(w, from);
-            const double2 bj = (jp != 0 && lane == r2) ? w : got;
-            if (lane == src || (jp != 0 && lane == r2)) w = got;
+            const int r2 = hb + ((j + jp) & (H - 1));
+            const bool mine = (jp != 0 && lane == r2);
+            const double2 got = shfl2(w, mine ? src : r2);
+            const double2 bj = mine ? w : got;
+            if (lane == src || mine) w = got;
             w.x -= lv * bj.x;  // zero multiplier outside rows j+1..j+lm
             w.y -= lv * bj.y;
             if (lane == src) {
               ysave = w;
               w = incCur;
             }
-            if ((j & 31) == 31) {  // end of a block of 32 columns
-              x[j - 31 + lane] = ysave;
+            if ((j & (H - 1)) == H - 1) {  // end of a block of H columns
+              x[j - (H - 1) + hl] = ysave;
               incCur = incNext;
             }
           }
@@ -857,22 +882,22 @@ __global__ void __launch_bounds__(kWPBr * 32) k_subst_real(SolveArgs a) {
       }
       cp_async_wait<0>();
       // the last (partial) block of y values and y[T-1]
-      const int base = ((T - 1) >> 5) << 5;
-      if ((T - 1) & 31) {
-        if (base + lane <= T - 2) x[base + lane] = ysave;
+      const int base = ((T - 1) >> LH) << LH;
+      if ((T - 1) & (H - 1)) {
+        if (base + hl <= T - 2) x[base + hl] = ysave;
       }
-      if (lane == ((T - 1) & 31)) x[T - 1] = w;
+      if (hl == ((T - 1) & (H - 1))) x[T - 1] = w;
     }
     __syncwarp();
     // ================= backward: U (kl+ku super-diagonals, reciprocal diagonal) =================
-    // lane l owns p = l (mod 32) in two registers: w0 for (p>>5) even, w1 for odd.
-    // Blocks of 32 columns j = T-1-32b-s; the owner of j takes position j-64.
+    // lane l owns p = l (mod H) in two registers: w0 for (p/H) even, w1 for odd.
+    // Blocks of H columns j = T-1-H*b-s; the owner of j takes position j-2H.
     {
       double2 w0 = zero2(), w1 = zero2();
       {
-        const int ih = (T - 1 - lane) & 31, ph = T - 1 - ih, pl = ph - 32;
-        if (ph >= 0) { if ((ph >> 5) & 1) w1 = x[ph]; else w0 = x[ph]; }
-        if (pl >= 0) { if ((pl >> 5) & 1) w1 = x[pl]; else w0 = x[pl]; }
+        const int ih = (T - 1 - hl) & (H - 1), ph = T - 1 - ih, pl = ph - H;
+        if (ph >= 0) { if ((ph >> LH) & 1) w1 = x[ph]; else w0 = x[ph]; }
+        if (pl >= 0) { if ((pl >> LH) & 1) w1 = x[pl]; else w0 = x[pl]; }
       }
       const int nchunks = (T + kCW - 1) / kCW;  // chunk c: columns T-1-c*kCW-q, q < kCW
       auto issue = [&](int c) {
@@ -880,9 +905,9 @@ __global__ void __launch_bounds__(kWPBr * 32) k_subst_real(SolveArgs a) {
           const int jhi = T - 1 - c * kCW, jlo = max(0, jhi - kCW + 1), nc = jhi - jlo + 1;
           double* dst = ring + (size_t)(c % kNBUF) * kCW * a.ring_cols;
           const int per = u_rows / 2;
-          for (int e = lane; e < nc * per; e += 32) {
-            const int q = e / per, r = e - q * per;  // q counts down from jhi
-            cp_async16(dst + q * a.ring_cols + 2 * r, ab + (size_t)(jhi - q) * ldab + 2 * r);
+          for (int e = lane; e < nc * NC * per; e += 32) {
+            const int q = e / (NC * per), rem = e - q * (NC * per), cc = rem / per, r = rem - cc * per;  // q counts down from jhi
+            cp_async16(dst + q * a.ring_cols + cc * rc + 2 * r, ab + (size_t)(jhi - q) * cstr + cc * ldab + 2 * r);
           }
         }
         cp_async_commit();
@@ -891,47 +916,47 @@ __global__ void __launch_bounds__(kWPBr * 32) k_subst_real(SolveArgs a) {
 #pragma unroll
       for (int c = 0; c < kNBUF - 1; ++c) issue(c);
       auto own_col = [&](int b) {  // column of block b finished by this lane (may be < 0)
-        const int top = T - 1 - 32 * b;
-        return top - ((top - lane) & 31);
+        const int top = T - 1 - H * b;
+        return top - ((top - hl) & (H - 1));
       };
       int jl = own_col(0);
-      double2 incCur = (jl - 64 >= 0) ? x[jl - 64] : zero2();
-      int cfCur = (jl >= 0) ? a.colflip[jl] : 0;
+      double2 incCur = (jl - 2 * H >= 0) ? x[jl - 2 * H] : zero2();
+      int cfCur = (jl >= 0) ? cflip[jl] : 0;
       double2 incNext = zero2(), xsave = zero2();
       int cfNext = 0, jn = jl;
       for (int c = 0; c < nchunks; ++c) {
         const int k0 = c * kCW;  // steps taken before this chunk
-        if ((k0 & 31) == 0) {
-          jn = own_col((k0 >> 5) + 1);
-          incNext = (jn - 64 >= 0) ? x[jn - 64] : zero2();
-          cfNext = (jn >= 0) ? a.colflip[jn] : 0;
+        if ((k0 & (H - 1)) == 0) {
+          jn = own_col((k0 >> LH) + 1);
+          incNext = (jn - 2 * H >= 0) ? x[jn - 2 * H] : zero2();
+          cfNext = (jn >= 0) ? cflip[jn] : 0;
         }
         __syncwarp();
         issue(c + kNBUF - 1);
         cp_async_wait<kNBUF - 1>();
         __syncwarp();
-        const double* cb = ring + (size_t)(c % kNBUF) * kCW * a.ring_cols;
+        const double* cb = ring + (size_t)(c % kNBUF) * kCW * a.ring_cols + cls * rc;
 #pragma unroll
         for (int q = 0; q < kCW; ++q) {
           const int k = k0 + q;
           const int j = T - 1 - k;
           if (j >= 0) {
-            const int src = j & 31, sel = (j >> 5) & 1;
+            const int src = hb + (j & (H - 1)), sel = (j >> LH) & 1;
             const double* col = cb + q * a.ring_cols;
-            const int ih = (j - lane) & 31, il = ih + 32;
+            const int ih = (j - hl) & (H - 1), il = ih + H;
             const double h = (ih >= 1 && ih <= kv) ? col[kv - ih] : 0.0;
             const double l_ = (il <= kv) ? col[kv - il] : 0.0;
             const double d = col[kv];
             const double2 yj = shfl2(sel ? w1 : w0, src);
             const double2 xj = make_double2(yj.x * d, yj.y * d);
-            const int hreg = ((j - ih) >> 5) & 1;
+            const int hreg = ((j - ih) >> LH) & 1;
             if (hreg) { w1.x -= h * xj.x; w1.y -= h * xj.y; w0.x -= l_ * xj.x; w0.y -= l_ * xj.y; }
             else      { w0.x -= h * xj.x; w0.y -= h * xj.y; w1.x -= l_ * xj.x; w1.y -= l_ * xj.y; }
             if (lane == src) {
               xsave = flip_col(xj, cfCur);
               if (sel) w1 = incCur; else w0 = incCur;
             }
-            if ((k & 31) == 31) {  // end of a block of 32 columns
+            if ((k & (H - 1)) == H - 1) {  // end of a block of H columns
               if (jl >= 0) x[jl] = xsave;
               jl = jn;
               incCur = incNext;
@@ -941,7 +966,7 @@ __global__ void __launch_bounds__(kWPBr * 32) k_subst_real(SolveArgs a) {
         }
       }
       cp_async_wait<0>();
-      if ((T & 31) != 0 && jl >= 0) x[jl] = xsave;  // the last (partial) block
+      if ((T & (H - 1)) != 0 && jl >= 0) x[jl] = xsave;  // the last (partial) block
     }
   }
   __syncwarp();
@@ -995,14 +1020,17 @@ __global__ void __launch_bounds__(kWPB * 32) k_rhs_nl(SolveArgs a, NLArgs n) {
     }
     r = cadd(r, cscale(kh, a.ch[a.nprev]));
     if (act && a.rowflip) r = flip_row(r, a.rowflip[t]);
-    a.work[base + t] = r;
+    // class order for the split solve; inactive systems (E = I) keep row t at
+    // the position of column t, where k_kstd_out reads it back
+    a.work[(size_t)sid * a.wst + (a.row_pos ? (act ? a.row_pos[t] : a.col_pos[t]) : t)] = r;
   }
 }
 
 // ------------------------------------------------------------------------------
 // After the substitutions: K_std_i = L aux (0 for inactive systems), the stage
 // output (the new state in the last stage, zero on inactive systems), and the
-// non-finite check.  One warp per (kx,ky) system.
+// non-finite check.  One warp per (kx,ky) system.  With a class split the
+// solution is read back from class order (L's columns are stored remapped).
 // ------------------------------------------------------------------------------
 __global__ void __launch_bounds__(kWPB * 32) k_kstd_out(SolveArgs a) {
   __shared__ double2 cls[kWPB][kMaxGroups];
@@ -1017,14 +1045,14 @@ __global__ void __launch_bounds__(kWPB * 32) k_kstd_out(SolveArgs a) {
     cls[warp][lane] = (lane < a.L.ngroups) ? cmul(ipow(a.kx[kx], a.L.gkx[lane]), ipow(a.ky[ky], a.L.gky[lane])) : zero2();
   __syncwarp();
   const size_t base = (size_t)sid * T;
-  const double2* x = a.work + base;
+  const double2* x = a.work + (size_t)sid * a.wst;  // solution (class order when split)
   const bool zero_out = a.last_stage && !act;
   bool bad = false;
   for (int t = lane; t < T; t += 32) {
-    const double2 v = zero_out ? zero2() : x[t];
+    const double2 v = zero_out ? zero2() : x[a.col_pos ? a.col_pos[t] : t];
     bad |= !(isfinite(v.x) && isfinite(v.y));
     if (a.out != a.work || zero_out) a.out[base + t] = v;
-    if (a.Kstd_out) a.Kstd_out[base + t] = act ? ell_row(a.L, t, cls[warp], x) : zero2();
+    if (a.Kstd_out) a.Kstd_out[base + t] = act ? ell_row(a.Lp, t, cls[warp], x) : zero2();
   }
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.flags, 1u);
 }
@@ -1339,14 +1367,19 @@ void launch_solve_real(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
   k_rhs_nl<<<(nsys + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a, n);
   if (a.nact > 0) {
     const size_t sm = (size_t)kWPBr * kNBUF * kCW * a.ring_cols * sizeof(double);
-    set_smem(k_subst_real, sm);
-    k_subst_real<<<(a.nact + kWPBr - 1) / kWPBr, kWPBr * 32, sm, s>>>(a);
+    if (a.ncls == 2) {
+      set_smem(k_subst_real<16>, sm);
+      k_subst_real<16><<<(a.nact + kWPBr - 1) / kWPBr, kWPBr * 32, sm, s>>>(a);
+    } else {
+      set_smem(k_subst_real<32>, sm);
+      k_subst_real<32><<<(a.nact + kWPBr - 1) / kWPBr, kWPBr * 32, sm, s>>>(a);
+    }
   }
   k_kstd_out<<<(nsys + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
 }
 void launch_factor_real(const FactorArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;
-  k_factor_real<<<(a.nact + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
+  k_factor_real<<<dim3((a.nact + kWPB - 1) / kWPB, a.ncls), kWPB * 32, 0, s>>>(a);
 }
 void launch_zero_step(const ZeroArgs& a, cudaStream_t s) {
   if (a.nsys <= 0) return;

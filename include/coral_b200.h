@@ -67,6 +67,10 @@ typedef struct coral_handle coral_handle;
 #define CORAL_Q_SYS_KU 600           /* + isys: super-diagonals of the evolution band */
 #define CORAL_Q_SYS_REAL 700         /* + isys: 1 if its LU factors are stored real-scaled (8-byte entries),
                                         0 if complex (16-byte entries) */
+#define CORAL_Q_SYS_CLASSES 800      /* + isys: independent blocks its solve is split into (1 or 2) */
+#define CORAL_Q_SYS_CLASS_T 900      /* + isys: positions per block (= SYS_T when not split)        */
+#define CORAL_Q_SYS_CLASS_KL 1000    /* + isys: sub-diagonals of one block's band                   */
+#define CORAL_Q_SYS_CLASS_KU 1100    /* + isys: super-diagonals of one block's band                 */
 
 /*
  * Create a solver from the text of coral.equations and coral.parameters.in.

@@ -133,23 +133,54 @@ def test_cfg0_100_steps_within_1e10():
     pl.close()
 
 
-@pytest.mark.parametrize("complex_factors", [False, True])
-def test_both_factor_paths_match_oracle(complex_factors, monkeypatch):
-    """The real-scaled factors (recipes whose variables/equations admit the +-i
-    scaling, like Rayleigh-Benard) and the general complex factors give the
-    same steps."""
-    if complex_factors:
+@pytest.mark.parametrize("path", ["split", "unsplit", "complex"])
+def test_all_factor_paths_match_oracle(path, monkeypatch):
+    """The three solve paths give the same steps: real-scaled factors split into
+    the two independent (Chebyshev parity) blocks of every system, real-scaled
+    factors of the whole system, and the general complex factors."""
+    monkeypatch.delenv("CORAL_COMPLEX_FACTORS", raising=False)
+    monkeypatch.delenv("CORAL_NO_CLASS_SPLIT", raising=False)
+    if path == "complex":
         monkeypatch.setenv("CORAL_COMPLEX_FACTORS", "1")
-    else:
-        monkeypatch.delenv("CORAL_COMPLEX_FACTORS", raising=False)
+    elif path == "unsplit":
+        monkeypatch.setenv("CORAL_NO_CLASS_SPLIT", "1")
     eq = equations("rrbc_stressfree_ek1e-4_ra5e7", **{"5.d7": "3.d4", "1.d4": "3.d2"})
     par = params(12, 16, 24, dt=1e-4)
     ref = co.Solver(eq, par)
     pl = _pl(eq, par)
+    assert pl.query(700) == (0 if path == "complex" else 1)
+    assert pl.query(800) == (2 if path == "split" else 1)
+    if path == "split":
+        assert 2 * pl.query(900) == pl.T[0]
     _random_state(ref, pl, 11, amp=1e-2)
     for _ in range(3):
         ref.step(1e-4)
     pl.march_forward(1e-4, 3)
     pl.synchronize()
     assert _rel(pl.get_field(0), ref.field[0]) < 1e-11
+    pl.close()
+
+
+@pytest.mark.parametrize("split", [True, False])
+def test_split_solve_rbc_noslip_matches_oracle(split, monkeypatch):
+    """No-slip Rayleigh-Benard (the benchmark recipe) at NZ = 48 with and without
+    the block split, against the oracle over a few ARS_222 steps."""
+    monkeypatch.delenv("CORAL_COMPLEX_FACTORS", raising=False)
+    if split:
+        monkeypatch.delenv("CORAL_NO_CLASS_SPLIT", raising=False)
+    else:
+        monkeypatch.setenv("CORAL_NO_CLASS_SPLIT", "1")
+    eq = equations("rbc_noslip_ra1e8", **{"1.d8": "1.d5"})
+    par = params(16, 12, 48, dt=1e-5)
+    ref = co.Solver(eq, par)
+    pl = _pl(eq, par)
+    assert pl.query(800) == (2 if split else 1)
+    _random_state(ref, pl, 5, amp=1e-2)
+    for _ in range(3):
+        ref.step(1e-5)
+    pl.march_forward(1e-5, 3)
+    pl.synchronize()
+    assert _rel(pl.get_field(0), ref.field[0]) < 1e-11
+    for s in range(len(ref.zlay)):
+        assert _rel(pl.get_mean_field(s), ref.zfield[s]) < 1e-11
     pl.close()
