@@ -83,6 +83,7 @@ struct KSys {
   unsigned char* colflip_cls = nullptr;
   DevEll Lp;
   double2* work = nullptr;
+  double2* work2 = nullptr;  // thread-per-block layout of the active systems' vectors (split only)
   std::vector<std::vector<int>> tab_t;   // per var: [NZ][kTabW]
   std::vector<std::vector<double>> tab_v;
   std::vector<int*> d_tab_t;
@@ -318,10 +319,19 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
         if (c >= 0) c = k.ops.col_cls_pos[c];
       k.Lp = upload_ell(mem, lp);
     }
-    if (k.real) k.abr = mem.get<double>((size_t)h->nact * k.Tc * k.ncls * k.ldab_s);
-    else k.ab = mem.get<double2>((size_t)h->nact * k.T * k.ldab);
-    // pivot rows padded to 8 bytes, one row per system and class
-    k.dpiv = mem.get<unsigned char>((size_t)h->nact * k.ncls * ((k.Tc + 7) & ~7));
+    if (k.ncls == 2) {
+      // thread-per-block layouts: groups of 32 blocks (block = 2 act + class) side by side
+      const size_t ngroups = ((size_t)h->nact * 2 + 31) / 32;
+      k.abr = mem.get<double>(ngroups * k.Tc * k.ldab_s * 32);
+      k.dpiv = mem.get<unsigned char>(ngroups * k.Tc * 32);
+      k.work2 = mem.get<double2>(ngroups * k.Tc * 32);
+      CK(cudaMemset(k.work2, 0, ngroups * k.Tc * 32 * sizeof(double2)));
+    } else {
+      if (k.real) k.abr = mem.get<double>((size_t)h->nact * k.Tc * k.ldab_s);
+      else k.ab = mem.get<double2>((size_t)h->nact * k.T * k.ldab);
+      // pivot rows padded to 8 bytes, one row per system
+      k.dpiv = mem.get<unsigned char>((size_t)h->nact * ((k.Tc + 7) & ~7));
+    }
     k.info = mem.get<int>((size_t)std::max(h->nact, 1));
     for (int v = 0; v < k.ops.nV; ++v) {
       std::vector<int> tt;
@@ -553,6 +563,8 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       sa.col_pos = k.col_pos;
       sa.colflip_cls = k.colflip_cls;
       sa.Lp = k.Lp;
+      sa.work2 = k.work2;
+      sa.nblk = k.ncls * h->nact;
       {
         const int kv = sa.kl + sa.ku;
         const int u_rows = (kv + 2) & ~1, l_rows = ((kv + 1 + sa.kl + 1) & ~1) - ((kv + 1) & ~1);
@@ -601,6 +613,7 @@ void factorize(coral_handle* h, double dt) {
     fa.Tc = k.Tc;
     fa.cls_row = k.cls_row;
     fa.col_pos = k.col_pos;
+    fa.tpb = k.work2 != nullptr;
     fa.nact = h->nact;
     fa.M = k.M;
     fa.L = k.L;

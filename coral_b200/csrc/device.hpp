@@ -124,6 +124,12 @@ struct SolveArgs {
   const int* col_pos;    // [T] class position of a variable column (null: unsplit)
   const unsigned char* colflip_cls;  // [ncls*Tc] colflip in class order
   DevEll Lp;             // L with its columns in class positions (= L when unsplit)
+  // thread-per-block solve (class split): block b = 2 act + class, lane b % 32 of
+  // group b / 32; factors abr[((g Tc + j) ldab + r) 32 + lane], pivots
+  // dpiv[(g Tc + j) 32 + lane], right-hand sides / solutions of the active
+  // systems work2[(g Tc + j) 32 + lane]; inactive systems stay in work
+  double2* work2;        // null: warp-per-system layouts
+  int nblk;              // ncls * nact
 };
 void launch_solve(const SolveArgs& a, cudaStream_t s);
 // real-scaled factors (unsplit: kl <= 31, kl+ku <= 63; class split: kl <= 15,
@@ -149,6 +155,7 @@ struct FactorArgs {
   int ncls, Tc;
   const int* cls_row;    // [ncls*Tc] equation row of a class position, -1 = identity padding
   const int* col_pos;    // [T] class position of a variable column
+  int tpb;               // 1: interleaved thread-per-block factor layout (see SolveArgs::work2)
 };
 void launch_factor(const FactorArgs& a, cudaStream_t s);
 void launch_factor_real(const FactorArgs& a, cudaStream_t s);

@@ -33,12 +33,13 @@ __device__ __forceinline__ double2 mul_mi(double2 a) {
 // sin(pi/3), from the mathematics
 #define CORAL_SIN60 0.86602540378443864676372317075293618
 
-// In-place-by-pingpong batched FFT of nl lines of length p.N stored in A (line
-// stride p.N).  B is scratch of the same size.  Returns the buffer that holds
-// the result.  INV = false: exp(-i), INV = true: exp(+i); no normalisation.
+// Ping-pong batched FFT of nl lines of length p.N stored in A (line stride LS)
+// with a plan chosen at run time (lengths without a compile-time plan).  B is
+// scratch of the same size.  Returns the buffer that holds the result.
+// INV = false: exp(-i), INV = true: exp(+i); no normalisation.
 // Must be called by all threads of the CTA (contains __syncthreads).
 template <bool INV>
-__device__ double2* fft_lines(double2* A, double2* B, int nl, const FftPlan& p) {
+__device__ double2* fft_lines(double2* A, double2* B, int nl, int LS, const FftPlan& p) {
   double2* src = A;
   double2* dst = B;
   const int N = p.N;
@@ -52,8 +53,8 @@ __device__ double2* fft_lines(double2* A, double2* B, int nl, const FftPlan& p) 
       const int line = idx / nb;
       const int j = idx - line * nb;
       const int k = j % Ns;
-      const double2* sl = src + line * N;
-      double2* dl = dst + line * N;
+      const double2* sl = src + line * LS;
+      double2* dl = dst + line * LS;
       const int od = (j / Ns) * Ns * R + k;
       if (R == 4) {
         double2 a0 = sl[j], a1 = sl[j + nb], a2 = sl[j + 2 * nb], a3 = sl[j + 3 * nb];
@@ -102,95 +103,210 @@ __device__ double2* fft_lines(double2* A, double2* B, int nl, const FftPlan& p) 
   return src;
 }
 
-// ---- compile-time plans --------------------------------------------------------
-// The same Stockham scheme with the transform length known at compile time:
-// radices, strides and all index arithmetic fold into constants.
-struct PlanC {
+// ---- compile-time plans: register passes ----------------------------------------
+// With the length N known at compile time the transform runs as a few passes of
+// radix 16, 9, 8, 4, 3 or 2 (odd radices first: their strided stores in the
+// first pass hit distinct shared-memory banks).  Each thread computes whole
+// radix-R butterflies in registers: it loads its R inputs, applies the twiddles,
+// waits for every thread to have loaded (so the pass can write in place), and
+// stores its R outputs at their Stockham (self-sorting) positions.  Only one
+// line buffer is needed.
+struct PlanR {
   int nst;
-  int r[16];
+  int r[12];
 };
-__host__ __device__ constexpr PlanC make_planc(int N) {
-  PlanC p{0, {}};
-  int n = N;
-  while (n % 4 == 0) { p.r[p.nst++] = 4; n /= 4; }
-  while (n % 3 == 0) { p.r[p.nst++] = 3; n /= 3; }
-  while (n % 2 == 0) { p.r[p.nst++] = 2; n /= 2; }
+__host__ __device__ constexpr PlanR make_planr(int N) {
+  PlanR p{0, {}};
+  int n = N, a = 0, b = 0;
+  while (n % 3 == 0) { n /= 3; ++b; }
+  while (n % 2 == 0) { n /= 2; ++a; }
+  if (n != 1) return PlanR{0, {}};
+  for (; b >= 2; b -= 2) p.r[p.nst++] = 9;
+  if (b == 1) p.r[p.nst++] = 3;
+  while (a > 0) {
+    if (a == 6) { p.r[p.nst++] = 8; p.r[p.nst++] = 8; a = 0; }
+    else if (a == 5) { p.r[p.nst++] = 8; p.r[p.nst++] = 4; a = 0; }
+    else if (a >= 4) { p.r[p.nst++] = 16; a -= 4; }
+    else if (a == 3) { p.r[p.nst++] = 8; a = 0; }
+    else if (a == 2) { p.r[p.nst++] = 4; a = 0; }
+    else { p.r[p.nst++] = 2; a = 0; }
+  }
   return p;
 }
 
-template <int N, int R, int Ns, bool INV>
-__device__ __forceinline__ void fft_stage_t(const double2* __restrict__ src, double2* __restrict__ dst, int nl,
-                                            const double2* __restrict__ tw) {
-  constexpr int nb = N / R;
-  constexpr int tstride = N / (Ns * R);
-  const int total = nl * nb;
-  for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-    const int line = idx / nb;
-    const int j = idx - line * nb;
-    const int k = j % Ns;
-    const double2* sl = src + line * N;
-    double2* dl = dst + line * N;
-    const int od = (j / Ns) * Ns * R + k;
-    if constexpr (R == 4) {
-      double2 a0 = sl[j], a1 = sl[j + nb], a2 = sl[j + 2 * nb], a3 = sl[j + 3 * nb];
+// cos / sin of 2 pi m / 16 and 2 pi m / 9, from the mathematics (40-digit values)
+#define CORAL_C16_1 0.923879532511286756128183189396788287   // cos(pi/8)
+#define CORAL_S16_1 0.382683432365089771728459984030398867   // sin(pi/8)
+#define CORAL_SQRT1_2 0.707106781186547524400844362104849039 // cos(pi/4)
+#define CORAL_C9_1 0.766044443118978035202392650555416674    // cos(2 pi/9)
+#define CORAL_S9_1 0.642787609686539326322643409907263433    // sin(2 pi/9)
+#define CORAL_C9_2 0.173648177666930348851716626769314796    // cos(4 pi/9)
+#define CORAL_S9_2 0.984807753012208059366743024589523014    // sin(4 pi/9)
+#define CORAL_C9_4 (-0.93969262078590838405410927732473147)  // cos(8 pi/9)
+#define CORAL_S9_4 0.342020143325668733044099614682259581    // sin(8 pi/9)
+
+// a * exp(-i t) (forward) or a * exp(+i t) (inverse), given c = cos t, s = sin t
+template <bool INV>
+__device__ __forceinline__ double2 rot(double2 a, double c, double s) {
+  return INV ? make_double2(a.x * c - a.y * s, a.x * s + a.y * c) : make_double2(a.x * c + a.y * s, a.y * c - a.x * s);
+}
+
+template <bool INV>
+__device__ __forceinline__ void dft3(double2& a0, double2& a1, double2& a2) {
+  const double2 t = cadd(a1, a2), d = csub(a1, a2);
+  const double2 m = make_double2(a0.x - 0.5 * t.x, a0.y - 0.5 * t.y);
+  const double sd = INV ? -CORAL_SIN60 : CORAL_SIN60;
+  const double2 isd = make_double2(-sd * d.y, sd * d.x);  // i s d
+  a0 = cadd(a0, t);
+  a1 = csub(m, isd);
+  a2 = cadd(m, isd);
+}
+template <bool INV>
+__device__ __forceinline__ void dft4(double2& a0, double2& a1, double2& a2, double2& a3) {
+  const double2 t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = mul_mi<INV>(csub(a1, a3));
+  a0 = cadd(t0, t2);
+  a1 = cadd(t1, t3);
+  a2 = csub(t0, t2);
+  a3 = csub(t1, t3);
+}
+
+// in-register DFT of length R, natural order in and out
+template <int R, bool INV>
+__device__ __forceinline__ void dft(double2 (&x)[R]) {
+  if constexpr (R == 2) {
+    const double2 t = x[0];
+    x[0] = cadd(t, x[1]);
+    x[1] = csub(t, x[1]);
+  } else if constexpr (R == 3) {
+    dft3<INV>(x[0], x[1], x[2]);
+  } else if constexpr (R == 4) {
+    dft4<INV>(x[0], x[1], x[2], x[3]);
+  } else if constexpr (R == 8) {
+    // n = 2 n1 + n2, k = k1 + 4 k2
+    dft4<INV>(x[0], x[2], x[4], x[6]);
+    dft4<INV>(x[1], x[3], x[5], x[7]);
+    x[3] = rot<INV>(x[3], CORAL_SQRT1_2, CORAL_SQRT1_2);
+    x[5] = mul_mi<INV>(x[5]);
+    x[7] = rot<INV>(x[7], -CORAL_SQRT1_2, CORAL_SQRT1_2);
+    double2 y[8];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      y[k1] = cadd(x[2 * k1], x[2 * k1 + 1]);
+      y[k1 + 4] = csub(x[2 * k1], x[2 * k1 + 1]);
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = y[k];
+  } else if constexpr (R == 9) {
+    // n = 3 n1 + n2, k = k1 + 3 k2
+    dft3<INV>(x[0], x[3], x[6]);
+    dft3<INV>(x[1], x[4], x[7]);
+    dft3<INV>(x[2], x[5], x[8]);
+    // A_{n2}[k1] sits in x[n2 + 3 k1]; twiddle by w9^(n2 k1)
+    x[4] = rot<INV>(x[4], CORAL_C9_1, CORAL_S9_1);
+    x[7] = rot<INV>(x[7], CORAL_C9_2, CORAL_S9_2);
+    x[5] = rot<INV>(x[5], CORAL_C9_2, CORAL_S9_2);
+    x[8] = rot<INV>(x[8], CORAL_C9_4, CORAL_S9_4);
+    dft3<INV>(x[0], x[1], x[2]);  // k1 = 0 -> X[0], X[3], X[6]
+    dft3<INV>(x[3], x[4], x[5]);  // k1 = 1 -> X[1], X[4], X[7]
+    dft3<INV>(x[6], x[7], x[8]);  // k1 = 2 -> X[2], X[5], X[8]
+    double2 y[9];
+#pragma unroll
+    for (int k1 = 0; k1 < 3; ++k1)
+#pragma unroll
+      for (int k2 = 0; k2 < 3; ++k2) y[k1 + 3 * k2] = x[3 * k1 + k2];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) x[k] = y[k];
+  } else if constexpr (R == 16) {
+    // n = 4 n1 + n2, k = k1 + 4 k2
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) dft4<INV>(x[n2], x[n2 + 4], x[n2 + 8], x[n2 + 12]);
+    // A_{n2}[k1] sits in x[n2 + 4 k1]; twiddle by w16^(n2 k1)
+    x[5] = rot<INV>(x[5], CORAL_C16_1, CORAL_S16_1);      // 1
+    x[9] = rot<INV>(x[9], CORAL_SQRT1_2, CORAL_SQRT1_2);  // 2
+    x[13] = rot<INV>(x[13], CORAL_S16_1, CORAL_C16_1);    // 3
+    x[6] = rot<INV>(x[6], CORAL_SQRT1_2, CORAL_SQRT1_2);  // 2
+    x[10] = mul_mi<INV>(x[10]);                            // 4
+    x[14] = rot<INV>(x[14], -CORAL_SQRT1_2, CORAL_SQRT1_2);  // 6
+    x[7] = rot<INV>(x[7], CORAL_S16_1, CORAL_C16_1);      // 3
+    x[11] = rot<INV>(x[11], -CORAL_SQRT1_2, CORAL_SQRT1_2);  // 6
+    x[15] = rot<INV>(x[15], -CORAL_C16_1, -CORAL_S16_1);  // 9
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) dft4<INV>(x[4 * k1], x[4 * k1 + 1], x[4 * k1 + 2], x[4 * k1 + 3]);
+    double2 y[16];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+      for (int k2 = 0; k2 < 4; ++k2) y[k1 + 4 * k2] = x[4 * k1 + k2];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) x[k] = y[k];
+  }
+}
+
+// One in-place pass of radix R over nl lines (line stride LS) by NT threads;
+// NLMAX bounds nl (registers hold ceil(NLMAX N / (R NT)) butterflies per thread).
+template <int N, int R, int Ns, bool INV, int NT, int NLMAX>
+__device__ __forceinline__ void fft_pass(double2* A, int nl, int LS, const double2* __restrict__ tw) {
+  constexpr int NB = N / R;               // butterflies per line
+  constexpr int TS = N / (Ns * R);        // twiddle stride
+  constexpr int BPT = (NLMAX * NB + NT - 1) / NT;
+  const int total = nl * NB;
+  double2 v[BPT][R];
+#pragma unroll
+  for (int i = 0; i < BPT; ++i) {
+    const int b = threadIdx.x + i * NT;
+    if (b < total) {
+      const int line = b / NB, j = b - line * NB;
+      const double2* sl = A + line * LS + j;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[i][r] = sl[r * NB];
       if constexpr (Ns > 1) {
-        double2 w1 = tw[k * tstride], w2 = tw[2 * k * tstride], w3 = tw[3 * k * tstride];
-        if (INV) { w1 = cconj(w1); w2 = cconj(w2); w3 = cconj(w3); }
-        a1 = cmul(a1, w1); a2 = cmul(a2, w2); a3 = cmul(a3, w3);
+        const int k = j % Ns;
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          double2 w = tw[r * k * TS];
+          if (INV) w = cconj(w);
+          v[i][r] = cmul(v[i][r], w);
+        }
       }
-      double2 t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = mul_mi<INV>(csub(a1, a3));
-      dl[od] = cadd(t0, t2);
-      dl[od + Ns] = cadd(t1, t3);
-      dl[od + 2 * Ns] = csub(t0, t2);
-      dl[od + 3 * Ns] = csub(t1, t3);
-    } else if constexpr (R == 3) {
-      double2 a0 = sl[j], a1 = sl[j + nb], a2 = sl[j + 2 * nb];
-      if constexpr (Ns > 1) {
-        double2 w1 = tw[k * tstride], w2 = tw[2 * k * tstride];
-        if (INV) { w1 = cconj(w1); w2 = cconj(w2); }
-        a1 = cmul(a1, w1); a2 = cmul(a2, w2);
-      }
-      double2 t = cadd(a1, a2), d = csub(a1, a2);
-      double2 m = make_double2(a0.x - 0.5 * t.x, a0.y - 0.5 * t.y);
-      const double sd = INV ? -CORAL_SIN60 : CORAL_SIN60;
-      double2 isd = make_double2(-sd * d.y, sd * d.x);
-      dl[od] = cadd(a0, t);
-      dl[od + Ns] = csub(m, isd);
-      dl[od + 2 * Ns] = cadd(m, isd);
-    } else {
-      double2 a0 = sl[j], a1 = sl[j + nb];
-      if constexpr (Ns > 1) {
-        double2 w1 = tw[k * tstride];
-        if (INV) w1 = cconj(w1);
-        a1 = cmul(a1, w1);
-      }
-      dl[od] = cadd(a0, a1);
-      dl[od + Ns] = csub(a0, a1);
+      dft<R, INV>(v[i]);
     }
   }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < BPT; ++i) {
+    const int b = threadIdx.x + i * NT;
+    if (b < total) {
+      const int line = b / NB, j = b - line * NB;
+      double2* dl = A + line * LS + (j / Ns) * Ns * R + (j % Ns);
+#pragma unroll
+      for (int r = 0; r < R; ++r) dl[r * Ns] = v[i][r];
+    }
+  }
+  __syncthreads();
 }
 
-template <int N, int S, int Ns, bool INV>
-__device__ __forceinline__ double2* fft_stages_t(double2* src, double2* dst, int nl, const double2* tw) {
-  constexpr PlanC P = make_planc(N);
-  if constexpr (S >= P.nst) {
-    return src;
-  } else {
+template <int N, int S, int Ns, bool INV, int NT, int NLMAX>
+__device__ __forceinline__ void fft_passes(double2* A, int nl, int LS, const double2* tw) {
+  constexpr PlanR P = make_planr(N);
+  if constexpr (S < P.nst) {
     constexpr int R = P.r[S];
-    fft_stage_t<N, R, Ns, INV>(src, dst, nl, tw);
-    __syncthreads();
-    return fft_stages_t<N, S + 1, Ns * R, INV>(dst, src, nl, tw);
+    fft_pass<N, R, Ns, INV, NT, NLMAX>(A, nl, LS, tw);
+    fft_passes<N, S + 1, Ns * R, INV, NT, NLMAX>(A, nl, LS, tw);
   }
 }
 
-// Batched FFT with a compile-time length NC, or the runtime plan when NC == 0.
-template <int NC, bool INV>
-__device__ __forceinline__ double2* fft_lines_n(double2* A, double2* B, int nl, const FftPlan& p) {
+// Batched FFT of nl <= NLMAX lines (line stride LS) by NT threads: compile-time
+// length NC in place in A (B unused), or the runtime plan (NC == 0) ping-ponging
+// through B.  Returns the buffer holding the result.  The caller synchronises
+// before (inputs written) and may read the result directly after.
+template <int NC, bool INV, int NT, int NLMAX>
+__device__ __forceinline__ double2* fft_lines_n(double2* A, double2* B, int nl, int LS, const FftPlan& p) {
   if constexpr (NC == 0) {
-    return fft_lines<INV>(A, B, nl, p);
+    return fft_lines<INV>(A, B, nl, LS, p);
   } else {
-    static_assert(make_planc(NC).nst > 0, "transform length must be 2^a 3^b");
-    return fft_stages_t<NC, 0, 1, INV>(A, B, nl, p.tw);
+    static_assert(make_planr(NC).nst > 0, "transform length must be 2^a 3^b");
+    fft_passes<NC, 0, 1, INV, NT, NLMAX>(A, nl, LS, p.tw);
+    return A;
   }
 }
 

@@ -11,6 +11,7 @@
 // The x<->y exchange of the reference's slab decomposition
 // (src/slabs.fftw3mpi/domain_decomposition.f90:152-183) is the change of
 // layout between the y pass and the x pass, done in shared memory.
+#include <algorithm>
 #include <cstdio>
 
 #include "device.hpp"
@@ -21,8 +22,17 @@ namespace {
 
 constexpr int kNB1 = 4;  // n lines per CTA, inverse / forward y pass
 constexpr int kNB2 = 8;  // n lines per CTA, x passes (packed in pairs)
-constexpr int kXB3 = 8;  // x columns per CTA, inverse z pass (packed in pairs)
+constexpr int kXB3 = 16; // x columns per CTA, inverse z pass (packed in pairs)
+constexpr int kQC = 5;   // quadratic variables per FFT batch, forward z pass (one radix-9 / radix-8
+                         // butterfly per thread at NZAA = 288)
+constexpr int kPadXY = 2;  // line stride N + 2 in the x / y passes, whose loads and stores
+                           // walk 4 interleaved lines: 2 line + position hits 8 distinct
+                           // 16-byte bank groups
 constexpr int kThreads = 256;
+// CTAs per SM the transform kernels are compiled for (caps their registers;
+// measured best at 384^2 x 192: 3 for the x / y passes, 4 for the z passes)
+constexpr int kMinBlocksXY = 3;
+constexpr int kMinBlocksZ = 4;
 constexpr int kWPB = 8;  // warps (systems) per CTA in the per-system kernels
 
 __device__ __forceinline__ double2 zero2() { return make_double2(0.0, 0.0); }
@@ -41,14 +51,14 @@ __device__ __forceinline__ double2 ipow(double k, int e) {
 //  c2r_transform steps 1-2 and the 0.5 of the x padding, transforms.f90:172-198)
 // ------------------------------------------------------------------------------
 template <int NF>
-__global__ void __launch_bounds__(kThreads) k_inv_y(Dims d, const FullVarDev* fv, StateSet st,
+__global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_inv_y(Dims d, const FullVarDev* fv, StateSet st,
                                                      const double2* plain_spec, const double* kxv,
                                                      const double* kyv, double2* Y1, FftPlan py) {
   extern __shared__ double2 sm[];
   const int f = blockIdx.x, n0 = blockIdx.y * kNB1, kx = blockIdx.z;
-  const int NYA = NF ? NF : d.NYA;
+  const int NYA = NF ? NF : d.NYA, LS = NYA + kPadXY;
   double2* A = sm;
-  double2* B = sm + kNB1 * NYA;
+  double2* B = sm + kNB1 * LS;  // runtime plan only
   for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
     const int ln = idx % kNB1, iy = idx / kNB1, n = n0 + ln;
     double2 c = zero2();
@@ -88,15 +98,15 @@ __global__ void __launch_bounds__(kThreads) k_inv_y(Dims d, const FullVarDev* fv
         }
       }
     }
-    A[ln * NYA + iy] = c;
+    A[ln * LS + iy] = c;
   }
   __syncthreads();
-  const double2* R = fft_lines_n<NF, true>(A, B, kNB1, py);
+  const double2* R = fft_lines_n<NF, true, kThreads, kNB1>(A, B, kNB1, LS, py);
   for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
     const int ln = idx % kNB1, y = idx / kNB1, n = n0 + ln;
     if (n < d.NZ) {
       const double s = (n == 0) ? 1.0 : 0.5;  // (x2 on Chebyshev index 0) * (0.5 of the x padding)
-      Y1[(((size_t)f * NYA + y) * d.NXH + kx) * d.NZ + n] = cscale(R[ln * NYA + y], s);
+      Y1[(((size_t)f * NYA + y) * d.NXH + kx) * d.NZ + n] = cscale(R[ln * LS + y], s);
     }
   }
 }
@@ -106,13 +116,13 @@ __global__ void __launch_bounds__(kThreads) k_inv_y(Dims d, const FullVarDev* fv
 // two real output lines per complex FFT
 // ------------------------------------------------------------------------------
 template <int NF>
-__global__ void __launch_bounds__(kThreads) k_inv_x(Dims d, const double2* Y1, double* Y2, FftPlan px) {
+__global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_inv_x(Dims d, const double2* Y1, double* Y2, FftPlan px) {
   extern __shared__ double2 sm[];
   const int f = blockIdx.x, n0 = blockIdx.y * kNB2, y = blockIdx.z;
-  const int NXA = NF ? NF : d.NXA, NP = kNB2 / 2;
+  const int NXA = NF ? NF : d.NXA, NP = kNB2 / 2, LS = NXA + kPadXY;
   double2* A = sm;
-  double2* B = sm + NP * NXA;
-  for (int idx = threadIdx.x; idx < NP * NXA; idx += blockDim.x) A[idx] = zero2();
+  double2* B = sm + NP * LS;  // runtime plan only
+  for (int idx = threadIdx.x; idx < NP * LS; idx += blockDim.x) A[idx] = zero2();
   __syncthreads();
   for (int idx = threadIdx.x; idx < NP * d.NXH; idx += blockDim.x) {
     const int m = idx % NP, kx = idx / NP, na = n0 + 2 * m;
@@ -120,17 +130,17 @@ __global__ void __launch_bounds__(kThreads) k_inv_x(Dims d, const double2* Y1, d
     double2 a = (na < d.NZ) ? src[na] : zero2();
     double2 b = (na + 1 < d.NZ) ? src[na + 1] : zero2();
     if (kx == 0) {
-      A[m * NXA] = make_double2(a.x, b.x);  // c2r reads only the real part of the DC term
+      A[m * LS] = make_double2(a.x, b.x);  // c2r reads only the real part of the DC term
     } else {
-      A[m * NXA + kx] = make_double2(a.x - b.y, a.y + b.x);        // a + i b
-      A[m * NXA + NXA - kx] = make_double2(a.x + b.y, b.x - a.y);  // conj(a) + i conj(b)
+      A[m * LS + kx] = make_double2(a.x - b.y, a.y + b.x);        // a + i b
+      A[m * LS + NXA - kx] = make_double2(a.x + b.y, b.x - a.y);  // conj(a) + i conj(b)
     }
   }
   __syncthreads();
-  const double2* R = fft_lines_n<NF, true>(A, B, NP, px);
+  const double2* R = fft_lines_n<NF, true, kThreads, kNB2 / 2>(A, B, NP, LS, px);
   for (int idx = threadIdx.x; idx < NP * NXA; idx += blockDim.x) {
     const int m = idx % NP, x = idx / NP, na = n0 + 2 * m;
-    double2 z = R[m * NXA + x];
+    double2 z = R[m * LS + x];
     double* dst = Y2 + (((size_t)f * d.NYA + y) * NXA + x) * d.NZ;
     if (na < d.NZ) dst[na] = z.x;
     if (na + 1 < d.NZ) dst[na + 1] = z.y;
@@ -147,7 +157,7 @@ __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, doub
 // compute_cfl_based_timestep (marching.f90:219-238) for the first three full variables
 // ------------------------------------------------------------------------------
 template <int NF>
-__global__ void __launch_bounds__(kThreads) k_inv_z(Dims d, const double* Y2, double* phys, FftPlan pz,
+__global__ void __launch_bounds__(kThreads, kMinBlocksZ) k_inv_z(Dims d, const double* Y2, double* phys, FftPlan pz,
                                                      const double2* dct_tw, const double* wz,
                                                      unsigned long long* cfl_bits) {
   extern __shared__ double2 sm[];
@@ -176,7 +186,7 @@ __global__ void __launch_bounds__(kThreads) k_inv_z(Dims d, const double* Y2, do
     A[m * N + n] = make_double2(va.x - vb.y, va.y + vb.x);  // va + i vb
   }
   __syncthreads();
-  const double2* R = fft_lines_n<NF, true>(A, B, NP, pz);
+  const double2* R = fft_lines_n<NF, true, kThreads, kXB3 / 2>(A, B, NP, N, pz);
   double mx = 0.0;
   const int which = (f < 3) ? f : -1;
   for (int idx = threadIdx.x; idx < NP * N; idx += blockDim.x) {
@@ -211,55 +221,61 @@ __global__ void __launch_bounds__(kThreads) k_inv_z(Dims d, const double* Y2, do
 // pair of x columns; also partial volume averages for KE (output.f90:84-102)
 // ------------------------------------------------------------------------------
 template <int NF>
-__global__ void __launch_bounds__(kThreads) k_fwd_z(Dims d, int nf, QuadDesc q, const double* phys, double* Q2,
+__global__ void __launch_bounds__(kThreads, kMinBlocksZ) k_fwd_z(Dims d, int nf, QuadDesc q, const double* phys, double* Q2,
                                                      FftPlan pz, const double2* dct_tw, const double* wz,
                                                      double* ke_partial) {
   extern __shared__ double2 sm[];
   __shared__ double red[3][kThreads / 32];
   const int x0 = blockIdx.x * 2, y = blockIdx.y;
-  const int N = NF ? NF : d.NZA, nq = q.nq;
-  double* P = reinterpret_cast<double*>(sm);  // [nf][2][N]
-  double2* A = sm + nf * N;                    // nq lines
-  double2* B = A + nq * N;
+  const int N = NF ? NF : d.NZA, nq = q.nq, nb = min(nq, kQC);
+  double* P = reinterpret_cast<double*>(sm);  // [nf][2][N], z in Makhoul order
+  double2* A = sm + nf * N;                    // nb lines
+  double2* B = A + nb * N;                     // runtime plan only
   for (int idx = threadIdx.x; idx < nf * 2 * N; idx += blockDim.x) {
     const int fv = idx / (2 * N), r = idx - fv * 2 * N;
-    const int xc = x0 + r / N, z = r % N;
-    P[idx] = (xc < d.NXA) ? phys[(((size_t)fv * d.NYA + y) * d.NXA + xc) * N + z] : 0.0;
+    const int c = r / N, z = r - c * N;
+    const int m = (z & 1) ? (N - 1 - (z >> 1)) : (z >> 1);  // Makhoul position of z
+    const int xc = x0 + c;
+    P[idx - z + m] = (xc < d.NXA) ? phys[(((size_t)fv * d.NYA + y) * d.NXA + xc) * N + z] : 0.0;
   }
   __syncthreads();
   double ke[3] = {0.0, 0.0, 0.0};
-  for (int idx = threadIdx.x; idx < nq * N; idx += blockDim.x) {
-    const int qi = idx / N, m = idx - qi * N;
-    const int z = (m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1;  // Makhoul reordering
-    const int v1 = q.v1[qi], v2 = q.v2[qi];
-    double pa, pb;
-    if (v1 < 0) { pa = P[(v2 * 2) * N + z]; pb = P[(v2 * 2 + 1) * N + z]; }
-    else if (v2 < 0) { pa = P[(v1 * 2) * N + z]; pb = P[(v1 * 2 + 1) * N + z]; }
-    else {
-      pa = P[(v1 * 2) * N + z] * P[(v2 * 2) * N + z];
-      pb = P[(v1 * 2 + 1) * N + z] * P[(v2 * 2 + 1) * N + z];
+  for (int q0 = 0; q0 < nq; q0 += kQC) {  // batches of kQC quadratic variables
+    const int nc = min(kQC, nq - q0);
+    for (int idx = threadIdx.x; idx < nc * N; idx += blockDim.x) {
+      const int qi = idx / N, m = idx - qi * N, qg = q0 + qi;
+      const int z = (m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1;  // Makhoul reordering
+      const int v1 = q.v1[qg], v2 = q.v2[qg];
+      double pa, pb;
+      if (v1 < 0) { pa = P[(v2 * 2) * N + m]; pb = P[(v2 * 2 + 1) * N + m]; }
+      else if (v2 < 0) { pa = P[(v1 * 2) * N + m]; pb = P[(v1 * 2 + 1) * N + m]; }
+      else {
+        pa = P[(v1 * 2) * N + m] * P[(v2 * 2) * N + m];
+        pb = P[(v1 * 2 + 1) * N + m] * P[(v2 * 2 + 1) * N + m];
+      }
+      A[qi * N + m] = make_double2(pa, pb);
+      if (ke_partial) {
+        for (int j = 0; j < 3; ++j)
+          if (q.ke_q[j] == qg) ke[j] += wz[z] * (pa + ((x0 + 1 < d.NXA) ? pb : 0.0));
+      }
     }
-    A[qi * N + m] = make_double2(pa, pb);
-    if (ke_partial) {
-      for (int j = 0; j < 3; ++j)
-        if (q.ke_q[j] == qi) ke[j] += wz[z] * (pa + ((x0 + 1 < d.NXA) ? pb : 0.0));
+    __syncthreads();
+    const double2* R = fft_lines_n<NF, false, kThreads, kQC>(A, B, nc, N, pz);
+    for (int idx = threadIdx.x; idx < nc * d.NZ; idx += blockDim.x) {
+      const int qi = idx / d.NZ, n = idx - qi * d.NZ;
+      const double2 Z = R[qi * N + n];
+      const double2 Zc = cconj(R[qi * N + ((N - n) % N)]);
+      const double2 va = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
+      const double2 dd = csub(Z, Zc);
+      const double2 vb = make_double2(0.5 * dd.y, -0.5 * dd.x);  // (Z - Zc) / 2i
+      const double2 w = dct_tw[n];                                // exp(-i pi n / 2N)
+      const double xa = 2.0 * (w.x * va.x - w.y * va.y);
+      const double xb = 2.0 * (w.x * vb.x - w.y * vb.y);
+      double* dst = Q2 + (((size_t)(q0 + qi) * d.NYA + y) * d.NXA + x0) * d.NZ;
+      dst[n] = xa;
+      if (x0 + 1 < d.NXA) dst[d.NZ + n] = xb;
     }
-  }
-  __syncthreads();
-  const double2* R = fft_lines_n<NF, false>(A, B, nq, pz);
-  for (int idx = threadIdx.x; idx < nq * d.NZ; idx += blockDim.x) {
-    const int qi = idx / d.NZ, n = idx - qi * d.NZ;
-    const double2 Z = R[qi * N + n];
-    const double2 Zc = cconj(R[qi * N + ((N - n) % N)]);
-    const double2 va = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
-    const double2 dd = csub(Z, Zc);
-    const double2 vb = make_double2(0.5 * dd.y, -0.5 * dd.x);  // (Z - Zc) / 2i
-    const double2 w = dct_tw[n];                                // exp(-i pi n / 2N)
-    const double xa = 2.0 * (w.x * va.x - w.y * va.y);
-    const double xb = 2.0 * (w.x * vb.x - w.y * vb.y);
-    double* dst = Q2 + (((size_t)qi * d.NYA + y) * d.NXA + x0) * d.NZ;
-    dst[n] = xa;
-    if (x0 + 1 < d.NXA) dst[d.NZ + n] = xb;
+    __syncthreads();  // A is refilled by the next batch
   }
   if (ke_partial) {
     for (int j = 0; j < 3; ++j) {
@@ -280,23 +296,23 @@ __global__ void __launch_bounds__(kThreads) k_fwd_z(Dims d, int nf, QuadDesc q, 
 // forward transform, pass 2: x r2c, keep kx < NX/2 (transforms.f90:255-267)
 // ------------------------------------------------------------------------------
 template <int NF>
-__global__ void __launch_bounds__(kThreads) k_fwd_x(Dims d, const double* Q2, double2* Q1, FftPlan px) {
+__global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_fwd_x(Dims d, const double* Q2, double2* Q1, FftPlan px) {
   extern __shared__ double2 sm[];
   const int qi = blockIdx.x, n0 = blockIdx.y * kNB2, y = blockIdx.z;
-  const int NXA = NF ? NF : d.NXA, NP = kNB2 / 2;
+  const int NXA = NF ? NF : d.NXA, NP = kNB2 / 2, LS = NXA + kPadXY;
   double2* A = sm;
-  double2* B = sm + NP * NXA;
+  double2* B = sm + NP * LS;  // runtime plan only
   for (int idx = threadIdx.x; idx < NP * NXA; idx += blockDim.x) {
     const int m = idx % NP, x = idx / NP, na = n0 + 2 * m;
     const double* src = Q2 + (((size_t)qi * d.NYA + y) * NXA + x) * d.NZ;
-    A[m * NXA + x] = make_double2(na < d.NZ ? src[na] : 0.0, na + 1 < d.NZ ? src[na + 1] : 0.0);
+    A[m * LS + x] = make_double2(na < d.NZ ? src[na] : 0.0, na + 1 < d.NZ ? src[na + 1] : 0.0);
   }
   __syncthreads();
-  const double2* R = fft_lines_n<NF, false>(A, B, NP, px);
+  const double2* R = fft_lines_n<NF, false, kThreads, kNB2 / 2>(A, B, NP, LS, px);
   for (int idx = threadIdx.x; idx < NP * d.NXH; idx += blockDim.x) {
     const int m = idx % NP, kx = idx / NP, na = n0 + 2 * m;
-    const double2 Z = R[m * NXA + kx];
-    const double2 Zc = cconj(R[m * NXA + ((NXA - kx) % NXA)]);
+    const double2 Z = R[m * LS + kx];
+    const double2 Zc = cconj(R[m * LS + ((NXA - kx) % NXA)]);
     const double2 a = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
     const double2 dd = csub(Z, Zc);
     const double2 b = make_double2(0.5 * dd.y, -0.5 * dd.x);
@@ -311,13 +327,13 @@ __global__ void __launch_bounds__(kThreads) k_fwd_x(Dims d, const double* Q2, do
 // 1/(NXAA NYAA NZAA) normalisation (transforms.f90:280-296)
 // ------------------------------------------------------------------------------
 template <int NF>
-__global__ void __launch_bounds__(kThreads) k_fwd_y(Dims d, const double2* Q1, double2* qspec, double scale,
+__global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_fwd_y(Dims d, const double2* Q1, double2* qspec, double scale,
                                                      FftPlan py) {
   extern __shared__ double2 sm[];
   const int qi = blockIdx.x, n0 = blockIdx.y * kNB1, kx = blockIdx.z;
-  const int NYA = NF ? NF : d.NYA;
+  const int NYA = NF ? NF : d.NYA, LS = NYA + kPadXY;
   double2* A = sm;
-  double2* B = sm + kNB1 * NYA;
+  double2* B = sm + kNB1 * LS;  // runtime plan only
   for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
     const int ln = idx % kNB1, y = idx / kNB1, n = n0 + ln;
     double2 v = zero2();
@@ -325,13 +341,13 @@ __global__ void __launch_bounds__(kThreads) k_fwd_y(Dims d, const double2* Q1, d
       v = Q1[(((size_t)qi * NYA + y) * d.NXH + kx) * d.NZ + n];
       if (n == 0) v = cscale(v, 0.5);
     }
-    A[ln * NYA + y] = v;
+    A[ln * LS + y] = v;
   }
   __syncthreads();
-  const double2* R = fft_lines_n<NF, false>(A, B, kNB1, py);
+  const double2* R = fft_lines_n<NF, false, kThreads, kNB1>(A, B, kNB1, LS, py);
   for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
     const int ln = idx % kNB1, ky = idx / kNB1, n = n0 + ln;
-    if (n < d.NZ) qspec[(((size_t)qi * d.NXH + kx) * NYA + ky) * d.NZ + n] = cscale(R[ln * NYA + ky], scale);
+    if (n < d.NZ) qspec[(((size_t)qi * d.NXH + kx) * NYA + ky) * d.NZ + n] = cscale(R[ln * LS + ky], scale);
   }
 }
 
@@ -974,6 +990,171 @@ __global__ void __launch_bounds__(kWPBr * 32) k_subst_real(SolveArgs a) {
 
 
 // ------------------------------------------------------------------------------
+// Thread-per-block solve of the independent blocks (class split).  Block
+// b = ncls * act + class is handled by one thread; the 32 blocks of a group lie
+// side by side in memory (abr[((g Tc + j) ldab + r) 32 + lane]), so every factor
+// row, pivot byte and vector entry a warp touches in one step is one contiguous
+// 256 / 32 / 512-byte row.  A thread keeps its band window in its own
+// shared-memory column (slot stride kTpbThreads), where the data-dependent
+// row interchange is a plain indexed access.
+// ------------------------------------------------------------------------------
+constexpr int kTpbThreads = 128;
+
+// DGBTF2 on one block, in the interleaved layout: the algorithm, pivot choice
+// and update order of k_factor_real.
+__global__ void __launch_bounds__(kTpbThreads) k_factor_tpb(FactorArgs a) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.ncls * a.nact) return;
+  const int sys = b / a.ncls, cls = b - sys * a.ncls;
+  const int T = a.Tc, kl = a.kl, ku = a.ku, kv = kl + ku, ldab = a.ldab;
+  const int sid = a.act_list[sys];
+  const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
+  double2 cm[kMaxGroups], cl[kMaxGroups];
+#pragma unroll
+  for (int g = 0; g < kMaxGroups; ++g) {
+    cm[g] = (g < a.M.ngroups) ? cmul(ipow(a.kx[kx], a.M.gkx[g]), ipow(a.ky[ky], a.M.gky[g])) : zero2();
+    cl[g] = (g < a.L.ngroups) ? cmul(ipow(a.kx[kx], a.L.gkx[g]), ipow(a.ky[ky], a.L.gky[g])) : zero2();
+  }
+  double* F = a.abr + (size_t)(b >> 5) * T * ldab * 32 + (b & 31);
+  auto at = [&](int j, int r) -> double& { return F[((size_t)j * ldab + r) * 32]; };
+  for (int j = 0; j < T; ++j)
+    for (int r = 0; r < ldab; ++r) at(j, r) = 0.0;
+  for (int i = 0; i < T; ++i) {
+    const int t = a.cls_row[cls * T + i];  // equation row of class position i
+    if (t < 0) {
+      at(i, kv) = 1.0;  // identity padding
+      continue;
+    }
+    const int rf = a.rowflip[t];
+    for (int pass = 0; pass < 2; ++pass) {
+      const DevEll& op = pass ? a.L : a.M;
+      for (int k = 0; k < op.width; ++k) {
+        const double v = op.v(t, k);
+        if (v == 0.0) continue;  // empty slot
+        const int c = op.col(t, k), g = op.grp(t, k);
+        const int jc = a.col_pos[c] - cls * T;  // column in the class
+        double2 cv = zero2();
+#pragma unroll
+        for (int gg = 0; gg < kMaxGroups; ++gg)
+          if (g == gg) cv = pass ? cl[gg] : cm[gg];
+        double2 z = cscale(cv, v);
+        if (pass) z = cscale(z, a.zsca);
+        z = flip_col(flip_row(z, rf), a.colflip[c]);
+        at(jc, kv + i - jc) += z.x;
+      }
+    }
+  }
+  unsigned char* P = a.dpiv + (size_t)(b >> 5) * T * 32 + (b & 31);
+  int ju = 0, info = 0;
+  for (int j = 0; j < T; ++j) {
+    const int km = min(kl, T - 1 - j);
+    int jp = 0;
+    double mag = fabs(at(j, kv));
+    for (int i = 1; i <= km; ++i) {
+      const double m2 = fabs(at(j, kv + i));
+      if (m2 > mag) { mag = m2; jp = i; }  // first maximum
+    }
+    P[(size_t)j * 32] = (unsigned char)jp;
+    if (at(j, kv + jp) == 0.0) {
+      if (info == 0) info = j + 1;
+      continue;
+    }
+    ju = max(ju, min(j + ku + jp, T - 1));
+    if (jp != 0) {
+      for (int c = j; c <= ju; ++c) {
+        double& p1 = at(c, kv + j + jp - c);
+        double& p0 = at(c, kv + j - c);
+        const double t0 = p0;
+        p0 = p1;
+        p1 = t0;
+      }
+    }
+    const double r = 1.0 / at(j, kv);
+    if (km > 0) {
+      for (int i = 1; i <= km; ++i) at(j, kv + i) *= r;
+      for (int c = j + 1; c <= ju; ++c) {
+        const double u = at(c, kv + j - c);
+        for (int i = 1; i <= km; ++i) at(c, kv + j + i - c) -= at(j, kv + i) * u;
+      }
+    }
+    at(j, kv) = r;
+  }
+  if (info) atomicMax(a.info + sys, info);
+}
+
+// Forward (P, L: the column sweep with the row interchanges interleaved, as the
+// reference's band solve) then backward (U, row form: each x_j subtracts the
+// known x_{j+i} in decreasing column order, the order in which the column sweep
+// reaches it) for one block.  KL, KV bound kl and kl+ku (registers hold one L
+// column / one U row); the window holds positions j..j+kl (forward, W1 slots)
+// or j..j+kv (backward, KV+1 slots).
+template <int KL, int KV>
+__global__ void __launch_bounds__(kTpbThreads) k_subst_tpb(SolveArgs a) {
+  constexpr int W1 = (KL + 2 <= 16) ? 16 : 32;  // power of 2 >= KL + 2
+  constexpr int W2 = KV + 1;
+  constexpr int S = kTpbThreads;                // slot stride
+  extern __shared__ double2 swin[];
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.nblk) return;  // no warp-collective operations below
+  const int T = a.Tc, kl = a.kl, kv = a.kl + a.ku, ldab = a.ldab;
+  const int cls = b % a.ncls;
+  const size_t gb = (size_t)(b >> 5) * T;
+  const double* F = a.abr + gb * ldab * 32 + (b & 31);
+  const unsigned char* P = a.dpiv + gb * 32 + (b & 31);
+  double2* X = a.work2 + gb * 32 + (b & 31);
+  const unsigned char* cflip = a.colflip_cls + (size_t)cls * T;
+  double2* win = swin + threadIdx.x;
+  // ---- forward: positions j..j+kl in slots p mod W1 ----
+  for (int p = 0; p <= kl && p < T; ++p) win[(p & (W1 - 1)) * S] = X[(size_t)p * 32];
+  for (int j = 0; j < T - 1; ++j) {
+    const int km = min(kl, T - 1 - j);
+    double lv[KL];
+#pragma unroll
+    for (int i = 0; i < KL; ++i) lv[i] = (i < km) ? F[((size_t)j * ldab + kv + 1 + i) * 32] : 0.0;
+    const int jp = P[(size_t)j * 32];
+    const double2 inc = (j + kl + 1 < T) ? X[(size_t)(j + kl + 1) * 32] : zero2();
+    const double2 bj = win[((j + jp) & (W1 - 1)) * S];
+    if (jp) win[((j + jp) & (W1 - 1)) * S] = win[(j & (W1 - 1)) * S];
+#pragma unroll
+    for (int i = 0; i < KL; ++i) {
+      if (i < km) {
+        double2 w = win[((j + 1 + i) & (W1 - 1)) * S];
+        w.x -= lv[i] * bj.x;
+        w.y -= lv[i] * bj.y;
+        win[((j + 1 + i) & (W1 - 1)) * S] = w;
+      }
+    }
+    X[(size_t)j * 32] = bj;
+    if (j + kl + 1 < T) win[((j + kl + 1) & (W1 - 1)) * S] = inc;
+  }
+  if (T > 0) X[(size_t)(T - 1) * 32] = win[((T - 1) & (W1 - 1)) * S];
+  // ---- backward: x_{j+1}..x_{j+kv} in slots p mod W2 ----
+  int sj = (T - 1) % W2;  // slot of position j
+  for (int j = T - 1; j >= 0; --j) {
+    const int im = min(kv, T - 1 - j);
+    double u[KV];
+#pragma unroll
+    for (int i = 0; i < KV; ++i) u[i] = (i < im) ? F[((size_t)(j + 1 + i) * ldab + kv - 1 - i) * 32] : 0.0;
+    const double dinv = F[((size_t)j * ldab + kv) * 32];  // U's diagonal is stored as its reciprocal
+    double2 acc = X[(size_t)j * 32];
+#pragma unroll
+    for (int i = KV - 1; i >= 0; --i) {
+      if (i < im) {
+        int sl = sj + 1 + i;
+        if (sl >= W2) sl -= W2;
+        const double2 xv = win[sl * S];
+        acc.x -= u[i] * xv.x;
+        acc.y -= u[i] * xv.y;
+      }
+    }
+    const double2 xj = make_double2(acc.x * dinv, acc.y * dinv);
+    win[sj * S] = xj;
+    X[(size_t)j * 32] = flip_col(xj, cflip[j]);
+    sj = (sj == 0) ? W2 - 1 : sj - 1;
+  }
+}
+
+// ------------------------------------------------------------------------------
 // Stage right-hand side with the NL assembly fused in, one warp per (kx,ky) system
 // (marching.f90:16-21, 93-125, 319-367):
 //   Khat_i = sum_terms (i kx)^a (i ky)^b dsca trunc(I^Iz M^mz) qhat    (0 for inactive)
@@ -988,7 +1169,8 @@ __global__ void __launch_bounds__(kWPB * 32) k_rhs_nl(SolveArgs a, NLArgs n) {
   if (sid >= nsys) return;
   const int T = a.T, NZ = a.d.NZ;
   const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
-  const bool act = a.act_index[sid] >= 0;
+  const int aidx = a.act_index[sid];
+  const bool act = aidx >= 0;
   const bool origin = (kx == 0 && ky == 0);
   if (lane < kMaxGroups) {
     cms[warp][lane] = (lane < a.M.ngroups) ? cmul(ipow(a.kx[kx], a.M.gkx[lane]), ipow(a.ky[ky], a.M.gky[lane])) : zero2();
@@ -1022,7 +1204,12 @@ __global__ void __launch_bounds__(kWPB * 32) k_rhs_nl(SolveArgs a, NLArgs n) {
     if (act && a.rowflip) r = flip_row(r, a.rowflip[t]);
     // class order for the split solve; inactive systems (E = I) keep row t at
     // the position of column t, where k_kstd_out reads it back
-    a.work[(size_t)sid * a.wst + (a.row_pos ? (act ? a.row_pos[t] : a.col_pos[t]) : t)] = r;
+    if (a.work2 && act) {
+      const int pos = a.row_pos[t], c = pos >= a.Tc ? 1 : 0, bb = aidx * a.ncls + c;
+      a.work2[((size_t)(bb >> 5) * a.Tc + pos - c * a.Tc) * 32 + (bb & 31)] = r;
+    } else {
+      a.work[(size_t)sid * a.wst + (a.row_pos ? (act ? a.row_pos[t] : a.col_pos[t]) : t)] = r;
+    }
   }
 }
 
@@ -1047,12 +1234,33 @@ __global__ void __launch_bounds__(kWPB * 32) k_kstd_out(SolveArgs a) {
   const size_t base = (size_t)sid * T;
   const double2* x = a.work + (size_t)sid * a.wst;  // solution (class order when split)
   const bool zero_out = a.last_stage && !act;
+  const bool tpb = a.work2 && act;
+  const int aidx = a.act_index[sid];
+  auto xat = [&](int c) -> double2 {  // solution at class position c
+    if (tpb) {
+      const int k = c >= a.Tc ? 1 : 0, bb = aidx * a.ncls + k;
+      return a.work2[((size_t)(bb >> 5) * a.Tc + c - k * a.Tc) * 32 + (bb & 31)];
+    }
+    return x[c];
+  };
   bool bad = false;
   for (int t = lane; t < T; t += 32) {
-    const double2 v = zero_out ? zero2() : x[a.col_pos ? a.col_pos[t] : t];
+    const double2 v = zero_out ? zero2() : xat(a.col_pos ? a.col_pos[t] : t);
     bad |= !(isfinite(v.x) && isfinite(v.y));
     if (a.out != a.work || zero_out) a.out[base + t] = v;
-    if (a.Kstd_out) a.Kstd_out[base + t] = act ? ell_row(a.Lp, t, cls[warp], x) : zero2();
+    if (a.Kstd_out) {
+      double2 ks = zero2();
+      if (act) {
+#pragma unroll 4
+        for (int k = 0; k < a.Lp.width; ++k) {
+          const int cg = a.Lp.cg[(size_t)k * a.Lp.rows + t];
+          const double lv = a.Lp.val[(size_t)k * a.Lp.rows + t];
+          const double2 xv = xat(cg & 0xFFFFFF);
+          ks = cadd(ks, cmul(cls[warp][cg >> 24], make_double2(lv * xv.x, lv * xv.y)));
+        }
+      }
+      a.Kstd_out[base + t] = ks;
+    }
   }
   if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.flags, 1u);
 }
@@ -1268,7 +1476,7 @@ template <int NF>
 struct InvY {
   static void run(const Dims& d, int nf, const FullVarDev* fv, StateSet st, const double2* plain_spec,
                   const double* kx, const double* ky, double2* Y1, const FftPlan& py, cudaStream_t s) {
-    size_t sm = 2 * kNB1 * (size_t)d.NYA * sizeof(double2);
+    size_t sm = (NF ? 1 : 2) * kNB1 * (size_t)(d.NYA + kPadXY) * sizeof(double2);
     set_smem(k_inv_y<NF>, sm);
     dim3 g(nf, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
     k_inv_y<NF><<<g, kThreads, sm, s>>>(d, fv, st, plain_spec, kx, ky, Y1, py);
@@ -1277,7 +1485,7 @@ struct InvY {
 template <int NF>
 struct InvX {
   static void run(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s) {
-    size_t sm = 2 * (kNB2 / 2) * (size_t)d.NXA * sizeof(double2);
+    size_t sm = (NF ? 1 : 2) * (kNB2 / 2) * (size_t)(d.NXA + kPadXY) * sizeof(double2);
     set_smem(k_inv_x<NF>, sm);
     dim3 g(nf, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
     k_inv_x<NF><<<g, kThreads, sm, s>>>(d, Y1, Y2, px);
@@ -1287,7 +1495,7 @@ template <int NF>
 struct InvZ {
   static void run(const Dims& d, int nf, const double* Y2, double* phys, const FftPlan& pz, const double2* dct_tw,
                   const double* wz, unsigned long long* cfl_bits, cudaStream_t s) {
-    size_t sm = 2 * (kXB3 / 2) * (size_t)d.NZA * sizeof(double2);
+    size_t sm = (NF ? 1 : 2) * (kXB3 / 2) * (size_t)d.NZA * sizeof(double2);
     set_smem(k_inv_z<NF>, sm);
     dim3 g(nf, (d.NXA + kXB3 - 1) / kXB3, d.NYA);
     k_inv_z<NF><<<g, kThreads, sm, s>>>(d, Y2, phys, pz, dct_tw, wz, cfl_bits);
@@ -1297,7 +1505,7 @@ template <int NF>
 struct FwdZ {
   static void run(const Dims& d, int nf, const QuadDesc& q, const double* phys, double* Q2, const FftPlan& pz,
                   const double2* dct_tw, const double* wz, double* ke_partial, cudaStream_t s) {
-    size_t sm = (size_t)nf * d.NZA * sizeof(double2) + 2 * (size_t)q.nq * d.NZA * sizeof(double2);
+    size_t sm = (size_t)nf * d.NZA * sizeof(double2) + (NF ? 1 : 2) * (size_t)std::min(q.nq, kQC) * d.NZA * sizeof(double2);
     set_smem(k_fwd_z<NF>, sm);
     dim3 g((d.NXA + 1) / 2, d.NYA);
     k_fwd_z<NF><<<g, kThreads, sm, s>>>(d, nf, q, phys, Q2, pz, dct_tw, wz, ke_partial);
@@ -1306,7 +1514,7 @@ struct FwdZ {
 template <int NF>
 struct FwdX {
   static void run(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s) {
-    size_t sm = 2 * (kNB2 / 2) * (size_t)d.NXA * sizeof(double2);
+    size_t sm = (NF ? 1 : 2) * (kNB2 / 2) * (size_t)(d.NXA + kPadXY) * sizeof(double2);
     set_smem(k_fwd_x<NF>, sm);
     dim3 g(nq, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
     k_fwd_x<NF><<<g, kThreads, sm, s>>>(d, Q2, Q1, px);
@@ -1316,7 +1524,7 @@ template <int NF>
 struct FwdY {
   static void run(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
                   cudaStream_t s) {
-    size_t sm = 2 * kNB1 * (size_t)d.NYA * sizeof(double2);
+    size_t sm = (NF ? 1 : 2) * kNB1 * (size_t)(d.NYA + kPadXY) * sizeof(double2);
     set_smem(k_fwd_y<NF>, sm);
     dim3 g(nq, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
     k_fwd_y<NF><<<g, kThreads, sm, s>>>(d, Q1, qspec, scale, py);
@@ -1365,6 +1573,22 @@ void launch_factor(const FactorArgs& a, cudaStream_t s) {
 void launch_solve_real(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
   const int nsys = a.d.NXH * a.d.NYA;
   k_rhs_nl<<<(nsys + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a, n);
+  if (a.work2) {
+    if (a.nblk > 0) {
+      const int kv = a.kl + a.ku, grid = (a.nblk + kTpbThreads - 1) / kTpbThreads;
+      if (a.kl == 9 && kv == 23) {
+        const size_t sm = (size_t)kTpbThreads * 24 * sizeof(double2);
+        set_smem(k_subst_tpb<9, 23>, sm);
+        k_subst_tpb<9, 23><<<grid, kTpbThreads, sm, s>>>(a);
+      } else {
+        const size_t sm = (size_t)kTpbThreads * 32 * sizeof(double2);
+        set_smem(k_subst_tpb<15, 31>, sm);
+        k_subst_tpb<15, 31><<<grid, kTpbThreads, sm, s>>>(a);
+      }
+    }
+    k_kstd_out<<<(nsys + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
+    return;
+  }
   if (a.nact > 0) {
     const size_t sm = (size_t)kWPBr * kNBUF * kCW * a.ring_cols * sizeof(double);
     if (a.ncls == 2) {
@@ -1379,6 +1603,11 @@ void launch_solve_real(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
 }
 void launch_factor_real(const FactorArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;
+  if (a.tpb) {
+    const int nb = a.ncls * a.nact;
+    k_factor_tpb<<<(nb + kTpbThreads - 1) / kTpbThreads, kTpbThreads, 0, s>>>(a);
+    return;
+  }
   k_factor_real<<<dim3((a.nact + kWPB - 1) / kWPB, a.ncls), kWPB * 32, 0, s>>>(a);
 }
 void launch_zero_step(const ZeroArgs& a, cudaStream_t s) {
