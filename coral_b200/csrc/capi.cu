@@ -525,6 +525,7 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       na.ky = h->d_ky;
       na.act_index = h->d_act_index;
       na.Khat = k.Khat[i];
+      na.nq = h->nQ;
       SolveArgs sa{};
       sa.d = d;
       sa.T = k.T;

@@ -84,6 +84,7 @@ struct NLArgs {
   const double* ky;
   const int* act_index;  // [kx*NYA+ky] -> factor slot, -1 for dealiased modes and (0,0)
   double2* Khat;
+  int nq;                // quadratic variables in qspec
 };
 void launch_nl(const NLArgs& a, cudaStream_t s);
 

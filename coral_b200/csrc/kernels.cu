@@ -1155,114 +1155,140 @@ __global__ void __launch_bounds__(kTpbThreads) k_subst_tpb(SolveArgs a) {
 }
 
 // ------------------------------------------------------------------------------
-// Stage right-hand side with the NL assembly fused in, one warp per (kx,ky) system
+// Stage right-hand side with the NL assembly fused in, one CTA per (kx,ky) system
 // (marching.f90:16-21, 93-125, 319-367):
 //   Khat_i = sum_terms (i kx)^a (i ky)^b dsca trunc(I^Iz M^mz) qhat    (0 for inactive)
 //   rhs    = M field + sum_{j<i} (dt a(i,j) Kstd_j + dt ahat(i+1,j) Khat_j) + dt ahat(i+1,i) Khat_i
-// rows flagged in rowflip are multiplied by -i for the real-scaled solve.
+// The system's quadratic-variable coefficients and state are first staged in
+// shared memory with coalesced loads, so the row gathers run from shared memory.
+// Active systems: rows flagged in rowflip are multiplied by -i for the real-scaled
+// solve and the right-hand side goes to the solve's work layout.  Inactive systems
+// (E = I): the right-hand side is the stage output itself (zero in the last
+// stage), K_std_i = 0.
 // ------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kWPB * 32) k_rhs_nl(SolveArgs a, NLArgs n) {
-  __shared__ double2 cms[kWPB][kMaxGroups], cns[kWPB][kMaxGroups];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int sid = blockIdx.x * kWPB + warp;
-  const int nsys = a.d.NXH * a.d.NYA;
-  if (sid >= nsys) return;
+constexpr int kRhsThreads = 256;
+
+__global__ void __launch_bounds__(kRhsThreads) k_rhs_nl(SolveArgs a, NLArgs n) {
+  extern __shared__ double2 shr[];
+  __shared__ double2 cms[kMaxGroups], cns[kMaxGroups];
+  const int sid = blockIdx.x;
   const int T = a.T, NZ = a.d.NZ;
   const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
   const int aidx = a.act_index[sid];
   const bool act = aidx >= 0;
   const bool origin = (kx == 0 && ky == 0);
-  if (lane < kMaxGroups) {
-    cms[warp][lane] = (lane < a.M.ngroups) ? cmul(ipow(a.kx[kx], a.M.gkx[lane]), ipow(a.ky[ky], a.M.gky[lane])) : zero2();
-    cns[warp][lane] = (lane < n.NL.ngroups) ? cmul(ipow(a.kx[kx], n.NL.gkx[lane]), ipow(a.ky[ky], n.NL.gky[lane])) : zero2();
+  if (threadIdx.x < kMaxGroups) {
+    const int g = threadIdx.x;
+    cms[g] = (g < a.M.ngroups) ? cmul(ipow(a.kx[kx], a.M.gkx[g]), ipow(a.ky[ky], a.M.gky[g])) : zero2();
+    cns[g] = (g < n.NL.ngroups) ? cmul(ipow(a.kx[kx], n.NL.gkx[g]), ipow(a.ky[ky], n.NL.gky[g])) : zero2();
   }
-  __syncwarp();
-  const double2* field = a.field + (size_t)sid * T;
-  const size_t qcol = ((size_t)kx * a.d.NYA + ky) * NZ;            // (kx,ky) column of quad var 0
-  const size_t qstride = (size_t)a.d.NXH * a.d.NYA * NZ;           // between quad vars
   const size_t base = (size_t)sid * T;
-  for (int t = lane; t < T; t += 32) {
+  const int nqz = act ? n.nq * NZ : 0;
+  double2* qs = shr;         // [quad][n] of this (kx,ky)
+  double2* fs = shr + nqz;   // state of this system
+  {
+    const size_t qstride = (size_t)a.d.NXH * a.d.NYA * NZ;  // between quad vars
+    for (int idx = threadIdx.x; idx < nqz; idx += kRhsThreads) {
+      const int q = idx / NZ, nn = idx - q * NZ;
+      qs[idx] = n.qspec[q * qstride + (size_t)sid * NZ + nn];
+    }
+    const double2* field = a.field + base;
+    for (int t = threadIdx.x; t < T; t += kRhsThreads) fs[t] = field[t];
+  }
+  __syncthreads();
+  const bool zero_out = a.last_stage && !act;
+  bool bad = false;
+  for (int t = threadIdx.x; t < T; t += kRhsThreads) {
     double2 kh = zero2();
     if (act) {
       for (int k = 0; k < n.NL.width; ++k) {
         const double v = n.NL.v(t, k);
         if (v == 0.0) break;  // slots are filled in order; exact zeros are not stored
         const int cg = n.NL.cg[(size_t)k * n.NL.rows + t];
-        const int c = cg & 0xFFFFFF;
-        const int qv = c / NZ, nn = c - qv * NZ;
-        const double2 qh = n.qspec[qv * qstride + qcol + nn];
-        kh = cadd(kh, cmul(cns[warp][cg >> 24], make_double2(v * qh.x, v * qh.y)));
+        const double2 qh = qs[cg & 0xFFFFFF];  // column = quad * NZ + n
+        kh = cadd(kh, cmul(cns[cg >> 24], make_double2(v * qh.x, v * qh.y)));
       }
     }
     n.Khat[base + t] = kh;
-    double2 r = origin ? zero2() : ell_row(a.M, t, cms[warp], field);
+    double2 r = zero2();
+    if (!origin) {
+#pragma unroll 4
+      for (int k = 0; k < a.M.width; ++k) {
+        const int cg = a.M.cg[(size_t)k * a.M.rows + t];
+        const double v = a.M.val[(size_t)k * a.M.rows + t];
+        const double2 xv = fs[cg & 0xFFFFFF];
+        r = cadd(r, cmul(cms[cg >> 24], make_double2(v * xv.x, v * xv.y)));
+      }
+    }
     for (int j = 0; j < a.nprev; ++j) {
       r = cadd(r, cscale(a.Kstd[j][base + t], a.ca[j]));
       r = cadd(r, cscale(a.Khat[j][base + t], a.ch[j]));
     }
     r = cadd(r, cscale(kh, a.ch[a.nprev]));
-    if (act && a.rowflip) r = flip_row(r, a.rowflip[t]);
-    // class order for the split solve; inactive systems (E = I) keep row t at
-    // the position of column t, where k_kstd_out reads it back
-    if (a.work2 && act) {
-      const int pos = a.row_pos[t], c = pos >= a.Tc ? 1 : 0, bb = aidx * a.ncls + c;
-      a.work2[((size_t)(bb >> 5) * a.Tc + pos - c * a.Tc) * 32 + (bb & 31)] = r;
+    if (act) {
+      if (a.rowflip) r = flip_row(r, a.rowflip[t]);
+      if (a.work2) {  // thread-per-block layout, class order
+        const int pos = a.row_pos[t], c = pos >= a.Tc ? 1 : 0, bb = aidx * a.ncls + c;
+        a.work2[((size_t)(bb >> 5) * a.Tc + pos - c * a.Tc) * 32 + (bb & 31)] = r;
+      } else {
+        a.work[(size_t)sid * a.wst + (a.row_pos ? a.row_pos[t] : t)] = r;
+      }
     } else {
-      a.work[(size_t)sid * a.wst + (a.row_pos ? (act ? a.row_pos[t] : a.col_pos[t]) : t)] = r;
+      const double2 v = zero_out ? zero2() : r;
+      bad |= !(isfinite(v.x) && isfinite(v.y));
+      a.out[base + t] = v;
+      if (a.Kstd_out) a.Kstd_out[base + t] = zero2();
     }
   }
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(a.flags, 1u);
 }
 
 // ------------------------------------------------------------------------------
-// After the substitutions: K_std_i = L aux (0 for inactive systems), the stage
-// output (the new state in the last stage, zero on inactive systems), and the
-// non-finite check.  One warp per (kx,ky) system.  With a class split the
-// solution is read back from class order (L's columns are stored remapped).
+// After the substitutions, one CTA per active system: the solution is staged in
+// shared memory (from the solve's layout), then K_std_i = L x, the stage output
+// (the new state in the last stage) and the non-finite check.
 // ------------------------------------------------------------------------------
-__global__ void __launch_bounds__(kWPB * 32) k_kstd_out(SolveArgs a) {
-  __shared__ double2 cls[kWPB][kMaxGroups];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int sid = blockIdx.x * kWPB + warp;
-  const int nsys = a.d.NXH * a.d.NYA;
-  if (sid >= nsys) return;
-  const int T = a.T;
+__global__ void __launch_bounds__(kRhsThreads) k_kstd_out(SolveArgs a) {
+  extern __shared__ double2 xs[];
+  __shared__ double2 cls[kMaxGroups];
+  const int aidx = blockIdx.x;
+  const int sid = a.act_list[aidx];
+  const int T = a.T, Tc = a.Tc, npos = a.ncls * a.Tc;
   const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
-  const bool act = a.act_index[sid] >= 0;
-  if (lane < kMaxGroups)
-    cls[warp][lane] = (lane < a.L.ngroups) ? cmul(ipow(a.kx[kx], a.L.gkx[lane]), ipow(a.ky[ky], a.L.gky[lane])) : zero2();
-  __syncwarp();
-  const size_t base = (size_t)sid * T;
-  const double2* x = a.work + (size_t)sid * a.wst;  // solution (class order when split)
-  const bool zero_out = a.last_stage && !act;
-  const bool tpb = a.work2 && act;
-  const int aidx = a.act_index[sid];
-  auto xat = [&](int c) -> double2 {  // solution at class position c
-    if (tpb) {
-      const int k = c >= a.Tc ? 1 : 0, bb = aidx * a.ncls + k;
-      return a.work2[((size_t)(bb >> 5) * a.Tc + c - k * a.Tc) * 32 + (bb & 31)];
+  if (threadIdx.x < kMaxGroups) {
+    const int g = threadIdx.x;
+    cls[g] = (g < a.Lp.ngroups) ? cmul(ipow(a.kx[kx], a.Lp.gkx[g]), ipow(a.ky[ky], a.Lp.gky[g])) : zero2();
+  }
+  if (a.work2) {
+    // (j, class) pairs: the two classes of one j are adjacent 16-byte entries
+    for (int idx = threadIdx.x; idx < npos; idx += kRhsThreads) {
+      const int j = idx / a.ncls, c = idx - j * a.ncls, bb = aidx * a.ncls + c;
+      xs[c * Tc + j] = a.work2[((size_t)(bb >> 5) * Tc + j) * 32 + (bb & 31)];
     }
-    return x[c];
-  };
+  } else {
+    const double2* x = a.work + (size_t)sid * a.wst;
+    for (int p = threadIdx.x; p < npos; p += kRhsThreads) xs[p] = x[p];
+  }
+  __syncthreads();
+  const size_t base = (size_t)sid * T;
   bool bad = false;
-  for (int t = lane; t < T; t += 32) {
-    const double2 v = zero_out ? zero2() : xat(a.col_pos ? a.col_pos[t] : t);
+  for (int t = threadIdx.x; t < T; t += kRhsThreads) {
+    const double2 v = xs[a.col_pos ? a.col_pos[t] : t];
     bad |= !(isfinite(v.x) && isfinite(v.y));
-    if (a.out != a.work || zero_out) a.out[base + t] = v;
+    if (a.out != a.work || a.work2) a.out[base + t] = v;
     if (a.Kstd_out) {
       double2 ks = zero2();
-      if (act) {
 #pragma unroll 4
-        for (int k = 0; k < a.Lp.width; ++k) {
-          const int cg = a.Lp.cg[(size_t)k * a.Lp.rows + t];
-          const double lv = a.Lp.val[(size_t)k * a.Lp.rows + t];
-          const double2 xv = xat(cg & 0xFFFFFF);
-          ks = cadd(ks, cmul(cls[warp][cg >> 24], make_double2(lv * xv.x, lv * xv.y)));
-        }
+      for (int k = 0; k < a.Lp.width; ++k) {
+        const int cg = a.Lp.cg[(size_t)k * a.Lp.rows + t];
+        const double lv = a.Lp.val[(size_t)k * a.Lp.rows + t];
+        const double2 xv = xs[cg & 0xFFFFFF];
+        ks = cadd(ks, cmul(cls[cg >> 24], make_double2(lv * xv.x, lv * xv.y)));
       }
       a.Kstd_out[base + t] = ks;
     }
   }
-  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(a.flags, 1u);
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(a.flags, 1u);
 }
 
 // ------------------------------------------------------------------------------
@@ -1572,7 +1598,13 @@ void launch_factor(const FactorArgs& a, cudaStream_t s) {
 }
 void launch_solve_real(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
   const int nsys = a.d.NXH * a.d.NYA;
-  k_rhs_nl<<<(nsys + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a, n);
+  {
+    const size_t sm = ((size_t)n.nq * a.d.NZ + a.T) * sizeof(double2);
+    set_smem(k_rhs_nl, sm);
+    k_rhs_nl<<<nsys, kRhsThreads, sm, s>>>(a, n);
+  }
+  const size_t smx = (size_t)a.ncls * a.Tc * sizeof(double2);
+  if (smx > 48 * 1024) set_smem(k_kstd_out, smx);
   if (a.work2) {
     if (a.nblk > 0) {
       const int kv = a.kl + a.ku, grid = (a.nblk + kTpbThreads - 1) / kTpbThreads;
@@ -1586,20 +1618,16 @@ void launch_solve_real(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
         k_subst_tpb<15, 31><<<grid, kTpbThreads, sm, s>>>(a);
       }
     }
-    k_kstd_out<<<(nsys + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
+    if (a.nact > 0) k_kstd_out<<<a.nact, kRhsThreads, smx, s>>>(a);
     return;
   }
+  // whole systems (no class split): one warp per system
   if (a.nact > 0) {
     const size_t sm = (size_t)kWPBr * kNBUF * kCW * a.ring_cols * sizeof(double);
-    if (a.ncls == 2) {
-      set_smem(k_subst_real<16>, sm);
-      k_subst_real<16><<<(a.nact + kWPBr - 1) / kWPBr, kWPBr * 32, sm, s>>>(a);
-    } else {
-      set_smem(k_subst_real<32>, sm);
-      k_subst_real<32><<<(a.nact + kWPBr - 1) / kWPBr, kWPBr * 32, sm, s>>>(a);
-    }
+    set_smem(k_subst_real<32>, sm);
+    k_subst_real<32><<<(a.nact + kWPBr - 1) / kWPBr, kWPBr * 32, sm, s>>>(a);
+    k_kstd_out<<<a.nact, kRhsThreads, smx, s>>>(a);
   }
-  k_kstd_out<<<(nsys + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
 }
 void launch_factor_real(const FactorArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;
