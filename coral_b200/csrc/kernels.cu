@@ -33,6 +33,7 @@ constexpr int kThreads = 256;
 // measured best at 384^2 x 192: 3 for the x / y passes, 4 for the z passes)
 constexpr int kMinBlocksXY = 3;
 constexpr int kMinBlocksZ = 4;
+constexpr int kMinBlocksZF = 2;  // fused z passes (two FFT batches in one kernel)
 constexpr int kWPB = 8;  // warps (systems) per CTA in the per-system kernels
 
 __device__ __forceinline__ double2 zero2() { return make_double2(0.0, 0.0); }
@@ -274,6 +275,138 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksZ) k_fwd_z(Dims d, int nf,
       double* dst = Q2 + (((size_t)(q0 + qi) * d.NYA + y) * d.NXA + x0) * d.NZ;
       dst[n] = xa;
       if (x0 + 1 < d.NXA) dst[d.NZ + n] = xb;
+    }
+    __syncthreads();  // A is refilled by the next batch
+  }
+  if (ke_partial) {
+    for (int j = 0; j < 3; ++j) {
+      double v = ke[j];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if ((threadIdx.x & 31) == 0) red[j][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+      double s = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
+      ke_partial[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 3 + threadIdx.x] = s;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------
+// z passes of one stage fused: z REDFT01 of the full variables (transforms.f90:
+// 216-223), the CFL maxima (marching.f90:219-238), the pointwise products
+// (marching.f90:279-291), the KE partial averages (output.f90:84-102) and the z
+// REDFT10 of the quadratic variables (transforms.f90:243-249), for one pair of
+// x columns; the physical fields never leave shared memory.  The inverse
+// transform leaves the physical values in Makhoul order (position m holds
+// z = 2m, or 2(N-1-m)+1 for m >= N/2), which is the order the forward transform
+// takes, so the products are formed position by position.
+// ------------------------------------------------------------------------------
+constexpr int kFC = 4;  // full variables per inverse FFT batch
+
+template <int NF>
+__global__ void __launch_bounds__(kThreads, kMinBlocksZF) k_z_fused(Dims d, int nf, QuadDesc q, const double* Y2,
+                                                                    double* Q2, FftPlan pz, const double2* dct_tw,
+                                                                    const double* wz, unsigned long long* cfl_bits,
+                                                                    double* ke_partial) {
+  extern __shared__ double2 sm[];
+  __shared__ double red[3][kThreads / 32];
+  const int x0 = blockIdx.x * 2, y = blockIdx.y;
+  const int N = NF ? NF : d.NZA, nq = q.nq, nb = min(nq, kQC);
+  const bool has_b = x0 + 1 < d.NXA;
+  double2* Fv = sm;          // nf lines: columns x0 (re) and x0+1 (im) of each full variable
+  double2* A = sm + nf * N;  // nb lines of quadratic variables
+  double2* B = A + nb * N;   // runtime plan only (max(kFC, kQC) lines)
+  // ---- inverse: X_n and X_{N-n} of both columns, twiddled, packed as va + i vb ----
+  for (int idx = threadIdx.x; idx < nf * N; idx += blockDim.x) {
+    const int f = idx / N, n = idx - f * N;
+    const double* sa = Y2 + (((size_t)f * d.NYA + y) * d.NXA + x0) * d.NZ;
+    const double* sb = sa + d.NZ;
+    double a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+    if (n < d.NZ) a0 = sa[n];
+    if (n > 0 && N - n < d.NZ) a1 = sa[N - n];
+    if (has_b) {
+      if (n < d.NZ) b0 = sb[n];
+      if (n > 0 && N - n < d.NZ) b1 = sb[N - n];
+    }
+    const double2 w = cconj(dct_tw[n]);  // exp(+i pi n / 2N)
+    const double2 va = cmul(w, make_double2(a0, -a1));
+    const double2 vb = cmul(w, make_double2(b0, -b1));
+    Fv[idx] = make_double2(va.x - vb.y, va.y + vb.x);
+  }
+  __syncthreads();
+  for (int f0 = 0; f0 < nf; f0 += kFC) {
+    const int nl = min(kFC, nf - f0);
+    const double2* R = fft_lines_n<NF, true, kThreads, kFC>(Fv + f0 * N, B, nl, N, pz);
+    if (R != Fv + f0 * N) {  // runtime plan with the result in the scratch lines
+      for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) Fv[f0 * N + idx] = R[idx];
+      __syncthreads();
+    }
+  }
+  // ---- CFL maxima of |u|, |v|, |w| / wz over both columns ----
+  if (cfl_bits) {
+    const int ncf = min(nf, 3);
+    double mx[3] = {0.0, 0.0, 0.0};
+    for (int idx = threadIdx.x; idx < ncf * N; idx += blockDim.x) {
+      const int f = idx / N, m = idx - f * N;
+      const int z = (m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1;
+      const double2 v = Fv[idx];
+      const double s = (f == 2) ? 1.0 / wz[z] : 1.0;
+      double a = fabs(v.x) * s;
+      if (has_b) a = fmax(a, fabs(v.y) * s);
+#pragma unroll
+      for (int j = 0; j < 3; ++j)
+        if (f == j) mx[j] = fmax(mx[j], a);
+    }
+    for (int j = 0; j < 3; ++j) {
+      double v = mx[j];
+      for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+      if ((threadIdx.x & 31) == 0) red[j][threadIdx.x >> 5] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < ncf) {
+      double m2 = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m2 = fmax(m2, red[threadIdx.x][w]);
+      atomic_max_nonneg(cfl_bits + threadIdx.x, m2);
+    }
+    __syncthreads();
+  }
+  // ---- products and forward transforms, in batches of kQC quadratic variables ----
+  double ke[3] = {0.0, 0.0, 0.0};
+  for (int q0 = 0; q0 < nq; q0 += kQC) {
+    const int nc = min(kQC, nq - q0);
+    for (int idx = threadIdx.x; idx < nc * N; idx += blockDim.x) {
+      const int qi = idx / N, m = idx - qi * N, qg = q0 + qi;
+      const int v1 = q.v1[qg], v2 = q.v2[qg];
+      double pa, pb;
+      if (v1 < 0) { pa = Fv[v2 * N + m].x; pb = Fv[v2 * N + m].y; }
+      else if (v2 < 0) { pa = Fv[v1 * N + m].x; pb = Fv[v1 * N + m].y; }
+      else {
+        const double2 f1 = Fv[v1 * N + m], f2 = Fv[v2 * N + m];
+        pa = f1.x * f2.x;
+        pb = f1.y * f2.y;
+      }
+      A[qi * N + m] = make_double2(pa, pb);
+      if (ke_partial) {
+        const int z = (m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1;
+        for (int j = 0; j < 3; ++j)
+          if (q.ke_q[j] == qg) ke[j] += wz[z] * (pa + (has_b ? pb : 0.0));
+      }
+    }
+    __syncthreads();
+    const double2* R = fft_lines_n<NF, false, kThreads, kQC>(A, B, nc, N, pz);
+    for (int idx = threadIdx.x; idx < nc * d.NZ; idx += blockDim.x) {
+      const int qi = idx / d.NZ, n = idx - qi * d.NZ;
+      const double2 Z = R[qi * N + n];
+      const double2 Zc = cconj(R[qi * N + ((N - n) % N)]);
+      const double2 va = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
+      const double2 dd = csub(Z, Zc);
+      const double2 vb = make_double2(0.5 * dd.y, -0.5 * dd.x);  // (Z - Zc) / 2i
+      const double2 w = dct_tw[n];                                // exp(-i pi n / 2N)
+      double* dst = Q2 + (((size_t)(q0 + qi) * d.NYA + y) * d.NXA + x0) * d.NZ;
+      dst[n] = 2.0 * (w.x * va.x - w.y * va.y);
+      if (has_b) dst[d.NZ + n] = 2.0 * (w.x * vb.x - w.y * vb.y);
     }
     __syncthreads();  // A is refilled by the next batch
   }
@@ -1085,11 +1218,128 @@ __global__ void __launch_bounds__(kTpbThreads) k_factor_tpb(FactorArgs a) {
 // Forward (P, L: the column sweep with the row interchanges interleaved, as the
 // reference's band solve) then backward (U, row form: each x_j subtracts the
 // known x_{j+i} in decreasing column order, the order in which the column sweep
-// reaches it) for one block.  KL, KV bound kl and kl+ku (registers hold one L
-// column / one U row); the window holds positions j..j+kl (forward, W1 slots)
-// or j..j+kv (backward, KV+1 slots).
-template <int KL, int KV>
+// reaches it) for one block.  The band is compile-time (kl = KL, kl + ku = KV,
+// column stride LD = ldab), so every factor offset is an immediate from one
+// per-column pointer; each step's factor values are loaded one step ahead.
+// Band entries outside the matrix are stored zeros, so the forward sweep runs
+// unpredicated (it only touches dead window slots near the end); the backward
+// rows within KV of the last column take the guarded loop.
+template <int KL, int KV, int LD>
 __global__ void __launch_bounds__(kTpbThreads) k_subst_tpb(SolveArgs a) {
+  constexpr int W1 = (KL + 2 <= 16) ? 16 : 32;  // power of 2 >= KL + 2
+  constexpr int W2 = KV + 1;
+  constexpr int S = kTpbThreads;                // slot stride
+  constexpr size_t CS = (size_t)LD * 32;        // column stride (doubles)
+  extern __shared__ double2 swin[];
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.nblk) return;  // no warp-collective operations below
+  const int T = a.Tc;
+  const int cls = b % a.ncls;
+  const size_t gb = (size_t)(b >> 5) * T;
+  const double* F = a.abr + gb * CS + (b & 31);
+  const unsigned char* P = a.dpiv + gb * 32 + (b & 31);
+  double2* X = a.work2 + gb * 32 + (b & 31);
+  const unsigned char* cflip = a.colflip_cls + (size_t)cls * T;
+  double2* win = swin + threadIdx.x;
+  // ---- forward: positions j..j+KL in slots p mod W1 ----
+  for (int p = 0; p <= KL && p < T; ++p) win[(p & (W1 - 1)) * S] = X[(size_t)p * 32];
+  if (T > 1) {
+    double lv[KL], lvn[KL];
+    int jpn = P[0];
+    double2 incn = (KL + 1 < T) ? X[(size_t)(KL + 1) * 32] : zero2();
+#pragma unroll
+    for (int i = 0; i < KL; ++i) lvn[i] = F[(KV + 1 + i) * 32];
+    for (int j = 0; j < T - 1; ++j) {
+#pragma unroll
+      for (int i = 0; i < KL; ++i) lv[i] = lvn[i];
+      const int jp = jpn;
+      const double2 inc = incn;
+      if (j + 1 < T - 1) {  // next column's multipliers, pivot and incoming entry
+        const double* Fn = F + (size_t)(j + 1) * CS;
+#pragma unroll
+        for (int i = 0; i < KL; ++i) lvn[i] = Fn[(KV + 1 + i) * 32];
+        jpn = P[(size_t)(j + 1) * 32];
+        incn = (j + KL + 2 < T) ? X[(size_t)(j + KL + 2) * 32] : zero2();
+      }
+      const int s0 = j & (W1 - 1);
+      const int sp = (j + jp) & (W1 - 1);
+      const double2 bj = win[sp * S];
+      if (jp) win[sp * S] = win[s0 * S];
+#pragma unroll
+      for (int i = 0; i < KL; ++i) {
+        const int sl = (s0 + 1 + i) & (W1 - 1);
+        double2 w = win[sl * S];
+        w.x -= lv[i] * bj.x;
+        w.y -= lv[i] * bj.y;
+        win[sl * S] = w;
+      }
+      X[(size_t)j * 32] = bj;
+      if (j + KL + 1 < T) win[((j + KL + 1) & (W1 - 1)) * S] = inc;
+    }
+  }
+  if (T > 0) X[(size_t)(T - 1) * 32] = win[((T - 1) & (W1 - 1)) * S];
+  // ---- backward: x_{j+1}..x_{j+KV} in slots p mod W2 ----
+  int sj = (T - 1) % W2;  // slot of position j
+  int j = T - 1;
+  for (; j >= 0 && j + KV >= T; --j) {  // rows within KV of the end
+    const double* Fj = F + (size_t)j * CS;
+    double2 acc = X[(size_t)j * 32];
+    for (int i = T - 2 - j; i >= 0; --i) {
+      int sl = sj + 1 + i;
+      if (sl >= W2) sl -= W2;
+      const double u = Fj[((1 + i) * LD + KV - 1 - i) * 32];
+      const double2 xv = win[sl * S];
+      acc.x -= u * xv.x;
+      acc.y -= u * xv.y;
+    }
+    const double dinv = Fj[KV * 32];  // U's diagonal is stored as its reciprocal
+    const double2 xj = make_double2(acc.x * dinv, acc.y * dinv);
+    win[sj * S] = xj;
+    X[(size_t)j * 32] = flip_col(xj, cflip[j]);
+    sj = (sj == 0) ? W2 - 1 : sj - 1;
+  }
+  if (j >= 0) {
+    double u[KV], un[KV];
+    double dinv, dinvn;
+    double2 yn;
+    {
+      const double* Fj = F + (size_t)j * CS;
+#pragma unroll
+      for (int i = 0; i < KV; ++i) un[i] = Fj[((1 + i) * LD + KV - 1 - i) * 32];
+      dinvn = Fj[KV * 32];
+      yn = X[(size_t)j * 32];
+    }
+    for (; j >= 0; --j) {
+#pragma unroll
+      for (int i = 0; i < KV; ++i) u[i] = un[i];
+      dinv = dinvn;
+      double2 acc = yn;
+      if (j > 0) {  // next row (j - 1)
+        const double* Fn = F + (size_t)(j - 1) * CS;
+#pragma unroll
+        for (int i = 0; i < KV; ++i) un[i] = Fn[((1 + i) * LD + KV - 1 - i) * 32];
+        dinvn = Fn[KV * 32];
+        yn = X[(size_t)(j - 1) * 32];
+      }
+#pragma unroll
+      for (int i = KV - 1; i >= 0; --i) {
+        int sl = sj + 1 + i;
+        if (sl >= W2) sl -= W2;
+        const double2 xv = win[sl * S];
+        acc.x -= u[i] * xv.x;
+        acc.y -= u[i] * xv.y;
+      }
+      const double2 xj = make_double2(acc.x * dinv, acc.y * dinv);
+      win[sj * S] = xj;
+      X[(size_t)j * 32] = flip_col(xj, cflip[j]);
+      sj = (sj == 0) ? W2 - 1 : sj - 1;
+    }
+  }
+}
+
+// The same solve for any band within (KL, KV) = (15, 31), kl and ku read at run time.
+template <int KL, int KV>
+__global__ void __launch_bounds__(kTpbThreads) k_subst_tpb_rt(SolveArgs a) {
   constexpr int W1 = (KL + 2 <= 16) ? 16 : 32;  // power of 2 >= KL + 2
   constexpr int W2 = KV + 1;
   constexpr int S = kTpbThreads;                // slot stride
@@ -1201,12 +1451,25 @@ __global__ void __launch_bounds__(kRhsThreads) k_rhs_nl(SolveArgs a, NLArgs n) {
   for (int t = threadIdx.x; t < T; t += kRhsThreads) {
     double2 kh = zero2();
     if (act) {
-      for (int k = 0; k < n.NL.width; ++k) {
-        const double v = n.NL.v(t, k);
-        if (v == 0.0) break;  // slots are filled in order; exact zeros are not stored
-        const int cg = n.NL.cg[(size_t)k * n.NL.rows + t];
-        const double2 qh = qs[cg & 0xFFFFFF];  // column = quad * NZ + n
-        kh = cadd(kh, cmul(cns[cg >> 24], make_double2(v * qh.x, v * qh.y)));
+      // slots in batches of 4 independent loads; slots are filled in order and
+      // exact zeros are not stored, so a zero ends the row
+      for (int k0 = 0; k0 < n.NL.width; k0 += 4) {
+        int cg[4];
+        double v[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const bool ok = k0 + u < n.NL.width;
+          cg[u] = ok ? n.NL.cg[(size_t)(k0 + u) * n.NL.rows + t] : 0;
+          v[u] = ok ? n.NL.val[(size_t)(k0 + u) * n.NL.rows + t] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (v[u] != 0.0) {
+            const double2 qh = qs[cg[u] & 0xFFFFFF];  // column = quad * NZ + n
+            kh = cadd(kh, cmul(cns[cg[u] >> 24], make_double2(v[u] * qh.x, v[u] * qh.y)));
+          }
+        }
+        if (v[3] == 0.0) break;
       }
     }
     n.Khat[base + t] = kh;
@@ -1538,6 +1801,18 @@ struct FwdZ {
   }
 };
 template <int NF>
+struct ZFused {
+  static void run(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* Q2, const FftPlan& pz,
+                  const double2* dct_tw, const double* wz, unsigned long long* cfl_bits, double* ke_partial,
+                  cudaStream_t s) {
+    const size_t lines = (size_t)nf + std::min(q.nq, kQC) + (NF ? 0 : std::max(kFC, kQC));
+    const size_t sm = lines * d.NZA * sizeof(double2);
+    set_smem(k_z_fused<NF>, sm);
+    dim3 g((d.NXA + 1) / 2, d.NYA);
+    k_z_fused<NF><<<g, kThreads, sm, s>>>(d, nf, q, Y2, Q2, pz, dct_tw, wz, cfl_bits, ke_partial);
+  }
+};
+template <int NF>
 struct FwdX {
   static void run(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s) {
     size_t sm = (NF ? 1 : 2) * (kNB2 / 2) * (size_t)(d.NXA + kPadXY) * sizeof(double2);
@@ -1560,6 +1835,11 @@ struct FwdY {
 void launch_inv_y(const Dims& d, int nf, const FullVarDev* fv, StateSet st, const double2* plain_spec,
                   const double* kx, const double* ky, double2* Y1, const FftPlan& py, cudaStream_t s) {
   dispatch_len<InvY>(d.NYA, d, nf, fv, st, plain_spec, kx, ky, Y1, py, s);
+}
+void launch_z_fused(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* Q2, const FftPlan& pz,
+                    const double2* dct_tw, const double* wz, unsigned long long* cfl_bits, double* ke_partial,
+                    cudaStream_t s) {
+  dispatch_len<ZFused>(d.NZA, d, nf, q, Y2, Q2, pz, dct_tw, wz, cfl_bits, ke_partial, s);
 }
 void launch_inv_x(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s) {
   dispatch_len<InvX>(d.NXA, d, nf, Y1, Y2, px, s);
@@ -1608,15 +1888,21 @@ void launch_solve_real(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
   if (a.work2) {
     if (a.nblk > 0) {
       const int kv = a.kl + a.ku, grid = (a.nblk + kTpbThreads - 1) / kTpbThreads;
-      if (a.kl == 9 && kv == 23) {
-        const size_t sm = (size_t)kTpbThreads * 24 * sizeof(double2);
-        set_smem(k_subst_tpb<9, 23>, sm);
-        k_subst_tpb<9, 23><<<grid, kTpbThreads, sm, s>>>(a);
-      } else {
+      // band (kl, kl+ku) = (9, 23) of the plane-layer recipes compiled, any other
+      // band within (15, 31) through the run-time-band kernel
+#define CORAL_TPB_CASE(KL_, KV_)                                                     \
+  if (a.kl == KL_ && kv == KV_ && a.ldab == ((KL_ + KV_ + 2) & ~1)) {                 \
+    constexpr int LD_ = (KL_ + KV_ + 2) & ~1;                                         \
+    const size_t sm = (size_t)kTpbThreads * (KV_ + 1 > 16 ? KV_ + 1 : 16) * sizeof(double2); \
+    set_smem(k_subst_tpb<KL_, KV_, LD_>, sm);                                         \
+    k_subst_tpb<KL_, KV_, LD_><<<grid, kTpbThreads, sm, s>>>(a);                     \
+  } else
+      CORAL_TPB_CASE(9, 23) {
         const size_t sm = (size_t)kTpbThreads * 32 * sizeof(double2);
-        set_smem(k_subst_tpb<15, 31>, sm);
-        k_subst_tpb<15, 31><<<grid, kTpbThreads, sm, s>>>(a);
+        set_smem(k_subst_tpb_rt<15, 31>, sm);
+        k_subst_tpb_rt<15, 31><<<grid, kTpbThreads, sm, s>>>(a);
       }
+#undef CORAL_TPB_CASE
     }
     if (a.nact > 0) k_kstd_out<<<a.nact, kRhsThreads, smx, s>>>(a);
     return;
