@@ -123,7 +123,7 @@ struct coral_handle {
   int nF = 0, nQ = 0, nact = 0;
   int* d_act_index = nullptr;
   int* d_act_list = nullptr;
-  double *d_kx = nullptr, *d_ky = nullptr, *d_wz = nullptr;
+  double *d_kx = nullptr, *d_ky = nullptr, *d_wz = nullptr, *d_wzinv = nullptr;
   FftPlan py{}, px{}, pz{};
   double2* dct_tw = nullptr;
   FullVarDev* d_fv = nullptr;
@@ -234,6 +234,11 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
   h->d_kx = mem.upload(g.kx);
   h->d_ky = mem.upload(g.ky);
   h->d_wz = mem.upload(g.zweights());
+  {
+    std::vector<double> wi = g.zweights();
+    for (double& w : wi) w = 1.0 / w;
+    h->d_wzinv = mem.upload(wi);
+  }
   std::vector<int> act_index(nsys, -1), act_list;
   for (int ix = 0; ix < g.NXH; ++ix)
     for (int iy = 0; iy < g.NYAA; ++iy)
@@ -507,7 +512,7 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
     // quadratic variables overwrite Y2 in place, each CTA reading and writing only
     // its own (y, x pair) columns
     B(3);
-    launch_z_fused(d, h->nF, h->quads, h->Y2, h->Y2, h->pz, h->dct_tw, h->d_wz, h->cfl_bits,
+    launch_z_fused(d, h->nF, h->quads, h->Y2, h->Y2, h->pz, h->dct_tw, h->d_wz, h->d_wzinv, h->cfl_bits,
                    i == 0 ? h->ke_partial : nullptr, h->stream);
     E();
     B(4); launch_fwd_x(d, h->nQ, h->Y2, h->Y1, h->px, h->stream); E();

@@ -72,10 +72,11 @@ void launch_fwd_z(const Dims& d, int nf, const QuadDesc& q, const double* phys, 
                   const double2* dct_tw, const double* wz, double* ke_partial, cudaStream_t s);
 // the z passes of a timestep stage fused: z DCT-III of the nf full variables from
 // Y2, CFL maxima (cfl_bits, when non-null), products, KE partial averages (when
-// ke_partial is non-null) and z DCT-II of the quadratic variables into Q2
+// ke_partial is non-null) and z DCT-II of the quadratic variables into Q2;
+// wzinv[z] = 1 / wz[z]
 void launch_z_fused(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* Q2, const FftPlan& pz,
-                    const double2* dct_tw, const double* wz, unsigned long long* cfl_bits, double* ke_partial,
-                    cudaStream_t s);
+                    const double2* dct_tw, const double* wz, const double* wzinv, unsigned long long* cfl_bits,
+                    double* ke_partial, cudaStream_t s);
 void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s);
 void launch_fwd_y(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
                   cudaStream_t s);

@@ -307,29 +307,34 @@ constexpr int kFC = 4;  // full variables per inverse FFT batch
 
 template <int NF>
 __global__ void __launch_bounds__(kThreads, kMinBlocksZF) k_z_fused(Dims d, int nf, QuadDesc q, const double* Y2,
-                                                                    double* Q2, FftPlan pz, const double2* dct_tw,
-                                                                    const double* wz, unsigned long long* cfl_bits,
-                                                                    double* ke_partial) {
+                                                                     double* Q2, FftPlan pz, const double2* dct_tw,
+                                                                     const double* wz, const double* wzinv,
+                                                                     unsigned long long* cfl_bits, double* ke_partial) {
   extern __shared__ double2 sm[];
   __shared__ double red[3][kThreads / 32];
+  __shared__ int qv[2][kMaxQuad];
   const int x0 = blockIdx.x * 2, y = blockIdx.y;
-  const int N = NF ? NF : d.NZA, nq = q.nq, nb = min(nq, kQC);
+  // compiled lengths: NZAA = 3 NZ / 2 (the launcher checks it)
+  const int N = NF ? NF : d.NZA, NZ = NF ? 2 * NF / 3 : d.NZ;
+  const int nq = q.nq, nb = min(nq, kQC);
   const bool has_b = x0 + 1 < d.NXA;
+  const size_t vstride = (size_t)d.NYA * d.NXA * NZ;  // between variables of Y2 / Q2
+  const size_t col0 = ((size_t)y * d.NXA + x0) * NZ;  // column x0 of variable 0
+  if (threadIdx.x < kMaxQuad) {
+    qv[0][threadIdx.x] = q.v1[threadIdx.x];
+    qv[1][threadIdx.x] = q.v2[threadIdx.x];
+  }
   double2* Fv = sm;          // nf lines: columns x0 (re) and x0+1 (im) of each full variable
   double2* A = sm + nf * N;  // nb lines of quadratic variables
   double2* B = A + nb * N;   // runtime plan only (max(kFC, kQC) lines)
   // ---- inverse: X_n and X_{N-n} of both columns, twiddled, packed as va + i vb ----
   for (int idx = threadIdx.x; idx < nf * N; idx += blockDim.x) {
     const int f = idx / N, n = idx - f * N;
-    const double* sa = Y2 + (((size_t)f * d.NYA + y) * d.NXA + x0) * d.NZ;
-    const double* sb = sa + d.NZ;
-    double a0 = 0, a1 = 0, b0 = 0, b1 = 0;
-    if (n < d.NZ) a0 = sa[n];
-    if (n > 0 && N - n < d.NZ) a1 = sa[N - n];
-    if (has_b) {
-      if (n < d.NZ) b0 = sb[n];
-      if (n > 0 && N - n < d.NZ) b1 = sb[N - n];
-    }
+    const double* sa = Y2 + f * vstride + col0;
+    const double* sb = sa + NZ;
+    const bool lo = n < NZ, hi = n > 0 && N - n < NZ;
+    const double a0 = lo ? sa[n] : 0.0, a1 = hi ? sa[N - n] : 0.0;
+    const double b0 = (lo && has_b) ? sb[n] : 0.0, b1 = (hi && has_b) ? sb[N - n] : 0.0;
     const double2 w = cconj(dct_tw[n]);  // exp(+i pi n / 2N)
     const double2 va = cmul(w, make_double2(a0, -a1));
     const double2 vb = cmul(w, make_double2(b0, -b1));
@@ -350,9 +355,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksZF) k_z_fused(Dims d, int 
     double mx[3] = {0.0, 0.0, 0.0};
     for (int idx = threadIdx.x; idx < ncf * N; idx += blockDim.x) {
       const int f = idx / N, m = idx - f * N;
-      const int z = (m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1;
       const double2 v = Fv[idx];
-      const double s = (f == 2) ? 1.0 / wz[z] : 1.0;
+      double s = 1.0;
+      if (f == 2) s = wzinv[(m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1];
       double a = fabs(v.x) * s;
       if (has_b) a = fmax(a, fabs(v.y) * s);
 #pragma unroll
@@ -378,35 +383,39 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksZF) k_z_fused(Dims d, int 
     const int nc = min(kQC, nq - q0);
     for (int idx = threadIdx.x; idx < nc * N; idx += blockDim.x) {
       const int qi = idx / N, m = idx - qi * N, qg = q0 + qi;
-      const int v1 = q.v1[qg], v2 = q.v2[qg];
+      const int v1 = qv[0][qg], v2 = qv[1][qg];
       double pa, pb;
-      if (v1 < 0) { pa = Fv[v2 * N + m].x; pb = Fv[v2 * N + m].y; }
-      else if (v2 < 0) { pa = Fv[v1 * N + m].x; pb = Fv[v1 * N + m].y; }
-      else {
+      if (v1 < 0 || v2 < 0) {
+        const double2 f1 = Fv[(v1 < 0 ? v2 : v1) * N + m];
+        pa = f1.x;
+        pb = f1.y;
+      } else {
         const double2 f1 = Fv[v1 * N + m], f2 = Fv[v2 * N + m];
         pa = f1.x * f2.x;
         pb = f1.y * f2.y;
       }
-      A[qi * N + m] = make_double2(pa, pb);
+      A[idx] = make_double2(pa, pb);
       if (ke_partial) {
         const int z = (m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1;
+#pragma unroll
         for (int j = 0; j < 3; ++j)
           if (q.ke_q[j] == qg) ke[j] += wz[z] * (pa + (has_b ? pb : 0.0));
       }
     }
     __syncthreads();
     const double2* R = fft_lines_n<NF, false, kThreads, kQC>(A, B, nc, N, pz);
-    for (int idx = threadIdx.x; idx < nc * d.NZ; idx += blockDim.x) {
-      const int qi = idx / d.NZ, n = idx - qi * d.NZ;
+    double* dst0 = Q2 + q0 * vstride + col0;
+    for (int idx = threadIdx.x; idx < nc * NZ; idx += blockDim.x) {
+      const int qi = idx / NZ, n = idx - qi * NZ;
       const double2 Z = R[qi * N + n];
-      const double2 Zc = cconj(R[qi * N + ((N - n) % N)]);
+      const double2 Zc = cconj(R[qi * N + (n == 0 ? 0 : N - n)]);
       const double2 va = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
       const double2 dd = csub(Z, Zc);
       const double2 vb = make_double2(0.5 * dd.y, -0.5 * dd.x);  // (Z - Zc) / 2i
       const double2 w = dct_tw[n];                                // exp(-i pi n / 2N)
-      double* dst = Q2 + (((size_t)(q0 + qi) * d.NYA + y) * d.NXA + x0) * d.NZ;
+      double* dst = dst0 + qi * vstride;
       dst[n] = 2.0 * (w.x * va.x - w.y * va.y);
-      if (has_b) dst[d.NZ + n] = 2.0 * (w.x * vb.x - w.y * vb.y);
+      if (has_b) dst[NZ + n] = 2.0 * (w.x * vb.x - w.y * vb.y);
     }
     __syncthreads();  // A is refilled by the next batch
   }
@@ -1592,22 +1601,28 @@ __global__ void k_zero_step(ZeroArgs a) {
     r = r + a.ch[i] * kh[t];
     b[t] = r;
   }
+  // band solve with the factors staged in shared memory; the updates of one
+  // column run across the lanes (each entry sees the same sequence of updates)
+  const int kl = z.kl, kv = z.kl + z.ku, ldab = z.ldab;
+  double* fab = smd + T;
+  for (int e = lane; e < T * ldab; e += 32) fab[e] = z.ab[e];
   __syncwarp();
-  if (lane == 0) {
-    const int kl = z.kl, kv = z.kl + z.ku, ldab = z.ldab;
-    for (int j = 0; j < T - 1; ++j) {
-      const int p = j + z.dpiv[j];
-      if (p != j) { double tmp = b[p]; b[p] = b[j]; b[j] = tmp; }
-      const int lm = min(kl, T - 1 - j);
-      for (int q = 1; q <= lm; ++q) b[j + q] -= z.ab[(size_t)j * ldab + kv + q] * b[j];
-    }
-    for (int j = T - 1; j >= 0; --j) {
-      const double bj = b[j] * z.ab[(size_t)j * ldab + kv];
-      b[j] = bj;
-      for (int q = 1; q <= kv && j - q >= 0; ++q) b[j - q] -= z.ab[(size_t)j * ldab + kv - q] * bj;
-    }
+  for (int j = 0; j < T - 1; ++j) {
+    const int p = j + z.dpiv[j];
+    if (lane == 0 && p != j) { const double tmp = b[p]; b[p] = b[j]; b[j] = tmp; }
+    __syncwarp();
+    const double bj = b[j];
+    const int lm = min(kl, T - 1 - j);
+    for (int q = 1 + lane; q <= lm; q += 32) b[j + q] -= fab[j * ldab + kv + q] * bj;
+    __syncwarp();
   }
-  __syncwarp();
+  for (int j = T - 1; j >= 0; --j) {
+    const double bj = b[j] * fab[j * ldab + kv];
+    __syncwarp();
+    if (lane == 0) b[j] = bj;
+    for (int q = 1 + lane; q <= kv && j - q >= 0; q += 32) b[j - q] -= fab[j * ldab + kv - q] * bj;
+    __syncwarp();
+  }
   double* out = a.last_stage ? z.field : z.aux;
   if (!a.last_stage)
     for (int t = lane; t < T; t += 32) z.Kstd[i][t] = ell_row_real(z.L, t, b);
@@ -1803,13 +1818,17 @@ struct FwdZ {
 template <int NF>
 struct ZFused {
   static void run(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* Q2, const FftPlan& pz,
-                  const double2* dct_tw, const double* wz, unsigned long long* cfl_bits, double* ke_partial,
-                  cudaStream_t s) {
+                  const double2* dct_tw, const double* wz, const double* wzinv, unsigned long long* cfl_bits,
+                  double* ke_partial, cudaStream_t s) {
+    if (NF != 0 && 3 * d.NZ != 2 * NF) {  // compiled lengths assume NZAA = 3 NZ / 2
+      ZFused<0>::run(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, s);
+      return;
+    }
     const size_t lines = (size_t)nf + std::min(q.nq, kQC) + (NF ? 0 : std::max(kFC, kQC));
     const size_t sm = lines * d.NZA * sizeof(double2);
     set_smem(k_z_fused<NF>, sm);
     dim3 g((d.NXA + 1) / 2, d.NYA);
-    k_z_fused<NF><<<g, kThreads, sm, s>>>(d, nf, q, Y2, Q2, pz, dct_tw, wz, cfl_bits, ke_partial);
+    k_z_fused<NF><<<g, kThreads, sm, s>>>(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial);
   }
 };
 template <int NF>
@@ -1837,9 +1856,9 @@ void launch_inv_y(const Dims& d, int nf, const FullVarDev* fv, StateSet st, cons
   dispatch_len<InvY>(d.NYA, d, nf, fv, st, plain_spec, kx, ky, Y1, py, s);
 }
 void launch_z_fused(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* Q2, const FftPlan& pz,
-                    const double2* dct_tw, const double* wz, unsigned long long* cfl_bits, double* ke_partial,
-                    cudaStream_t s) {
-  dispatch_len<ZFused>(d.NZA, d, nf, q, Y2, Q2, pz, dct_tw, wz, cfl_bits, ke_partial, s);
+                    const double2* dct_tw, const double* wz, const double* wzinv, unsigned long long* cfl_bits,
+                    double* ke_partial, cudaStream_t s) {
+  dispatch_len<ZFused>(d.NZA, d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, s);
 }
 void launch_inv_x(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s) {
   dispatch_len<InvX>(d.NXA, d, nf, Y1, Y2, px, s);
@@ -1926,9 +1945,10 @@ void launch_factor_real(const FactorArgs& a, cudaStream_t s) {
 }
 void launch_zero_step(const ZeroArgs& a, cudaStream_t s) {
   if (a.nsys <= 0) return;
-  int Tmax = 1;
-  for (int i = 0; i < a.nsys; ++i) Tmax = a.sys[i].T > Tmax ? a.sys[i].T : Tmax;
-  k_zero_step<<<a.nsys, 32, (size_t)Tmax * sizeof(double), s>>>(a);
+  size_t sm = 8;
+  for (int i = 0; i < a.nsys; ++i) sm = std::max(sm, (size_t)a.sys[i].T * (1 + a.sys[i].ldab) * sizeof(double));
+  set_smem(k_zero_step, sm);
+  k_zero_step<<<a.nsys, 32, sm, s>>>(a);
 }
 void launch_zero_factor(const ZeroArgs& a, cudaStream_t s) {
   if (a.nsys <= 0) return;
