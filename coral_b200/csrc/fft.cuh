@@ -285,6 +285,32 @@ __device__ __forceinline__ void fft_pass(double2* A, int nl, int LS, const doubl
   __syncthreads();
 }
 
+// The first pass (Ns = 1, no twiddles) with its inputs produced by ld(line, k)
+// (k = position in the line) instead of read from shared memory; it writes its
+// outputs in place into A, which nothing reads during the pass, so it needs no
+// barrier between loads and stores.
+template <int N, int R, bool INV, int NT, int NLMAX, class Load>
+__device__ __forceinline__ void fft_pass_first(double2* A, int nl, int LS, Load&& ld) {
+  constexpr int NB = N / R;
+  constexpr int BPT = (NLMAX * NB + NT - 1) / NT;
+  const int total = nl * NB;
+#pragma unroll
+  for (int i = 0; i < BPT; ++i) {
+    const int b = threadIdx.x + i * NT;
+    if (b < total) {
+      const int line = b / NB, j = b - line * NB;
+      double2 v[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = ld(line, j + r * NB);
+      dft<R, INV>(v);
+      double2* dl = A + line * LS + j * R;
+#pragma unroll
+      for (int r = 0; r < R; ++r) dl[r] = v[r];
+    }
+  }
+  __syncthreads();
+}
+
 template <int N, int S, int Ns, bool INV, int NT, int NLMAX>
 __device__ __forceinline__ void fft_passes(double2* A, int nl, int LS, const double2* tw) {
   constexpr PlanR P = make_planr(N);
@@ -299,6 +325,27 @@ __device__ __forceinline__ void fft_passes(double2* A, int nl, int LS, const dou
 // length NC in place in A (B unused), or the runtime plan (NC == 0) ping-ponging
 // through B.  Returns the buffer holding the result.  The caller synchronises
 // before (inputs written) and may read the result directly after.
+// The same with the inputs produced by ld(line, k) (see fft_pass_first); the
+// caller need not synchronise before.  Runtime plans stage the inputs in A first.
+template <int NC, bool INV, int NT, int NLMAX, class Load>
+__device__ __forceinline__ double2* fft_lines_ld(double2* A, double2* B, int nl, int LS, const FftPlan& p,
+                                                 Load&& ld) {
+  if constexpr (NC == 0) {
+    for (int idx = threadIdx.x; idx < nl * p.N; idx += blockDim.x) {
+      const int line = idx / p.N, k = idx - line * p.N;
+      A[line * LS + k] = ld(line, k);
+    }
+    __syncthreads();
+    return fft_lines<INV>(A, B, nl, LS, p);
+  } else {
+    constexpr PlanR P = make_planr(NC);
+    static_assert(P.nst > 0, "transform length must be 2^a 3^b");
+    fft_pass_first<NC, P.r[0], INV, NT, NLMAX>(A, nl, LS, ld);
+    fft_passes<NC, 1, P.r[0], INV, NT, NLMAX>(A, nl, LS, p.tw);
+    return A;
+  }
+}
+
 template <int NC, bool INV, int NT, int NLMAX>
 __device__ __forceinline__ double2* fft_lines_n(double2* A, double2* B, int nl, int LS, const FftPlan& p) {
   if constexpr (NC == 0) {

@@ -327,23 +327,23 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksZF) k_z_fused(Dims d, int 
   double2* Fv = sm;          // nf lines: columns x0 (re) and x0+1 (im) of each full variable
   double2* A = sm + nf * N;  // nb lines of quadratic variables
   double2* B = A + nb * N;   // runtime plan only (max(kFC, kQC) lines)
-  // ---- inverse: X_n and X_{N-n} of both columns, twiddled, packed as va + i vb ----
-  for (int idx = threadIdx.x; idx < nf * N; idx += blockDim.x) {
-    const int f = idx / N, n = idx - f * N;
-    const double* sa = Y2 + f * vstride + col0;
-    const double* sb = sa + NZ;
-    const bool lo = n < NZ, hi = n > 0 && N - n < NZ;
-    const double a0 = lo ? sa[n] : 0.0, a1 = hi ? sa[N - n] : 0.0;
-    const double b0 = (lo && has_b) ? sb[n] : 0.0, b1 = (hi && has_b) ? sb[N - n] : 0.0;
-    const double2 w = cconj(dct_tw[n]);  // exp(+i pi n / 2N)
-    const double2 va = cmul(w, make_double2(a0, -a1));
-    const double2 vb = cmul(w, make_double2(b0, -b1));
-    Fv[idx] = make_double2(va.x - vb.y, va.y + vb.x);
-  }
-  __syncthreads();
+  // ---- inverse: X_n and X_{N-n} of both columns, twiddled, packed as va + i vb,
+  //      produced inside the first FFT pass ----
+  __syncthreads();  // qv
   for (int f0 = 0; f0 < nf; f0 += kFC) {
     const int nl = min(kFC, nf - f0);
-    const double2* R = fft_lines_n<NF, true, kThreads, kFC>(Fv + f0 * N, B, nl, N, pz);
+    auto ld = [&](int line, int n) -> double2 {
+      const double* sa = Y2 + (f0 + line) * vstride + col0;
+      const double* sb = sa + NZ;
+      const bool lo = n < NZ, hi = n > 0 && N - n < NZ;
+      const double a0 = lo ? sa[n] : 0.0, a1 = hi ? sa[N - n] : 0.0;
+      const double b0 = (lo && has_b) ? sb[n] : 0.0, b1 = (hi && has_b) ? sb[N - n] : 0.0;
+      const double2 w = cconj(dct_tw[n]);  // exp(+i pi n / 2N)
+      const double2 va = cmul(w, make_double2(a0, -a1));
+      const double2 vb = cmul(w, make_double2(b0, -b1));
+      return make_double2(va.x - vb.y, va.y + vb.x);
+    };
+    const double2* R = fft_lines_ld<NF, true, kThreads, kFC>(Fv + f0 * N, B, nl, N, pz, ld);
     if (R != Fv + f0 * N) {  // runtime plan with the result in the scratch lines
       for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) Fv[f0 * N + idx] = R[idx];
       __syncthreads();
@@ -381,8 +381,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksZF) k_z_fused(Dims d, int 
   double ke[3] = {0.0, 0.0, 0.0};
   for (int q0 = 0; q0 < nq; q0 += kQC) {
     const int nc = min(kQC, nq - q0);
-    for (int idx = threadIdx.x; idx < nc * N; idx += blockDim.x) {
-      const int qi = idx / N, m = idx - qi * N, qg = q0 + qi;
+    // products formed inside the first FFT pass (and the KE sums on the way)
+    auto ld = [&](int qi, int m) -> double2 {
+      const int qg = q0 + qi;
       const int v1 = qv[0][qg], v2 = qv[1][qg];
       double pa, pb;
       if (v1 < 0 || v2 < 0) {
@@ -394,16 +395,15 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksZF) k_z_fused(Dims d, int 
         pa = f1.x * f2.x;
         pb = f1.y * f2.y;
       }
-      A[idx] = make_double2(pa, pb);
       if (ke_partial) {
         const int z = (m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1;
 #pragma unroll
         for (int j = 0; j < 3; ++j)
           if (q.ke_q[j] == qg) ke[j] += wz[z] * (pa + (has_b ? pb : 0.0));
       }
-    }
-    __syncthreads();
-    const double2* R = fft_lines_n<NF, false, kThreads, kQC>(A, B, nc, N, pz);
+      return make_double2(pa, pb);
+    };
+    const double2* R = fft_lines_ld<NF, false, kThreads, kQC>(A, B, nc, N, pz, ld);
     double* dst0 = Q2 + q0 * vstride + col0;
     for (int idx = threadIdx.x; idx < nc * NZ; idx += blockDim.x) {
       const int qi = idx / NZ, n = idx - qi * NZ;
