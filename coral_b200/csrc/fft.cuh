@@ -289,7 +289,10 @@ __device__ __forceinline__ void fft_pass(double2* A, int nl, int LS, const doubl
 // (k = position in the line) instead of read from shared memory; it writes its
 // outputs in place into A, which nothing reads during the pass, so it needs no
 // barrier between loads and stores.
-template <int N, int R, bool INV, int NT, int NLMAX, class Load>
+// LINE_FAST: consecutive threads take consecutive lines at the same position
+// (so that interleaved lines of a global array load together); otherwise
+// consecutive positions of one line.
+template <int N, int R, bool INV, int NT, int NLMAX, bool LINE_FAST, class Load>
 __device__ __forceinline__ void fft_pass_first(double2* A, int nl, int LS, Load&& ld) {
   constexpr int NB = N / R;
   constexpr int BPT = (NLMAX * NB + NT - 1) / NT;
@@ -298,7 +301,8 @@ __device__ __forceinline__ void fft_pass_first(double2* A, int nl, int LS, Load&
   for (int i = 0; i < BPT; ++i) {
     const int b = threadIdx.x + i * NT;
     if (b < total) {
-      const int line = b / NB, j = b - line * NB;
+      const int line = LINE_FAST ? b % nl : b / NB;
+      const int j = LINE_FAST ? b / nl : b - line * NB;
       double2 v[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) v[r] = ld(line, j + r * NB);
@@ -327,7 +331,7 @@ __device__ __forceinline__ void fft_passes(double2* A, int nl, int LS, const dou
 // before (inputs written) and may read the result directly after.
 // The same with the inputs produced by ld(line, k) (see fft_pass_first); the
 // caller need not synchronise before.  Runtime plans stage the inputs in A first.
-template <int NC, bool INV, int NT, int NLMAX, class Load>
+template <int NC, bool INV, int NT, int NLMAX, bool LINE_FAST = false, class Load>
 __device__ __forceinline__ double2* fft_lines_ld(double2* A, double2* B, int nl, int LS, const FftPlan& p,
                                                  Load&& ld) {
   if constexpr (NC == 0) {
@@ -340,7 +344,7 @@ __device__ __forceinline__ double2* fft_lines_ld(double2* A, double2* B, int nl,
   } else {
     constexpr PlanR P = make_planr(NC);
     static_assert(P.nst > 0, "transform length must be 2^a 3^b");
-    fft_pass_first<NC, P.r[0], INV, NT, NLMAX>(A, nl, LS, ld);
+    fft_pass_first<NC, P.r[0], INV, NT, NLMAX, LINE_FAST>(A, nl, LS, ld);
     fft_passes<NC, 1, P.r[0], INV, NT, NLMAX>(A, nl, LS, p.tw);
     return A;
   }

@@ -60,8 +60,10 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_inv_y(Dims d, const 
   const int NYA = NF ? NF : d.NYA, LS = NYA + kPadXY;
   double2* A = sm;
   double2* B = sm + kNB1 * LS;  // runtime plan only
-  for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
-    const int ln = idx % kNB1, iy = idx / kNB1, n = n0 + ln;
+  // the spectral build of (line ln = Chebyshev n0 + ln, ky index iy), produced
+  // inside the first FFT pass
+  auto ld = [&](int ln, int iy) -> double2 {
+    const int n = n0 + ln;
     double2 c = zero2();
     if (n < d.NZ) {
       if (plain_spec) {
@@ -99,10 +101,9 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_inv_y(Dims d, const 
         }
       }
     }
-    A[ln * LS + iy] = c;
-  }
-  __syncthreads();
-  const double2* R = fft_lines_n<NF, true, kThreads, kNB1>(A, B, kNB1, LS, py);
+    return c;
+  };
+  const double2* R = fft_lines_ld<NF, true, kThreads, kNB1, true>(A, B, kNB1, LS, py, ld);
   for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
     const int ln = idx % kNB1, y = idx / kNB1, n = n0 + ln;
     if (n < d.NZ) {
@@ -123,22 +124,23 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_inv_x(Dims d, const 
   const int NXA = NF ? NF : d.NXA, NP = kNB2 / 2, LS = NXA + kPadXY;
   double2* A = sm;
   double2* B = sm + NP * LS;  // runtime plan only
-  for (int idx = threadIdx.x; idx < NP * LS; idx += blockDim.x) A[idx] = zero2();
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < NP * d.NXH; idx += blockDim.x) {
-    const int m = idx % NP, kx = idx / NP, na = n0 + 2 * m;
-    const double2* src = Y1 + (((size_t)f * d.NYA + y) * d.NXH + kx) * d.NZ;
-    double2 a = (na < d.NZ) ? src[na] : zero2();
-    double2 b = (na + 1 < d.NZ) ? src[na + 1] : zero2();
-    if (kx == 0) {
-      A[m * LS] = make_double2(a.x, b.x);  // c2r reads only the real part of the DC term
-    } else {
-      A[m * LS + kx] = make_double2(a.x - b.y, a.y + b.x);        // a + i b
-      A[m * LS + NXA - kx] = make_double2(a.x + b.y, b.x - a.y);  // conj(a) + i conj(b)
-    }
-  }
-  __syncthreads();
-  const double2* R = fft_lines_n<NF, true, kThreads, kNB2 / 2>(A, B, NP, LS, px);
+  // position p of line m (Chebyshev pair na, na+1): the Hermitian extension of
+  // both coefficient rows packed as a + i b, zero padding in between; produced
+  // inside the first FFT pass
+  const double2* src0 = Y1 + ((size_t)f * d.NYA + y) * d.NXH * d.NZ;
+  auto ld = [&](int m, int p) -> double2 {
+    const int na = n0 + 2 * m;
+    const bool lo = p < d.NXH, hi = p > NXA - d.NXH;  // kx = p, or kx = NXA - p (conjugate)
+    if (!lo && !hi) return zero2();
+    const int kx = lo ? p : NXA - p;
+    const double2* src = src0 + (size_t)kx * d.NZ;
+    const double2 a = (na < d.NZ) ? src[na] : zero2();
+    const double2 b = (na + 1 < d.NZ) ? src[na + 1] : zero2();
+    if (p == 0) return make_double2(a.x, b.x);  // c2r reads only the real part of the DC term
+    return lo ? make_double2(a.x - b.y, a.y + b.x)    // a + i b
+              : make_double2(a.x + b.y, b.x - a.y);   // conj(a) + i conj(b)
+  };
+  const double2* R = fft_lines_ld<NF, true, kThreads, kNB2 / 2, true>(A, B, NP, LS, px, ld);
   for (int idx = threadIdx.x; idx < NP * NXA; idx += blockDim.x) {
     const int m = idx % NP, x = idx / NP, na = n0 + 2 * m;
     double2 z = R[m * LS + x];
@@ -444,13 +446,15 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_fwd_x(Dims d, const 
   const int NXA = NF ? NF : d.NXA, NP = kNB2 / 2, LS = NXA + kPadXY;
   double2* A = sm;
   double2* B = sm + NP * LS;  // runtime plan only
-  for (int idx = threadIdx.x; idx < NP * NXA; idx += blockDim.x) {
-    const int m = idx % NP, x = idx / NP, na = n0 + 2 * m;
-    const double* src = Q2 + (((size_t)qi * d.NYA + y) * NXA + x) * d.NZ;
-    A[m * LS + x] = make_double2(na < d.NZ ? src[na] : 0.0, na + 1 < d.NZ ? src[na + 1] : 0.0);
-  }
-  __syncthreads();
-  const double2* R = fft_lines_n<NF, false, kThreads, kNB2 / 2>(A, B, NP, LS, px);
+  // rows na, na+1 of column x packed as one complex value, produced inside the
+  // first FFT pass
+  const double* src0 = Q2 + ((size_t)qi * d.NYA + y) * NXA * d.NZ;
+  auto ld = [&](int m, int x) -> double2 {
+    const int na = n0 + 2 * m;
+    const double* src = src0 + (size_t)x * d.NZ;
+    return make_double2(na < d.NZ ? src[na] : 0.0, na + 1 < d.NZ ? src[na + 1] : 0.0);
+  };
+  const double2* R = fft_lines_ld<NF, false, kThreads, kNB2 / 2, true>(A, B, NP, LS, px, ld);
   for (int idx = threadIdx.x; idx < NP * d.NXH; idx += blockDim.x) {
     const int m = idx % NP, kx = idx / NP, na = n0 + 2 * m;
     const double2 Z = R[m * LS + kx];
@@ -476,17 +480,17 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_fwd_y(Dims d, const 
   const int NYA = NF ? NF : d.NYA, LS = NYA + kPadXY;
   double2* A = sm;
   double2* B = sm + kNB1 * LS;  // runtime plan only
-  for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
-    const int ln = idx % kNB1, y = idx / kNB1, n = n0 + ln;
+  // produced inside the first FFT pass
+  auto ld = [&](int ln, int y) -> double2 {
+    const int n = n0 + ln;
     double2 v = zero2();
     if (n < d.NZ) {
       v = Q1[(((size_t)qi * NYA + y) * d.NXH + kx) * d.NZ + n];
       if (n == 0) v = cscale(v, 0.5);
     }
-    A[ln * LS + y] = v;
-  }
-  __syncthreads();
-  const double2* R = fft_lines_n<NF, false, kThreads, kNB1>(A, B, kNB1, LS, py);
+    return v;
+  };
+  const double2* R = fft_lines_ld<NF, false, kThreads, kNB1, true>(A, B, kNB1, LS, py, ld);
   for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
     const int ln = idx % kNB1, ky = idx / kNB1, n = n0 + ln;
     if (n < d.NZ) qspec[(((size_t)qi * d.NXH + kx) * NYA + ky) * d.NZ + n] = cscale(R[ln * LS + ky], scale);
