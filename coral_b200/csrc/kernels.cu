@@ -29,6 +29,17 @@ constexpr int kPadXY = 2;  // line stride N + 2 in the x / y passes, whose loads
                            // walk 4 interleaved lines: 2 line + position hits 8 distinct
                            // 16-byte bank groups
 constexpr int kThreads = 256;
+// x / y passes: threads per CTA for nl lines of a compiled length N, the most
+// butterflies of any pass rounded up to whole warps (one butterfly per thread
+// per pass); 256 for the run-time plans
+__host__ __device__ constexpr int xy_threads(int N, int nl) {
+  if (N == 0) return 256;
+  const PlanR p = make_planr(N);
+  int m = 32;
+  for (int i = 0; i < p.nst; ++i) m = (nl * N / p.r[i] > m) ? nl * N / p.r[i] : m;
+  return (m + 31) / 32 * 32;
+}
+#define kThreadsXY xy_threads(NF, 4)
 // CTAs per SM the transform kernels are compiled for (caps their registers;
 // measured best at 384^2 x 192: 3 for the x / y passes, 4 for the z passes)
 constexpr int kMinBlocksXY = 3;
@@ -52,7 +63,7 @@ __device__ __forceinline__ double2 ipow(double k, int e) {
 //  c2r_transform steps 1-2 and the 0.5 of the x padding, transforms.f90:172-198)
 // ------------------------------------------------------------------------------
 template <int NF>
-__global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_inv_y(Dims d, const FullVarDev* fv, StateSet st,
+__global__ void __launch_bounds__(kThreadsXY, kMinBlocksXY) k_inv_y(Dims d, const FullVarDev* fv, StateSet st,
                                                      const double2* plain_spec, const double* kxv,
                                                      const double* kyv, double2* Y1, FftPlan py) {
   extern __shared__ double2 sm[];
@@ -103,7 +114,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_inv_y(Dims d, const 
     }
     return c;
   };
-  const double2* R = fft_lines_ld<NF, true, kThreads, kNB1, true>(A, B, kNB1, LS, py, ld);
+  const double2* R = fft_lines_ld<NF, true, kThreadsXY, kNB1, true>(A, B, kNB1, LS, py, ld);
   for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
     const int ln = idx % kNB1, y = idx / kNB1, n = n0 + ln;
     if (n < d.NZ) {
@@ -118,7 +129,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_inv_y(Dims d, const 
 // two real output lines per complex FFT
 // ------------------------------------------------------------------------------
 template <int NF>
-__global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_inv_x(Dims d, const double2* Y1, double* Y2, FftPlan px) {
+__global__ void __launch_bounds__(kThreadsXY, kMinBlocksXY) k_inv_x(Dims d, const double2* Y1, double* Y2, FftPlan px) {
   extern __shared__ double2 sm[];
   const int f = blockIdx.x, n0 = blockIdx.y * kNB2, y = blockIdx.z;
   const int NXA = NF ? NF : d.NXA, NP = kNB2 / 2, LS = NXA + kPadXY;
@@ -140,7 +151,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_inv_x(Dims d, const 
     return lo ? make_double2(a.x - b.y, a.y + b.x)    // a + i b
               : make_double2(a.x + b.y, b.x - a.y);   // conj(a) + i conj(b)
   };
-  const double2* R = fft_lines_ld<NF, true, kThreads, kNB2 / 2, true>(A, B, NP, LS, px, ld);
+  const double2* R = fft_lines_ld<NF, true, kThreadsXY, kNB2 / 2, true>(A, B, NP, LS, px, ld);
   for (int idx = threadIdx.x; idx < NP * NXA; idx += blockDim.x) {
     const int m = idx % NP, x = idx / NP, na = n0 + 2 * m;
     double2 z = R[m * LS + x];
@@ -440,7 +451,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksZF) k_z_fused(Dims d, int 
 // forward transform, pass 2: x r2c, keep kx < NX/2 (transforms.f90:255-267)
 // ------------------------------------------------------------------------------
 template <int NF>
-__global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_fwd_x(Dims d, const double* Q2, double2* Q1, FftPlan px) {
+__global__ void __launch_bounds__(kThreadsXY, kMinBlocksXY) k_fwd_x(Dims d, const double* Q2, double2* Q1, FftPlan px) {
   extern __shared__ double2 sm[];
   const int qi = blockIdx.x, n0 = blockIdx.y * kNB2, y = blockIdx.z;
   const int NXA = NF ? NF : d.NXA, NP = kNB2 / 2, LS = NXA + kPadXY;
@@ -454,7 +465,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_fwd_x(Dims d, const 
     const double* src = src0 + (size_t)x * d.NZ;
     return make_double2(na < d.NZ ? src[na] : 0.0, na + 1 < d.NZ ? src[na + 1] : 0.0);
   };
-  const double2* R = fft_lines_ld<NF, false, kThreads, kNB2 / 2, true>(A, B, NP, LS, px, ld);
+  const double2* R = fft_lines_ld<NF, false, kThreadsXY, kNB2 / 2, true>(A, B, NP, LS, px, ld);
   for (int idx = threadIdx.x; idx < NP * d.NXH; idx += blockDim.x) {
     const int m = idx % NP, kx = idx / NP, na = n0 + 2 * m;
     const double2 Z = R[m * LS + kx];
@@ -473,7 +484,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_fwd_x(Dims d, const 
 // 1/(NXAA NYAA NZAA) normalisation (transforms.f90:280-296)
 // ------------------------------------------------------------------------------
 template <int NF>
-__global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_fwd_y(Dims d, const double2* Q1, double2* qspec, double scale,
+__global__ void __launch_bounds__(kThreadsXY, kMinBlocksXY) k_fwd_y(Dims d, const double2* Q1, double2* qspec, double scale,
                                                      FftPlan py) {
   extern __shared__ double2 sm[];
   const int qi = blockIdx.x, n0 = blockIdx.y * kNB1, kx = blockIdx.z;
@@ -490,7 +501,7 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksXY) k_fwd_y(Dims d, const 
     }
     return v;
   };
-  const double2* R = fft_lines_ld<NF, false, kThreads, kNB1, true>(A, B, kNB1, LS, py, ld);
+  const double2* R = fft_lines_ld<NF, false, kThreadsXY, kNB1, true>(A, B, kNB1, LS, py, ld);
   for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
     const int ln = idx % kNB1, ky = idx / kNB1, n = n0 + ln;
     if (n < d.NZ) qspec[(((size_t)qi * d.NXH + kx) * NYA + ky) * d.NZ + n] = cscale(R[ln * LS + ky], scale);
@@ -1451,9 +1462,14 @@ __global__ void __launch_bounds__(kRhsThreads) k_rhs_nl(SolveArgs a, NLArgs n) {
   double2* fs = shr + nqz;   // state of this system
   {
     const size_t qstride = (size_t)a.d.NXH * a.d.NYA * NZ;  // between quad vars
-    for (int idx = threadIdx.x; idx < nqz; idx += kRhsThreads) {
-      const int q = idx / NZ, nn = idx - q * NZ;
-      qs[idx] = n.qspec[q * qstride + (size_t)sid * NZ + nn];
+    if (act) {
+      // flat index idx = q NZ + nn, advanced without a division per element
+      int q = threadIdx.x / NZ, nn = threadIdx.x - q * NZ;
+      for (int idx = threadIdx.x; idx < nqz; idx += kRhsThreads) {
+        qs[idx] = n.qspec[q * qstride + (size_t)sid * NZ + nn];
+        nn += kRhsThreads;
+        while (nn >= NZ) { nn -= NZ; ++q; }
+      }
     }
     const double2* field = a.field + base;
     for (int t = threadIdx.x; t < T; t += kRhsThreads) fs[t] = field[t];
@@ -1496,9 +1512,12 @@ __global__ void __launch_bounds__(kRhsThreads) k_rhs_nl(SolveArgs a, NLArgs n) {
         r = cadd(r, cmul(cms[cg >> 24], make_double2(v * xv.x, v * xv.y)));
       }
     }
-    for (int j = 0; j < a.nprev; ++j) {
-      r = cadd(r, cscale(a.Kstd[j][base + t], a.ca[j]));
-      r = cadd(r, cscale(a.Khat[j][base + t], a.ch[j]));
+#pragma unroll
+    for (int j = 0; j < kMaxStages - 1; ++j) {  // static indices into the argument arrays
+      if (j < a.nprev) {
+        r = cadd(r, cscale(a.Kstd[j][base + t], a.ca[j]));
+        r = cadd(r, cscale(a.Khat[j][base + t], a.ch[j]));
+      }
     }
     r = cadd(r, cscale(kh, a.ch[a.nprev]));
     if (act) {
@@ -1537,8 +1556,9 @@ __global__ void __launch_bounds__(kRhsThreads) k_kstd_out(SolveArgs a) {
   }
   if (a.work2) {
     // (j, class) pairs: the two classes of one j are adjacent 16-byte entries
-    for (int idx = threadIdx.x; idx < npos; idx += kRhsThreads) {
-      const int j = idx / a.ncls, c = idx - j * a.ncls, bb = aidx * a.ncls + c;
+    // (the thread-per-block layout always has two classes)
+    for (int idx = threadIdx.x; idx < 2 * Tc; idx += kRhsThreads) {
+      const int j = idx >> 1, c = idx & 1, bb = 2 * aidx + c;
       xs[c * Tc + j] = a.work2[((size_t)(bb >> 5) * Tc + j) * 32 + (bb & 31)];
     }
   } else {
@@ -1787,7 +1807,7 @@ struct InvY {
     size_t sm = (NF ? 1 : 2) * kNB1 * (size_t)(d.NYA + kPadXY) * sizeof(double2);
     set_smem(k_inv_y<NF>, sm);
     dim3 g(nf, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
-    k_inv_y<NF><<<g, kThreads, sm, s>>>(d, fv, st, plain_spec, kx, ky, Y1, py);
+    k_inv_y<NF><<<g, kThreadsXY, sm, s>>>(d, fv, st, plain_spec, kx, ky, Y1, py);
   }
 };
 template <int NF>
@@ -1796,7 +1816,7 @@ struct InvX {
     size_t sm = (NF ? 1 : 2) * (kNB2 / 2) * (size_t)(d.NXA + kPadXY) * sizeof(double2);
     set_smem(k_inv_x<NF>, sm);
     dim3 g(nf, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
-    k_inv_x<NF><<<g, kThreads, sm, s>>>(d, Y1, Y2, px);
+    k_inv_x<NF><<<g, kThreadsXY, sm, s>>>(d, Y1, Y2, px);
   }
 };
 template <int NF>
@@ -1841,7 +1861,7 @@ struct FwdX {
     size_t sm = (NF ? 1 : 2) * (kNB2 / 2) * (size_t)(d.NXA + kPadXY) * sizeof(double2);
     set_smem(k_fwd_x<NF>, sm);
     dim3 g(nq, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
-    k_fwd_x<NF><<<g, kThreads, sm, s>>>(d, Q2, Q1, px);
+    k_fwd_x<NF><<<g, kThreadsXY, sm, s>>>(d, Q2, Q1, px);
   }
 };
 template <int NF>
@@ -1851,7 +1871,7 @@ struct FwdY {
     size_t sm = (NF ? 1 : 2) * kNB1 * (size_t)(d.NYA + kPadXY) * sizeof(double2);
     set_smem(k_fwd_y<NF>, sm);
     dim3 g(nq, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
-    k_fwd_y<NF><<<g, kThreads, sm, s>>>(d, Q1, qspec, scale, py);
+    k_fwd_y<NF><<<g, kThreadsXY, sm, s>>>(d, Q1, qspec, scale, py);
   }
 };
 
