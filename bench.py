@@ -39,7 +39,8 @@ CONFIGS = {
                             NX=192, NY=192, NZ=96, dt=5e-6, seed=1, Ra=5e7),
 }
 METRIC = "timesteps/s at 384^2x192 (FP64 path)"
-PHASES = ("inv_y", "inv_x", "inv_z", "z_products", "fwd_x", "fwd_y", "nl_assembly", "solve", "mean_systems")
+PHASES = ("inv_y", "inv_x", "inv_z", "z_products", "fwd_x", "fwd_y", "nl_assembly", "rhs_nl", "mean_systems",
+          "substitution", "kstd_out")
 
 
 def dist_env():
@@ -133,7 +134,7 @@ def make_ic(cfg, pl):
 PHASE_KERNELS = {
     "inv_y": "k_inv_y", "inv_x": "k_inv_x", "inv_z": "k_inv_z", "z_products": "k_z_fused",
     "fwd_x": "k_fwd_x", "fwd_y": "k_fwd_y", "nl_assembly": "k_nl",
-    "solve": "k_rhs_nl + k_subst_real + k_kstd_out", "mean_systems": "k_zero_step",
+    "rhs_nl": "k_rhs_nl", "mean_systems": "k_zero_step", "substitution": "k_subst_tpb", "kstd_out": "k_kstd_out",
 }
 
 
@@ -158,16 +159,24 @@ def phase_bytes(g, nsys, nact, T, ncls, Tc, kl, ku, stages, factor_bytes):
         "fwd_x": y2(nQ) + y1(nQ),
         "fwd_y": y1(nQ) + y1(nQ),
     }
-    # solve: LU factors (2 kl + ku + 1 band entries per column of each block,
-    # plus one pivot byte) and quadratic-variable coefficients of the active
-    # systems; for every system the state read, the K arrays read and written
-    # and the outputs
-    tot = 0
+    # the solve, kernel by kernel, averaged over the stages (stage i reads the
+    # K arrays of the i earlier stages; the last stage writes no K_std):
+    #   rhs_nl: state, K arrays and quadratic coefficients in, K_hat and the
+    #     right-hand side (inactive systems: the stage output) out
+    #   substitution: LU factors (2 kl + ku + 1 band entries and one pivot byte
+    #     per column of each block) and the block vectors (right-hand side in,
+    #     intermediate out and in, solution out)
+    #   kstd_out: solution in, stage output and K_std out (active systems)
+    rhs = sub = kst = 0
+    nblk_cols = nact * ncls * Tc
     for i in range(stages):
         last = (i == stages - 1)
-        per_sys = 16 * T * (1 + 2 * i + 1 + 1 + (0 if last else 1))
-        tot += nsys * per_sys + nact * (ncls * Tc * (factor_bytes * (2 * kl + ku + 1) + 1) + 16 * nQ * NZ)
-    out["solve"] = tot / stages
+        rhs += nsys * 16 * T * (1 + 2 * i + 1 + 1) + nact * 16 * nQ * NZ + (nsys - nact) * 16 * T * (0 if last else 1)
+        sub += nblk_cols * (factor_bytes * (2 * kl + ku + 1) + 1) + 4 * 16 * nblk_cols
+        kst += 16 * nblk_cols + nact * 16 * T * (1 if last else 2)
+    out["rhs_nl"] = rhs / stages
+    out["substitution"] = sub / stages
+    out["kstd_out"] = kst / stages
     return out
 
 
@@ -339,13 +348,41 @@ def read_traffic(kernels):
     return None
 
 
-def cpu_baseline(cfg, eq, par, max_seconds=20.0, processes=1):
+def _solve_worker(job):
+    """Repeated zgbtrs on the sampled factors for about `seconds`; returns the
+    number of solves (runs in a spawned process of the CPU baseline)."""
+    facs, kl, ku, b, seconds = job
+    import time as _t
+    import scipy.linalg.lapack as _lapack
+    n = 0
+    t0 = _t.perf_counter()
+    while _t.perf_counter() - t0 < seconds:
+        for lu, piv in facs:
+            _lapack.zgbtrs(lu, kl, ku, b, piv)
+        n += len(facs)
+    return n
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(cfg, eq, par, max_seconds=20.0, processes=None):
     """The oracle (CPU restatement, FP64) timed on a bounded sample of the same
-    workload: one inverse and one forward 3-D transform at full size, the band
-    LU solves of a sample of (kx,ky) systems and the operator applications of a
-    sample of kx slabs; the step time is extrapolated to the full step."""
+    workload with `processes` host threads (default: all): one inverse and one
+    forward 3-D transform at full size (scipy.fft workers), the band LU solves
+    of a sample of (kx,ky) systems and the operator applications of a sample of
+    kx slabs (a spawned process pool for the solves, a thread pool for the
+    sparse products), as throughput; the step time is extrapolated to the full
+    step.""" 
+    from concurrent.futures import ThreadPoolExecutor
     from oracle import coral_oracle as co
+    import scipy.fft as sfft
     import scipy.linalg.lapack as lapack
+    processes = processes or host_threads()
     t_start = time.perf_counter()
     s = co.Solver.__new__(co.Solver)
     s.recipe = co.parse_equations(eq)
@@ -366,12 +403,13 @@ def cpu_baseline(cfg, eq, par, max_seconds=20.0, processes=1):
     rng = np.random.default_rng(0)
     # (a) transforms at full size
     spec = rng.standard_normal((g.NXH, g.NYAA, g.NZ)) + 1j * rng.standard_normal((g.NXH, g.NYAA, g.NZ))
-    t0 = time.perf_counter()
-    ph = co.spec_to_phys(spec, g)
-    t_inv = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    co.phys_to_spec(ph * ph, g)
-    t_fwd = time.perf_counter() - t0
+    with sfft.set_workers(processes):
+        t0 = time.perf_counter()
+        ph = co.spec_to_phys(spec, g)
+        t_inv = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        co.phys_to_spec(ph * ph, g)
+        t_fwd = time.perf_counter() - t0
     del ph, spec
     # (b) band LU solve per system: factor a handful, time zgbtrs on them
     kl = ku = 0
@@ -393,26 +431,34 @@ def cpu_baseline(cfg, eq, par, max_seconds=20.0, processes=1):
         lu, piv, info = lapack.zgbtrf(ab, kl, ku)
         facs.append((lu, piv))
     b = rng.standard_normal(T) + 1j * rng.standard_normal(T)
-    reps = 0
-    t0 = time.perf_counter()
-    while True:
-        for lu, piv in facs:
-            lapack.zgbtrs(lu, kl, ku, b, piv)
-        reps += 1
-        if time.perf_counter() - t0 > 1.0:
-            break
-    t_solve = (time.perf_counter() - t0) / (reps * nsample)
-    # (c) mass / stiffness applications on one kx slab
+
     X = (rng.standard_normal((g.NYAA, T)) + 1j * rng.standard_normal((g.NYAA, T)))
-    t0 = time.perf_counter()
-    for _, B in mass + stif:
-        (B @ X.T)
-    t_mv = (time.perf_counter() - t0) / g.NYAA
+
+    def mv_slab(_):
+        for _, B in mass + stif:
+            (B @ X.T)
+
+    if processes > 1:
+        # band solves in a spawned process pool (the LAPACK wrapper holds the
+        # interpreter lock): total solves of all workers over the wall time
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(processes) as pp:
+            pp.map(_solve_worker, [(facs[:1], kl, ku, b, 0.0)] * processes)  # start the workers
+            t0 = time.perf_counter()
+            counts = pp.map(_solve_worker, [(facs, kl, ku, b, 2.0)] * processes)
+            t_solve = (time.perf_counter() - t0) / sum(counts)
+    else:
+        t_solve = 2.0 / _solve_worker((facs, kl, ku, b, 2.0))
+    with ThreadPoolExecutor(processes) as pool:
+        # (c) mass / stiffness applications, one kx slab per task
+        t0 = time.perf_counter()
+        list(pool.map(mv_slab, range(processes)))
+        t_mv = (time.perf_counter() - t0) / (processes * g.NYAA)
     nsys = g.NXH * g.NYAA
     nact = int(g.active.sum())
     step = s.nstages * (nF * t_inv + nQ * t_fwd + nact * t_solve + nsys * t_mv)
     return {"value": 1.0 / step, "unit": "timesteps/s", "cores": processes, "kind": "port",
-            "sample": ("oracle (numpy/scipy FP64, %d thread) timed on: 1 inverse + 1 forward 3-D transform at "
+            "sample": ("oracle (numpy/scipy FP64, %d host threads) timed on: 1 inverse + 1 forward 3-D transform at "
                        "%dx%dx%d, zgbtrs on %d of the %d (kx,ky) systems (T=%d, kl=%d, ku=%d), M/L applications "
                        "on one kx slab; extrapolated to %d stages x (%d inverse + %d forward transforms + %d solves "
                        "+ %d operator applications); sample took %.1f s"

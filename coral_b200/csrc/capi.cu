@@ -478,6 +478,8 @@ int full_vars_to_phys(coral_handle* h, bool use_field, bool cfl) {
   return 3;
 }
 
+constexpr int kProfileClasses = 11;  // coral_profile_step
+
 struct PhaseTimer {
   cudaStream_t s;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev;
@@ -579,7 +581,9 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
         sa.ring_cols = k.ncls * std::max(u_rows, l_rows);
       }
       if (k.real) {
-        B(7); launch_solve_real(sa, na, h->stream); E();
+        B(7); launch_rhs_nl(sa, na, h->stream); E();
+        B(9); launch_subst(sa, h->stream); E();
+        B(10); launch_kstd_out(sa, h->stream); E();
         nl += 3;
       } else {
         B(6); launch_nl(na, h->stream); E();
@@ -1120,7 +1124,7 @@ int coral_stream(coral_handle* h, void** stream) {
 
 int coral_profile_step(coral_handle* h, double dt, double* ms, int n) {
   return guarded(h, [&] {
-    if (!ms || n < 9) throw CoralError(CORAL_EBADARG, "need 9 timing slots");
+    if (!ms || n < kProfileClasses) throw CoralError(CORAL_EBADARG, "need 11 timing slots");
     if (!(dt > 0.0)) throw CoralError(CORAL_EBADARG, "dt must be > 0");
     if (h->dt_factored != dt) factorize(h, dt);
     PhaseTimer pt{h->stream, {}};

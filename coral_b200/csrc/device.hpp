@@ -144,6 +144,10 @@ void launch_solve(const SolveArgs& a, cudaStream_t s);
 // kl+ku <= 31 per class): right-hand side with the NL assembly fused in,
 // substitutions, then K_std and outputs (three kernels)
 void launch_solve_real(const SolveArgs& a, const NLArgs& n, cudaStream_t s);
+// its three kernels one by one
+void launch_rhs_nl(const SolveArgs& a, const NLArgs& n, cudaStream_t s);
+void launch_subst(const SolveArgs& a, cudaStream_t s);
+void launch_kstd_out(const SolveArgs& a, cudaStream_t s);
 
 struct FactorArgs {
   Dims d;

@@ -1919,15 +1919,14 @@ void launch_factor(const FactorArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;
   k_factor<<<(a.nact + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
 }
-void launch_solve_real(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
+void launch_rhs_nl(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
   const int nsys = a.d.NXH * a.d.NYA;
-  {
-    const size_t sm = ((size_t)n.nq * a.d.NZ + a.T) * sizeof(double2);
-    set_smem(k_rhs_nl, sm);
-    k_rhs_nl<<<nsys, kRhsThreads, sm, s>>>(a, n);
-  }
-  const size_t smx = (size_t)a.ncls * a.Tc * sizeof(double2);
-  if (smx > 48 * 1024) set_smem(k_kstd_out, smx);
+  const size_t sm = ((size_t)n.nq * a.d.NZ + a.T) * sizeof(double2);
+  set_smem(k_rhs_nl, sm);
+  k_rhs_nl<<<nsys, kRhsThreads, sm, s>>>(a, n);
+}
+void launch_subst(const SolveArgs& a, cudaStream_t s) {
+  if (a.nact <= 0) return;
   if (a.work2) {
     if (a.nblk > 0) {
       const int kv = a.kl + a.ku, grid = (a.nblk + kTpbThreads - 1) / kTpbThreads;
@@ -1947,16 +1946,23 @@ void launch_solve_real(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
       }
 #undef CORAL_TPB_CASE
     }
-    if (a.nact > 0) k_kstd_out<<<a.nact, kRhsThreads, smx, s>>>(a);
     return;
   }
   // whole systems (no class split): one warp per system
-  if (a.nact > 0) {
-    const size_t sm = (size_t)kWPBr * kNBUF * kCW * a.ring_cols * sizeof(double);
-    set_smem(k_subst_real<32>, sm);
-    k_subst_real<32><<<(a.nact + kWPBr - 1) / kWPBr, kWPBr * 32, sm, s>>>(a);
-    k_kstd_out<<<a.nact, kRhsThreads, smx, s>>>(a);
-  }
+  const size_t sm = (size_t)kWPBr * kNBUF * kCW * a.ring_cols * sizeof(double);
+  set_smem(k_subst_real<32>, sm);
+  k_subst_real<32><<<(a.nact + kWPBr - 1) / kWPBr, kWPBr * 32, sm, s>>>(a);
+}
+void launch_kstd_out(const SolveArgs& a, cudaStream_t s) {
+  if (a.nact <= 0) return;
+  const size_t smx = (size_t)a.ncls * a.Tc * sizeof(double2);
+  if (smx > 48 * 1024) set_smem(k_kstd_out, smx);
+  k_kstd_out<<<a.nact, kRhsThreads, smx, s>>>(a);
+}
+void launch_solve_real(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
+  launch_rhs_nl(a, n, s);
+  launch_subst(a, s);
+  launch_kstd_out(a, s);
 }
 void launch_factor_real(const FactorArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;

@@ -172,7 +172,8 @@ class PlaneLayer:
         self._check(self._lib.coral_stream(self._h, ctypes.byref(v)))
         return v.value or 0
 
-    PHASES = ("inv_y", "inv_x", "inv_z", "z_products", "fwd_x", "fwd_y", "nl_assembly", "solve", "mean_systems")
+    PHASES = ("inv_y", "inv_x", "inv_z", "z_products", "fwd_x", "fwd_y", "nl_assembly", "rhs_nl", "mean_systems",
+              "substitution", "kstd_out")
 
     def profile_step(self, dt):
         """One eager step with CUDA events per kernel class; returns {phase: ms}."""

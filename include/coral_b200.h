@@ -163,9 +163,10 @@ int coral_stream(coral_handle* h, void** stream);
  * kernel class; ms[k] receives the device time of class k summed over the
  * stages (k = 0 inverse y pass, 1 inverse x pass, 2 inverse z pass (0: fused
  * into class 3), 3 z passes with the products (inverse z, CFL maxima, products,
- * forward z), 4 forward x pass, 5 forward y pass, 6 NL assembly (0: fused into
- * class 7), 7 right-hand side + NL assembly + banded solve + K_std, 8 mean
- * systems).  n >= 9.
+ * forward z), 4 forward x pass, 5 forward y pass, 6 NL assembly (complex
+ * factors only), 7 right-hand side with the NL assembly (real-scaled factors)
+ * or stage update + banded solve (complex factors), 8 mean systems,
+ * 9 banded substitutions, 10 K_std and stage output).  n >= 11.
  * The step advances the state exactly like coral_march(h, dt, 1).
  * (The reference has wall-clock prints only, plane_layer_main.f90:166-171.)
  */
