@@ -79,7 +79,7 @@ struct KSys {
   // class split of the real-scaled solve (SystemOps::ncls == 2); when unsplit:
   // ncls = 1, Tc = T, the band (kl_s, ku_s, ldab_s) of the whole system, work = aux
   int ncls = 1, Tc = 0, kl_s = 0, ku_s = 0, ldab_s = 0, wst = 0;
-  int *row_pos = nullptr, *col_pos = nullptr, *cls_row = nullptr;
+  int *row_pos = nullptr, *col_pos = nullptr, *cls_row = nullptr, *cls_col = nullptr;
   unsigned char* colflip_cls = nullptr;
   DevEll Lp;
   double2* work = nullptr;
@@ -316,6 +316,11 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
       k.row_pos = mem.upload(k.ops.row_cls_pos);
       k.col_pos = mem.upload(k.ops.col_cls_pos);
       k.cls_row = mem.upload(k.ops.cls_row);
+      {
+        std::vector<int> cc(2 * (size_t)k.Tc, -1);  // class position -> variable column
+        for (int t = 0; t < k.T; ++t) cc[k.ops.col_cls_pos[t]] = t;
+        k.cls_col = mem.upload(cc);
+      }
       std::vector<unsigned char> cf(2 * (size_t)k.Tc, 0);
       for (int t = 0; t < k.T; ++t) cf[k.ops.col_cls_pos[t]] = k.ops.col_flip[t];
       k.colflip_cls = mem.upload(cf);
@@ -575,6 +580,7 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       sa.Lp = k.Lp;
       sa.work2 = k.work2;
       sa.nblk = k.ncls * h->nact;
+      sa.cls_col = k.cls_col;
       {
         const int kv = sa.kl + sa.ku;
         const int u_rows = (kv + 2) & ~1, l_rows = ((kv + 1 + sa.kl + 1) & ~1) - ((kv + 1) & ~1);

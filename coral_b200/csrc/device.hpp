@@ -138,6 +138,8 @@ struct SolveArgs {
   // systems work2[(g Tc + j) 32 + lane]; inactive systems stay in work
   double2* work2;        // null: warp-per-system layouts
   int nblk;              // ncls * nact
+  const int* cls_col;    // [ncls*Tc] variable column of a class position, -1 = padding: the
+                         // thread-per-block solve writes its solution straight into out
 };
 void launch_solve(const SolveArgs& a, cudaStream_t s);
 // real-scaled factors (unsplit: kl <= 31, kl+ku <= 63; class split: kl <= 15,

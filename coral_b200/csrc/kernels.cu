@@ -316,63 +316,84 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksZ) k_fwd_z(Dims d, int nf,
 // z = 2m, or 2(N-1-m)+1 for m >= N/2), which is the order the forward transform
 // takes, so the products are formed position by position.
 // ------------------------------------------------------------------------------
-constexpr int kFC = 4;  // full variables per inverse FFT batch
+
+// Threads of the fused z kernel for nl lines of a compiled length N: enough for
+// one butterfly per thread in the odd and radix-8/16 passes and two in the
+// radix-2/4 passes (N = 288, 8 lines: 288 threads, every pass balanced).
+__host__ __device__ constexpr int z_threads(int N, int nl) {
+  if (N == 0) return 256;
+  const PlanR p = make_planr(N);
+  int m = 32;
+  for (int i = 0; i < p.nst; ++i) {
+    const int b = nl * N / p.r[i], per = (p.r[i] <= 4) ? (b + 1) / 2 : b;
+    m = per > m ? per : m;
+  }
+  return (m + 31) / 32 * 32;
+}
+constexpr int kZPairs = 2;               // x-column pairs per CTA
+constexpr int kZLines = 4 * kZPairs;     // lines per FFT batch (4 full variables x 2 pairs)
+#define kThreadsZF z_threads(NF, kZLines)
 
 template <int NF>
-__global__ void __launch_bounds__(kThreads, kMinBlocksZF) k_z_fused(Dims d, int nf, QuadDesc q, const double* Y2,
-                                                                     double* Q2, FftPlan pz, const double2* dct_tw,
-                                                                     const double* wz, const double* wzinv,
-                                                                     unsigned long long* cfl_bits, double* ke_partial) {
+__global__ void __launch_bounds__(kThreadsZF, kMinBlocksZF) k_z_fused(Dims d, int nf, QuadDesc q, const double* Y2,
+                                                                       double* Q2, FftPlan pz, const double2* dct_tw,
+                                                                       const double* wz, const double* wzinv,
+                                                                       unsigned long long* cfl_bits, double* ke_partial) {
+  constexpr int NT = kThreadsZF;
   extern __shared__ double2 sm[];
-  __shared__ double red[3][kThreads / 32];
+  __shared__ double red[3][(NT + 31) / 32];
   __shared__ int qv[2][kMaxQuad];
-  const int x0 = blockIdx.x * 2, y = blockIdx.y;
+  const int x0 = blockIdx.x * 2 * kZPairs, y = blockIdx.y;
   // compiled lengths: NZAA = 3 NZ / 2 (the launcher checks it)
   const int N = NF ? NF : d.NZA, NZ = NF ? 2 * NF / 3 : d.NZ;
-  const int nq = q.nq, nb = min(nq, kQC);
-  const bool has_b = x0 + 1 < d.NXA;
+  const int nq = q.nq;
   const size_t vstride = (size_t)d.NYA * d.NXA * NZ;  // between variables of Y2 / Q2
   const size_t col0 = ((size_t)y * d.NXA + x0) * NZ;  // column x0 of variable 0
   if (threadIdx.x < kMaxQuad) {
     qv[0][threadIdx.x] = q.v1[threadIdx.x];
     qv[1][threadIdx.x] = q.v2[threadIdx.x];
   }
-  double2* Fv = sm;          // nf lines: columns x0 (re) and x0+1 (im) of each full variable
-  double2* A = sm + nf * N;  // nb lines of quadratic variables
-  double2* B = A + nb * N;   // runtime plan only (max(kFC, kQC) lines)
+  // line l of a batch: variable l / kZPairs, column pair l % kZPairs (columns
+  // x0 + 2p (re) and x0 + 2p + 1 (im))
+  auto col_ok = [&](int c) { return x0 + c < d.NXA; };
+  double2* Fv = sm;                   // nf * kZPairs lines of the full variables
+  double2* A = Fv + nf * kZPairs * N; // kZLines lines of quadratic variables
+  double2* B = A + kZLines * N;       // runtime plan only (kZLines lines)
   // ---- inverse: X_n and X_{N-n} of both columns, twiddled, packed as va + i vb,
   //      produced inside the first FFT pass ----
   __syncthreads();  // qv
-  for (int f0 = 0; f0 < nf; f0 += kFC) {
-    const int nl = min(kFC, nf - f0);
+  for (int l0 = 0; l0 < nf * kZPairs; l0 += kZLines) {
+    const int nl = min(kZLines, nf * kZPairs - l0);
     auto ld = [&](int line, int n) -> double2 {
-      const double* sa = Y2 + (f0 + line) * vstride + col0;
+      const int lg = l0 + line, f = lg / kZPairs, pr = lg - f * kZPairs;
+      const bool ha = col_ok(2 * pr), hb = col_ok(2 * pr + 1);
+      const double* sa = Y2 + f * vstride + col0 + (size_t)(2 * pr) * NZ;
       const double* sb = sa + NZ;
       const bool lo = n < NZ, hi = n > 0 && N - n < NZ;
-      const double a0 = lo ? sa[n] : 0.0, a1 = hi ? sa[N - n] : 0.0;
-      const double b0 = (lo && has_b) ? sb[n] : 0.0, b1 = (hi && has_b) ? sb[N - n] : 0.0;
+      const double a0 = (lo && ha) ? sa[n] : 0.0, a1 = (hi && ha) ? sa[N - n] : 0.0;
+      const double b0 = (lo && hb) ? sb[n] : 0.0, b1 = (hi && hb) ? sb[N - n] : 0.0;
       const double2 w = cconj(dct_tw[n]);  // exp(+i pi n / 2N)
       const double2 va = cmul(w, make_double2(a0, -a1));
       const double2 vb = cmul(w, make_double2(b0, -b1));
       return make_double2(va.x - vb.y, va.y + vb.x);
     };
-    const double2* R = fft_lines_ld<NF, true, kThreads, kFC>(Fv + f0 * N, B, nl, N, pz, ld);
-    if (R != Fv + f0 * N) {  // runtime plan with the result in the scratch lines
-      for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) Fv[f0 * N + idx] = R[idx];
+    const double2* R = fft_lines_ld<NF, true, NT, kZLines>(Fv + l0 * N, B, nl, N, pz, ld);
+    if (R != Fv + l0 * N) {  // runtime plan with the result in the scratch lines
+      for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) Fv[l0 * N + idx] = R[idx];
       __syncthreads();
     }
   }
-  // ---- CFL maxima of |u|, |v|, |w| / wz over both columns ----
+  // ---- CFL maxima of |u|, |v|, |w| / wz over all columns ----
   if (cfl_bits) {
     const int ncf = min(nf, 3);
     double mx[3] = {0.0, 0.0, 0.0};
-    for (int idx = threadIdx.x; idx < ncf * N; idx += blockDim.x) {
-      const int f = idx / N, m = idx - f * N;
+    for (int idx = threadIdx.x; idx < ncf * kZPairs * N; idx += blockDim.x) {
+      const int lg = idx / N, m = idx - lg * N, f = lg / kZPairs, pr = lg - f * kZPairs;
       const double2 v = Fv[idx];
       double s = 1.0;
       if (f == 2) s = wzinv[(m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1];
-      double a = fabs(v.x) * s;
-      if (has_b) a = fmax(a, fabs(v.y) * s);
+      double a = col_ok(2 * pr) ? fabs(v.x) * s : 0.0;
+      if (col_ok(2 * pr + 1)) a = fmax(a, fabs(v.y) * s);
 #pragma unroll
       for (int j = 0; j < 3; ++j)
         if (f == j) mx[j] = fmax(mx[j], a);
@@ -390,21 +411,21 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksZF) k_z_fused(Dims d, int 
     }
     __syncthreads();
   }
-  // ---- products and forward transforms, in batches of kQC quadratic variables ----
+  // ---- products and forward transforms, kZLines (quadratic variable, pair) lines a batch ----
   double ke[3] = {0.0, 0.0, 0.0};
-  for (int q0 = 0; q0 < nq; q0 += kQC) {
-    const int nc = min(kQC, nq - q0);
+  for (int l0 = 0; l0 < nq * kZPairs; l0 += kZLines) {
+    const int nc = min(kZLines, nq * kZPairs - l0);
     // products formed inside the first FFT pass (and the KE sums on the way)
-    auto ld = [&](int qi, int m) -> double2 {
-      const int qg = q0 + qi;
+    auto ld = [&](int line, int m) -> double2 {
+      const int lg = l0 + line, qg = lg / kZPairs, pr = lg - qg * kZPairs;
       const int v1 = qv[0][qg], v2 = qv[1][qg];
       double pa, pb;
       if (v1 < 0 || v2 < 0) {
-        const double2 f1 = Fv[(v1 < 0 ? v2 : v1) * N + m];
+        const double2 f1 = Fv[((v1 < 0 ? v2 : v1) * kZPairs + pr) * N + m];
         pa = f1.x;
         pb = f1.y;
       } else {
-        const double2 f1 = Fv[v1 * N + m], f2 = Fv[v2 * N + m];
+        const double2 f1 = Fv[(v1 * kZPairs + pr) * N + m], f2 = Fv[(v2 * kZPairs + pr) * N + m];
         pa = f1.x * f2.x;
         pb = f1.y * f2.y;
       }
@@ -412,23 +433,24 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksZF) k_z_fused(Dims d, int 
         const int z = (m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1;
 #pragma unroll
         for (int j = 0; j < 3; ++j)
-          if (q.ke_q[j] == qg) ke[j] += wz[z] * (pa + (has_b ? pb : 0.0));
+          if (q.ke_q[j] == qg)
+            ke[j] += wz[z] * ((col_ok(2 * pr) ? pa : 0.0) + (col_ok(2 * pr + 1) ? pb : 0.0));
       }
       return make_double2(pa, pb);
     };
-    const double2* R = fft_lines_ld<NF, false, kThreads, kQC>(A, B, nc, N, pz, ld);
-    double* dst0 = Q2 + q0 * vstride + col0;
+    const double2* R = fft_lines_ld<NF, false, NT, kZLines>(A, B, nc, N, pz, ld);
     for (int idx = threadIdx.x; idx < nc * NZ; idx += blockDim.x) {
-      const int qi = idx / NZ, n = idx - qi * NZ;
-      const double2 Z = R[qi * N + n];
-      const double2 Zc = cconj(R[qi * N + (n == 0 ? 0 : N - n)]);
+      const int li = idx / NZ, n = idx - li * NZ;
+      const int lg = l0 + li, qg = lg / kZPairs, pr = lg - qg * kZPairs;
+      const double2 Z = R[li * N + n];
+      const double2 Zc = cconj(R[li * N + (n == 0 ? 0 : N - n)]);
       const double2 va = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
       const double2 dd = csub(Z, Zc);
       const double2 vb = make_double2(0.5 * dd.y, -0.5 * dd.x);  // (Z - Zc) / 2i
       const double2 w = dct_tw[n];                                // exp(-i pi n / 2N)
-      double* dst = dst0 + qi * vstride;
-      dst[n] = 2.0 * (w.x * va.x - w.y * va.y);
-      if (has_b) dst[NZ + n] = 2.0 * (w.x * vb.x - w.y * vb.y);
+      double* dst = Q2 + qg * vstride + col0 + (size_t)(2 * pr) * NZ;
+      if (col_ok(2 * pr)) dst[n] = 2.0 * (w.x * va.x - w.y * va.y);
+      if (col_ok(2 * pr + 1)) dst[NZ + n] = 2.0 * (w.x * vb.x - w.y * vb.y);
     }
     __syncthreads();  // A is refilled by the next batch
   }
@@ -1264,6 +1286,9 @@ __global__ void __launch_bounds__(kTpbThreads) k_subst_tpb(SolveArgs a) {
   const unsigned char* P = a.dpiv + gb * 32 + (b & 31);
   double2* X = a.work2 + gb * 32 + (b & 31);
   const unsigned char* cflip = a.colflip_cls + (size_t)cls * T;
+  const int* ccol = a.cls_col + (size_t)cls * T;
+  double2* out = a.out + (size_t)a.act_list[b / a.ncls] * a.T;  // this system's stage output
+  bool bad = false;
   double2* win = swin + threadIdx.x;
   // ---- forward: positions j..j+KL in slots p mod W1 ----
   for (int p = 0; p <= KL && p < T; ++p) win[(p & (W1 - 1)) * S] = X[(size_t)p * 32];
@@ -1319,7 +1344,14 @@ __global__ void __launch_bounds__(kTpbThreads) k_subst_tpb(SolveArgs a) {
     const double dinv = Fj[KV * 32];  // U's diagonal is stored as its reciprocal
     const double2 xj = make_double2(acc.x * dinv, acc.y * dinv);
     win[sj * S] = xj;
-    X[(size_t)j * 32] = flip_col(xj, cflip[j]);
+    {  // the solution, scaled back, straight into the stage output (original order)
+      const int t = ccol[j];
+      if (t >= 0) {
+        const double2 xo = flip_col(xj, cflip[j]);
+        bad |= !(isfinite(xo.x) && isfinite(xo.y));
+        out[t] = xo;
+      }
+    }
     sj = (sj == 0) ? W2 - 1 : sj - 1;
   }
   if (j >= 0) {
@@ -1355,10 +1387,19 @@ __global__ void __launch_bounds__(kTpbThreads) k_subst_tpb(SolveArgs a) {
       }
       const double2 xj = make_double2(acc.x * dinv, acc.y * dinv);
       win[sj * S] = xj;
-      X[(size_t)j * 32] = flip_col(xj, cflip[j]);
+      {  // the solution, scaled back, straight into the stage output (original order)
+        const int t = ccol[j];
+        if (t >= 0) {
+          const double2 xo = flip_col(xj, cflip[j]);
+          bad |= !(isfinite(xo.x) && isfinite(xo.y));
+          out[t] = xo;
+        }
+      }
       sj = (sj == 0) ? W2 - 1 : sj - 1;
     }
   }
+  // non-finite check (no warp-collective operation: lanes of a partial warp returned early)
+  if (bad) atomicOr(a.flags, 1u);
 }
 
 // The same solve for any band within (KL, KV) = (15, 31), kl and ku read at run time.
@@ -1377,6 +1418,9 @@ __global__ void __launch_bounds__(kTpbThreads) k_subst_tpb_rt(SolveArgs a) {
   const unsigned char* P = a.dpiv + gb * 32 + (b & 31);
   double2* X = a.work2 + gb * 32 + (b & 31);
   const unsigned char* cflip = a.colflip_cls + (size_t)cls * T;
+  const int* ccol = a.cls_col + (size_t)cls * T;
+  double2* out = a.out + (size_t)a.act_list[b / a.ncls] * a.T;  // this system's stage output
+  bool bad = false;
   double2* win = swin + threadIdx.x;
   // ---- forward: positions j..j+kl in slots p mod W1 ----
   for (int p = 0; p <= kl && p < T; ++p) win[(p & (W1 - 1)) * S] = X[(size_t)p * 32];
@@ -1423,9 +1467,17 @@ __global__ void __launch_bounds__(kTpbThreads) k_subst_tpb_rt(SolveArgs a) {
     }
     const double2 xj = make_double2(acc.x * dinv, acc.y * dinv);
     win[sj * S] = xj;
-    X[(size_t)j * 32] = flip_col(xj, cflip[j]);
+    {  // the solution, scaled back, straight into the stage output (original order)
+      const int t = ccol[j];
+      if (t >= 0) {
+        const double2 xo = flip_col(xj, cflip[j]);
+        bad |= !(isfinite(xo.x) && isfinite(xo.y));
+        out[t] = xo;
+      }
+    }
     sj = (sj == 0) ? W2 - 1 : sj - 1;
   }
+  if (bad) atomicOr(a.flags, 1u);
 }
 
 // ------------------------------------------------------------------------------
@@ -1548,36 +1600,36 @@ __global__ void __launch_bounds__(kRhsThreads) k_kstd_out(SolveArgs a) {
   __shared__ double2 cls[kMaxGroups];
   const int aidx = blockIdx.x;
   const int sid = a.act_list[aidx];
-  const int T = a.T, Tc = a.Tc, npos = a.ncls * a.Tc;
+  const int T = a.T;
   const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
+  // thread-per-block solve: the solution is already in out, original order, and
+  // only K_std remains (L with its original columns); whole-system solve: the
+  // solution is in work (class order = original order), copied to out here
+  const bool in_out = a.work2 != nullptr;
+  const DevEll& L = in_out ? a.L : a.Lp;
   if (threadIdx.x < kMaxGroups) {
     const int g = threadIdx.x;
-    cls[g] = (g < a.Lp.ngroups) ? cmul(ipow(a.kx[kx], a.Lp.gkx[g]), ipow(a.ky[ky], a.Lp.gky[g])) : zero2();
+    cls[g] = (g < L.ngroups) ? cmul(ipow(a.kx[kx], L.gkx[g]), ipow(a.ky[ky], L.gky[g])) : zero2();
   }
-  if (a.work2) {
-    // (j, class) pairs: the two classes of one j are adjacent 16-byte entries
-    // (the thread-per-block layout always has two classes)
-    for (int idx = threadIdx.x; idx < 2 * Tc; idx += kRhsThreads) {
-      const int j = idx >> 1, c = idx & 1, bb = 2 * aidx + c;
-      xs[c * Tc + j] = a.work2[((size_t)(bb >> 5) * Tc + j) * 32 + (bb & 31)];
-    }
-  } else {
-    const double2* x = a.work + (size_t)sid * a.wst;
-    for (int p = threadIdx.x; p < npos; p += kRhsThreads) xs[p] = x[p];
+  const size_t base = (size_t)sid * T;
+  {
+    const double2* x = in_out ? a.out + base : a.work + (size_t)sid * a.wst;
+    for (int p = threadIdx.x; p < T; p += kRhsThreads) xs[p] = x[p];
   }
   __syncthreads();
-  const size_t base = (size_t)sid * T;
   bool bad = false;
   for (int t = threadIdx.x; t < T; t += kRhsThreads) {
-    const double2 v = xs[a.col_pos ? a.col_pos[t] : t];
-    bad |= !(isfinite(v.x) && isfinite(v.y));
-    if (a.out != a.work || a.work2) a.out[base + t] = v;
+    if (!in_out) {
+      const double2 v = xs[t];
+      bad |= !(isfinite(v.x) && isfinite(v.y));
+      if (a.out != a.work) a.out[base + t] = v;
+    }
     if (a.Kstd_out) {
       double2 ks = zero2();
 #pragma unroll 4
-      for (int k = 0; k < a.Lp.width; ++k) {
-        const int cg = a.Lp.cg[(size_t)k * a.Lp.rows + t];
-        const double lv = a.Lp.val[(size_t)k * a.Lp.rows + t];
+      for (int k = 0; k < L.width; ++k) {
+        const int cg = L.cg[(size_t)k * L.rows + t];
+        const double lv = L.val[(size_t)k * L.rows + t];
         const double2 xv = xs[cg & 0xFFFFFF];
         ks = cadd(ks, cmul(cls[cg >> 24], make_double2(lv * xv.x, lv * xv.y)));
       }
@@ -1848,11 +1900,12 @@ struct ZFused {
       ZFused<0>::run(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, s);
       return;
     }
-    const size_t lines = (size_t)nf + std::min(q.nq, kQC) + (NF ? 0 : std::max(kFC, kQC));
+    const size_t lines = (size_t)nf * kZPairs + kZLines + (NF ? 0 : kZLines);
     const size_t sm = lines * d.NZA * sizeof(double2);
     set_smem(k_z_fused<NF>, sm);
-    dim3 g((d.NXA + 1) / 2, d.NYA);
-    k_z_fused<NF><<<g, kThreads, sm, s>>>(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial);
+    dim3 g((d.NXA + 2 * kZPairs - 1) / (2 * kZPairs), d.NYA);
+    k_z_fused<NF><<<g, z_threads(NF, kZLines), sm, s>>>(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits,
+                                                       ke_partial);
   }
 };
 template <int NF>
@@ -1955,7 +2008,8 @@ void launch_subst(const SolveArgs& a, cudaStream_t s) {
 }
 void launch_kstd_out(const SolveArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;
-  const size_t smx = (size_t)a.ncls * a.Tc * sizeof(double2);
+  if (a.work2 && !a.Kstd_out) return;  // solution already in out, no K_std in the last stage
+  const size_t smx = (size_t)a.T * sizeof(double2);
   if (smx > 48 * 1024) set_smem(k_kstd_out, smx);
   k_kstd_out<<<a.nact, kRhsThreads, smx, s>>>(a);
 }
