@@ -105,8 +105,9 @@ __device__ double2* fft_lines(double2* A, double2* B, int nl, int LS, const FftP
 
 // ---- compile-time plans: register passes ----------------------------------------
 // With the length N known at compile time the transform runs as a few passes of
-// radix 16, 9, 8, 4, 3 or 2 (odd radices first: their strided stores in the
-// first pass hit distinct shared-memory banks).  Each thread computes whole
+// radix 24, 18, 16, 9, 8, 4, 3 or 2 (in the three-pass plans odd radices come
+// first: their strided stores in the first pass hit distinct shared-memory banks;
+// the two-pass plans trade that for one pass fewer).  Each thread computes whole
 // radix-R butterflies in registers: it loads its R inputs, applies the twiddles,
 // waits for every thread to have loaded (so the pass can write in place), and
 // stores its R outputs at their Stockham (self-sorting) positions.  Only one
@@ -134,6 +135,16 @@ __host__ __device__ constexpr PlanR make_planr(int N) {
   return p;
 }
 
+// Two-pass plans (more registers per thread, one barrier pair fewer):
+// 288 = 18 x 16, 576 = 24 x 24; other lengths keep make_planr.
+__host__ __device__ constexpr PlanR make_planr2(int N) {
+  if (N == 288) return PlanR{2, {18, 16}};
+  if (N == 576) return PlanR{2, {24, 24}};
+  return make_planr(N);
+}
+// plan variant PV: 0 = make_planr, 1 = make_planr2
+__host__ __device__ constexpr PlanR plan_of(int N, int PV) { return PV ? make_planr2(N) : make_planr(N); }
+
 // cos / sin of 2 pi m / 16 and 2 pi m / 9, from the mathematics (40-digit values)
 #define CORAL_C16_1 0.923879532511286756128183189396788287   // cos(pi/8)
 #define CORAL_S16_1 0.382683432365089771728459984030398867   // sin(pi/8)
@@ -144,6 +155,27 @@ __host__ __device__ constexpr PlanR make_planr(int N) {
 #define CORAL_S9_2 0.984807753012208059366743024589523014    // sin(4 pi/9)
 #define CORAL_C9_4 (-0.93969262078590838405410927732473147)  // cos(8 pi/9)
 #define CORAL_S9_4 0.342020143325668733044099614682259581    // sin(8 pi/9)
+
+// cos / sin of 2 pi m / 18 and 2 pi m / 24 (m = 0, 1, ...), from the mathematics
+__device__ constexpr double kC18[9] = {1.0, 0.93969262078590838405410927732473147, 0.766044443118978035202392650555416674,
+                                       0.5, 0.173648177666930348851716626769314796, -0.173648177666930348851716626769314796,
+                                       -0.5, -0.766044443118978035202392650555416674, -0.93969262078590838405410927732473147};
+__device__ constexpr double kS18[9] = {0.0, 0.342020143325668733044099614682259581, 0.642787609686539326322643409907263433,
+                                       0.866025403784438646763723170752936183, 0.984807753012208059366743024589523014,
+                                       0.984807753012208059366743024589523014, 0.866025403784438646763723170752936183,
+                                       0.642787609686539326322643409907263433, 0.342020143325668733044099614682259581};
+__device__ constexpr double kC24[15] = {1.0, 0.965925826289068286749743199728897368, 0.866025403784438646763723170752936183,
+                                        0.707106781186547524400844362104849039, 0.5, 0.258819045102520762348898837624048328,
+                                        0.0, -0.258819045102520762348898837624048328, -0.5,
+                                        -0.707106781186547524400844362104849039, -0.866025403784438646763723170752936183,
+                                        -0.965925826289068286749743199728897368, -1.0,
+                                        -0.965925826289068286749743199728897368, -0.866025403784438646763723170752936183};
+__device__ constexpr double kS24[15] = {0.0, 0.258819045102520762348898837624048328, 0.5,
+                                        0.707106781186547524400844362104849039, 0.866025403784438646763723170752936183,
+                                        0.965925826289068286749743199728897368, 1.0, 0.965925826289068286749743199728897368,
+                                        0.866025403784438646763723170752936183, 0.707106781186547524400844362104849039, 0.5,
+                                        0.258819045102520762348898837624048328, 0.0, -0.258819045102520762348898837624048328,
+                                        -0.5};
 
 // a * exp(-i t) (forward) or a * exp(+i t) (inverse), given c = cos t, s = sin t
 template <bool INV>
@@ -216,6 +248,47 @@ __device__ __forceinline__ void dft(double2 (&x)[R]) {
       for (int k2 = 0; k2 < 3; ++k2) y[k1 + 3 * k2] = x[3 * k1 + k2];
 #pragma unroll
     for (int k = 0; k < 9; ++k) x[k] = y[k];
+  } else if constexpr (R == 18) {
+    // n = 2 n1 + n2, k = k1 + 9 k2: two 9-point DFTs, twiddles w18^k1, butterflies
+    double2 e[9], o[9];
+#pragma unroll
+    for (int n1 = 0; n1 < 9; ++n1) {
+      e[n1] = x[2 * n1];
+      o[n1] = x[2 * n1 + 1];
+    }
+    dft<9, INV>(e);
+    dft<9, INV>(o);
+#pragma unroll
+    for (int k1 = 1; k1 < 9; ++k1) o[k1] = rot<INV>(o[k1], kC18[k1], kS18[k1]);
+#pragma unroll
+    for (int k1 = 0; k1 < 9; ++k1) {
+      x[k1] = cadd(e[k1], o[k1]);
+      x[k1 + 9] = csub(e[k1], o[k1]);
+    }
+  } else if constexpr (R == 24) {
+    // n = 3 n1 + n2, k = k1 + 8 k2: three 8-point DFTs, twiddles w24^(n2 k1), 3-point DFTs
+    double2 a0[8], a1[8], a2[8];
+#pragma unroll
+    for (int n1 = 0; n1 < 8; ++n1) {
+      a0[n1] = x[3 * n1];
+      a1[n1] = x[3 * n1 + 1];
+      a2[n1] = x[3 * n1 + 2];
+    }
+    dft<8, INV>(a0);
+    dft<8, INV>(a1);
+    dft<8, INV>(a2);
+#pragma unroll
+    for (int k1 = 1; k1 < 8; ++k1) {
+      a1[k1] = rot<INV>(a1[k1], kC24[k1], kS24[k1]);
+      a2[k1] = rot<INV>(a2[k1], kC24[2 * k1], kS24[2 * k1]);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 8; ++k1) {
+      dft3<INV>(a0[k1], a1[k1], a2[k1]);
+      x[k1] = a0[k1];
+      x[k1 + 8] = a1[k1];
+      x[k1 + 16] = a2[k1];
+    }
   } else if constexpr (R == 16) {
     // n = 4 n1 + n2, k = k1 + 4 k2
 #pragma unroll
@@ -315,13 +388,13 @@ __device__ __forceinline__ void fft_pass_first(double2* A, int nl, int LS, Load&
   __syncthreads();
 }
 
-template <int N, int S, int Ns, bool INV, int NT, int NLMAX>
+template <int N, int S, int Ns, bool INV, int NT, int NLMAX, int PV = 0>
 __device__ __forceinline__ void fft_passes(double2* A, int nl, int LS, const double2* tw) {
-  constexpr PlanR P = make_planr(N);
+  constexpr PlanR P = plan_of(N, PV);
   if constexpr (S < P.nst) {
     constexpr int R = P.r[S];
     fft_pass<N, R, Ns, INV, NT, NLMAX>(A, nl, LS, tw);
-    fft_passes<N, S + 1, Ns * R, INV, NT, NLMAX>(A, nl, LS, tw);
+    fft_passes<N, S + 1, Ns * R, INV, NT, NLMAX, PV>(A, nl, LS, tw);
   }
 }
 
@@ -331,7 +404,7 @@ __device__ __forceinline__ void fft_passes(double2* A, int nl, int LS, const dou
 // before (inputs written) and may read the result directly after.
 // The same with the inputs produced by ld(line, k) (see fft_pass_first); the
 // caller need not synchronise before.  Runtime plans stage the inputs in A first.
-template <int NC, bool INV, int NT, int NLMAX, bool LINE_FAST = false, class Load>
+template <int NC, bool INV, int NT, int NLMAX, bool LINE_FAST = false, int PV = 0, class Load>
 __device__ __forceinline__ double2* fft_lines_ld(double2* A, double2* B, int nl, int LS, const FftPlan& p,
                                                  Load&& ld) {
   if constexpr (NC == 0) {
@@ -342,10 +415,10 @@ __device__ __forceinline__ double2* fft_lines_ld(double2* A, double2* B, int nl,
     __syncthreads();
     return fft_lines<INV>(A, B, nl, LS, p);
   } else {
-    constexpr PlanR P = make_planr(NC);
+    constexpr PlanR P = plan_of(NC, PV);
     static_assert(P.nst > 0, "transform length must be 2^a 3^b");
     fft_pass_first<NC, P.r[0], INV, NT, NLMAX, LINE_FAST>(A, nl, LS, ld);
-    fft_passes<NC, 1, P.r[0], INV, NT, NLMAX>(A, nl, LS, p.tw);
+    fft_passes<NC, 1, P.r[0], INV, NT, NLMAX, PV>(A, nl, LS, p.tw);
     return A;
   }
 }

@@ -29,22 +29,32 @@ constexpr int kPadXY = 2;  // line stride N + 2 in the x / y passes, whose loads
                            // walk 4 interleaved lines: 2 line + position hits 8 distinct
                            // 16-byte bank groups
 constexpr int kThreads = 256;
+// FFT plans of the time-step transforms (fft.cuh plan_of): the x passes and the
+// fused z passes use the two-pass plans (576 = 24 x 24, 288 = 18 x 16); the y
+// passes, whose first pass gathers its inputs (spectral build, strided
+// coefficients), keep the three-pass plans with their shorter per-thread load
+// chains (measured at 384^2 x 192)
+constexpr int kPlanHot = 1;
+constexpr int kPlanY = 0;
 // x / y passes: threads per CTA for nl lines of a compiled length N, the most
 // butterflies of any pass rounded up to whole warps (one butterfly per thread
 // per pass); 256 for the run-time plans
-__host__ __device__ constexpr int xy_threads(int N, int nl) {
+__host__ __device__ constexpr int xy_threads(int N, int nl, int pv) {
   if (N == 0) return 256;
-  const PlanR p = make_planr(N);
+  const PlanR p = plan_of(N, pv);
   int m = 32;
   for (int i = 0; i < p.nst; ++i) m = (nl * N / p.r[i] > m) ? nl * N / p.r[i] : m;
   return (m + 31) / 32 * 32;
 }
-#define kThreadsXY xy_threads(NF, 4)
-// CTAs per SM the transform kernels are compiled for (caps their registers;
-// measured best at 384^2 x 192: 3 for the x / y passes, 4 for the z passes)
-constexpr int kMinBlocksXY = 3;
+#define kThreadsX xy_threads(NF, 4, kPlanHot)
+#define kThreadsY xy_threads(NF, 4, kPlanY)
+// CTAs per SM the kernels with two-pass plans are compiled for: registers
+// capped at no fewer than 128 per thread
+__host__ __device__ constexpr int hot_min_blocks(int nt) { return 65536 / (nt * 128) > 1 ? 65536 / (nt * 128) : 1; }
+// CTAs per SM of the y passes (measured best at 384^2 x 192) and of the
+// separate z passes of the transform API paths
+constexpr int kMinBlocksY = 3;
 constexpr int kMinBlocksZ = 4;
-constexpr int kMinBlocksZF = 2;  // fused z passes (two FFT batches in one kernel)
 constexpr int kWPB = 8;  // warps (systems) per CTA in the per-system kernels
 
 __device__ __forceinline__ double2 zero2() { return make_double2(0.0, 0.0); }
@@ -63,7 +73,7 @@ __device__ __forceinline__ double2 ipow(double k, int e) {
 //  c2r_transform steps 1-2 and the 0.5 of the x padding, transforms.f90:172-198)
 // ------------------------------------------------------------------------------
 template <int NF>
-__global__ void __launch_bounds__(kThreadsXY, kMinBlocksXY) k_inv_y(Dims d, const FullVarDev* fv, StateSet st,
+__global__ void __launch_bounds__(kThreadsY, kMinBlocksY) k_inv_y(Dims d, const FullVarDev* fv, StateSet st,
                                                      const double2* plain_spec, const double* kxv,
                                                      const double* kyv, double2* Y1, FftPlan py) {
   extern __shared__ double2 sm[];
@@ -114,7 +124,7 @@ __global__ void __launch_bounds__(kThreadsXY, kMinBlocksXY) k_inv_y(Dims d, cons
     }
     return c;
   };
-  const double2* R = fft_lines_ld<NF, true, kThreadsXY, kNB1, true>(A, B, kNB1, LS, py, ld);
+  const double2* R = fft_lines_ld<NF, true, kThreadsY, kNB1, true, kPlanY>(A, B, kNB1, LS, py, ld);
   for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
     const int ln = idx % kNB1, y = idx / kNB1, n = n0 + ln;
     if (n < d.NZ) {
@@ -129,7 +139,7 @@ __global__ void __launch_bounds__(kThreadsXY, kMinBlocksXY) k_inv_y(Dims d, cons
 // two real output lines per complex FFT
 // ------------------------------------------------------------------------------
 template <int NF>
-__global__ void __launch_bounds__(kThreadsXY, kMinBlocksXY) k_inv_x(Dims d, const double2* Y1, double* Y2, FftPlan px) {
+__global__ void __launch_bounds__(kThreadsX, hot_min_blocks(kThreadsX)) k_inv_x(Dims d, const double2* Y1, double* Y2, FftPlan px) {
   extern __shared__ double2 sm[];
   const int f = blockIdx.x, n0 = blockIdx.y * kNB2, y = blockIdx.z;
   const int NXA = NF ? NF : d.NXA, NP = kNB2 / 2, LS = NXA + kPadXY;
@@ -151,7 +161,7 @@ __global__ void __launch_bounds__(kThreadsXY, kMinBlocksXY) k_inv_x(Dims d, cons
     return lo ? make_double2(a.x - b.y, a.y + b.x)    // a + i b
               : make_double2(a.x + b.y, b.x - a.y);   // conj(a) + i conj(b)
   };
-  const double2* R = fft_lines_ld<NF, true, kThreadsXY, kNB2 / 2, true>(A, B, NP, LS, px, ld);
+  const double2* R = fft_lines_ld<NF, true, kThreadsX, kNB2 / 2, true, kPlanHot>(A, B, NP, LS, px, ld);
   for (int idx = threadIdx.x; idx < NP * NXA; idx += blockDim.x) {
     const int m = idx % NP, x = idx / NP, na = n0 + 2 * m;
     double2 z = R[m * LS + x];
@@ -318,11 +328,11 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksZ) k_fwd_z(Dims d, int nf,
 // ------------------------------------------------------------------------------
 
 // Threads of the fused z kernel for nl lines of a compiled length N: enough for
-// one butterfly per thread in the odd and radix-8/16 passes and two in the
-// radix-2/4 passes (N = 288, 8 lines: 288 threads, every pass balanced).
+// one butterfly per thread in the radix >= 8 passes and two in the radix-2/4
+// passes (N = 288, 8 lines, plan 18 x 16: 160 threads).
 __host__ __device__ constexpr int z_threads(int N, int nl) {
   if (N == 0) return 256;
-  const PlanR p = make_planr(N);
+  const PlanR p = plan_of(N, kPlanHot);
   int m = 32;
   for (int i = 0; i < p.nst; ++i) {
     const int b = nl * N / p.r[i], per = (p.r[i] <= 4) ? (b + 1) / 2 : b;
@@ -335,7 +345,7 @@ constexpr int kZLines = 4 * kZPairs;     // lines per FFT batch (4 full variable
 #define kThreadsZF z_threads(NF, kZLines)
 
 template <int NF>
-__global__ void __launch_bounds__(kThreadsZF, kMinBlocksZF) k_z_fused(Dims d, int nf, QuadDesc q, const double* Y2,
+__global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fused(Dims d, int nf, QuadDesc q, const double* Y2,
                                                                        double* Q2, FftPlan pz, const double2* dct_tw,
                                                                        const double* wz, const double* wzinv,
                                                                        unsigned long long* cfl_bits, double* ke_partial) {
@@ -377,7 +387,7 @@ __global__ void __launch_bounds__(kThreadsZF, kMinBlocksZF) k_z_fused(Dims d, in
       const double2 vb = cmul(w, make_double2(b0, -b1));
       return make_double2(va.x - vb.y, va.y + vb.x);
     };
-    const double2* R = fft_lines_ld<NF, true, NT, kZLines>(Fv + l0 * N, B, nl, N, pz, ld);
+    const double2* R = fft_lines_ld<NF, true, NT, kZLines, false, kPlanHot>(Fv + l0 * N, B, nl, N, pz, ld);
     if (R != Fv + l0 * N) {  // runtime plan with the result in the scratch lines
       for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) Fv[l0 * N + idx] = R[idx];
       __syncthreads();
@@ -438,7 +448,7 @@ __global__ void __launch_bounds__(kThreadsZF, kMinBlocksZF) k_z_fused(Dims d, in
       }
       return make_double2(pa, pb);
     };
-    const double2* R = fft_lines_ld<NF, false, NT, kZLines>(A, B, nc, N, pz, ld);
+    const double2* R = fft_lines_ld<NF, false, NT, kZLines, false, kPlanHot>(A, B, nc, N, pz, ld);
     for (int idx = threadIdx.x; idx < nc * NZ; idx += blockDim.x) {
       const int li = idx / NZ, n = idx - li * NZ;
       const int lg = l0 + li, qg = lg / kZPairs, pr = lg - qg * kZPairs;
@@ -473,7 +483,7 @@ __global__ void __launch_bounds__(kThreadsZF, kMinBlocksZF) k_z_fused(Dims d, in
 // forward transform, pass 2: x r2c, keep kx < NX/2 (transforms.f90:255-267)
 // ------------------------------------------------------------------------------
 template <int NF>
-__global__ void __launch_bounds__(kThreadsXY, kMinBlocksXY) k_fwd_x(Dims d, const double* Q2, double2* Q1, FftPlan px) {
+__global__ void __launch_bounds__(kThreadsX, hot_min_blocks(kThreadsX)) k_fwd_x(Dims d, const double* Q2, double2* Q1, FftPlan px) {
   extern __shared__ double2 sm[];
   const int qi = blockIdx.x, n0 = blockIdx.y * kNB2, y = blockIdx.z;
   const int NXA = NF ? NF : d.NXA, NP = kNB2 / 2, LS = NXA + kPadXY;
@@ -487,7 +497,7 @@ __global__ void __launch_bounds__(kThreadsXY, kMinBlocksXY) k_fwd_x(Dims d, cons
     const double* src = src0 + (size_t)x * d.NZ;
     return make_double2(na < d.NZ ? src[na] : 0.0, na + 1 < d.NZ ? src[na + 1] : 0.0);
   };
-  const double2* R = fft_lines_ld<NF, false, kThreadsXY, kNB2 / 2, true>(A, B, NP, LS, px, ld);
+  const double2* R = fft_lines_ld<NF, false, kThreadsX, kNB2 / 2, true, kPlanHot>(A, B, NP, LS, px, ld);
   for (int idx = threadIdx.x; idx < NP * d.NXH; idx += blockDim.x) {
     const int m = idx % NP, kx = idx / NP, na = n0 + 2 * m;
     const double2 Z = R[m * LS + kx];
@@ -506,7 +516,7 @@ __global__ void __launch_bounds__(kThreadsXY, kMinBlocksXY) k_fwd_x(Dims d, cons
 // 1/(NXAA NYAA NZAA) normalisation (transforms.f90:280-296)
 // ------------------------------------------------------------------------------
 template <int NF>
-__global__ void __launch_bounds__(kThreadsXY, kMinBlocksXY) k_fwd_y(Dims d, const double2* Q1, double2* qspec, double scale,
+__global__ void __launch_bounds__(kThreadsY, kMinBlocksY) k_fwd_y(Dims d, const double2* Q1, double2* qspec, double scale,
                                                      FftPlan py) {
   extern __shared__ double2 sm[];
   const int qi = blockIdx.x, n0 = blockIdx.y * kNB1, kx = blockIdx.z;
@@ -523,7 +533,7 @@ __global__ void __launch_bounds__(kThreadsXY, kMinBlocksXY) k_fwd_y(Dims d, cons
     }
     return v;
   };
-  const double2* R = fft_lines_ld<NF, false, kThreadsXY, kNB1, true>(A, B, kNB1, LS, py, ld);
+  const double2* R = fft_lines_ld<NF, false, kThreadsY, kNB1, true, kPlanY>(A, B, kNB1, LS, py, ld);
   for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
     const int ln = idx % kNB1, ky = idx / kNB1, n = n0 + ln;
     if (n < d.NZ) qspec[(((size_t)qi * d.NXH + kx) * NYA + ky) * d.NZ + n] = cscale(R[ln * LS + ky], scale);
@@ -1859,7 +1869,7 @@ struct InvY {
     size_t sm = (NF ? 1 : 2) * kNB1 * (size_t)(d.NYA + kPadXY) * sizeof(double2);
     set_smem(k_inv_y<NF>, sm);
     dim3 g(nf, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
-    k_inv_y<NF><<<g, kThreadsXY, sm, s>>>(d, fv, st, plain_spec, kx, ky, Y1, py);
+    k_inv_y<NF><<<g, kThreadsY, sm, s>>>(d, fv, st, plain_spec, kx, ky, Y1, py);
   }
 };
 template <int NF>
@@ -1868,7 +1878,7 @@ struct InvX {
     size_t sm = (NF ? 1 : 2) * (kNB2 / 2) * (size_t)(d.NXA + kPadXY) * sizeof(double2);
     set_smem(k_inv_x<NF>, sm);
     dim3 g(nf, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
-    k_inv_x<NF><<<g, kThreadsXY, sm, s>>>(d, Y1, Y2, px);
+    k_inv_x<NF><<<g, kThreadsX, sm, s>>>(d, Y1, Y2, px);
   }
 };
 template <int NF>
@@ -1914,7 +1924,7 @@ struct FwdX {
     size_t sm = (NF ? 1 : 2) * (kNB2 / 2) * (size_t)(d.NXA + kPadXY) * sizeof(double2);
     set_smem(k_fwd_x<NF>, sm);
     dim3 g(nq, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
-    k_fwd_x<NF><<<g, kThreadsXY, sm, s>>>(d, Q2, Q1, px);
+    k_fwd_x<NF><<<g, kThreadsX, sm, s>>>(d, Q2, Q1, px);
   }
 };
 template <int NF>
@@ -1924,7 +1934,7 @@ struct FwdY {
     size_t sm = (NF ? 1 : 2) * kNB1 * (size_t)(d.NYA + kPadXY) * sizeof(double2);
     set_smem(k_fwd_y<NF>, sm);
     dim3 g(nq, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
-    k_fwd_y<NF><<<g, kThreadsXY, sm, s>>>(d, Q1, qspec, scale, py);
+    k_fwd_y<NF><<<g, kThreadsY, sm, s>>>(d, Q1, qspec, scale, py);
   }
 };
 
