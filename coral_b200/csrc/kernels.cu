@@ -25,6 +25,7 @@ constexpr int kNB2 = 8;  // n lines per CTA, x passes (packed in pairs)
 constexpr int kXB3 = 16; // x columns per CTA, inverse z pass (packed in pairs)
 constexpr int kQC = 5;   // quadratic variables per FFT batch, forward z pass (one radix-9 / radix-8
                          // butterfly per thread at NZAA = 288)
+constexpr int kPadY = 2;   // line stride of the y passes (kNB1 interleaved lines)
 constexpr int kPadXY = 2;  // line stride N + 2 in the x / y passes, whose loads and stores
                            // walk 4 interleaved lines: 2 line + position hits 8 distinct
                            // 16-byte bank groups
@@ -78,7 +79,7 @@ __global__ void __launch_bounds__(kThreadsY, kMinBlocksY) k_inv_y(Dims d, const 
                                                      const double* kyv, double2* Y1, FftPlan py) {
   extern __shared__ double2 sm[];
   const int f = blockIdx.x, n0 = blockIdx.y * kNB1, kx = blockIdx.z;
-  const int NYA = NF ? NF : d.NYA, LS = NYA + kPadXY;
+  const int NYA = NF ? NF : d.NYA, LS = NYA + kPadY;
   double2* A = sm;
   double2* B = sm + kNB1 * LS;  // runtime plan only
   // the spectral build of (line ln = Chebyshev n0 + ln, ky index iy), produced
@@ -341,8 +342,12 @@ __host__ __device__ constexpr int z_threads(int N, int nl) {
   return (m + 31) / 32 * 32;
 }
 constexpr int kZPairs = 2;               // x-column pairs per CTA
-constexpr int kZLines = 4 * kZPairs;     // lines per FFT batch (4 full variables x 2 pairs)
-#define kThreadsZF z_threads(NF, kZLines)
+constexpr int kZLines = 4 * kZPairs;     // lines per inverse FFT batch (4 full variables x 2 pairs)
+constexpr int kZFwd = 9;                 // lines per forward FFT batch ((quadratic variable, pair) lines)
+__host__ __device__ constexpr int z_threads_fused(int N) {
+  return z_threads(N, kZLines) > z_threads(N, kZFwd) ? z_threads(N, kZLines) : z_threads(N, kZFwd);
+}
+#define kThreadsZF z_threads_fused(NF)
 
 template <int NF>
 __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fused(Dims d, int nf, QuadDesc q, const double* Y2,
@@ -367,8 +372,8 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
   // x0 + 2p (re) and x0 + 2p + 1 (im))
   auto col_ok = [&](int c) { return x0 + c < d.NXA; };
   double2* Fv = sm;                   // nf * kZPairs lines of the full variables
-  double2* A = Fv + nf * kZPairs * N; // kZLines lines of quadratic variables
-  double2* B = A + kZLines * N;       // runtime plan only (kZLines lines)
+  double2* A = Fv + nf * kZPairs * N; // kZFwd lines of quadratic variables
+  double2* B = A + kZFwd * N;         // runtime plan only (max(kZLines, kZFwd) lines)
   // ---- inverse: X_n and X_{N-n} of both columns, twiddled, packed as va + i vb,
   //      produced inside the first FFT pass ----
   __syncthreads();  // qv
@@ -421,10 +426,10 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
     }
     __syncthreads();
   }
-  // ---- products and forward transforms, kZLines (quadratic variable, pair) lines a batch ----
+  // ---- products and forward transforms, kZFwd (quadratic variable, pair) lines a batch ----
   double ke[3] = {0.0, 0.0, 0.0};
-  for (int l0 = 0; l0 < nq * kZPairs; l0 += kZLines) {
-    const int nc = min(kZLines, nq * kZPairs - l0);
+  for (int l0 = 0; l0 < nq * kZPairs; l0 += kZFwd) {
+    const int nc = min(kZFwd, nq * kZPairs - l0);
     // products formed inside the first FFT pass (and the KE sums on the way)
     auto ld = [&](int line, int m) -> double2 {
       const int lg = l0 + line, qg = lg / kZPairs, pr = lg - qg * kZPairs;
@@ -448,7 +453,7 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
       }
       return make_double2(pa, pb);
     };
-    const double2* R = fft_lines_ld<NF, false, NT, kZLines, false, kPlanHot>(A, B, nc, N, pz, ld);
+    const double2* R = fft_lines_ld<NF, false, NT, kZFwd, false, kPlanHot>(A, B, nc, N, pz, ld);
     for (int idx = threadIdx.x; idx < nc * NZ; idx += blockDim.x) {
       const int li = idx / NZ, n = idx - li * NZ;
       const int lg = l0 + li, qg = lg / kZPairs, pr = lg - qg * kZPairs;
@@ -520,7 +525,7 @@ __global__ void __launch_bounds__(kThreadsY, kMinBlocksY) k_fwd_y(Dims d, const 
                                                      FftPlan py) {
   extern __shared__ double2 sm[];
   const int qi = blockIdx.x, n0 = blockIdx.y * kNB1, kx = blockIdx.z;
-  const int NYA = NF ? NF : d.NYA, LS = NYA + kPadXY;
+  const int NYA = NF ? NF : d.NYA, LS = NYA + kPadY;
   double2* A = sm;
   double2* B = sm + kNB1 * LS;  // runtime plan only
   // produced inside the first FFT pass
@@ -1866,7 +1871,7 @@ template <int NF>
 struct InvY {
   static void run(const Dims& d, int nf, const FullVarDev* fv, StateSet st, const double2* plain_spec,
                   const double* kx, const double* ky, double2* Y1, const FftPlan& py, cudaStream_t s) {
-    size_t sm = (NF ? 1 : 2) * kNB1 * (size_t)(d.NYA + kPadXY) * sizeof(double2);
+    size_t sm = (NF ? 1 : 2) * kNB1 * (size_t)(d.NYA + kPadY) * sizeof(double2);
     set_smem(k_inv_y<NF>, sm);
     dim3 g(nf, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
     k_inv_y<NF><<<g, kThreadsY, sm, s>>>(d, fv, st, plain_spec, kx, ky, Y1, py);
@@ -1910,11 +1915,11 @@ struct ZFused {
       ZFused<0>::run(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, s);
       return;
     }
-    const size_t lines = (size_t)nf * kZPairs + kZLines + (NF ? 0 : kZLines);
+    const size_t lines = (size_t)nf * kZPairs + kZFwd + (NF ? 0 : std::max(kZLines, kZFwd));
     const size_t sm = lines * d.NZA * sizeof(double2);
     set_smem(k_z_fused<NF>, sm);
     dim3 g((d.NXA + 2 * kZPairs - 1) / (2 * kZPairs), d.NYA);
-    k_z_fused<NF><<<g, z_threads(NF, kZLines), sm, s>>>(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits,
+    k_z_fused<NF><<<g, z_threads_fused(NF), sm, s>>>(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits,
                                                        ke_partial);
   }
 };
@@ -1931,7 +1936,7 @@ template <int NF>
 struct FwdY {
   static void run(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
                   cudaStream_t s) {
-    size_t sm = (NF ? 1 : 2) * kNB1 * (size_t)(d.NYA + kPadXY) * sizeof(double2);
+    size_t sm = (NF ? 1 : 2) * kNB1 * (size_t)(d.NYA + kPadY) * sizeof(double2);
     set_smem(k_fwd_y<NF>, sm);
     dim3 g(nq, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
     k_fwd_y<NF><<<g, kThreadsY, sm, s>>>(d, Q1, qspec, scale, py);
