@@ -33,6 +33,8 @@ CONFIGS = {
                          NX=64, NY=64, NZ=48, dt=1e-4, seed=0, Ra=1e5),
     "rbc_96x96x192": dict(eq="rbc_noslip_ra1e8.equations", par="rbc_noslip_ra1e8_96x96x192.parameters.in",
                           NX=96, NY=96, NZ=192, dt=1e-6, seed=2, Ra=1e8),
+    "rbc_192x192x192": dict(eq="rbc_noslip_ra1e8.equations", par="rbc_noslip_ra1e8_192x192x192.parameters.in",
+                            NX=192, NY=192, NZ=192, dt=1e-6, seed=2, Ra=1e8),
     "rbc_32x32x192": dict(eq="rbc_noslip_ra1e8.equations", par="rbc_noslip_ra1e8_32x32x192.parameters.in",
                           NX=32, NY=32, NZ=192, dt=1e-6, seed=2, Ra=1e8),
     "rrbc_192x192x96": dict(eq="rrbc_stressfree_ek1e-4_ra5e7.equations", par="rrbc_stressfree_192x192x96.parameters.in",

@@ -82,6 +82,10 @@ struct KSys {
   int *row_pos = nullptr, *col_pos = nullptr, *cls_row = nullptr, *cls_col = nullptr;
   unsigned char* colflip_cls = nullptr;
   DevEll Lp;
+  // operator-stationary K_std: tile windows and window-relative L
+  int* tile_win = nullptr;
+  int tile_lwin_max = 0;
+  DevEll Lw;
   double2* work = nullptr;
   double2* work2 = nullptr;  // thread-per-block layout of the active systems' vectors (split only)
   std::vector<std::vector<int>> tab_t;   // per var: [NZ][kTabW]
@@ -328,6 +332,33 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
       for (int& c : lp.col)
         if (c >= 0) c = k.ops.col_cls_pos[c];
       k.Lp = upload_ell(mem, lp);
+    }
+    if (k.ncls == 2) {
+      // K_std in tiles of kTileRows rows: per tile the window of solution columns
+      // its rows of L touch, and L with columns relative to that window
+      const int ntiles = (k.T + kTileRows - 1) / kTileRows;
+      std::vector<int> tw(2 * (size_t)ntiles, 0);
+      EllOp lw = k.ops.L;
+      for (int tile = 0; tile < ntiles; ++tile) {
+        const int t0 = tile * kTileRows, t1 = std::min(k.T, t0 + kTileRows);
+        int lo = 1 << 30, hi = -1;
+        for (int t = t0; t < t1; ++t)
+          for (int kk = 0; kk < lw.width; ++kk) {
+            const int c = lw.col[(size_t)t * lw.width + kk];
+            if (c >= 0) { lo = std::min(lo, c); hi = std::max(hi, c); }
+          }
+        if (hi < 0) lo = 0;
+        tw[2 * (size_t)tile] = lo;
+        tw[2 * (size_t)tile + 1] = hi - lo + 1 > 0 ? hi - lo + 1 : 0;
+        k.tile_lwin_max = std::max(k.tile_lwin_max, tw[2 * (size_t)tile + 1]);
+        for (int t = t0; t < t1; ++t)
+          for (int kk = 0; kk < lw.width; ++kk) {
+            int& c = lw.col[(size_t)t * lw.width + kk];
+            if (c >= 0) c -= lo;
+          }
+      }
+      k.tile_win = mem.upload(tw);
+      k.Lw = upload_ell(mem, lw);
     }
     if (k.ncls == 2) {
       // thread-per-block layouts: groups of 32 blocks (block = 2 act + class) side by side
@@ -581,6 +612,9 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       sa.work2 = k.work2;
       sa.nblk = k.ncls * h->nact;
       sa.cls_col = k.cls_col;
+      sa.tile_win = k.tile_win;
+      sa.tile_lwin_max = k.tile_lwin_max;
+      sa.Lw = k.Lw;
       {
         const int kv = sa.kl + sa.ku;
         const int u_rows = (kv + 2) & ~1, l_rows = ((kv + 1 + sa.kl + 1) & ~1) - ((kv + 1) & ~1);

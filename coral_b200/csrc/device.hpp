@@ -15,6 +15,7 @@ constexpr int kMaxQuad = 16;    // quadratic variables
 constexpr int kMaxFull = 8;     // full variables
 constexpr int kMaxFullTerms = 8;
 constexpr int kTabW = 5;        // Galerkin -> Chebyshev entries per Chebyshev row
+constexpr int kTileRows = 128;  // rows per tile of the operator-stationary K_std kernel
 
 // Row-list operator: y[r] = sum_k coef[grp(r,k)] * val(r,k) * x[col(r,k)].
 // Stored slot-major ([k][r]) so that a warp reading rows r..r+31 of one slot
@@ -140,6 +141,12 @@ struct SolveArgs {
   int nblk;              // ncls * nact
   const int* cls_col;    // [ncls*Tc] variable column of a class position, -1 = padding: the
                          // thread-per-block solve writes its solution straight into out
+  // operator-stationary K_std (null tile_win: k_kstd_out): rows in tiles of
+  // kTileRows; tile_win[2 tile + .] = (start, width) of the solution columns the
+  // tile's rows of L touch; Lw = L with its columns relative to that window
+  const int* tile_win;
+  int tile_lwin_max;     // widest window
+  DevEll Lw;
 };
 void launch_solve(const SolveArgs& a, cudaStream_t s);
 // real-scaled factors (unsplit: kl <= 31, kl+ku <= 63; class split: kl <= 15,

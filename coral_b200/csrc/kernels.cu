@@ -1655,6 +1655,59 @@ __global__ void __launch_bounds__(kRhsThreads) k_kstd_out(SolveArgs a) {
 }
 
 // ------------------------------------------------------------------------------
+// Operator-stationary K_std: a CTA takes one tile of kTileRows rows and kTileSys
+// active systems.  Each thread keeps its row of L (columns relative to the
+// tile's solution window) in registers; the CTA first stages the windows of all
+// its systems (coalesced loads from the stage output), then evaluates its row
+// for the systems one after the other.  Same arithmetic and order as
+// k_kstd_out.
+// ------------------------------------------------------------------------------
+constexpr int kTileSys = 8;  // systems per CTA
+constexpr int kLW = 16;      // register slots: L entries per row (wider L takes k_kstd_out)
+
+__global__ void __launch_bounds__(kTileRows, 4) k_kstd_tiles(SolveArgs a) {
+  extern __shared__ double2 xw[];
+  __shared__ double2 cls[kTileSys][kMaxGroups];
+  const int T = a.T;
+  const int tile = blockIdx.x, t = tile * kTileRows + threadIdx.x;
+  const bool row_ok = t < T;
+  const int llo = a.tile_win[2 * tile], lw = a.tile_win[2 * tile + 1];
+  const int a0 = blockIdx.y * kTileSys;
+  const int ns = min(kTileSys, a.nact - a0);
+  if (threadIdx.x < kTileSys * kMaxGroups) {
+    const int u = threadIdx.x / kMaxGroups, g = threadIdx.x - u * kMaxGroups;
+    const int sid = a.act_list[a0 + (u < ns ? u : 0)];
+    const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
+    cls[u][g] = (g < a.L.ngroups) ? cmul(ipow(a.kx[kx], a.L.gkx[g]), ipow(a.ky[ky], a.L.gky[g])) : zero2();
+  }
+  for (int u = 0; u < ns; ++u) {
+    const double2* x = a.out + (size_t)a.act_list[a0 + u] * T + llo;
+    for (int i = threadIdx.x; i < lw; i += kTileRows) xw[u * lw + i] = x[i];
+  }
+  __syncthreads();
+  if (!row_ok) return;
+  int lcg[kLW];
+  double lv[kLW];
+#pragma unroll
+  for (int k = 0; k < kLW; ++k) {
+    const bool ok = k < a.Lw.width;
+    lcg[k] = ok ? a.Lw.cg[k * a.Lw.rows + t] : 0;
+    lv[k] = ok ? a.Lw.val[k * a.Lw.rows + t] : 0.0;
+  }
+  for (int u = 0; u < ns; ++u) {
+    const double2* x = xw + u * lw;
+    double2 ks = zero2();
+#pragma unroll
+    for (int k = 0; k < kLW; ++k)
+      if (lv[k] != 0.0) {
+        const double2 xv = x[lcg[k] & 0xFFFFFF];
+        ks = cadd(ks, cmul(cls[u][lcg[k] >> 24], make_double2(lv[k] * xv.x, lv[k] * xv.y)));
+      }
+    a.Kstd_out[(size_t)a.act_list[a0 + u] * T + t] = ks;
+  }
+}
+
+// ------------------------------------------------------------------------------
 // mean (kx = ky = 0) systems: real arithmetic, one warp per system
 // ------------------------------------------------------------------------------
 __device__ double ell_row_real(const DevEll& op, int t, const double* x) {
@@ -2024,6 +2077,13 @@ void launch_subst(const SolveArgs& a, cudaStream_t s) {
 void launch_kstd_out(const SolveArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;
   if (a.work2 && !a.Kstd_out) return;  // solution already in out, no K_std in the last stage
+  if (a.work2 && a.tile_win && a.Lw.width <= kLW) {
+    const size_t sm = (size_t)kTileSys * a.tile_lwin_max * sizeof(double2);
+    set_smem(k_kstd_tiles, sm);
+    const dim3 g((a.T + kTileRows - 1) / kTileRows, (a.nact + kTileSys - 1) / kTileSys);
+    k_kstd_tiles<<<g, kTileRows, sm, s>>>(a);
+    return;
+  }
   const size_t smx = (size_t)a.T * sizeof(double2);
   if (smx > 48 * 1024) set_smem(k_kstd_out, smx);
   k_kstd_out<<<a.nact, kRhsThreads, smx, s>>>(a);
