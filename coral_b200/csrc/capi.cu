@@ -82,6 +82,9 @@ struct KSys {
   int *row_pos = nullptr, *col_pos = nullptr, *cls_row = nullptr, *cls_col = nullptr;
   unsigned char* colflip_cls = nullptr;
   DevEll Lp;
+  // per class column, band entries nonzero in any block (thread-per-block layout)
+  unsigned long long* cmask = nullptr;
+  unsigned *lmask = nullptr, *umask = nullptr;
   // operator-stationary K_std: tile windows and window-relative L
   int* tile_win = nullptr;
   int tile_lwin_max = 0;
@@ -366,6 +369,9 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
       k.abr = mem.get<double>(ngroups * k.Tc * k.ldab_s * 32);
       k.dpiv = mem.get<unsigned char>(ngroups * k.Tc * 32);
       k.work2 = mem.get<double2>(ngroups * k.Tc * 32);
+      k.cmask = mem.get<unsigned long long>(k.Tc);
+      k.lmask = mem.get<unsigned>(k.Tc);
+      k.umask = mem.get<unsigned>(k.Tc);
       CK(cudaMemset(k.work2, 0, ngroups * k.Tc * 32 * sizeof(double2)));
     } else {
       if (k.real) k.abr = mem.get<double>((size_t)h->nact * k.Tc * k.ldab_s);
@@ -612,6 +618,8 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       sa.work2 = k.work2;
       sa.nblk = k.ncls * h->nact;
       sa.cls_col = k.cls_col;
+      sa.lmask = k.lmask;
+      sa.umask = k.umask;
       sa.tile_win = k.tile_win;
       sa.tile_lwin_max = k.tile_lwin_max;
       sa.Lw = k.Lw;
@@ -666,6 +674,9 @@ void factorize(coral_handle* h, double dt) {
     fa.cls_row = k.cls_row;
     fa.col_pos = k.col_pos;
     fa.tpb = k.work2 != nullptr;
+    fa.cmask = k.cmask;
+    fa.lmask = k.lmask;
+    fa.umask = k.umask;
     fa.nact = h->nact;
     fa.M = k.M;
     fa.L = k.L;

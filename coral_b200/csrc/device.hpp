@@ -147,6 +147,10 @@ struct SolveArgs {
   const int* tile_win;
   int tile_lwin_max;     // widest window
   DevEll Lw;
+  // band entries that are zero in every block are not loaded (FactorArgs::lmask,
+  // umask; null: load all)
+  const unsigned* lmask;
+  const unsigned* umask;
 };
 void launch_solve(const SolveArgs& a, cudaStream_t s);
 // real-scaled factors (unsplit: kl <= 31, kl+ku <= 63; class split: kl <= 15,
@@ -177,6 +181,13 @@ struct FactorArgs {
   const int* cls_row;    // [ncls*Tc] equation row of a class position, -1 = identity padding
   const int* col_pos;    // [T] class position of a variable column
   int tpb;               // 1: interleaved thread-per-block factor layout (see SolveArgs::work2)
+  // thread-per-block layout: per class column j, the band rows nonzero in any
+  // block (cmask, bit r = band row r), and derived from it the L rows
+  // (lmask[j], bit i = row kl+ku+1+i of column j) and the U entries of row j
+  // (umask[j], bit i = entry (j, j+1+i)) that are nonzero in any block
+  unsigned long long* cmask;
+  unsigned* lmask;
+  unsigned* umask;
 };
 void launch_factor(const FactorArgs& a, cudaStream_t s);
 void launch_factor_real(const FactorArgs& a, cudaStream_t s);

@@ -1276,6 +1276,35 @@ __global__ void __launch_bounds__(kTpbThreads) k_factor_tpb(FactorArgs a) {
   if (info) atomicMax(a.info + sys, info);
 }
 
+// Band rows that are nonzero in any block, per class column: one warp per
+// (group, column) tests the 32 blocks of its group row by row (lanes beyond
+// the last block count as zero).
+__global__ void __launch_bounds__(256) k_mask_cols(FactorArgs a) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int g = blockIdx.x, j = blockIdx.y * 8 + w;
+  const int T = a.Tc, ldab = a.ldab;
+  if (j >= T) return;
+  const bool ok = g * 32 + lane < a.ncls * a.nact;
+  const double* F = a.abr + ((size_t)g * T + j) * ldab * 32 + lane;
+  unsigned long long bits = 0;
+  for (int r = 0; r < ldab; ++r) {
+    const double v = ok ? F[(size_t)r * 32] : 0.0;
+    if (__any_sync(0xffffffffu, v != 0.0)) bits |= 1ull << r;
+  }
+  if (lane == 0 && bits) atomicOr(a.cmask + j, bits);
+}
+// lmask / umask from cmask (see FactorArgs)
+__global__ void k_mask_rows(FactorArgs a) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int T = a.Tc, kl = a.kl, kv = a.kl + a.ku;
+  if (j >= T) return;
+  a.lmask[j] = (unsigned)((a.cmask[j] >> (kv + 1)) & ((1ull << kl) - 1));
+  unsigned u = 0;
+  for (int i = 0; i < kv; ++i)
+    if (j + 1 + i < T && ((a.cmask[j + 1 + i] >> (kv - 1 - i)) & 1ull)) u |= 1u << i;
+  a.umask[j] = u;
+}
+
 // Forward (P, L: the column sweep with the row interchanges interleaved, as the
 // reference's band solve) then backward (U, row form: each x_j subtracts the
 // known x_{j+i} in decreasing column order, the order in which the column sweep
@@ -1307,12 +1336,18 @@ __global__ void __launch_bounds__(kTpbThreads) k_subst_tpb(SolveArgs a) {
   double2* win = swin + threadIdx.x;
   // ---- forward: positions j..j+KL in slots p mod W1 ----
   for (int p = 0; p <= KL && p < T; ++p) win[(p & (W1 - 1)) * S] = X[(size_t)p * 32];
+  // L rows / U entries that are zero in every block are not loaded
+  const unsigned* lmask = a.lmask;
+  const unsigned* umask = a.umask;
   if (T > 1) {
     double lv[KL], lvn[KL];
     int jpn = P[0];
     double2 incn = (KL + 1 < T) ? X[(size_t)(KL + 1) * 32] : zero2();
+    {
+      const unsigned lm = lmask ? lmask[0] : ~0u;
 #pragma unroll
-    for (int i = 0; i < KL; ++i) lvn[i] = F[(KV + 1 + i) * 32];
+      for (int i = 0; i < KL; ++i) lvn[i] = ((lm >> i) & 1u) ? F[(KV + 1 + i) * 32] : 0.0;
+    }
     for (int j = 0; j < T - 1; ++j) {
 #pragma unroll
       for (int i = 0; i < KL; ++i) lv[i] = lvn[i];
@@ -1320,8 +1355,9 @@ __global__ void __launch_bounds__(kTpbThreads) k_subst_tpb(SolveArgs a) {
       const double2 inc = incn;
       if (j + 1 < T - 1) {  // next column's multipliers, pivot and incoming entry
         const double* Fn = F + (size_t)(j + 1) * CS;
+        const unsigned lm = lmask ? lmask[j + 1] : ~0u;
 #pragma unroll
-        for (int i = 0; i < KL; ++i) lvn[i] = Fn[(KV + 1 + i) * 32];
+        for (int i = 0; i < KL; ++i) lvn[i] = ((lm >> i) & 1u) ? Fn[(KV + 1 + i) * 32] : 0.0;
         jpn = P[(size_t)(j + 1) * 32];
         incn = (j + KL + 2 < T) ? X[(size_t)(j + KL + 2) * 32] : zero2();
       }
@@ -1375,8 +1411,9 @@ __global__ void __launch_bounds__(kTpbThreads) k_subst_tpb(SolveArgs a) {
     double2 yn;
     {
       const double* Fj = F + (size_t)j * CS;
+      const unsigned um = umask ? umask[j] : ~0u;
 #pragma unroll
-      for (int i = 0; i < KV; ++i) un[i] = Fj[((1 + i) * LD + KV - 1 - i) * 32];
+      for (int i = 0; i < KV; ++i) un[i] = ((um >> i) & 1u) ? Fj[((1 + i) * LD + KV - 1 - i) * 32] : 0.0;
       dinvn = Fj[KV * 32];
       yn = X[(size_t)j * 32];
     }
@@ -1387,8 +1424,9 @@ __global__ void __launch_bounds__(kTpbThreads) k_subst_tpb(SolveArgs a) {
       double2 acc = yn;
       if (j > 0) {  // next row (j - 1)
         const double* Fn = F + (size_t)(j - 1) * CS;
+        const unsigned um = umask ? umask[j - 1] : ~0u;
 #pragma unroll
-        for (int i = 0; i < KV; ++i) un[i] = Fn[((1 + i) * LD + KV - 1 - i) * 32];
+        for (int i = 0; i < KV; ++i) un[i] = ((um >> i) & 1u) ? Fn[((1 + i) * LD + KV - 1 - i) * 32] : 0.0;
         dinvn = Fn[KV * 32];
         yn = X[(size_t)(j - 1) * 32];
       }
@@ -1568,7 +1606,9 @@ __global__ void __launch_bounds__(kRhsThreads) k_rhs_nl(SolveArgs a, NLArgs n) {
         if (v[3] == 0.0) break;
       }
     }
-    n.Khat[base + t] = kh;
+    // K_hat of the last stage is used only here, from the register (the next step
+    // starts from K_hat_0)
+    if (!a.last_stage) n.Khat[base + t] = kh;
     double2 r = zero2();
     if (!origin) {
 #pragma unroll 4
@@ -2098,6 +2138,11 @@ void launch_factor_real(const FactorArgs& a, cudaStream_t s) {
   if (a.tpb) {
     const int nb = a.ncls * a.nact;
     k_factor_tpb<<<(nb + kTpbThreads - 1) / kTpbThreads, kTpbThreads, 0, s>>>(a);
+    if (a.cmask && a.ldab <= 64 && a.kl + a.ku <= 32 && a.kl <= 32) {
+      cudaMemsetAsync(a.cmask, 0, (size_t)a.Tc * sizeof(unsigned long long), s);
+      k_mask_cols<<<dim3((nb + 31) / 32, (a.Tc + 7) / 8), 256, 0, s>>>(a);
+      k_mask_rows<<<(a.Tc + 127) / 128, 128, 0, s>>>(a);
+    }
     return;
   }
   k_factor_real<<<dim3((a.nact + kWPB - 1) / kWPB, a.ncls), kWPB * 32, 0, s>>>(a);
