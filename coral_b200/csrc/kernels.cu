@@ -49,6 +49,11 @@ __host__ __device__ constexpr int xy_threads(int N, int nl, int pv) {
 }
 #define kThreadsX xy_threads(NF, 4, kPlanHot)
 #define kThreadsY xy_threads(NF, 4, kPlanY)
+// the pipelined forward y pass reads its first-pass inputs from shared memory:
+// plan and threads of its own
+constexpr int kPlanYF = 1;
+#define kThreadsYF xy_threads(NF, 4, kPlanYF)
+#define kMinBlocksYF (kPlanYF ? hot_min_blocks(kThreadsYF) : kMinBlocksY)
 // CTAs per SM the kernels with two-pass plans are compiled for: registers
 // capped at no fewer than 128 per thread
 __host__ __device__ constexpr int hot_min_blocks(int nt) { return 65536 / (nt * 128) > 1 ? 65536 / (nt * 128) : 1; }
@@ -59,6 +64,23 @@ constexpr int kMinBlocksZ = 4;
 constexpr int kWPB = 8;  // warps (systems) per CTA in the per-system kernels
 
 __device__ __forceinline__ double2 zero2() { return make_double2(0.0, 0.0); }
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+// 16 bytes, or zeros when !valid (then gmem is not read)
+__device__ __forceinline__ void cp_async16z(void* smem, const void* gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? 16 : 0;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(n) : "memory");
+}
+
 
 __device__ __forceinline__ double2 ipow(double k, int e) {
   // (i k)^e by repeated multiplication, as Fortran's complex**integer
@@ -545,6 +567,56 @@ __global__ void __launch_bounds__(kThreadsY, kMinBlocksY) k_fwd_y(Dims d, const 
   }
 }
 
+// The same pass for compiled lengths as a persistent kernel: each CTA walks the
+// tiles (quadratic variable, block of kNB1 Chebyshev rows, kx) with a stride of
+// the grid size; the next tile's input is copied into a staging buffer with
+// cp.async while the current tile's later FFT passes and stores run (the first
+// pass reads the staging buffer and frees it).
+template <int NF>
+__global__ void __launch_bounds__(kThreadsYF, kMinBlocksYF) k_fwd_y_pipe(Dims d, int nq, const double2* Q1,
+                                                                        double2* qspec, double scale, FftPlan py) {
+  extern __shared__ double2 sm[];
+  constexpr int NYA = NF;
+  constexpr PlanR P = plan_of(NF, kPlanYF);
+  const int LS = NYA + kPadY;
+  double2* A = sm;                 // kNB1 lines, stride LS
+  double2* stg = A + kNB1 * LS;    // staged input [y][kNB1]
+  const int nnb = (d.NZ + kNB1 - 1) / kNB1;
+  const int ntiles = nq * nnb * d.NXH;
+  const size_t ystride = (size_t)d.NXH * d.NZ;
+  auto issue = [&](int tile) {
+    if (tile < ntiles) {
+      const int qi = tile % nq, r = tile / nq, nb = r % nnb, kx = r / nnb, n0 = nb * kNB1;
+      const double2* src = Q1 + ((size_t)qi * NYA * d.NXH + kx) * d.NZ + n0;
+      for (int e = threadIdx.x; e < NYA * kNB1; e += blockDim.x) {
+        const int y = e / kNB1, ln = e - y * kNB1;
+        const bool ok = n0 + ln < d.NZ;
+        cp_async16z(stg + e, ok ? src + y * ystride + ln : Q1, ok);
+      }
+    }
+    cp_async_commit();
+  };
+  issue(blockIdx.x);
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int qi = tile % nq, r = tile / nq, nb = r % nnb, kx = r / nnb, n0 = nb * kNB1;
+    cp_async_wait<0>();
+    __syncthreads();
+    auto ld = [&](int ln, int y) -> double2 {
+      const double2 v = stg[y * kNB1 + ln];
+      return (n0 + ln == 0) ? cscale(v, 0.5) : v;
+    };
+    fft_pass_first<NF, P.r[0], false, kThreadsYF, kNB1, true>(A, kNB1, LS, ld);  // ends with a barrier
+    issue(tile + gridDim.x);
+    fft_passes<NF, 1, P.r[0], false, kThreadsYF, kNB1, kPlanYF>(A, kNB1, LS, py.tw);
+    for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
+      const int ln = idx % kNB1, ky = idx / kNB1, n = n0 + ln;
+      if (n < d.NZ) qspec[(((size_t)qi * d.NXH + kx) * NYA + ky) * d.NZ + n] = cscale(A[ln * LS + ky], scale);
+    }
+    __syncthreads();  // A is rewritten by the next tile's first pass
+  }
+  cp_async_wait<0>();
+}
+
 // remove_vertical_mean_of_quadratic_var (PL_IMEX_timestepping.f90:223-235)
 __global__ void k_remove_zmean(Dims d, double2* qs) {
   const size_t col = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -975,16 +1047,6 @@ __global__ void __launch_bounds__(kWPB * 32) k_factor_real(FactorArgs a) {
 constexpr int kWPBr = 4;   // warps per CTA
 constexpr int kCW = 8;     // factor columns per ring chunk (divides 32)
 constexpr int kNBUF = 4;   // ring chunks per warp
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
 
 __device__ __forceinline__ double2 shfl2(double2 v, int src) {
   return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
@@ -1960,6 +2022,16 @@ void dispatch_len(int n, Args&&... args) {
   }
 }
 
+// CTAs of a persistent kernel: as many as fit on the device at once
+template <class K>
+int persistent_ctas(K kernel, int threads, size_t smem) {
+  int dev = 0, nsm = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem);
+  return std::max(1, nsm * std::max(per, 1));
+}
+
 template <int NF>
 struct InvY {
   static void run(const Dims& d, int nf, const FullVarDev* fv, StateSet st, const double2* plain_spec,
@@ -2029,6 +2101,16 @@ template <int NF>
 struct FwdY {
   static void run(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
                   cudaStream_t s) {
+    if constexpr (NF != 0) {
+      // persistent pipelined kernel: as many CTAs as fit on the device at once
+      const size_t sm = (kNB1 * (size_t)(NF + kPadY) + (size_t)NF * kNB1) * sizeof(double2);
+      set_smem(k_fwd_y_pipe<NF>, sm);
+      static int nct = 0;
+      if (!nct) nct = persistent_ctas(k_fwd_y_pipe<NF>, kThreadsYF, sm);
+      const int ntiles = nq * ((d.NZ + kNB1 - 1) / kNB1) * d.NXH;
+      k_fwd_y_pipe<NF><<<std::min(nct, ntiles), kThreadsYF, sm, s>>>(d, nq, Q1, qspec, scale, py);
+      return;
+    }
     size_t sm = (NF ? 1 : 2) * kNB1 * (size_t)(d.NYA + kPadY) * sizeof(double2);
     set_smem(k_fwd_y<NF>, sm);
     dim3 g(nq, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
