@@ -135,17 +135,19 @@ def make_ic(cfg, pl):
 # kernels of each timed phase (names as ncu lists them)
 PHASE_KERNELS = {
     "inv_y": "k_inv_y", "inv_x": "k_inv_x", "inv_z": "k_inv_z", "z_products": "k_z_fused",
-    "fwd_x": "k_fwd_x", "fwd_y": "k_fwd_y", "nl_assembly": "k_nl",
-    "rhs_nl": "k_rhs_nl", "mean_systems": "k_zero_step", "substitution": "k_subst_tpb", "kstd_out": "k_kstd_out",
+    "fwd_x": "k_fwd_x", "fwd_y": "k_fwd_y_pipe", "nl_assembly": "k_nl",
+    "rhs_nl": "k_rhs_tiles", "mean_systems": "k_zero_step", "substitution": "k_subst_tpb", "kstd_out": "k_kstd_tiles",
 }
 
 
-def phase_bytes(g, nsys, nact, T, ncls, Tc, kl, ku, stages, factor_bytes):
+def phase_bytes(g, nsys, nact, T, ncls, Tc, kl, ku, stages, factor_bytes, factor_entries=0):
     """Algorithmic HBM bytes of one launch of each phase (averaged over the
     stages): every array a phase must read from or write to HBM once.
     g: dict with NXH, NYA, NXA, NZ, NZA, nF (full variables), nQ (quadratic
     variables).  Transform intermediates are 16-byte complex where the data are
-    complex (after an x r2c / before an x c2r) and 8-byte real otherwise."""
+    complex (after an x r2c / before an x c2r) and 8-byte real otherwise.
+    factor_entries: LU band entries per block that the substitution reads (the
+    entries nonzero in some block; 0 = the whole band, 2 kl + ku + 1 per column)."""
     NXH, NYA, NXA, NZ, NZA, nF, nQ = (g[k] for k in ("NXH", "NYA", "NXA", "NZ", "NZA", "nF", "nQ"))
     y1 = lambda nv: nv * NYA * NXH * NZ * 16   # [var][y][kx][n] complex
     y2 = lambda nv: nv * NYA * NXA * NZ * 8    # [var][y][x][n] real
@@ -165,16 +167,18 @@ def phase_bytes(g, nsys, nact, T, ncls, Tc, kl, ku, stages, factor_bytes):
     # K arrays of the i earlier stages; the last stage writes no K_std):
     #   rhs_nl: state, K arrays and quadratic coefficients in, K_hat and the
     #     right-hand side (inactive systems: the stage output) out
-    #   substitution: LU factors (2 kl + ku + 1 band entries and one pivot byte
-    #     per column of each block) and the block vectors (right-hand side in,
-    #     intermediate out and in, solution out)
+    #   substitution: LU factors (the band entries that are nonzero in some
+    #     block, or all 2 kl + ku + 1 per column, and one pivot byte per column of
+    #     each block) and the block vectors (right-hand side in, intermediate out
+    #     and in, solution out)
     #   kstd_out: solution in, stage output and K_std out (active systems)
     rhs = sub = kst = 0
     nblk_cols = nact * ncls * Tc
     for i in range(stages):
         last = (i == stages - 1)
         rhs += nsys * 16 * T * (1 + 2 * i + 1 + 1) + nact * 16 * nQ * NZ + (nsys - nact) * 16 * T * (0 if last else 1)
-        sub += nblk_cols * (factor_bytes * (2 * kl + ku + 1) + 1) + 4 * 16 * nblk_cols
+        entries = factor_entries * nact * ncls if factor_entries else nblk_cols * (2 * kl + ku + 1)
+        sub += entries * factor_bytes + nblk_cols + 4 * 16 * nblk_cols
         kst += 16 * nblk_cols + nact * 16 * T * (1 if last else 2)
     out["rhs_nl"] = rhs / stages
     out["substitution"] = sub / stages
@@ -280,7 +284,8 @@ def run_ours(args, cfg):
     ncls, Tc, kl_c, ku_c = pl.query(800), pl.query(900), pl.query(1000), pl.query(1100)
     geo = {"NXH": pl.NXH, "NYA": pl.NYAA, "NXA": pl.NXAA, "NZ": pl.NZ, "NZA": pl.NZAA,
            "nF": pl.query(8), "nQ": pl.query(9)}
-    pbytes = phase_bytes(geo, nsys, nact, T, ncls, Tc, kl_c, ku_c, pl.stages, fbytes)
+    fentries = pl.query(1200)  # after the factorisation of the timed steps
+    pbytes = phase_bytes(geo, nsys, nact, T, ncls, Tc, kl_c, ku_c, pl.stages, fbytes, fentries)
     peak, src = read_peaks()
     phases = {}
     for k, b in pbytes.items():

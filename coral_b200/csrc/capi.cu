@@ -89,6 +89,9 @@ struct KSys {
   int* tile_win = nullptr;
   int tile_lwin_max = 0;
   DevEll Lw;
+  int* rhs_win = nullptr;
+  int rhs_win_max = 0;
+  DevEll Mw, NLw;
   double2* work = nullptr;
   double2* work2 = nullptr;  // thread-per-block layout of the active systems' vectors (split only)
   std::vector<std::vector<int>> tab_t;   // per var: [NZ][kTabW]
@@ -362,6 +365,54 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
       }
       k.tile_win = mem.upload(tw);
       k.Lw = upload_ell(mem, lw);
+      // the right-hand side in the same row tiles: the state window of M's
+      // columns, the Chebyshev range and the quadratic variables of the NL
+      // operator's columns (quad * NZ + n), and both operators relative to them
+      std::vector<int> rw((size_t)ntiles * kRhsWin, 0);
+      EllOp mw = k.ops.M, nw = k.ops.NLop;
+      const int NZ = g.NZ;
+      for (int tile = 0; tile < ntiles; ++tile) {
+        const int t0 = tile * kTileRows, t1 = std::min(k.T, t0 + kTileRows);
+        int mlo = 1 << 30, mhi = -1, nlo = 1 << 30, nhi = -1;
+        std::vector<int> slot(kMaxQuad, -1), qs;
+        for (int t = t0; t < t1; ++t) {
+          for (int kk = 0; kk < mw.width; ++kk) {
+            const int c = mw.col[(size_t)t * mw.width + kk];
+            if (c >= 0) { mlo = std::min(mlo, c); mhi = std::max(mhi, c); }
+          }
+          for (int kk = 0; kk < nw.width; ++kk) {
+            const int c = nw.col[(size_t)t * nw.width + kk];
+            if (c < 0) continue;
+            const int q = c / NZ, n = c - q * NZ;
+            if (q >= kMaxQuad) throw CoralError(CORAL_EUNSUPPORTED, "too many quadratic variables");
+            nlo = std::min(nlo, n);
+            nhi = std::max(nhi, n);
+            if (slot[q] < 0) { slot[q] = (int)qs.size(); qs.push_back(q); }
+          }
+        }
+        if (mhi < 0) mlo = mhi = 0;
+        if (nhi < 0) nlo = nhi = 0;
+        const int mwid = mhi - mlo + 1, nwid = nhi - nlo + 1;
+        int* r = rw.data() + (size_t)tile * kRhsWin;
+        r[0] = mlo; r[1] = mwid; r[2] = nlo; r[3] = nwid; r[4] = (int)qs.size();
+        for (size_t i = 0; i < qs.size(); ++i) r[5 + i] = qs[i];
+        k.rhs_win_max = std::max(k.rhs_win_max, mwid + (int)qs.size() * nwid);
+        for (int t = t0; t < t1; ++t) {
+          for (int kk = 0; kk < mw.width; ++kk) {
+            int& c = mw.col[(size_t)t * mw.width + kk];
+            if (c >= 0) c -= mlo;
+          }
+          for (int kk = 0; kk < nw.width; ++kk) {
+            int& c = nw.col[(size_t)t * nw.width + kk];
+            if (c < 0) continue;
+            const int q = c / NZ, n = c - q * NZ;
+            c = slot[q] * nwid + n - nlo;
+          }
+        }
+      }
+      k.rhs_win = mem.upload(rw);
+      k.Mw = upload_ell(mem, mw);
+      k.NLw = upload_ell(mem, nw);
     }
     if (k.ncls == 2) {
       // thread-per-block layouts: groups of 32 blocks (block = 2 act + class) side by side
@@ -622,6 +673,10 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       sa.umask = k.umask;
       sa.tile_win = k.tile_win;
       sa.tile_lwin_max = k.tile_lwin_max;
+      sa.rhs_win = k.rhs_win;
+      sa.rhs_win_max = k.rhs_win_max;
+      sa.Mw = k.Mw;
+      sa.NLw = k.NLw;
       sa.Lw = k.Lw;
       {
         const int kv = sa.kl + sa.ku;
@@ -992,6 +1047,20 @@ int coral_query(const coral_handle* hc, int what, long long* value) {
   if (base == CORAL_Q_SYS_CLASS_T && i < (int)h->ks.size()) { *value = h->ks[i].Tc; return 0; }
   if (base == CORAL_Q_SYS_CLASS_KL && i < (int)h->ks.size()) { *value = h->ks[i].kl_s; return 0; }
   if (base == CORAL_Q_SYS_CLASS_KU && i < (int)h->ks.size()) { *value = h->ks[i].ku_s; return 0; }
+  if (base == CORAL_Q_SYS_FACTOR_ENTRIES && i < (int)h->ks.size()) {
+    const KSys& k = h->ks[i];
+    *value = 0;
+    if (!k.lmask || h->dt_factored < 0.0) return 0;
+    std::vector<unsigned> lm(k.Tc), um(k.Tc);
+    if (cudaSetDevice(h->device) != cudaSuccess || cudaStreamSynchronize(h->stream) != cudaSuccess ||
+        cudaMemcpy(lm.data(), k.lmask, k.Tc * sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(um.data(), k.umask, k.Tc * sizeof(unsigned), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return CORAL_ECUDA;
+    long long n = 0;
+    for (int j = 0; j < k.Tc; ++j) n += 1 + __builtin_popcount(lm[j]) + __builtin_popcount(um[j]);
+    *value = n;
+    return 0;
+  }
   return CORAL_EBADARG;
 }
 

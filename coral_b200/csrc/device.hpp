@@ -16,6 +16,7 @@ constexpr int kMaxFull = 8;     // full variables
 constexpr int kMaxFullTerms = 8;
 constexpr int kTabW = 5;        // Galerkin -> Chebyshev entries per Chebyshev row
 constexpr int kTileRows = 128;  // rows per tile of the operator-stationary K_std kernel
+constexpr int kRhsWin = 5 + kMaxQuad;  // ints per tile of SolveArgs::rhs_win
 
 // Row-list operator: y[r] = sum_k coef[grp(r,k)] * val(r,k) * x[col(r,k)].
 // Stored slot-major ([k][r]) so that a warp reading rows r..r+31 of one slot
@@ -147,6 +148,16 @@ struct SolveArgs {
   const int* tile_win;
   int tile_lwin_max;     // widest window
   DevEll Lw;
+  // operator-stationary right-hand side (null rhs_win: k_rhs_nl): per tile of
+  // kTileRows rows, rhs_win[kRhsWin tile + .] = (start, width) of the state
+  // columns its rows of M touch, (start, width) of the Chebyshev range its rows
+  // of the NL operator touch, the number of quadratic variables they touch and
+  // those variables; Mw = M with columns relative to the state window, NLw = the
+  // NL operator with columns slot * width + n - start (slot: position of the
+  // variable in the tile's list)
+  const int* rhs_win;
+  int rhs_win_max;       // widest window (state + all slots), complex entries
+  DevEll Mw, NLw;
   // band entries that are zero in every block are not loaded (FactorArgs::lmask,
   // umask; null: load all)
   const unsigned* lmask;

@@ -1810,6 +1810,135 @@ __global__ void __launch_bounds__(kTileRows, 4) k_kstd_tiles(SolveArgs a) {
 }
 
 // ------------------------------------------------------------------------------
+// Operator-stationary right-hand side: a CTA takes one tile of kTileRows rows
+// and kRhsSys consecutive systems (active or not).  Each thread keeps its row of
+// M and of the NL operator (columns relative to the tile's windows) in
+// registers; the CTA copies the state window and the quadratic-variable windows
+// of its systems into shared memory with cp.async, then evaluates its row: first
+// K_hat and M x of every system from shared memory, then the earlier stages' K
+// arrays (loads of all systems in flight together), then the stores.  Same
+// arithmetic and order as k_rhs_nl.
+// ------------------------------------------------------------------------------
+constexpr int kRhsSys = 4;  // systems per CTA
+
+template <int RM, int RN>
+__global__ void __launch_bounds__(kTileRows, 6) k_rhs_tiles(SolveArgs a, NLArgs n) {
+  extern __shared__ double2 win[];
+  __shared__ double2 cms[kRhsSys][kMaxGroups], cns[kRhsSys][kMaxGroups];
+  const int T = a.T, NZ = a.d.NZ, nsys = a.d.NXH * a.d.NYA;
+  const int tile = blockIdx.y, t = tile * kTileRows + threadIdx.x;
+  const int* rw = a.rhs_win + tile * kRhsWin;
+  const int mlo = rw[0], mw = rw[1], nlo = rw[2], nw = rw[3], nqt = rw[4];
+  const int ws = mw + nqt * nw;  // window entries per system
+  const int s0 = blockIdx.x * kRhsSys, ns = min(kRhsSys, nsys - s0);
+  const size_t qstride = (size_t)nsys * NZ;  // between quadratic variables of qspec
+  for (int u = 0; u < ns; ++u) {
+    const int sid = s0 + u;
+    double2* w = win + u * ws;
+    const double2* f = a.field + (size_t)sid * T + mlo;
+    for (int i = threadIdx.x; i < mw; i += kTileRows) cp_async16(w + i, f + i);
+    if (a.act_index[sid] >= 0)
+      for (int i = threadIdx.x; i < nqt * nw; i += kTileRows) {
+        const int sl = i / nw, k = i - sl * nw;
+        cp_async16(w + mw + i, n.qspec + rw[5 + sl] * qstride + (size_t)sid * NZ + nlo + k);
+      }
+  }
+  cp_async_commit();
+  for (int i = threadIdx.x; i < kRhsSys * kMaxGroups; i += kTileRows) {
+    const int u = i / kMaxGroups, g = i - u * kMaxGroups;
+    const int sid = s0 + (u < ns ? u : 0);
+    const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
+    cms[u][g] = (g < a.Mw.ngroups) ? cmul(ipow(a.kx[kx], a.Mw.gkx[g]), ipow(a.ky[ky], a.Mw.gky[g])) : zero2();
+    cns[u][g] = (g < a.NLw.ngroups) ? cmul(ipow(a.kx[kx], a.NLw.gkx[g]), ipow(a.ky[ky], a.NLw.gky[g])) : zero2();
+  }
+  const bool row_ok = t < T;
+  const int tr = row_ok ? t : 0;
+  int mcg[RM], ncg[RN];
+  double mv[RM], nv[RN];
+#pragma unroll
+  for (int k = 0; k < RM; ++k) {
+    const bool ok = k < a.Mw.width;
+    mcg[k] = ok ? a.Mw.cg[(size_t)k * a.Mw.rows + tr] : 0;
+    mv[k] = ok ? a.Mw.val[(size_t)k * a.Mw.rows + tr] : 0.0;
+  }
+#pragma unroll
+  for (int k = 0; k < RN; ++k) {
+    const bool ok = k < a.NLw.width;
+    ncg[k] = ok ? a.NLw.cg[(size_t)k * a.NLw.rows + tr] : 0;
+    nv[k] = ok ? a.NLw.val[(size_t)k * a.NLw.rows + tr] : 0.0;
+  }
+  int ai[kRhsSys];
+#pragma unroll
+  for (int u = 0; u < kRhsSys; ++u) ai[u] = u < ns ? a.act_index[s0 + u] : -1;
+  cp_async_wait<0>();
+  __syncthreads();
+  if (!row_ok) return;  // no barrier below
+  // phase 1 (shared memory only): K_hat and M x of every system
+  double2 kh[kRhsSys], r[kRhsSys];
+#pragma unroll
+  for (int u = 0; u < kRhsSys; ++u) {
+    kh[u] = zero2();
+    r[u] = zero2();
+    if (u < ns) {
+      const double2* w = win + u * ws;
+      if (ai[u] >= 0) {
+#pragma unroll
+        for (int k = 0; k < RN; ++k)
+          if (nv[k] != 0.0) {
+            const double2 qh = w[mw + (ncg[k] & 0xFFFFFF)];
+            kh[u] = cadd(kh[u], cmul(cns[u][ncg[k] >> 24], make_double2(nv[k] * qh.x, nv[k] * qh.y)));
+          }
+      }
+      if (s0 + u != 0) {
+#pragma unroll
+        for (int k = 0; k < RM; ++k)
+          if (k < a.Mw.width) {
+            const double2 xv = w[mcg[k] & 0xFFFFFF];
+            r[u] = cadd(r[u], cmul(cms[u][mcg[k] >> 24], make_double2(mv[k] * xv.x, mv[k] * xv.y)));
+          }
+      }
+    }
+  }
+  // phase 2: the earlier stages' K arrays (no store in between: the loads of all
+  // systems can be in flight together)
+#pragma unroll
+  for (int j = 0; j < kMaxStages - 1; ++j) {  // static indices into the argument arrays
+    if (j < a.nprev) {
+#pragma unroll
+      for (int u = 0; u < kRhsSys; ++u)
+        if (u < ns) {
+          const size_t base = (size_t)(s0 + u) * T + t;
+          r[u] = cadd(r[u], cscale(a.Kstd[j][base], a.ca[j]));
+          r[u] = cadd(r[u], cscale(a.Khat[j][base], a.ch[j]));
+        }
+    }
+  }
+  // phase 3: stores
+  const int pos = a.row_pos[t], c = pos >= a.Tc ? 1 : 0, pc = pos - c * a.Tc;
+  const unsigned char rf = a.rowflip ? a.rowflip[t] : 0;
+  bool bad = false;
+#pragma unroll
+  for (int u = 0; u < kRhsSys; ++u) {
+    if (u >= ns) break;
+    const size_t base = (size_t)(s0 + u) * T;
+    // K_hat of the last stage is used only here, from the register
+    if (!a.last_stage) n.Khat[base + t] = kh[u];
+    double2 v = cadd(r[u], cscale(kh[u], a.ch[a.nprev]));
+    if (ai[u] >= 0) {
+      if (a.rowflip) v = flip_row(v, rf);
+      const int bb = ai[u] * a.ncls + c;
+      a.work2[((size_t)(bb >> 5) * a.Tc + pc) * 32 + (bb & 31)] = v;
+    } else {
+      if (a.last_stage) v = zero2();
+      bad |= !(isfinite(v.x) && isfinite(v.y));
+      a.out[base + t] = v;
+      if (a.Kstd_out) a.Kstd_out[base + t] = zero2();
+    }
+  }
+  if (bad) atomicOr(a.flags, 1u);
+}
+
+// ------------------------------------------------------------------------------
 // mean (kx = ky = 0) systems: real arithmetic, one warp per system
 // ------------------------------------------------------------------------------
 __device__ double ell_row_real(const DevEll& op, int t, const double* x) {
@@ -2162,7 +2291,19 @@ void launch_factor(const FactorArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;
   k_factor<<<(a.nact + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
 }
+template <int RM, int RN>
+static void launch_rhs_tiles(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
+  const int nsys = a.d.NXH * a.d.NYA;
+  const size_t sm = (size_t)kRhsSys * a.rhs_win_max * sizeof(double2);
+  set_smem(k_rhs_tiles<RM, RN>, sm);
+  const dim3 g((nsys + kRhsSys - 1) / kRhsSys, (a.T + kTileRows - 1) / kTileRows);
+  k_rhs_tiles<RM, RN><<<g, kTileRows, sm, s>>>(a, n);
+}
 void launch_rhs_nl(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
+  if (a.work2 && a.rhs_win && a.row_pos) {
+    if (a.Mw.width <= 4 && a.NLw.width <= 8) return launch_rhs_tiles<4, 8>(a, n, s);
+    if (a.Mw.width <= 8 && a.NLw.width <= 16) return launch_rhs_tiles<8, 16>(a, n, s);
+  }
   const int nsys = a.d.NXH * a.d.NYA;
   const size_t sm = ((size_t)n.nq * a.d.NZ + a.T) * sizeof(double2);
   set_smem(k_rhs_nl, sm);

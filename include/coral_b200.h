@@ -71,6 +71,10 @@ typedef struct coral_handle coral_handle;
 #define CORAL_Q_SYS_CLASS_T 900      /* + isys: positions per block (= SYS_T when not split)        */
 #define CORAL_Q_SYS_CLASS_KL 1000    /* + isys: sub-diagonals of one block's band                   */
 #define CORAL_Q_SYS_CLASS_KU 1100    /* + isys: super-diagonals of one block's band                 */
+#define CORAL_Q_SYS_FACTOR_ENTRIES 1200 /* + isys: LU band entries per block that the substitution reads
+                                        (L and U entries nonzero in some block, and the diagonal),
+                                        summed over the block's columns; 0 before coral_factorize or
+                                        when the solve reads the whole band */
 
 /*
  * Create a solver from the text of coral.equations and coral.parameters.in.

@@ -180,6 +180,12 @@ def test_split_solve_rbc_noslip_matches_oracle(split, monkeypatch):
         ref.step(1e-5)
     pl.march_forward(1e-5, 3)
     pl.synchronize()
+    # band entries the substitution reads: within the block band, at least the diagonal
+    Tc, kl, ku = pl.query(900), pl.query(1000), pl.query(1100)
+    if split:
+        assert Tc <= pl.query(1200) <= Tc * (2 * kl + ku + 1)
+    else:
+        assert pl.query(1200) == 0
     assert _rel(pl.get_field(0), ref.field[0]) < 1e-11
     for s in range(len(ref.zlay)):
         assert _rel(pl.get_mean_field(s), ref.zfield[s]) < 1e-11
