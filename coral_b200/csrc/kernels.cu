@@ -1782,10 +1782,12 @@ __global__ void __launch_bounds__(kTileRows, 4) k_kstd_tiles(SolveArgs a) {
     const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
     cls[u][g] = (g < a.L.ngroups) ? cmul(ipow(a.kx[kx], a.L.gkx[g]), ipow(a.ky[ky], a.L.gky[g])) : zero2();
   }
-  for (int u = 0; u < ns; ++u) {
+  for (int u = 0; u < ns; ++u) {  // cp.async: no register round trip per system
     const double2* x = a.out + (size_t)a.act_list[a0 + u] * T + llo;
-    for (int i = threadIdx.x; i < lw; i += kTileRows) xw[u * lw + i] = x[i];
+    for (int i = threadIdx.x; i < lw; i += kTileRows) cp_async16(xw + u * lw + i, x + i);
   }
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncthreads();
   if (!row_ok) return;
   int lcg[kLW];
