@@ -600,15 +600,17 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       StateSet st = state_set(h, i == 0);
       B(0); launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream); E();
       B(1); launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream); E();
-      CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
+      // the CFL maxima reported after a step are those of its last stage's fields
+      // (each stage's evaluation replaces them): only the last stage computes them
+      if (last) CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
       nl += 2;
     }
     // z passes fused (inverse DCT, CFL maxima, products, KE, forward DCT); the
     // quadratic variables overwrite Y2 in place, each CTA reading and writing only
     // its own (y, x pair) columns
     B(3);
-    launch_z_fused(d, h->nF, h->quads, h->Y2, h->Y2, h->pz, h->dct_tw, h->d_wz, h->d_wzinv, h->cfl_bits,
-                   i == 0 ? h->ke_partial : nullptr, h->stream);
+    launch_z_fused(d, h->nF, h->quads, h->Y2, h->Y2, h->pz, h->dct_tw, h->d_wz, h->d_wzinv,
+                   last ? h->cfl_bits : nullptr, i == 0 ? h->ke_partial : nullptr, h->stream);
     E();
     B(4); launch_fwd_x(d, h->nQ, h->Y2, h->Y1, h->px, h->stream); E();
     B(5); launch_fwd_y(d, h->nQ, h->Y1, h->qspec, scale, h->py, h->stream); E();

@@ -420,39 +420,79 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
       __syncthreads();
     }
   }
-  // ---- CFL maxima of |u|, |v|, |w| / wz over all columns ----
-  if (cfl_bits) {
-    const int ncf = min(nf, 3);
-    double mx[3] = {0.0, 0.0, 0.0};
-    for (int idx = threadIdx.x; idx < ncf * kZPairs * N; idx += blockDim.x) {
-      const int lg = idx / N, m = idx - lg * N, f = lg / kZPairs, pr = lg - f * kZPairs;
-      const double2 v = Fv[idx];
-      double s = 1.0;
-      if (f == 2) s = wzinv[(m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1];
-      double a = col_ok(2 * pr) ? fabs(v.x) * s : 0.0;
-      if (col_ok(2 * pr + 1)) a = fmax(a, fabs(v.y) * s);
+  // ---- CFL maxima of |u|, |v|, |w| / wz and the KE sums (z-weighted products
+  //      of the quadratic variables uu, vv, ww) over all columns, from the
+  //      physical values (Makhoul order: position m is grid point z) ----
+  if (cfl_bits || ke_partial) {
+    const int ncf = cfl_bits ? min(nf, 3) : 0;
+    double mx[3] = {0.0, 0.0, 0.0}, ke[3] = {0.0, 0.0, 0.0};
+    for (int idx = threadIdx.x; idx < kZPairs * N; idx += blockDim.x) {
+      const int pr = idx / N, m = idx - pr * N;
+      const bool oka = col_ok(2 * pr), okb = col_ok(2 * pr + 1);
+      const int z = (m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1;
 #pragma unroll
       for (int j = 0; j < 3; ++j)
-        if (f == j) mx[j] = fmax(mx[j], a);
+        if (j < ncf) {
+          const double2 v = Fv[(j * kZPairs + pr) * N + m];
+          const double s = (j == 2) ? wzinv[z] : 1.0;
+          double a = oka ? fabs(v.x) * s : 0.0;
+          if (okb) a = fmax(a, fabs(v.y) * s);
+          mx[j] = fmax(mx[j], a);
+        }
+      if (ke_partial) {
+        const double w = wz[z];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          const int qg = q.ke_q[j];
+          if (qg < 0) continue;
+          const int v1 = qv[0][qg], v2 = qv[1][qg];
+          double pa, pb;
+          if (v1 < 0 || v2 < 0) {
+            const double2 f1 = Fv[((v1 < 0 ? v2 : v1) * kZPairs + pr) * N + m];
+            pa = f1.x;
+            pb = f1.y;
+          } else {
+            const double2 f1 = Fv[(v1 * kZPairs + pr) * N + m], f2 = Fv[(v2 * kZPairs + pr) * N + m];
+            pa = f1.x * f2.x;
+            pb = f1.y * f2.y;
+          }
+          ke[j] += w * ((oka ? pa : 0.0) + (okb ? pb : 0.0));
+        }
+      }
     }
-    for (int j = 0; j < 3; ++j) {
-      double v = mx[j];
-      for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-      if ((threadIdx.x & 31) == 0) red[j][threadIdx.x >> 5] = v;
+    if (cfl_bits) {
+      for (int j = 0; j < 3; ++j) {
+        double v = mx[j];
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+        if ((threadIdx.x & 31) == 0) red[j][threadIdx.x >> 5] = v;
+      }
+      __syncthreads();
+      if (threadIdx.x < ncf) {
+        double m2 = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m2 = fmax(m2, red[threadIdx.x][w]);
+        atomic_max_nonneg(cfl_bits + threadIdx.x, m2);
+      }
+      __syncthreads();
     }
-    __syncthreads();
-    if (threadIdx.x < ncf) {
-      double m2 = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m2 = fmax(m2, red[threadIdx.x][w]);
-      atomic_max_nonneg(cfl_bits + threadIdx.x, m2);
+    if (ke_partial) {
+      for (int j = 0; j < 3; ++j) {
+        double v = ke[j];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0) red[j][threadIdx.x >> 5] = v;
+      }
+      __syncthreads();
+      if (threadIdx.x < 3) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
+        ke_partial[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 3 + threadIdx.x] = s;
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
   // ---- products and forward transforms, kZFwd (quadratic variable, pair) lines a batch ----
-  double ke[3] = {0.0, 0.0, 0.0};
   for (int l0 = 0; l0 < nq * kZPairs; l0 += kZFwd) {
     const int nc = min(kZFwd, nq * kZPairs - l0);
-    // products formed inside the first FFT pass (and the KE sums on the way)
+    // products formed inside the first FFT pass
     auto ld = [&](int line, int m) -> double2 {
       const int lg = l0 + line, qg = lg / kZPairs, pr = lg - qg * kZPairs;
       const int v1 = qv[0][qg], v2 = qv[1][qg];
@@ -465,13 +505,6 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
         const double2 f1 = Fv[(v1 * kZPairs + pr) * N + m], f2 = Fv[(v2 * kZPairs + pr) * N + m];
         pa = f1.x * f2.x;
         pb = f1.y * f2.y;
-      }
-      if (ke_partial) {
-        const int z = (m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1;
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-          if (q.ke_q[j] == qg)
-            ke[j] += wz[z] * ((col_ok(2 * pr) ? pa : 0.0) + (col_ok(2 * pr + 1) ? pb : 0.0));
       }
       return make_double2(pa, pb);
     };
@@ -490,19 +523,6 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
       if (col_ok(2 * pr + 1)) dst[NZ + n] = 2.0 * (w.x * vb.x - w.y * vb.y);
     }
     __syncthreads();  // A is refilled by the next batch
-  }
-  if (ke_partial) {
-    for (int j = 0; j < 3; ++j) {
-      double v = ke[j];
-      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-      if ((threadIdx.x & 31) == 0) red[j][threadIdx.x >> 5] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x < 3) {
-      double s = 0.0;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
-      ke_partial[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 3 + threadIdx.x] = s;
-    }
   }
 }
 

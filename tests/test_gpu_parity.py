@@ -190,3 +190,24 @@ def test_split_solve_rbc_noslip_matches_oracle(split, monkeypatch):
     for s in range(len(ref.zlay)):
         assert _rel(pl.get_mean_field(s), ref.zfield[s]) < 1e-11
     pl.close()
+
+
+@pytest.mark.parametrize("scheme", ["ARS_222", "ARS_111"])
+def test_diagnostics_match_oracle(scheme):
+    """CFL time step (from the last stage's fields) and kinetic energy (volume
+    averages of uu + vv + ww at the first stage) after a few steps, against the
+    oracle's compute_cfl_based_timestep and output_global_quantities values."""
+    eq = equations("rbc_noslip_ra1e8", **{"1.d8": "1.d5"})
+    par = params(16, 12, 48, dt=1e-5, scheme=scheme)
+    ref = co.Solver(eq, par)
+    pl = _pl(eq, par)
+    _random_state(ref, pl, 9, amp=1e-2)
+    for _ in range(2):
+        ref.step(1e-5)
+    pl.march_forward(1e-5, 2)
+    d = pl.diagnostics()
+    assert d["nonfinite"] is False
+    assert ref.cfl_dt is not None and ref.ke is not None
+    assert abs(d["cfl_dt"] - ref.cfl_dt) <= 1e-11 * abs(ref.cfl_dt)
+    assert abs(d["KE"] - ref.ke) <= 1e-11 * abs(ref.ke)
+    pl.close()
