@@ -104,6 +104,35 @@ __global__ void __launch_bounds__(kThreadsY, kMinBlocksY) k_inv_y(Dims d, const 
   const int NYA = NF ? NF : d.NYA, LS = NYA + kPadY;
   double2* A = sm;
   double2* B = sm + kNB1 * LS;  // runtime plan only
+  // the CTA's build tables in shared memory: per term and line the stencil's
+  // state indices and values, the term's state base at this kx and (i kx)^dx,
+  // so that the state loads of the first pass depend on no global load
+  __shared__ int s_tt[kMaxFullTerms][kNB1][kTabW];
+  __shared__ double s_tv[kMaxFullTerms][kNB1][kTabW];
+  __shared__ const double2* s_base[kMaxFullTerms];
+  __shared__ double2 s_kxf[kMaxFullTerms];
+  __shared__ int s_kt[kMaxFullTerms], s_zero[kMaxFullTerms], s_dx[kMaxFullTerms], s_dy[kMaxFullTerms];
+  __shared__ double s_dsca[kMaxFullTerms];
+  const int nterms = plain_spec ? 0 : fv[f].nterms;
+  for (int e = threadIdx.x; e < nterms * kNB1 * kTabW; e += blockDim.x) {
+    const int t = e / (kNB1 * kTabW), r = e - t * kNB1 * kTabW, ln = r / kTabW, k = r - ln * kTabW;
+    const FullTermDev& ft = fv[f].term[t];
+    const int n = n0 + ln;
+    s_tt[t][ln][k] = n < d.NZ ? ft.tab_t[n * kTabW + k] : -1;
+    s_tv[t][ln][k] = n < d.NZ ? ft.tab_v[n * kTabW + k] : 0.0;
+  }
+  if (threadIdx.x < nterms) {
+    const int t = threadIdx.x;
+    const FullTermDev& ft = fv[f].term[t];
+    s_zero[t] = ft.zero_kind;
+    s_dx[t] = ft.dx;
+    s_dy[t] = ft.dy;
+    s_dsca[t] = ft.dsca;
+    s_kt[t] = ft.zero_kind ? 0 : st.kT[ft.set];
+    s_base[t] = ft.zero_kind ? nullptr : st.k[ft.set] + (size_t)kx * NYA * st.kT[ft.set];
+    s_kxf[t] = ipow(kxv[kx], ft.dx);
+  }
+  __syncthreads();
   // the spectral build of (line ln = Chebyshev n0 + ln, ky index iy), produced
   // inside the first FFT pass
   auto ld = [&](int ln, int iy) -> double2 {
@@ -113,11 +142,10 @@ __global__ void __launch_bounds__(kThreadsY, kMinBlocksY) k_inv_y(Dims d, const 
       if (plain_spec) {
         c = plain_spec[((size_t)kx * NYA + iy) * d.NZ + n];
       } else {
-        const FullVarDev& v = fv[f];
-        for (int t = 0; t < v.nterms; ++t) {
-          const FullTermDev& ft = v.term[t];
-          if (ft.zero_kind) {
+        for (int t = 0; t < nterms; ++t) {
+          if (s_zero[t]) {
             if (kx == 0 && iy == 0) {
+              const FullTermDev& ft = fv[f].term[t];
               const double* zs = st.z[ft.set];
               double s = 0.0;
               for (int k = 0; k < kTabW; ++k) {
@@ -127,19 +155,20 @@ __global__ void __launch_bounds__(kThreadsY, kMinBlocksY) k_inv_y(Dims d, const 
               c.x += s * ft.dsca;
             }
           } else {
-            const double2* sv = st.k[ft.set] + ((size_t)kx * NYA + iy) * st.kT[ft.set];
+            const double2* sv = s_base[t] + (size_t)iy * s_kt[t];
             double2 s = zero2();
+#pragma unroll
             for (int k = 0; k < kTabW; ++k) {
-              int tt = ft.tab_t[n * kTabW + k];
+              const int tt = s_tt[t][ln][k];
               if (tt >= 0) {
-                double w = ft.tab_v[n * kTabW + k];
-                double2 x = sv[tt];
+                const double w = s_tv[t][ln][k];
+                const double2 x = sv[tt];
                 s.x += w * x.x;
                 s.y += w * x.y;
               }
             }
-            s = cscale(s, ft.dsca);
-            if (ft.dx || ft.dy) s = cmul(cmul(s, ipow(kxv[kx], ft.dx)), ipow(kyv[iy], ft.dy));
+            s = cscale(s, s_dsca[t]);
+            if (s_dx[t] || s_dy[t]) s = cmul(cmul(s, s_kxf[t]), ipow(kyv[iy], s_dy[t]));
             c = cadd(c, s);
           }
         }
