@@ -171,19 +171,31 @@ def phase_bytes(g, nsys, nact, T, ncls, Tc, kl, ku, stages, factor_bytes, factor
     #     block, or all 2 kl + ku + 1 per column, and one pivot byte per column of
     #     each block) and the block vectors (right-hand side in, intermediate out
     #     and in, solution out)
-    #   kstd_out: solution in, stage output and K_std out (active systems)
+    #   kstd_out: split systems: the solution (already in the stage output) in,
+    #     K_std out, in every stage but the last (which needs no K_std);
+    #     whole systems: solution in, stage output and K_std out
     rhs = sub = kst = 0
     nblk_cols = nact * ncls * Tc
     for i in range(stages):
         last = (i == stages - 1)
-        rhs += nsys * 16 * T * (1 + 2 * i + 1 + 1) + nact * 16 * nQ * NZ + (nsys - nact) * 16 * T * (0 if last else 1)
+        rhs += (nsys * 16 * T * (1 + 2 * i + (0 if last else 1) + 1) + nact * 16 * nQ * NZ
+                + (nsys - nact) * 16 * T * (0 if last else 1))
         entries = factor_entries * nact * ncls if factor_entries else nblk_cols * (2 * kl + ku + 1)
         sub += entries * factor_bytes + nblk_cols + 4 * 16 * nblk_cols
         kst += 16 * nblk_cols + nact * 16 * T * (1 if last else 2)
     out["rhs_nl"] = rhs / stages
     out["substitution"] = sub / stages
-    out["kstd_out"] = kst / stages
+    out["kstd_out"] = (2 * nact * 16 * T) if ncls == 2 else kst / stages
     return out
+
+
+def phase_launches(stages, ncls):
+    """Launches per step of each phase's kernel: one per stage, except the split
+    systems' K_std kernel, which the last stage skips."""
+    n = {k: stages for k in PHASE_KERNELS}
+    if ncls == 2:
+        n["kstd_out"] = max(stages - 1, 1)
+    return n
 
 
 def run_ours(args, cfg):
@@ -288,16 +300,17 @@ def run_ours(args, cfg):
     pbytes = phase_bytes(geo, nsys, nact, T, ncls, Tc, kl_c, ku_c, pl.stages, fbytes, fentries)
     peak, src = read_peaks()
     phases = {}
+    nlaunch = phase_launches(pl.stages, ncls)
     for k, b in pbytes.items():
         if prof[k] <= 0:
             continue
-        launch_ms = prof[k] / pl.stages
+        launch_ms = prof[k] / nlaunch[k]
         gbs = b / (launch_ms / 1e3) / 1e9 if launch_ms > 0 else None
         phases[k] = {"kernels": PHASE_KERNELS[k], "ms_per_launch": round(launch_ms, 4),
                      "algorithmic_bytes": b, "achieved_gbs": round(gbs, 1) if gbs else None,
                      "frac": round(gbs / peak, 4) if gbs else None}
     top = max(pbytes, key=lambda k: prof[k])
-    launch_ms = prof[top] / pl.stages
+    launch_ms = prof[top] / nlaunch[top]
     achieved = pbytes[top] / (launch_ms / 1e3) / 1e9
     traffic = read_traffic(PHASE_KERNELS[top])
     cpu = None

@@ -88,7 +88,7 @@ struct KSys {
   // operator-stationary K_std: tile windows and window-relative L
   int* tile_win = nullptr;
   int tile_lwin_max = 0;
-  DevEll Lw;
+  DevGEll Lw;
   int* rhs_win = nullptr;
   int rhs_win_max = 0;
   DevEll Mw, NLw;
@@ -196,6 +196,73 @@ DevEll upload_ell(DevAlloc& mem, const EllOp& op) {
     }
   e.cg = mem.upload(cg);
   e.val = mem.upload(val);
+  return e;
+}
+
+// The grouped form of an operator for the tile kernels (DevGEll): groups whose
+// (column, value) entries coincide in every row are merged (their coefficients
+// add), then each row's entries are laid out group by group in fixed slot
+// ranges.  Returns valid = 0 when the layout does not fit the register slots.
+DevGEll upload_gell(DevAlloc& mem, const EllOp& op) {
+  DevGEll e{};
+  e.rows = op.rows;
+  const int G = (int)op.groups.size();
+  // entries of group g in row t, in slot order
+  auto entries = [&](int t, int g) {
+    std::vector<std::pair<int, double>> v;
+    for (int k = 0; k < op.width; ++k) {
+      const size_t i = (size_t)t * op.width + k;
+      if (op.col[i] >= 0 && op.grp[i] == g) v.emplace_back(op.col[i], op.val[i]);
+    }
+    return v;
+  };
+  std::vector<int> cls(G, -1);   // merged group of each monomial group
+  std::vector<int> rep;          // representative monomial group of each merged group
+  for (int g = 0; g < G; ++g) {
+    for (size_t c = 0; c < rep.size() && cls[g] < 0; ++c) {
+      bool same = true;
+      for (int t = 0; t < op.rows && same; ++t) same = entries(t, g) == entries(t, rep[c]);
+      if (same) cls[g] = (int)c;
+    }
+    if (cls[g] < 0) {
+      cls[g] = (int)rep.size();
+      rep.push_back(g);
+    }
+  }
+  const int NG = (int)rep.size();
+  if (NG > kMaxGroups) return e;
+  std::vector<int> wid(NG, 0);
+  for (int t = 0; t < op.rows; ++t)
+    for (int c = 0; c < NG; ++c) wid[c] = std::max(wid[c], (int)entries(t, rep[c]).size());
+  int W = 0;
+  for (int c = 0; c < NG; ++c) W += wid[c];
+  if (W > kGSlots) return e;
+  for (int g = 0; g < G; ++g) {
+    const int c = cls[g];
+    if (e.nmono[c] >= kGMono) return DevGEll{};
+    e.mkx[c][e.nmono[c]] = op.groups[g].first;
+    e.mky[c][e.nmono[c]] = op.groups[g].second;
+    ++e.nmono[c];
+  }
+  std::vector<int> col((size_t)W * op.rows, 0);
+  std::vector<double> val((size_t)W * op.rows, 0.0);
+  int off = 0;
+  for (int c = 0; c < NG; ++c) {
+    for (int k = 0; k < wid[c]; ++k) e.slot_grp[off + k] = c;
+    for (int t = 0; t < op.rows; ++t) {
+      const auto v = entries(t, rep[c]);
+      for (size_t k = 0; k < v.size(); ++k) {
+        col[(size_t)(off + k) * op.rows + t] = v[k].first;
+        val[(size_t)(off + k) * op.rows + t] = v[k].second;
+      }
+    }
+    off += wid[c];
+  }
+  e.width = W;
+  e.ngroups = NG;
+  e.col = mem.upload(col);
+  e.val = mem.upload(val);
+  e.valid = 1;
   return e;
 }
 
@@ -364,7 +431,7 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
           }
       }
       k.tile_win = mem.upload(tw);
-      k.Lw = upload_ell(mem, lw);
+      k.Lw = upload_gell(mem, lw);
       // the right-hand side in the same row tiles: the state window of M's
       // columns, the Chebyshev range and the quadratic variables of the NL
       // operator's columns (quad * NZ + n), and both operators relative to them

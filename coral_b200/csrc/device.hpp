@@ -32,6 +32,24 @@ struct DevEll {
   __device__ __forceinline__ double v(int r, int k) const { return val[(size_t)k * rows + r]; }
 };
 
+// An operator row split by monomial group for the tile kernels: the slots of a
+// row are grouped (group of slot k = slot_grp[k], the same in every row, groups
+// in increasing slot order), so a row is evaluated as sum_g c_g (sum_k v_k x_k)
+// with one complex multiply per group.  Groups whose entries coincide in every
+// row are merged; the coefficient of a group is the sum of its monomials
+// (i kx)^mkx (i ky)^mky.
+constexpr int kGSlots = 16;  // slots of a grouped row (register-resident)
+constexpr int kGMono = 4;    // monomials of one merged group
+struct DevGEll {
+  int valid;            // 0: the operator has no grouped form within these limits
+  int rows, width, ngroups;
+  int slot_grp[kGSlots];
+  int nmono[kMaxGroups];
+  int mkx[kMaxGroups][kGMono], mky[kMaxGroups][kGMono];
+  const int* col;       // [width][rows] window-relative column, 0 in empty slots
+  const double* val;    // [width][rows], 0 in empty slots
+};
+
 // one term of a full variable build: dsca * (i kx)^dx (i ky)^dy * S_var g
 struct FullTermDev {
   int zero_kind;  // 1: mean variable (adds to the (0,0) mode only)
@@ -147,7 +165,7 @@ struct SolveArgs {
   // tile's rows of L touch; Lw = L with its columns relative to that window
   const int* tile_win;
   int tile_lwin_max;     // widest window
-  DevEll Lw;
+  DevGEll Lw;            // !valid: k_kstd_out
   // operator-stationary right-hand side (null rhs_win: k_rhs_nl): per tile of
   // kTileRows rows, rhs_win[kRhsWin tile + .] = (start, width) of the state
   // columns its rows of M touch, (start, width) of the Chebyshev range its rows

@@ -1807,14 +1807,46 @@ __global__ void __launch_bounds__(kRhsThreads) k_kstd_out(SolveArgs a) {
 
 // ------------------------------------------------------------------------------
 // Operator-stationary K_std: a CTA takes one tile of kTileRows rows and kTileSys
-// active systems.  Each thread keeps its row of L (columns relative to the
-// tile's solution window) in registers; the CTA first stages the windows of all
-// its systems (coalesced loads from the stage output), then evaluates its row
-// for the systems one after the other.  Same arithmetic and order as
-// k_kstd_out.
+// active systems.  Each thread keeps its row of L in grouped form (columns
+// relative to the tile's solution window) in registers; the CTA first copies the
+// windows of all its systems into shared memory (cp.async from the stage
+// output), then evaluates its row for the systems one after the other: per
+// monomial group a real sum, then one complex multiply by the group coefficient.
 // ------------------------------------------------------------------------------
 constexpr int kTileSys = 8;  // systems per CTA
-constexpr int kLW = 16;      // register slots: L entries per row (wider L takes k_kstd_out)
+constexpr int kLW = kGSlots;  // register slots of an L row (wider grouped L takes k_kstd_out)
+
+// coefficient of group g of a grouped operator at (kx, ky)
+__device__ __forceinline__ double2 gcoef(const DevGEll& G, int g, double kx, double ky) {
+  double2 c = zero2();
+  for (int m = 0; m < G.nmono[g]; ++m) c = cadd(c, cmul(ipow(kx, G.mkx[g][m]), ipow(ky, G.mky[g][m])));
+  return c;
+}
+// one grouped row (slots in registers) applied to x: real sums per group, one
+// complex multiply by the group coefficient c[g] per group
+template <int RW>
+__device__ __forceinline__ double2 grow(const DevGEll& G, const int* col, const double* val, const double2* x,
+                                        const double2* c) {
+  double2 r = zero2(), acc = zero2();
+  int lg = 0;
+#pragma unroll
+  for (int k = 0; k < RW; ++k) {
+    if (k < G.width) {
+      if (k > 0 && G.slot_grp[k] != lg) {
+        r = cadd(r, cmul(c[lg], acc));
+        acc = zero2();
+      }
+      lg = G.slot_grp[k];
+      if (val[k] != 0.0) {
+        const double2 xv = x[col[k]];
+        acc.x += val[k] * xv.x;
+        acc.y += val[k] * xv.y;
+      }
+    }
+  }
+  if (G.width > 0) r = cadd(r, cmul(c[lg], acc));
+  return r;
+}
 
 __global__ void __launch_bounds__(kTileRows, 4) k_kstd_tiles(SolveArgs a) {
   extern __shared__ double2 xw[];
@@ -1829,7 +1861,7 @@ __global__ void __launch_bounds__(kTileRows, 4) k_kstd_tiles(SolveArgs a) {
     const int u = threadIdx.x / kMaxGroups, g = threadIdx.x - u * kMaxGroups;
     const int sid = a.act_list[a0 + (u < ns ? u : 0)];
     const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
-    cls[u][g] = (g < a.L.ngroups) ? cmul(ipow(a.kx[kx], a.L.gkx[g]), ipow(a.ky[ky], a.L.gky[g])) : zero2();
+    cls[u][g] = (g < a.Lw.ngroups) ? gcoef(a.Lw, g, a.kx[kx], a.ky[ky]) : zero2();
   }
   for (int u = 0; u < ns; ++u) {  // cp.async: no register round trip per system
     const double2* x = a.out + (size_t)a.act_list[a0 + u] * T + llo;
@@ -1839,25 +1871,16 @@ __global__ void __launch_bounds__(kTileRows, 4) k_kstd_tiles(SolveArgs a) {
   cp_async_wait<0>();
   __syncthreads();
   if (!row_ok) return;
-  int lcg[kLW];
+  int lc[kLW];
   double lv[kLW];
 #pragma unroll
   for (int k = 0; k < kLW; ++k) {
     const bool ok = k < a.Lw.width;
-    lcg[k] = ok ? a.Lw.cg[k * a.Lw.rows + t] : 0;
+    lc[k] = ok ? a.Lw.col[k * a.Lw.rows + t] : 0;
     lv[k] = ok ? a.Lw.val[k * a.Lw.rows + t] : 0.0;
   }
-  for (int u = 0; u < ns; ++u) {
-    const double2* x = xw + u * lw;
-    double2 ks = zero2();
-#pragma unroll
-    for (int k = 0; k < kLW; ++k)
-      if (lv[k] != 0.0) {
-        const double2 xv = x[lcg[k] & 0xFFFFFF];
-        ks = cadd(ks, cmul(cls[u][lcg[k] >> 24], make_double2(lv[k] * xv.x, lv[k] * xv.y)));
-      }
-    a.Kstd_out[(size_t)a.act_list[a0 + u] * T + t] = ks;
-  }
+  for (int u = 0; u < ns; ++u)
+    a.Kstd_out[(size_t)a.act_list[a0 + u] * T + t] = grow<kLW>(a.Lw, lc, lv, xw + u * lw, cls[u]);
 }
 
 // ------------------------------------------------------------------------------
@@ -2391,7 +2414,7 @@ void launch_subst(const SolveArgs& a, cudaStream_t s) {
 void launch_kstd_out(const SolveArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;
   if (a.work2 && !a.Kstd_out) return;  // solution already in out, no K_std in the last stage
-  if (a.work2 && a.tile_win && a.Lw.width <= kLW) {
+  if (a.work2 && a.tile_win && a.Lw.valid && a.Lw.width <= kLW) {
     const size_t sm = (size_t)kTileSys * a.tile_lwin_max * sizeof(double2);
     set_smem(k_kstd_tiles, sm);
     const dim3 g((a.T + kTileRows - 1) / kTileRows, (a.nact + kTileSys - 1) / kTileSys);
