@@ -1894,6 +1894,7 @@ __global__ void __launch_bounds__(kTileRows, 4) k_kstd_tiles(SolveArgs a) {
 // arithmetic and order as k_rhs_nl.
 // ------------------------------------------------------------------------------
 constexpr int kRhsSys = 4;  // systems per CTA
+constexpr int kRhsStg = 4;  // window entries per thread with precomputed offsets (wider: plain loops)
 
 template <int RM, int RN>
 __global__ void __launch_bounds__(kTileRows, 6) k_rhs_tiles(SolveArgs a, NLArgs n) {
@@ -1906,16 +1907,45 @@ __global__ void __launch_bounds__(kTileRows, 6) k_rhs_tiles(SolveArgs a, NLArgs 
   const int ws = mw + nqt * nw;  // window entries per system
   const int s0 = blockIdx.x * kRhsSys, ns = min(kRhsSys, nsys - s0);
   const size_t qstride = (size_t)nsys * NZ;  // between quadratic variables of qspec
-  for (int u = 0; u < ns; ++u) {
-    const int sid = s0 + u;
-    double2* w = win + u * ws;
-    const double2* f = a.field + (size_t)sid * T + mlo;
-    for (int i = threadIdx.x; i < mw; i += kTileRows) cp_async16(w + i, f + i);
-    if (a.act_index[sid] >= 0)
-      for (int i = threadIdx.x; i < nqt * nw; i += kTileRows) {
-        const int sl = i / nw, k = i - sl * nw;
-        cp_async16(w + mw + i, n.qspec + rw[5 + sl] * qstride + (size_t)sid * NZ + nlo + k);
+  if (ws <= kRhsStg * kTileRows) {
+    // window entry e = threadIdx.x + j kTileRows: the same source offset for every
+    // system (plus the system's base), computed once
+    size_t off[kRhsStg];
+#pragma unroll
+    for (int j = 0; j < kRhsStg; ++j) {
+      const int e = threadIdx.x + j * kTileRows;
+      if (e < mw) {
+        off[j] = (size_t)(mlo + e);
+      } else {
+        const int i = e - mw, sl = i / nw, k = i - sl * nw;
+        off[j] = e < ws ? rw[5 + sl] * qstride + nlo + k : 0;
       }
+    }
+    for (int u = 0; u < ns; ++u) {
+      const int sid = s0 + u;
+      const bool act = a.act_index[sid] >= 0;
+      double2* w = win + u * ws;
+      const double2* f = a.field + (size_t)sid * T;
+      const double2* qb = n.qspec + (size_t)sid * NZ;
+#pragma unroll
+      for (int j = 0; j < kRhsStg; ++j) {
+        const int e = threadIdx.x + j * kTileRows;
+        if (e < mw) cp_async16(w + e, f + off[j]);
+        else if (e < ws && act) cp_async16(w + e, qb + off[j]);
+      }
+    }
+  } else {
+    for (int u = 0; u < ns; ++u) {
+      const int sid = s0 + u;
+      double2* w = win + u * ws;
+      const double2* f = a.field + (size_t)sid * T + mlo;
+      for (int i = threadIdx.x; i < mw; i += kTileRows) cp_async16(w + i, f + i);
+      if (a.act_index[sid] >= 0)
+        for (int i = threadIdx.x; i < nqt * nw; i += kTileRows) {
+          const int sl = i / nw, k = i - sl * nw;
+          cp_async16(w + mw + i, n.qspec + rw[5 + sl] * qstride + (size_t)sid * NZ + nlo + k);
+        }
+    }
   }
   cp_async_commit();
   for (int i = threadIdx.x; i < kRhsSys * kMaxGroups; i += kTileRows) {
@@ -1941,6 +1971,21 @@ __global__ void __launch_bounds__(kTileRows, 6) k_rhs_tiles(SolveArgs a, NLArgs 
     ncg[k] = ok ? a.NLw.cg[(size_t)k * a.NLw.rows + tr] : 0;
     nv[k] = ok ? a.NLw.val[(size_t)k * a.NLw.rows + tr] : 0.0;
   }
+  // shared-memory index and group of every slot
+  int nix[RN], ngr[RN], mix[RM], mgr[RM];
+#pragma unroll
+  for (int k = 0; k < RN; ++k) {
+    nix[k] = mw + (ncg[k] & 0xFFFFFF);
+    ngr[k] = ncg[k] >> 24;
+  }
+#pragma unroll
+  for (int k = 0; k < RM; ++k) {
+    mix[k] = mcg[k] & 0xFFFFFF;
+    mgr[k] = mcg[k] >> 24;
+  }
+  // M with the single monomial 1 (every recipe here): its coefficient is exactly
+  // 1 and the complex multiply is skipped (identical for finite values)
+  const bool m_unit = a.Mw.ngroups == 1 && a.Mw.gkx[0] == 0 && a.Mw.gky[0] == 0;
   int ai[kRhsSys];
 #pragma unroll
   for (int u = 0; u < kRhsSys; ++u) ai[u] = u < ns ? a.act_index[s0 + u] : -1;
@@ -1959,16 +2004,17 @@ __global__ void __launch_bounds__(kTileRows, 6) k_rhs_tiles(SolveArgs a, NLArgs 
 #pragma unroll
         for (int k = 0; k < RN; ++k)
           if (nv[k] != 0.0) {
-            const double2 qh = w[mw + (ncg[k] & 0xFFFFFF)];
-            kh[u] = cadd(kh[u], cmul(cns[u][ncg[k] >> 24], make_double2(nv[k] * qh.x, nv[k] * qh.y)));
+            const double2 qh = w[nix[k]];
+            kh[u] = cadd(kh[u], cmul(cns[u][ngr[k]], make_double2(nv[k] * qh.x, nv[k] * qh.y)));
           }
       }
       if (s0 + u != 0) {
 #pragma unroll
         for (int k = 0; k < RM; ++k)
           if (k < a.Mw.width) {
-            const double2 xv = w[mcg[k] & 0xFFFFFF];
-            r[u] = cadd(r[u], cmul(cms[u][mcg[k] >> 24], make_double2(mv[k] * xv.x, mv[k] * xv.y)));
+            const double2 xv = w[mix[k]];
+            const double2 p = make_double2(mv[k] * xv.x, mv[k] * xv.y);
+            r[u] = cadd(r[u], m_unit ? p : cmul(cms[u][mgr[k]], p));
           }
       }
     }
