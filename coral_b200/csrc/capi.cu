@@ -92,6 +92,7 @@ struct KSys {
   int* rhs_win = nullptr;
   int rhs_win_max = 0;
   DevEll Mw, NLw;
+  DevGEll NLg;
   double2* work = nullptr;
   double2* work2 = nullptr;  // thread-per-block layout of the active systems' vectors (split only)
   std::vector<std::vector<int>> tab_t;   // per var: [NZ][kTabW]
@@ -480,6 +481,7 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
       k.rhs_win = mem.upload(rw);
       k.Mw = upload_ell(mem, mw);
       k.NLw = upload_ell(mem, nw);
+      k.NLg = upload_gell(mem, nw);
     }
     if (k.ncls == 2) {
       // thread-per-block layouts: groups of 32 blocks (block = 2 act + class) side by side
@@ -746,6 +748,7 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       sa.rhs_win_max = k.rhs_win_max;
       sa.Mw = k.Mw;
       sa.NLw = k.NLw;
+      sa.NLg = k.NLg;
       sa.Lw = k.Lw;
       {
         const int kv = sa.kl + sa.ku;

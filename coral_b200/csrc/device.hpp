@@ -176,6 +176,7 @@ struct SolveArgs {
   const int* rhs_win;
   int rhs_win_max;       // widest window (state + all slots), complex entries
   DevEll Mw, NLw;
+  DevGEll NLg;           // NLw in grouped form (valid = 0: none)
   // band entries that are zero in every block are not loaded (FactorArgs::lmask,
   // umask; null: load all)
   const unsigned* lmask;

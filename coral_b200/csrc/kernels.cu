@@ -1896,7 +1896,10 @@ __global__ void __launch_bounds__(kTileRows, 4) k_kstd_tiles(SolveArgs a) {
 constexpr int kRhsSys = 4;  // systems per CTA
 constexpr int kRhsStg = 4;  // window entries per thread with precomputed offsets (wider: plain loops)
 
-template <int RM, int RN>
+// G0, G1, G2 > 0: the NL operator in grouped form (SolveArgs::NLg) with slot
+// ranges of these widths per monomial group, compiled: per group a real sum,
+// then one complex multiply by the group coefficient (RN = G0 + G1 + G2)
+template <int RM, int RN, int G0 = 0, int G1 = 0, int G2 = 0>
 __global__ void __launch_bounds__(kTileRows, 6) k_rhs_tiles(SolveArgs a, NLArgs n) {
   extern __shared__ double2 win[];
   __shared__ double2 cms[kRhsSys][kMaxGroups], cns[kRhsSys][kMaxGroups];
@@ -1953,7 +1956,10 @@ __global__ void __launch_bounds__(kTileRows, 6) k_rhs_tiles(SolveArgs a, NLArgs 
     const int sid = s0 + (u < ns ? u : 0);
     const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
     cms[u][g] = (g < a.Mw.ngroups) ? cmul(ipow(a.kx[kx], a.Mw.gkx[g]), ipow(a.ky[ky], a.Mw.gky[g])) : zero2();
-    cns[u][g] = (g < a.NLw.ngroups) ? cmul(ipow(a.kx[kx], a.NLw.gkx[g]), ipow(a.ky[ky], a.NLw.gky[g])) : zero2();
+    if constexpr (G0 > 0)
+      cns[u][g] = (g < a.NLg.ngroups) ? gcoef(a.NLg, g, a.kx[kx], a.ky[ky]) : zero2();
+    else
+      cns[u][g] = (g < a.NLw.ngroups) ? cmul(ipow(a.kx[kx], a.NLw.gkx[g]), ipow(a.ky[ky], a.NLw.gky[g])) : zero2();
   }
   const bool row_ok = t < T;
   const int tr = row_ok ? t : 0;
@@ -1965,18 +1971,25 @@ __global__ void __launch_bounds__(kTileRows, 6) k_rhs_tiles(SolveArgs a, NLArgs 
     mcg[k] = ok ? a.Mw.cg[(size_t)k * a.Mw.rows + tr] : 0;
     mv[k] = ok ? a.Mw.val[(size_t)k * a.Mw.rows + tr] : 0.0;
   }
+  constexpr bool kGrouped = G0 > 0;
+  static_assert(!kGrouped || G0 + G1 + G2 == RN, "grouped NL slots");
 #pragma unroll
   for (int k = 0; k < RN; ++k) {
-    const bool ok = k < a.NLw.width;
-    ncg[k] = ok ? a.NLw.cg[(size_t)k * a.NLw.rows + tr] : 0;
-    nv[k] = ok ? a.NLw.val[(size_t)k * a.NLw.rows + tr] : 0.0;
+    if constexpr (kGrouped) {
+      ncg[k] = a.NLg.col[(size_t)k * a.NLg.rows + tr];
+      nv[k] = a.NLg.val[(size_t)k * a.NLg.rows + tr];
+    } else {
+      const bool ok = k < a.NLw.width;
+      ncg[k] = ok ? a.NLw.cg[(size_t)k * a.NLw.rows + tr] : 0;
+      nv[k] = ok ? a.NLw.val[(size_t)k * a.NLw.rows + tr] : 0.0;
+    }
   }
   // shared-memory index and group of every slot
   int nix[RN], ngr[RN], mix[RM], mgr[RM];
 #pragma unroll
   for (int k = 0; k < RN; ++k) {
     nix[k] = mw + (ncg[k] & 0xFFFFFF);
-    ngr[k] = ncg[k] >> 24;
+    ngr[k] = kGrouped ? 0 : ncg[k] >> 24;
   }
 #pragma unroll
   for (int k = 0; k < RM; ++k) {
@@ -2001,12 +2014,28 @@ __global__ void __launch_bounds__(kTileRows, 6) k_rhs_tiles(SolveArgs a, NLArgs 
     if (u < ns) {
       const double2* w = win + u * ws;
       if (ai[u] >= 0) {
+        if constexpr (kGrouped) {
+          double2 acc[3] = {zero2(), zero2(), zero2()};
 #pragma unroll
-        for (int k = 0; k < RN; ++k)
-          if (nv[k] != 0.0) {
-            const double2 qh = w[nix[k]];
-            kh[u] = cadd(kh[u], cmul(cns[u][ngr[k]], make_double2(nv[k] * qh.x, nv[k] * qh.y)));
+          for (int k = 0; k < RN; ++k) {
+            const int g = k < G0 ? 0 : (k < G0 + G1 ? 1 : 2);
+            if (nv[k] != 0.0) {
+              const double2 qh = w[nix[k]];
+              acc[g].x += nv[k] * qh.x;
+              acc[g].y += nv[k] * qh.y;
+            }
           }
+          kh[u] = cmul(cns[u][0], acc[0]);
+          if (G1 > 0) kh[u] = cadd(kh[u], cmul(cns[u][1], acc[1]));
+          if (G2 > 0) kh[u] = cadd(kh[u], cmul(cns[u][2], acc[2]));
+        } else {
+#pragma unroll
+          for (int k = 0; k < RN; ++k)
+            if (nv[k] != 0.0) {
+              const double2 qh = w[nix[k]];
+              kh[u] = cadd(kh[u], cmul(cns[u][ngr[k]], make_double2(nv[k] * qh.x, nv[k] * qh.y)));
+            }
+        }
       }
       if (s0 + u != 0) {
 #pragma unroll
@@ -2411,16 +2440,28 @@ void launch_factor(const FactorArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;
   k_factor<<<(a.nact + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
 }
-template <int RM, int RN>
+template <int RM, int RN, int G0 = 0, int G1 = 0, int G2 = 0>
 static void launch_rhs_tiles(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
   const int nsys = a.d.NXH * a.d.NYA;
   const size_t sm = (size_t)kRhsSys * a.rhs_win_max * sizeof(double2);
-  set_smem(k_rhs_tiles<RM, RN>, sm);
+  set_smem(k_rhs_tiles<RM, RN, G0, G1, G2>, sm);
   const dim3 g((nsys + kRhsSys - 1) / kRhsSys, (a.T + kTileRows - 1) / kTileRows);
-  k_rhs_tiles<RM, RN><<<g, kTileRows, sm, s>>>(a, n);
+  k_rhs_tiles<RM, RN, G0, G1, G2><<<g, kTileRows, sm, s>>>(a, n);
+}
+// slot widths of the groups of a grouped operator (0 past its last group)
+static void group_widths(const DevGEll& G, int w[3]) {
+  w[0] = w[1] = w[2] = 0;
+  for (int k = 0; k < G.width; ++k)
+    if (G.slot_grp[k] < 3) ++w[G.slot_grp[k]];
 }
 void launch_rhs_nl(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
   if (a.work2 && a.rhs_win && a.row_pos) {
+    if (a.NLg.valid && a.NLg.ngroups == 3 && a.Mw.width <= 4) {
+      int w[3];
+      group_widths(a.NLg, w);
+      // the plane-layer recipes' NL operator: groups i kx, i ky, 1 of widths 3, 3, 2
+      if (w[0] == 3 && w[1] == 3 && w[2] == 2) return launch_rhs_tiles<4, 8, 3, 3, 2>(a, n, s);
+    }
     if (a.Mw.width <= 4 && a.NLw.width <= 8) return launch_rhs_tiles<4, 8>(a, n, s);
     if (a.Mw.width <= 8 && a.NLw.width <= 16) return launch_rhs_tiles<8, 16>(a, n, s);
   }
