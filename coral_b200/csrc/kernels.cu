@@ -1848,6 +1848,8 @@ __device__ __forceinline__ double2 grow(const DevGEll& G, const int* col, const 
   return r;
 }
 
+// G0..G3 > 0: the grouped L's slot ranges compiled (no run-time group test)
+template <int G0 = 0, int G1 = 0, int G2 = 0, int G3 = 0>
 __global__ void __launch_bounds__(kTileRows, 4) k_kstd_tiles(SolveArgs a) {
   extern __shared__ double2 xw[];
   __shared__ double2 cls[kTileSys][kMaxGroups];
@@ -1879,8 +1881,31 @@ __global__ void __launch_bounds__(kTileRows, 4) k_kstd_tiles(SolveArgs a) {
     lc[k] = ok ? a.Lw.col[k * a.Lw.rows + t] : 0;
     lv[k] = ok ? a.Lw.val[k * a.Lw.rows + t] : 0.0;
   }
-  for (int u = 0; u < ns; ++u)
-    a.Kstd_out[(size_t)a.act_list[a0 + u] * T + t] = grow<kLW>(a.Lw, lc, lv, xw + u * lw, cls[u]);
+  for (int u = 0; u < ns; ++u) {
+    double2 ks;
+    if constexpr (G0 > 0) {
+      constexpr int W = G0 + G1 + G2 + G3;
+      static_assert(W <= kLW, "grouped L slots");
+      const double2* x = xw + u * lw;
+      double2 acc[4] = {zero2(), zero2(), zero2(), zero2()};
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        const int g = k < G0 ? 0 : (k < G0 + G1 ? 1 : (k < G0 + G1 + G2 ? 2 : 3));
+        if (lv[k] != 0.0) {
+          const double2 xv = x[lc[k]];
+          acc[g].x += lv[k] * xv.x;
+          acc[g].y += lv[k] * xv.y;
+        }
+      }
+      ks = cmul(cls[u][0], acc[0]);
+      if (G1 > 0) ks = cadd(ks, cmul(cls[u][1], acc[1]));
+      if (G2 > 0) ks = cadd(ks, cmul(cls[u][2], acc[2]));
+      if (G3 > 0) ks = cadd(ks, cmul(cls[u][3], acc[3]));
+    } else {
+      ks = grow<kLW>(a.Lw, lc, lv, xw + u * lw, cls[u]);
+    }
+    a.Kstd_out[(size_t)a.act_list[a0 + u] * T + t] = ks;
+  }
 }
 
 // ------------------------------------------------------------------------------
@@ -2503,9 +2528,18 @@ void launch_kstd_out(const SolveArgs& a, cudaStream_t s) {
   if (a.work2 && !a.Kstd_out) return;  // solution already in out, no K_std in the last stage
   if (a.work2 && a.tile_win && a.Lw.valid && a.Lw.width <= kLW) {
     const size_t sm = (size_t)kTileSys * a.tile_lwin_max * sizeof(double2);
-    set_smem(k_kstd_tiles, sm);
     const dim3 g((a.T + kTileRows - 1) / kTileRows, (a.nact + kTileSys - 1) / kTileSys);
-    k_kstd_tiles<<<g, kTileRows, sm, s>>>(a);
+    int w[4] = {0, 0, 0, 0};
+    for (int k = 0; k < a.Lw.width; ++k)
+      if (a.Lw.slot_grp[k] < 4) ++w[a.Lw.slot_grp[k]];
+    if (a.Lw.ngroups == 4 && w[0] == 4 && w[1] == 6 && w[2] == 3 && w[3] == 3) {
+      // the plane-layer recipes' L: (kx^2 + ky^2), 1, kx, ky groups
+      set_smem(k_kstd_tiles<4, 6, 3, 3>, sm);
+      k_kstd_tiles<4, 6, 3, 3><<<g, kTileRows, sm, s>>>(a);
+      return;
+    }
+    set_smem(k_kstd_tiles<>, sm);
+    k_kstd_tiles<><<<g, kTileRows, sm, s>>>(a);
     return;
   }
   const size_t smx = (size_t)a.T * sizeof(double2);
