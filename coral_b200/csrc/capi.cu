@@ -143,6 +143,7 @@ struct coral_handle {
   double2 *Y1 = nullptr, *qspec = nullptr, *tmp_spec = nullptr;
   double *Y2 = nullptr, *fphys = nullptr, *tmp_phys = nullptr;
   double* ke_partial = nullptr;
+  double* ke_total = nullptr;  // device: total of ke_partial (coral_diagnostics)
   size_t n_ke_partial = 0;
   unsigned long long* cfl_bits = nullptr;
   unsigned int* flags = nullptr;
@@ -612,6 +613,7 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
   h->tmp_phys = mem.get<double>((size_t)g.NYAA * g.NXAA * g.NZAA);
   h->n_ke_partial = (size_t)((g.NXAA + 1) / 2) * g.NYAA * 3;
   h->ke_partial = mem.get<double>(h->n_ke_partial);
+  h->ke_total = mem.get<double>(1);
   CK(cudaMemset(h->ke_partial, 0, h->n_ke_partial * sizeof(double)));
   h->cfl_bits = mem.get<unsigned long long>(3);
   CK(cudaMemset(h->cfl_bits, 0, 3 * sizeof(unsigned long long)));
@@ -1347,10 +1349,13 @@ int coral_diagnostics(coral_handle* h, double* out3) {
     double w = std::max(v, mx[2]);
     double m = std::max(u, std::max(v, w));
     out3[0] = (h->nF >= 3 && m > 0.0) ? 1.0 / m : (h->nF >= 3 ? INFINITY : 1.0);
-    std::vector<double> part(h->n_ke_partial);
-    CK(cudaMemcpy(part.data(), h->ke_partial, part.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    // the partial sums are totalled on the device: 8 bytes come back, not the
+    // per-CTA array
+    launch_ke_sum(h->ke_partial, h->n_ke_partial, h->ke_total, h->stream);
+    ++h->launches;
     double ke = 0.0;
-    for (size_t i = 0; i < part.size(); ++i) ke += part[i];
+    CK(cudaMemcpyAsync(&ke, h->ke_total, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
     out3[1] = ke / g.NXAA / g.NYAA;
     unsigned int f = 0;
     CK(cudaMemcpy(&f, h->flags, sizeof(f), cudaMemcpyDeviceToHost));

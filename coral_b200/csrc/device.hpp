@@ -101,6 +101,8 @@ void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const Ff
 void launch_fwd_y(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
                   cudaStream_t s);
 void launch_remove_zmean(const Dims& d, double2* qspec_q, cudaStream_t s);
+// total of the n KE partial sums (one CTA, fixed order) into *out
+void launch_ke_sum(const double* part, size_t n, double* out, cudaStream_t s);
 
 struct NLArgs {
   Dims d;

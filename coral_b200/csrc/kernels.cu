@@ -47,7 +47,7 @@ __host__ __device__ constexpr int xy_threads(int N, int nl, int pv) {
   for (int i = 0; i < p.nst; ++i) m = (nl * N / p.r[i] > m) ? nl * N / p.r[i] : m;
   return (m + 31) / 32 * 32;
 }
-#define kThreadsX xy_threads(NF, 4, kPlanHot)
+#define kThreadsX xy_threads(NF, kNB2 / 2, kPlanHot)
 #define kThreadsY xy_threads(NF, 4, kPlanY)
 // the pipelined forward y pass reads its first-pass inputs from shared memory:
 // plan and threads of its own
@@ -2447,6 +2447,24 @@ void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const Ff
 void launch_fwd_y(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
                   cudaStream_t s) {
   dispatch_len<FwdY>(d.NYA, d, nq, Q1, qspec, scale, py, s);
+}
+// total of the KE partial sums written by the z kernels: one CTA, each thread a
+// strided sum, then a fixed-order tree
+__global__ void __launch_bounds__(1024) k_ke_sum(const double* part, size_t n, double* out) {
+  __shared__ double red[32];
+  double v = 0.0;
+  for (size_t i = threadIdx.x; i < n; i += blockDim.x) v += part[i];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) *out = v;
+  }
+}
+void launch_ke_sum(const double* part, size_t n, double* out, cudaStream_t s) {
+  k_ke_sum<<<1, 1024, 0, s>>>(part, n, out);
 }
 void launch_remove_zmean(const Dims& d, double2* qspec_q, cudaStream_t s) {
   k_remove_zmean<<<grid1d((size_t)d.NXH * d.NYA, 128), 128, 0, s>>>(d, qspec_q);

@@ -104,10 +104,17 @@ class PlaneLayer:
     def synchronize(self):
         self._check(self._lib.coral_synchronize(self._h))
 
-    def get_field(self, isys=0):
-        a = np.empty((self.NXH, self.NYAA, self.T[isys]), dtype=np.complex128)
-        self._check(self._lib.coral_get_field(self._h, isys, _dptr(a)))
-        return a
+    def get_field(self, isys=0, out=None):
+        """State of kxky system isys, (NX/2, NYAA, T) complex.  out: an existing
+        C-contiguous complex128 array of that shape to copy into (page-locked
+        memory makes the copy a DMA at full link speed)."""
+        shape = (self.NXH, self.NYAA, self.T[isys])
+        if out is None:
+            out = np.empty(shape, dtype=np.complex128)
+        elif out.shape != shape or out.dtype != np.complex128 or not out.flags.c_contiguous:
+            raise ValueError("out must be a C-contiguous complex128 array of shape %s" % (shape,))
+        self._check(self._lib.coral_get_field(self._h, isys, _dptr(out)))
+        return out
 
     def set_field(self, isys, field):
         a = np.ascontiguousarray(field, dtype=np.complex128)
