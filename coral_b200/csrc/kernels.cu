@@ -419,6 +419,18 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
     qv[0][threadIdx.x] = q.v1[threadIdx.x];
     qv[1][threadIdx.x] = q.v2[threadIdx.x];
   }
+  // compiled lengths: the FFT and DCT twiddles in shared memory
+  __shared__ double2 s_tw[NF ? NF : 1], s_dtw[NF ? NF : 1];
+  FftPlan pzl = pz;
+  const double2* dtw = dct_tw;
+  if constexpr (NF != 0) {
+    for (int i = threadIdx.x; i < NF; i += blockDim.x) {
+      s_tw[i] = pz.tw[i];
+      s_dtw[i] = dct_tw[i];
+    }
+    pzl.tw = s_tw;
+    dtw = s_dtw;
+  }
   // line l of a batch: variable l / kZPairs, column pair l % kZPairs (columns
   // x0 + 2p (re) and x0 + 2p + 1 (im))
   auto col_ok = [&](int c) { return x0 + c < d.NXA; };
@@ -438,12 +450,12 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
       const bool lo = n < NZ, hi = n > 0 && N - n < NZ;
       const double a0 = (lo && ha) ? sa[n] : 0.0, a1 = (hi && ha) ? sa[N - n] : 0.0;
       const double b0 = (lo && hb) ? sb[n] : 0.0, b1 = (hi && hb) ? sb[N - n] : 0.0;
-      const double2 w = cconj(dct_tw[n]);  // exp(+i pi n / 2N)
+      const double2 w = cconj(dtw[n]);  // exp(+i pi n / 2N)
       const double2 va = cmul(w, make_double2(a0, -a1));
       const double2 vb = cmul(w, make_double2(b0, -b1));
       return make_double2(va.x - vb.y, va.y + vb.x);
     };
-    const double2* R = fft_lines_ld<NF, true, NT, kZLines, false, kPlanHot>(Fv + l0 * N, B, nl, N, pz, ld);
+    const double2* R = fft_lines_ld<NF, true, NT, kZLines, false, kPlanHot>(Fv + l0 * N, B, nl, N, pzl, ld);
     if (R != Fv + l0 * N) {  // runtime plan with the result in the scratch lines
       for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) Fv[l0 * N + idx] = R[idx];
       __syncthreads();
@@ -537,7 +549,7 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
       }
       return make_double2(pa, pb);
     };
-    const double2* R = fft_lines_ld<NF, false, NT, kZFwd, false, kPlanHot>(A, B, nc, N, pz, ld);
+    const double2* R = fft_lines_ld<NF, false, NT, kZFwd, false, kPlanHot>(A, B, nc, N, pzl, ld);
     for (int idx = threadIdx.x; idx < nc * NZ; idx += blockDim.x) {
       const int li = idx / NZ, n = idx - li * NZ;
       const int lg = l0 + li, qg = lg / kZPairs, pr = lg - qg * kZPairs;
@@ -546,7 +558,7 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
       const double2 va = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
       const double2 dd = csub(Z, Zc);
       const double2 vb = make_double2(0.5 * dd.y, -0.5 * dd.x);  // (Z - Zc) / 2i
-      const double2 w = dct_tw[n];                                // exp(-i pi n / 2N)
+      const double2 w = dtw[n];                                   // exp(-i pi n / 2N)
       double* dst = Q2 + qg * vstride + col0 + (size_t)(2 * pr) * NZ;
       if (col_ok(2 * pr)) dst[n] = 2.0 * (w.x * va.x - w.y * va.y);
       if (col_ok(2 * pr + 1)) dst[NZ + n] = 2.0 * (w.x * vb.x - w.y * vb.y);
