@@ -751,6 +751,9 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       sa.Mw = k.Mw;
       sa.NLw = k.NLw;
       sa.NLg = k.NLg;
+      // CORAL_GENERIC_TILES=1: the run-time forms of the tile kernels (tests cover
+      // them with the plane-layer recipes, whose layouts are otherwise compiled)
+      sa.generic_tiles = std::getenv("CORAL_GENERIC_TILES") != nullptr;
       sa.Lw = k.Lw;
       {
         const int kv = sa.kl + sa.ku;

@@ -179,6 +179,7 @@ struct SolveArgs {
   int rhs_win_max;       // widest window (state + all slots), complex entries
   DevEll Mw, NLw;
   DevGEll NLg;           // NLw in grouped form (valid = 0: none)
+  int generic_tiles;     // 1: the tile kernels' run-time forms only (no compiled group layouts)
   // band entries that are zero in every block are not loaded (FactorArgs::lmask,
   // umask; null: load all)
   const unsigned* lmask;

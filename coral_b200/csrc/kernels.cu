@@ -2511,7 +2511,7 @@ static void group_widths(const DevGEll& G, int w[3]) {
 }
 void launch_rhs_nl(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
   if (a.work2 && a.rhs_win && a.row_pos) {
-    if (a.NLg.valid && a.NLg.ngroups == 3 && a.Mw.width <= 4) {
+    if (!a.generic_tiles && a.NLg.valid && a.NLg.ngroups == 3 && a.Mw.width <= 4) {
       int w[3];
       group_widths(a.NLg, w);
       // the plane-layer recipes' NL operator: groups i kx, i ky, 1 of widths 3, 3, 2
@@ -2562,7 +2562,7 @@ void launch_kstd_out(const SolveArgs& a, cudaStream_t s) {
     int w[4] = {0, 0, 0, 0};
     for (int k = 0; k < a.Lw.width; ++k)
       if (a.Lw.slot_grp[k] < 4) ++w[a.Lw.slot_grp[k]];
-    if (a.Lw.ngroups == 4 && w[0] == 4 && w[1] == 6 && w[2] == 3 && w[3] == 3) {
+    if (!a.generic_tiles && a.Lw.ngroups == 4 && w[0] == 4 && w[1] == 6 && w[2] == 3 && w[3] == 3) {
       // the plane-layer recipes' L: (kx^2 + ky^2), 1, kx, ky groups
       set_smem(k_kstd_tiles<4, 6, 3, 3>, sm);
       k_kstd_tiles<4, 6, 3, 3><<<g, kTileRows, sm, s>>>(a);

@@ -161,11 +161,16 @@ def test_all_factor_paths_match_oracle(path, monkeypatch):
     pl.close()
 
 
-@pytest.mark.parametrize("split", [True, False])
-def test_split_solve_rbc_noslip_matches_oracle(split, monkeypatch):
+@pytest.mark.parametrize("split,generic", [(True, False), (True, True), (False, False)])
+def test_split_solve_rbc_noslip_matches_oracle(split, generic, monkeypatch):
     """No-slip Rayleigh-Benard (the benchmark recipe) at NZ = 48 with and without
-    the block split, against the oracle over a few ARS_222 steps."""
+    the block split, against the oracle over a few ARS_222 steps; generic: the
+    tile kernels' run-time operator forms instead of the compiled group layouts."""
     monkeypatch.delenv("CORAL_COMPLEX_FACTORS", raising=False)
+    if generic:
+        monkeypatch.setenv("CORAL_GENERIC_TILES", "1")
+    else:
+        monkeypatch.delenv("CORAL_GENERIC_TILES", raising=False)
     if split:
         monkeypatch.delenv("CORAL_NO_CLASS_SPLIT", raising=False)
     else:
