@@ -1,0 +1,174 @@
+"""Error model of a split-precision form of the timestep (test infrastructure).
+
+TEST INFRASTRUCTURE ONLY, like ``coral_oracle``: a CPU model, not product code
+and not imported by the product.  It answers one design question before any
+tensor-core kernel is written: how accurate must the transforms be for the
+timestep to stay within a given relative error of the FP64 oracle?
+
+The model swaps the oracle's transforms (``spec_to_phys`` / ``phys_to_spec``,
+which restate src/slabs.fftw3mpi/transforms.f90:155-301) for variants in which
+
+* the z (Chebyshev) transform is a dense contraction with the REDFT01 /
+  REDFT10 matrices (NZAA x NZ and NZ x NZAA), both operands split into k
+  BF16 slices (round to nearest even), the slice products with i + j < k
+  (i + j <= 2 for k = 3: six products) formed exactly and accumulated either in
+  FP32 (a tensor-core accumulator) or exactly (FP64 here: the accumulation of
+  an integer-slice scheme is exact);
+* the x / y FFTs run in FP32 or FP64.
+
+Everything else (band LU, stage sums, the state) stays the oracle's FP64.  The
+state after n steps is compared with the FP64 oracle started from the same
+seeded initial condition as the benchmark (white-noise temperature, amplitude
+1e-3, times sin(pi z'), PCG64 seed 2; Ra = 1e8 no-slip recipe, dt = 1e-6).
+
+    python oracle/precision_model.py NX NZ STEPS
+"""
+import os
+import sys
+import time
+
+import numpy as np
+import scipy.fft as sfft
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+from oracle import coral_oracle as co  # noqa: E402
+
+
+def bf16(x):
+    """Round to the nearest BF16 value (ties to even), returned as float64."""
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32)
+    u = (u + (0x7FFF + ((u >> 16) & 1))) & np.uint32(0xFFFF0000)
+    return u.view(np.float32).astype(np.float64)
+
+
+def slices(x, k):
+    """x = s_0 + s_1 + ... + s_{k-1} + remainder, each s_i a BF16 value."""
+    out, r = [], np.asarray(x, dtype=np.float64)
+    for _ in range(k):
+        s = bf16(r)
+        out.append(s)
+        r = r - s
+    return out
+
+
+def gemm_sliced(A, B, k, fp32_acc):
+    """A @ B from the slice products with i + j < k; products are exact (8-bit
+    significands), accumulation in FP32 or exact (FP64)."""
+    As, Bs = slices(A, k), slices(B, k)
+    dt = np.float32 if fp32_acc else np.float64
+    acc = np.zeros((A.shape[0], B.shape[1]), dtype=dt)
+    for i in range(k):
+        for j in range(k - i):
+            acc += As[i].astype(dt) @ Bs[j].astype(dt)
+    return acc.astype(np.float64)
+
+
+_MATS = {}
+
+
+def dct_matrices(NZ, NZAA):
+    """REDFT01 of the zero-padded series (NZAA x NZ) and REDFT10 truncated to NZ
+    outputs (NZ x NZAA), unnormalised as FFTW's."""
+    if (NZ, NZAA) not in _MATS:
+        z = np.arange(NZAA)[:, None]
+        n = np.arange(NZ)[None, :]
+        C = np.cos(np.pi * n * (2 * z + 1) / (2.0 * NZAA))
+        inv = 2.0 * C
+        inv[:, 0] = 1.0
+        _MATS[(NZ, NZAA)] = (inv, 2.0 * C.T)
+    return _MATS[(NZ, NZAA)]
+
+
+def make_transforms(k, fp32_acc=True, fp32_fft=True):
+    """spec_to_phys / phys_to_spec with the z transform as a sliced contraction
+    (k = 0: the exact FP64 contraction) and the x / y FFTs in FP32 or FP64."""
+    cd = np.complex64 if fp32_fft else np.complex128
+    rd = np.float32 if fp32_fft else np.float64
+
+    def zgemm(M, cols):
+        return gemm_sliced(M, cols, k, fp32_acc) if k else M @ cols
+
+    def spec_to_phys(spec, g):
+        b = sfft.ifft(spec.astype(cd), axis=1, norm="forward")
+        b[:, :, 0] *= 2.0
+        X = np.zeros((g.NYAA, g.NXAA // 2 + 1, g.NZ), dtype=cd)
+        X[:, :g.NXH, :] = b.transpose(1, 0, 2) * 0.5
+        r = sfft.irfft(X, n=g.NXAA, axis=1, norm="forward")
+        inv, _ = dct_matrices(g.NZ, g.NZAA)
+        ph = zgemm(inv, r.reshape(-1, g.NZ).T.astype(np.float64))
+        return ph.T.reshape(g.NYAA, g.NXAA, g.NZAA)
+
+    def phys_to_spec(phys, g):
+        _, fwd = dct_matrices(g.NZ, g.NZAA)
+        a = zgemm(fwd, phys.reshape(-1, g.NZAA).T).T.reshape(g.NYAA, g.NXAA, g.NZ)
+        c = sfft.rfft(a.astype(rd), axis=1)[:, :g.NXH, :]
+        c = np.ascontiguousarray(c.transpose(1, 0, 2))
+        c[:, :, 0] *= 0.5
+        s = sfft.fft(c, axis=1).astype(np.complex128)
+        return s * (1.0 / (g.NXAA * g.NYAA * g.NZAA))
+
+    return spec_to_phys, phys_to_spec
+
+
+def benchmark_ic(solver, seed=2):
+    """The benchmark's initial condition (bench.make_ic) on the oracle."""
+    from coral_b200.initial_conditions import gauss_chebyshev_z
+    g = solver.g
+    rng = np.random.Generator(np.random.PCG64(seed))
+    zp = gauss_chebyshev_z(g.NZAA, 0.5, 1.0)
+    th = rng.uniform(-1e-3, 1e-3, size=(g.NXAA, g.NYAA, g.NZAA)) * np.sin(np.pi * zp)[None, None, :]
+    mean = th.mean(axis=(0, 1))
+    th -= mean[None, None, :]
+    solver.set_var_from_phys(0, 4, np.ascontiguousarray(th.transpose(1, 0, 2)))
+    solver.set_zero_var_from_phys(1, 0, mean)
+
+
+VARIANTS = [  # (label, slices, FP32 accumulation, FP32 FFTs)
+    ("3 BF16 slices, FP32 acc, FP32 FFTs", 3, True, True),
+    ("3 BF16 slices, FP32 acc, FP64 FFTs", 3, True, False),
+    ("exact z, FP32 FFTs", 0, True, True),
+    ("2 BF16 slices, FP32 acc, FP32 FFTs", 2, True, True),
+    ("3 BF16 slices, exact acc, FP64 FFTs", 3, False, False),
+    ("4 BF16 slices, exact acc, FP64 FFTs", 4, False, False),
+    ("5 BF16 slices, exact acc, FP64 FFTs", 5, False, False),
+]
+
+
+def main(NX, NZ, steps, checkpoints=(1, 10, 100)):
+    from tests.problems import equations, params
+    dt = 1e-6
+    eq, par = equations("rbc_noslip_ra1e8"), params(NX, NX, NZ, dt=dt)
+
+    def fresh():
+        s = co.Solver(eq, par)
+        benchmark_ic(s)
+        return s
+
+    keep = [c for c in checkpoints if c <= steps] or [steps]
+    base, ref = fresh(), {}
+    t0 = time.time()
+    for i in range(1, steps + 1):
+        base.step(dt)
+        if i in keep:
+            ref[i] = ([f.copy() for f in base.field], [z.copy() for z in base.zfield])
+    print("FP64 oracle, %dx%dx%d, %d steps: %.0f s" % (NX, NX, NZ, steps, time.time() - t0), flush=True)
+    s2p, p2s = co.spec_to_phys, co.phys_to_spec
+    for label, k, acc32, fft32 in VARIANTS:
+        co.spec_to_phys, co.phys_to_spec = make_transforms(k, acc32, fft32)
+        try:
+            m, out = fresh(), []
+            for i in range(1, steps + 1):
+                m.step(dt)
+                if i in keep:
+                    f, z = ref[i]
+                    e = max(np.linalg.norm(m.field[j] - f[j]) / np.linalg.norm(f[j]) for j in range(len(f)))
+                    ez = max(np.linalg.norm(m.zfield[j] - z[j]) / max(np.linalg.norm(z[j]), 1e-300)
+                             for j in range(len(z)))
+                    out.append("step %d: %.1e / %.1e" % (i, e, ez))
+        finally:
+            co.spec_to_phys, co.phys_to_spec = s2p, p2s
+        print("%-38s kxky / mean rel L2: %s" % (label, "; ".join(out)), flush=True)
+
+
+if __name__ == "__main__":
+    main(int(sys.argv[1]), int(sys.argv[2]), int(sys.argv[3]))
