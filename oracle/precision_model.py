@@ -14,6 +14,9 @@ which restate src/slabs.fftw3mpi/transforms.f90:155-301) for variants in which
   (i + j <= 2 for k = 3: six products) formed exactly and accumulated either in
   FP32 (a tensor-core accumulator) or exactly (FP64 here: the accumulation of
   an integer-slice scheme is exact);
+* or the z contraction uses int8 slices with one shared exponent per matrix
+  row and per data column, the slice products accumulated exactly (an integer
+  tensor-core GEMM accumulates in INT32) and combined in FP64;
 * the x / y FFTs run in FP32 or FP64.
 
 Everything else (band LU, stage sums, the state) stays the oracle's FP64.  The
@@ -63,6 +66,36 @@ def gemm_sliced(A, B, k, fp32_acc):
     return acc.astype(np.float64)
 
 
+def int8_slices(x, k, axis):
+    """Integer slices with one shared exponent per row (axis=1) or column
+    (axis=0): x = 2^e (d_0 + d_1 2^-7 + ... + d_{k-1} 2^-7(k-1)) / 127 + rem,
+    every d_s an integer in [-127, 127].  Returns the digit arrays (float64
+    holding integers) and the scale per row / column."""
+    m = np.abs(x).max(axis=axis, keepdims=True)
+    e = np.where(m > 0, np.ceil(np.log2(np.where(m > 0, m, 1.0))), 0.0)
+    scale = np.exp2(e)
+    r = x / scale * 127.0                     # |r| <= 127
+    out = []
+    for s in range(k):
+        d = np.rint(r)
+        out.append(d)
+        r = (r - d) * 128.0
+    return out, scale
+
+
+def gemm_int8(A, B, k):
+    """A @ B from int8 slices (shared exponent per row of A and per column of
+    B): the products with i + j < k are integer GEMMs (exact: |sum| < 2^31 for
+    K = 192), combined in FP64."""
+    As, sa = int8_slices(A, k, axis=1)
+    Bs, sb = int8_slices(B, k, axis=0)
+    acc = np.zeros((A.shape[0], B.shape[1]))
+    for i in range(k):
+        for j in range(k - i):
+            acc += (As[i] @ Bs[j]) * 2.0 ** (-7 * (i + j))   # integer-valued products, exact in FP64
+    return acc * (sa / 127.0) * (sb / 127.0)
+
+
 _MATS = {}
 
 
@@ -81,11 +114,15 @@ def dct_matrices(NZ, NZAA):
 
 def make_transforms(k, fp32_acc=True, fp32_fft=True):
     """spec_to_phys / phys_to_spec with the z transform as a sliced contraction
-    (k = 0: the exact FP64 contraction) and the x / y FFTs in FP32 or FP64."""
+    (k > 0: k BF16 slices; k < 0: -k int8 slices with exact integer
+    accumulation; k = 0: the exact FP64 contraction) and the x / y FFTs in FP32
+    or FP64."""
     cd = np.complex64 if fp32_fft else np.complex128
     rd = np.float32 if fp32_fft else np.float64
 
     def zgemm(M, cols):
+        if k < 0:
+            return gemm_int8(M, cols, -k)
         return gemm_sliced(M, cols, k, fp32_acc) if k else M @ cols
 
     def spec_to_phys(spec, g):
@@ -131,6 +168,9 @@ VARIANTS = [  # (label, slices, FP32 accumulation, FP32 FFTs)
     ("3 BF16 slices, exact acc, FP64 FFTs", 3, False, False),
     ("4 BF16 slices, exact acc, FP64 FFTs", 4, False, False),
     ("5 BF16 slices, exact acc, FP64 FFTs", 5, False, False),
+    ("4 int8 slices, INT32 acc, FP64 FFTs", -4, False, False),
+    ("5 int8 slices, INT32 acc, FP64 FFTs", -5, False, False),
+    ("6 int8 slices, INT32 acc, FP64 FFTs", -6, False, False),
 ]
 
 

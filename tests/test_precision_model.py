@@ -34,3 +34,15 @@ def test_contraction_form_matches_oracle_transforms():
     s2p4, _ = pm.make_transforms(4, fp32_acc=False, fp32_fft=False)
     c = s2p4(spec, g)
     assert np.abs(c - ph).max() <= 1e-8 * np.abs(ph).max()
+
+
+def test_int8_slice_contraction_accuracy():
+    """Integer slices (shared exponent per row / column, exact accumulation):
+    each slice adds ~7 bits relative to the row / column maximum."""
+    rng = np.random.default_rng(2)
+    inv, _ = pm.dct_matrices(48, 72)
+    B = rng.standard_normal((48, 40)) * np.exp(rng.uniform(-6, 0, (48, 1)))
+    ex = inv @ B
+    errs = [np.abs(pm.gemm_int8(inv, B, k) - ex).max() / np.abs(ex).max() for k in (3, 4, 5, 6)]
+    assert errs[0] < 1e-4 and errs[2] < 1e-8 and errs[3] < 1e-10
+    assert all(b < a for a, b in zip(errs, errs[1:]))
