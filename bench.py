@@ -52,6 +52,16 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(x, device):
+    """Max of a float over all ranks of the process group (a tensor on `device`:
+    the rank's GPU under NCCL, "cpu" under gloo)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def read_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -242,9 +252,7 @@ def run_ours(args, cfg):
     barrier()
     gpu_launches = pl.kernel_launches - launches0
     if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{dev}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, f"cuda:{dev}")
     ms_per_step = ms / args.steps
     value = world * args.steps / (ms / 1e3)
     diag = pl.diagnostics()
@@ -278,9 +286,7 @@ def run_ours(args, cfg):
     out = pl.get_field(0, out=pin_out)
     e2e_s = time.perf_counter() - t0
     if world > 1:
-        t = torch.tensor([e2e_s], device=f"cuda:{dev}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2e_s = max_over_ranks(e2e_s, f"cuda:{dev}")
     del out
     state_bytes = field.nbytes + sum(z.nbytes for z in zf)
     diag_bytes = 3 * 8 + 8 + 4  # CFL maxima, KE total, non-finite flag
