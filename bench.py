@@ -75,7 +75,15 @@ class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
     def __init__(self, index):
-        self.index = index
+        # nvidia-smi numbers GPUs physically, CUDA after CUDA_VISIBLE_DEVICES
+        # remapping: select the timed GPU by its UUID (read-only query)
+        self.index = str(index)
+        try:
+            import torch
+            u = str(torch.cuda.get_device_properties(index).uuid)
+            self.index = u if u.startswith("GPU-") else "GPU-" + u
+        except Exception:
+            pass
         self.proc = None
         self.lines = []
 
@@ -84,7 +92,7 @@ class ClockSampler:
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.index, "--query-gpu=" + q,
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)

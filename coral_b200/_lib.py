@@ -43,6 +43,12 @@ SIGNATURES = {
     "coral_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
     "coral_profile_step": (ctypes.c_int, [_P, ctypes.c_double, _D, ctypes.c_int]),
     "coral_spec_to_phys_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D, _P]),
+    "coral_set_timeseries": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "coral_set_timeseries_from_file": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "coral_timeseries": (ctypes.c_int, [_P, _D, ctypes.c_int]),
+    "coral_set_time": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_longlong]),
+    "coral_get_time": (ctypes.c_int, [_P, _D]),
+    "coral_run": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_char_p]),
 }
 
 _lib = None

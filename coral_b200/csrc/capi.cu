@@ -6,6 +6,8 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <sys/stat.h>
+#include <cerrno>
 #include <memory>
 #include <sstream>
 #include <string>
@@ -153,6 +155,19 @@ struct coral_handle {
   double graph_dt = -1.0;
   long long launches = 0;
   int launches_per_step = 0;
+  // timeseries objects of coral.timeseries (output_global_quantities,
+  // PL_IMEX_timestepping_output.f90:5-231): file name of each object and the
+  // per-CTA partial sums / totals on the device
+  std::vector<std::string> ts_file;
+  double* ts_partial = nullptr;   // [z_fused_ctas][kMaxTs]
+  size_t ts_ncta = 0;
+  double* ts_out = nullptr;       // [kMaxTs], totals of the last step's first stage
+  double* h_pin = nullptr;        // page-locked readback: kMaxTs timeseries values, 3 CFL maxima, flags
+  // time keeping of the driver loop (src/misc/timeKeeping.f90:22-49)
+  double time = 0.0, dt_current = 0.0, dt_target = 0.0;
+  long long i_timestep = 1, refactorizations = 0;
+  // timeseries rows not yet written: (i_timestep, time, values)
+  std::vector<std::pair<long long, std::vector<double>>> ts_rows;
 };
 
 namespace {
@@ -619,6 +634,15 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
   CK(cudaMemset(h->cfl_bits, 0, 3 * sizeof(unsigned long long)));
   h->flags = mem.get<unsigned int>(1);
   CK(cudaMemset(h->flags, 0, sizeof(unsigned int)));
+  h->ts_ncta = z_fused_ctas(h->d);
+  h->ts_partial = mem.get<double>(h->ts_ncta * kMaxTs);
+  h->ts_out = mem.get<double>(kMaxTs);
+  CK(cudaMemset(h->ts_out, 0, kMaxTs * sizeof(double)));
+  CK(cudaMallocHost(&h->h_pin, (kMaxTs + 4) * sizeof(double)));
+  // timings%init (timeKeeping.f90:57-70): dt_current = dt = dt_max, t = 0, step 1
+  h->dt_current = h->dt_target = P.dt_max;
+  h->time = 0.0;
+  h->i_timestep = 1;
   CK(cudaDeviceSynchronize());
 }
 
@@ -680,8 +704,13 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
     // quadratic variables overwrite Y2 in place, each CTA reading and writing only
     // its own (y, x pair) columns
     B(3);
-    launch_z_fused(d, h->nF, h->quads, h->Y2, h->Y2, h->pz, h->dct_tw, h->d_wz, h->d_wzinv,
-                   last ? h->cfl_bits : nullptr, i == 0 ? h->ke_partial : nullptr, h->stream);
+    {
+      // the first stage's fields also give the timeseries objects
+      QuadDesc q = h->quads;
+      q.ts_partial = (i == 0 && q.ts_n > 0) ? h->ts_partial : nullptr;
+      launch_z_fused(d, h->nF, q, h->Y2, h->Y2, h->pz, h->dct_tw, h->d_wz, h->d_wzinv,
+                     last ? h->cfl_bits : nullptr, i == 0 ? h->ke_partial : nullptr, h->stream);
+    }
     E();
     B(4); launch_fwd_x(d, h->nQ, h->Y2, h->Y1, h->px, h->stream); E();
     B(5); launch_fwd_y(d, h->nQ, h->Y1, h->qspec, scale, h->py, h->stream); E();
@@ -786,6 +815,11 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
       B(8); launch_zero_step(za, h->stream); E();
       ++nl;
     }
+  }
+  if (h->quads.ts_n > 0) {
+    launch_ts_reduce(h->ts_partial, h->ts_ncta, h->quads.ts_n, 1.0 / ((double)g.NXAA * (double)g.NYAA), h->ts_out,
+                     h->stream);
+    ++nl;
   }
   CK(cudaGetLastError());
   return nl;
@@ -1008,6 +1042,180 @@ std::vector<double> export_zero_var(coral_handle* h, ZSys& z, int v) {
   return prof;
 }
 
+// mkdir -p
+int mkdir_p(const std::string& path) {
+  std::string cur;
+  for (size_t i = 0; i <= path.size(); ++i) {
+    if (i == path.size() || path[i] == '/') {
+      if (!cur.empty() && ::mkdir(cur.c_str(), 0755) != 0 && errno != EEXIST) return -1;
+    }
+    if (i < path.size()) cur.push_back(path[i]);
+  }
+  return 0;
+}
+
+// cargo%cfl_based_DT from the CFL maxima of the last step's last stage
+// (compute_cfl_based_timestep, marching.f90:219-238, cflFactor_along_z = 1)
+double cfl_dt_of(const coral_handle* h, const unsigned long long bits[3]) {
+  const Geometry& g = *h->G;
+  double mx[3];
+  for (int i = 0; i < 3; ++i) std::memcpy(&mx[i], &bits[i], sizeof(double));
+  const double u = mx[0] * g.NXAA / g.Lx, v = mx[1] * g.NYAA / g.Ly;
+  const double w = std::max(v, mx[2]);
+  const double m = std::max(u, std::max(v, w));
+  return (h->nF >= 3 && m > 0.0) ? 1.0 / m : (h->nF >= 3 ? INFINITY : 1.0);
+}
+
+std::string trim(const std::string& t) {
+  size_t a = t.find_first_not_of(" \t\r\n"), b = t.find_last_not_of(" \t\r\n");
+  return a == std::string::npos ? std::string() : t.substr(a, b - a + 1);
+}
+
+// coral.timeseries (master_recipe%add_timeseries, PL_equations.f90:233-320 with
+// get_timeseriesVarName_period[_position], PL_string_to_data.f90:200-242):
+//   >>Volume_average :: NAME <<
+//   >>Horizontal_avg :: NAME ;; Position= K <<      (K: 1-based z grid index)
+// until >>EOF<<.  Positions beyond NZAA are ignored (as the reference does);
+// NAME is a full variable or a quadratic variable.  Objects are ordered as the
+// reference fills its buffer: full variables in recipe order, then quadratic
+// variables, each with its objects in file order.
+void set_timeseries(coral_handle* h, const std::string& text) {
+  struct Obj { int src, z; std::string file; };
+  std::vector<std::vector<Obj>> per_full(h->nF), per_quad(h->nQ);
+  std::istringstream in(text);
+  std::string line;
+  const int NZAA = h->G->NZAA;
+  while (std::getline(in, line)) {
+    if (line.size() >= 5 && line.compare(2, 3, "EOF") == 0) break;
+    if (trim(line).empty()) continue;
+    const std::string head = line.substr(0, std::min<size_t>(19, line.size()));
+    const size_t dc = line.find("::"), end = line.find("<<", 2);
+    if (dc == std::string::npos || end == std::string::npos || end < dc)
+      throw CoralError(CORAL_EPARSE, "coral.timeseries: cannot read line '" + line + "'");
+    std::string name;
+    int zpos = -1;
+    if (head == ">>Volume_average ::") {
+      name = trim(line.substr(dc + 2, end - dc - 2));
+    } else if (head == ">>Horizontal_avg ::") {
+      const size_t pp = line.find(";; Position=");
+      if (pp == std::string::npos || pp < dc)
+        throw CoralError(CORAL_EPARSE, "coral.timeseries: no ';; Position=' in '" + line + "'");
+      name = trim(line.substr(dc + 2, pp - dc - 2));
+      zpos = std::atoi(trim(line.substr(pp + 12, end - pp - 12)).c_str());
+      if (zpos > NZAA) continue;  // ignored, as by the reference
+      if (zpos < 1) throw CoralError(CORAL_EPARSE, "coral.timeseries: position must be >= 1 in '" + line + "'");
+    } else {
+      throw CoralError(CORAL_EPARSE, "coral.timeseries: lines must start with '>>Volume_average ::' or "
+                                     "'>>Horizontal_avg ::' ('" + line + "')");
+    }
+    char ext[32];
+    if (zpos < 0) std::snprintf(ext, sizeof(ext), "_volAvg.dat");
+    else std::snprintf(ext, sizeof(ext), "_XYavg_z%05d.dat", zpos);
+    for (int f = 0; f < h->nF; ++f)
+      if (h->R.full[f].name == name) per_full[f].push_back({f, zpos - 1, name + ext});
+    for (int q = 0; q < h->nQ; ++q)
+      if (h->R.quad[q].name == name) per_quad[q].push_back({-1 - q, zpos - 1, name + ext});
+  }
+  std::vector<Obj> all;
+  for (auto& v : per_full) all.insert(all.end(), v.begin(), v.end());
+  for (auto& v : per_quad) all.insert(all.end(), v.begin(), v.end());
+  if (all.size() > (size_t)kMaxTs)
+    throw CoralError(CORAL_EUNSUPPORTED, "coral.timeseries: more than " + std::to_string(kMaxTs) + " objects");
+  h->quads.ts_n = (int)all.size();
+  h->ts_file.clear();
+  for (size_t o = 0; o < all.size(); ++o) {
+    h->quads.ts_src[o] = all[o].src;
+    h->quads.ts_z[o] = all[o].z;
+    h->ts_file.push_back(all[o].file);
+  }
+  // the step graph bakes in the objects: capture it again
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
+  h->ts_rows.clear();
+}
+
+// Append the buffered timeseries rows to <dir>/Timeseries/*.dat: raw float64,
+// the value of step k at byte offset 8 (k - 1), a file started afresh when
+// step 1 is written (output_2Dbundled_dsca_in_unique_timeserie calls of
+// PL_IMEX_timestepping_output.f90:136-231).
+void flush_timeseries(coral_handle* h, const std::string& dir) {
+  if (h->ts_rows.empty()) return;
+  const std::string tsdir = dir + "/Timeseries";
+  FILE* probe = std::fopen((tsdir + "/.").c_str(), "rb");
+  if (probe) std::fclose(probe);
+  else if (mkdir_p(tsdir) != 0) throw CoralError(CORAL_EIO, "cannot create " + tsdir);
+  const int n = h->quads.ts_n;
+  for (int o = -1; o < n; ++o) {  // -1: time.dat
+    const std::string fn = tsdir + "/" + (o < 0 ? std::string("time.dat") : h->ts_file[o]);
+    const long long first = h->ts_rows.front().first;
+    FILE* f = std::fopen(fn.c_str(), first == 1 ? "wb" : "r+b");
+    if (!f) f = std::fopen(fn.c_str(), "wb");
+    if (!f) throw CoralError(CORAL_EIO, "cannot open " + fn);
+    std::vector<double> col;
+    col.reserve(h->ts_rows.size());
+    for (auto& r : h->ts_rows) col.push_back(r.second[o + 1]);
+    if (std::fseek(f, (long)((first - 1) * 8), SEEK_SET) != 0 ||
+        std::fwrite(col.data(), sizeof(double), col.size(), f) != col.size()) {
+      std::fclose(f);
+      throw CoralError(CORAL_EIO, "short write in " + fn);
+    }
+    std::fclose(f);
+  }
+  h->ts_rows.clear();
+}
+
+// The time loop of plane_layer_main.f90:138-205 for nsteps steps, with the
+// dt rules of timeKeeping.f90: after each step dt = CFL_C * cfl_based_DT
+// capped at dt_max (compare_dt_against_CFL, :78-89; stop below dt_min = 1e-9);
+// before each step, dt_current takes the target dt when they differ by more
+// than tolerance * dt_current, and the operators are refactorised
+// (update_dt_if_needed, :171-183; factorize_operators).  The timeseries
+// objects are recorded every step (time at the start of the step and the
+// values of its first stage) and written to <dir>/Timeseries every 20 steps
+// (buffer_length, PL_IMEX_timestepping.f90:159) and at the end.
+void run_loop(coral_handle* h, int nsteps, const char* outdir) {
+  if (nsteps < 0) throw CoralError(CORAL_EBADARG, "coral_run: nsteps must be >= 0");
+  const Parameters& P = h->P;
+  const double dt_min = 1e-9;
+  const int n = h->quads.ts_n;
+  for (int s = 0; s < nsteps; ++s) {
+    // check_for_update
+    if (std::fabs(h->dt_target - h->dt_current) > P.tolerance * h->dt_current) {
+      h->dt_current = h->dt_target;
+      ++h->refactorizations;
+    }
+    march(h, h->dt_current, 1);  // refactorises when dt_current changed
+    CK(cudaMemcpyAsync(h->h_pin + kMaxTs, h->cfl_bits, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       h->stream));
+    if (n > 0)
+      CK(cudaMemcpyAsync(h->h_pin, h->ts_out, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (n > 0 || outdir) {
+      std::vector<double> row(n + 1);
+      row[0] = h->time;
+      for (int o = 0; o < n; ++o) row[o + 1] = h->h_pin[o];
+      h->ts_rows.emplace_back(h->i_timestep, std::move(row));
+    }
+    unsigned long long bits[3];
+    std::memcpy(bits, h->h_pin + kMaxTs, sizeof(bits));
+    const double cfl = cfl_dt_of(h, bits);
+    // apply_cfl
+    double dt = cfl * P.CFL_C;
+    if (!(dt <= P.dt_max)) dt = P.dt_max;  // also when cfl is infinite or NaN
+    if (!(cfl == cfl)) throw CoralError(CORAL_ENONFINITE, "non-finite velocity maximum in the CFL criterion");
+    if (dt < dt_min) throw CoralError(CORAL_ENONFINITE, "minimal timestep reached (dt < 1e-9)");
+    h->dt_target = dt;
+    // increment
+    h->time += h->dt_current;
+    ++h->i_timestep;
+    if (outdir && h->ts_rows.size() >= 20) flush_timeseries(h, outdir);
+  }
+  if (outdir) flush_timeseries(h, outdir);
+  else h->ts_rows.clear();
+}
+
 template <typename F>
 int guarded(coral_handle* h, F&& f) {
   if (!h) return CORAL_EBADARG;
@@ -1049,12 +1257,14 @@ int coral_create(const char* equations_text, const char* parameters_text, const 
   } catch (const CoralError& e) {
     g_create_error = e.what();
     h->mem.free_all();
+    if (h->h_pin) cudaFreeHost(h->h_pin);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return e.code;
   } catch (const std::exception& e) {
     g_create_error = e.what();
     h->mem.free_all();
+    if (h->h_pin) cudaFreeHost(h->h_pin);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return CORAL_EBADARG;
@@ -1086,6 +1296,7 @@ void coral_destroy(coral_handle* h) {
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->graph) cudaGraphExecDestroy(h->graph);
   h->mem.free_all();
+  if (h->h_pin) cudaFreeHost(h->h_pin);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -1345,13 +1556,7 @@ int coral_diagnostics(coral_handle* h, double* out3) {
     CK(cudaStreamSynchronize(h->stream));
     unsigned long long bits[3];
     CK(cudaMemcpy(bits, h->cfl_bits, sizeof(bits), cudaMemcpyDeviceToHost));
-    double mx[3];
-    for (int i = 0; i < 3; ++i) std::memcpy(&mx[i], &bits[i], sizeof(double));
-    // compute_cfl_based_timestep (marching.f90:219-238), cflFactor_along_z = 1
-    double u = mx[0] * g.NXAA / g.Lx, v = mx[1] * g.NYAA / g.Ly;
-    double w = std::max(v, mx[2]);
-    double m = std::max(u, std::max(v, w));
-    out3[0] = (h->nF >= 3 && m > 0.0) ? 1.0 / m : (h->nF >= 3 ? INFINITY : 1.0);
+    out3[0] = cfl_dt_of(h, bits);
     // the partial sums are totalled on the device: 8 bytes come back, not the
     // per-CTA array
     launch_ke_sum(h->ke_partial, h->n_ke_partial, h->ke_total, h->stream);
@@ -1364,6 +1569,56 @@ int coral_diagnostics(coral_handle* h, double* out3) {
     CK(cudaMemcpy(&f, h->flags, sizeof(f), cudaMemcpyDeviceToHost));
     out3[2] = (f & 1u) ? 1.0 : 0.0;
   });
+}
+
+int coral_set_timeseries(coral_handle* h, const char* timeseries_text) {
+  return guarded(h, [&] {
+    if (!timeseries_text) throw CoralError(CORAL_EBADARG, "null text");
+    set_timeseries(h, timeseries_text);
+  });
+}
+
+int coral_set_timeseries_from_file(coral_handle* h, const char* path) {
+  return guarded(h, [&] {
+    if (!path) throw CoralError(CORAL_EBADARG, "null path");
+    set_timeseries(h, slurp(path));
+  });
+}
+
+int coral_timeseries(coral_handle* h, double* values, int n) {
+  return guarded(h, [&] {
+    const int m = h->quads.ts_n;
+    if (n < m || (m > 0 && !values)) throw CoralError(CORAL_EBADARG, "buffer smaller than the timeseries objects");
+    CK(cudaStreamSynchronize(h->stream));
+    if (m > 0) CK(cudaMemcpy(values, h->ts_out, m * sizeof(double), cudaMemcpyDeviceToHost));
+  });
+}
+
+int coral_set_time(coral_handle* h, double time, double dt, long long i_timestep) {
+  return guarded(h, [&] {
+    if (!(dt > 0.0) || i_timestep < 1) throw CoralError(CORAL_EBADARG, "dt must be > 0 and i_timestep >= 1");
+    // read_timings_from_file (timeKeeping.f90:92-134) after its dt / 50: dt is
+    // capped at dt_max
+    const double d = dt <= h->P.dt_max ? dt : h->P.dt_max;
+    h->time = time;
+    h->dt_current = h->dt_target = d;
+    h->i_timestep = i_timestep;
+    h->ts_rows.clear();
+  });
+}
+
+int coral_get_time(coral_handle* h, double* out4) {
+  return guarded(h, [&] {
+    if (!out4) throw CoralError(CORAL_EBADARG, "null buffer");
+    out4[0] = h->time;
+    out4[1] = h->dt_current;
+    out4[2] = (double)h->i_timestep;
+    out4[3] = (double)h->refactorizations;
+  });
+}
+
+int coral_run(coral_handle* h, int nsteps, const char* output_directory) {
+  return guarded(h, [&] { run_loop(h, nsteps, output_directory); });
 }
 
 }  // extern "C"

@@ -70,10 +70,21 @@ struct StateSet {  // pointers of the coupled kxky systems for the full-variable
   const double* z[kMaxSets];
 };
 
+constexpr int kMaxTs = 16;      // timeseries objects (lines of coral.timeseries)
+
 struct QuadDesc {
   int nq;
   int v1[kMaxQuad], v2[kMaxQuad];
   int ke_q[3];  // quadratic variables whose volume averages form KE (uu, vv, ww), -1 if absent
+  // Timeseries objects of output_global_quantities (PL_IMEX_timestepping_output.f90:5-127),
+  // evaluated on the first stage's physical fields when ts_partial is non-null:
+  // ts_src[o] >= 0: full variable ts_src[o]; < 0: quadratic variable -1 - ts_src[o];
+  // ts_z[o] < 0: volume average (Gauss-Chebyshev weights), else the horizontal average at
+  // grid level ts_z[o] (0-based z index of phys(NZAA, NXAA, NYAA)).  Per-CTA partial sums
+  // go to ts_partial[cta * kMaxTs + o].
+  int ts_n;
+  int ts_src[kMaxTs], ts_z[kMaxTs];
+  double* ts_partial;
 };
 
 struct Dims {
@@ -101,8 +112,13 @@ void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const Ff
 void launch_fwd_y(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
                   cudaStream_t s);
 void launch_remove_zmean(const Dims& d, double2* qspec_q, cudaStream_t s);
+// CTAs of launch_z_fused (rows of its KE and timeseries partial sums)
+size_t z_fused_ctas(const Dims& d);
 // total of the n KE partial sums (one CTA, fixed order) into *out
 void launch_ke_sum(const double* part, size_t n, double* out, cudaStream_t s);
+// timeseries: out[o] = scale * sum over the ncta rows of part[cta * kMaxTs + o]
+// (fixed order, deterministic), o < nobj (timeseries.cu)
+void launch_ts_reduce(const double* part, size_t ncta, int nobj, double scale, double* out, cudaStream_t s);
 
 struct NLArgs {
   Dims d;

@@ -14,7 +14,11 @@
 #include <algorithm>
 #include <cstdio>
 
+#include <string>
+
+#include "../../include/coral_b200.h"
 #include "device.hpp"
+#include "host.hpp"
 
 namespace coral {
 
@@ -528,6 +532,41 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
         ke_partial[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 3 + threadIdx.x] = s;
       }
       __syncthreads();
+    }
+    // timeseries objects, one at a time (one accumulator register)
+    if (ke_partial && q.ts_partial) {
+      const size_t cta = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+      for (int o = 0; o < q.ts_n; ++o) {
+        const int src = q.ts_src[o], zsel = q.ts_z[o];
+        const int fa = src >= 0 ? src : qv[0][-1 - src], fb = src >= 0 ? -1 : qv[1][-1 - src];
+        double acc = 0.0;
+        for (int idx = threadIdx.x; idx < kZPairs * N; idx += blockDim.x) {
+          const int pr = idx / N, m = idx - pr * N;
+          const int z = (m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1;
+          if (zsel >= 0 && z != zsel) continue;
+          double pa, pb;
+          if (fa < 0 || fb < 0) {
+            const double2 f1 = Fv[((fa < 0 ? fb : fa) * kZPairs + pr) * N + m];
+            pa = f1.x;
+            pb = f1.y;
+          } else {
+            const double2 f1 = Fv[(fa * kZPairs + pr) * N + m], f2 = Fv[(fb * kZPairs + pr) * N + m];
+            pa = f1.x * f2.x;
+            pb = f1.y * f2.y;
+          }
+          const double w = zsel >= 0 ? 1.0 : wz[z];
+          acc += w * ((col_ok(2 * pr) ? pa : 0.0) + (col_ok(2 * pr + 1) ? pb : 0.0));
+        }
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if ((threadIdx.x & 31) == 0) red[0][threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+          double s = 0.0;
+          for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[0][w];
+          q.ts_partial[cta * kMaxTs + o] = s;
+        }
+        __syncthreads();
+      }
     }
   }
   // ---- products and forward transforms, kZFwd (quadratic variable, pair) lines a batch ----
@@ -2309,12 +2348,21 @@ __global__ void k_check_finite(const double2* x, size_t n, unsigned int* flags) 
 
 int grid1d(size_t n, int bs) { return (int)((n + bs - 1) / bs); }
 
+// Raise a kernel's dynamic shared-memory limit when it needs more than the
+// default 48 KB; a refused attribute is reported with the kernel and the size
+// (instead of surfacing later as a generic launch failure).
 template <typename K>
-void set_smem(K kernel, size_t bytes) {
-  static size_t done = 0;
-  (void)done;
-  if (bytes > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+void set_smem_named(const char* name, K kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return;
+  const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // the refusal is reported here, not left for the next launch check
+    throw CoralError(CORAL_ECUDA, std::string("cudaFuncSetAttribute(") + name + ", dynamic shared memory " +
+                                      std::to_string(bytes) + " bytes): " + cudaGetErrorString(e));
+  }
 }
+// (variadic so that template argument lists pass through; the text names the call)
+#define set_smem(...) set_smem_named(#__VA_ARGS__, __VA_ARGS__)
 
 }  // namespace
 
@@ -2475,6 +2523,7 @@ __global__ void __launch_bounds__(1024) k_ke_sum(const double* part, size_t n, d
     if (threadIdx.x == 0) *out = v;
   }
 }
+size_t z_fused_ctas(const Dims& d) { return (size_t)((d.NXA + 2 * kZPairs - 1) / (2 * kZPairs)) * d.NYA; }
 void launch_ke_sum(const double* part, size_t n, double* out, cudaStream_t s) {
   k_ke_sum<<<1, 1024, 0, s>>>(part, n, out);
 }

@@ -21,28 +21,71 @@ using namespace coral;
 namespace {
 
 constexpr size_t kScratchBytes = size_t(64) << 20;  // 64 MiB, the stated maximum
+constexpr int kMaxModes = 1 << 16;                  // per direction, checked first
 __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
+// The device address of g_scratch, looked up once per device and CUDA context
+// with that device current (in host code the array's name is only a stand-in
+// for the symbol, not a device address).  The cache is keyed by the context's
+// unique id, so a cudaDeviceReset in the caller's process (a new primary
+// context, the module loaded again) triggers a fresh lookup.
+struct ScratchSlot {
+  unsigned long long ctx_id = 0;
+  void* addr = nullptr;
+};
 constexpr int kMaxDevices = 64;
 std::mutex g_mutex;
-void* g_scratch_addr[kMaxDevices] = {};
+ScratchSlot g_slot[kMaxDevices];
 
-// Device address of g_scratch on the current device, looked up once per device
-// (the array's name in host code is only a stand-in for the symbol).
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
+
+// id of the current CUDA context (0 if the driver cannot tell); the driver's
+// entry points are fetched through the runtime, so the library needs no link
+// against libcuda
+unsigned long long current_context_id() {
+  static CtxGetCurrentFn get_cur = nullptr;
+  static CtxGetIdFn get_id = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    cudaDriverEntryPointQueryResult q1, q2;
+    void* f1 = nullptr;
+    void* f2 = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+        q1 == cudaDriverEntryPointSuccess &&
+        cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+        q2 == cudaDriverEntryPointSuccess) {
+      get_cur = reinterpret_cast<CtxGetCurrentFn>(f1);
+      get_id = reinterpret_cast<CtxGetIdFn>(f2);
+    }
+  }
+  if (!get_cur || !get_id) return 0;
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (get_cur(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
+
 void* scratch_address() {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) throw CoralError(CORAL_ENODEV, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) throw CoralError(CORAL_EBADARG, "device index beyond the supported range");
+  // before the runtime has made the device's context current the id reads 0,
+  // which always triggers a lookup (cudaGetSymbolAddress creates the context)
+  const unsigned long long ctx = current_context_id();
   std::lock_guard<std::mutex> lock(g_mutex);
-  if (!g_scratch_addr[dev]) {
+  ScratchSlot& slot = g_slot[dev];
+  if (!slot.addr || slot.ctx_id != ctx || ctx == 0) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_scratch);
     if (e != cudaSuccess || !p)
       throw CoralError(CORAL_ECUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
-    g_scratch_addr[dev] = p;
+    slot.addr = p;
+    slot.ctx_id = ctx;
   }
-  return g_scratch_addr[dev];
+  return slot.addr;
 }
 
 // exp(-i pi k * f / N) for k < N, from sincospi: f = 2 gives the FFT twiddles,
@@ -81,8 +124,17 @@ size_t up256(size_t b) { return (b + 255) & ~size_t(255); }
 extern "C" int coral_spec_to_phys_noalloc(int NX, int NY, int NZ, const double* spec, double* phys, void* stream) {
   try {
     if (!spec || !phys) throw CoralError(CORAL_EBADARG, "coral_spec_to_phys_noalloc: null buffer");
-    if (NX <= 0 || NY <= 0 || NZ <= 0 || NX % 4 || NY % 4 || NZ % 4)
-      throw CoralError(CORAL_EBADARG, "coral_spec_to_phys_noalloc: NX, NY, NZ must be positive multiples of 4");
+    // sizes are checked before any arithmetic on them (3 N / 2 must not overflow)
+    if (NX <= 0 || NY <= 0 || NZ <= 0 || NX > kMaxModes || NY > kMaxModes || NZ > kMaxModes || NX % 4 || NY % 4 ||
+        NZ % 4)
+      throw CoralError(CORAL_EBADARG, "coral_spec_to_phys_noalloc: NX, NY, NZ must be multiples of 4 in [4, " +
+                                          std::to_string(kMaxModes) + "]");
+    // an error left pending by earlier, unrelated work is not this call's: it is
+    // reported as such and left in place for its owner
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess)
+      throw CoralError(CORAL_ECUDA, std::string("coral_spec_to_phys_noalloc: a CUDA error was already pending "
+                                                "before the call: ") + cudaGetErrorString(pending));
     const int NXA = 3 * NX / 2, NYA = 3 * NY / 2, NZA = 3 * NZ / 2, NXH = NX / 2;
     if (!smooth23(NXA) || !smooth23(NYA) || !smooth23(NZA))
       throw CoralError(CORAL_EBADARG, "coral_spec_to_phys_noalloc: grid sizes must be of the form 2^a 3^b");
@@ -117,6 +169,7 @@ extern "C" int coral_spec_to_phys_noalloc(int NX, int NY, int NZ, const double* 
     launch_inv_y(d, 1, nullptr, StateSet{}, reinterpret_cast<const double2*>(spec), nullptr, nullptr, Y1, py, s);
     launch_inv_x(d, 1, Y1, Y2, px, s);
     launch_inv_z(d, 1, Y2, phys, pz, td, nullptr, nullptr, s);
+    // nothing was pending at entry, so an error now comes from these launches
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) throw CoralError(CORAL_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
     return CORAL_OK;

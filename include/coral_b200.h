@@ -204,6 +204,46 @@ int coral_spec_to_phys_noalloc(int NX, int NY, int NZ, const double* spec, doubl
  */
 int coral_diagnostics(coral_handle* h, double* out3);
 
+/*
+ * Timeseries objects: the text of coral.timeseries (lines
+ * '>>Volume_average :: NAME <<' and '>>Horizontal_avg :: NAME ;; Position= K <<'
+ * up to '>>EOF<<', NAME a full or quadratic variable, K a 1-based z grid index;
+ * at most 16 objects).  Replaces master_recipe%add_timeseries
+ * (src/plane_layer/PL_equations.f90:233-320).  Every later step evaluates the
+ * objects on its first stage's physical fields, as output_global_quantities
+ * does (src/plane_layer/PL_IMEX_timestepping_output.f90:5-127).
+ */
+int coral_set_timeseries(coral_handle* h, const char* timeseries_text);
+int coral_set_timeseries_from_file(coral_handle* h, const char* path);
+/* Values of the objects at the last step, in the reference's buffer order
+ * (full variables in recipe order, then quadratic variables); n >= count. */
+int coral_timeseries(coral_handle* h, double* values, int n);
+
+/*
+ * Time keeping of the driver loop (src/misc/timeKeeping.f90): set the time,
+ * the current dt and the step index, e.g. from CheckPoints/dt.sav after the
+ * reference's dt / 50 restart rule (read_timings_from_file, :92-134; dt is
+ * capped at dt_max).  A new handle starts at t = 0, dt = dt_max, step 1.
+ * coral_get_time: out4 = (time, dt_current, i_timestep, refactorisations so far).
+ */
+int coral_set_time(coral_handle* h, double time, double dt, long long i_timestep);
+int coral_get_time(coral_handle* h, double* out4);
+
+/*
+ * The time loop of src/plane_layer/plane_layer_main.f90:138-205 for nsteps
+ * steps: before each step dt_current takes the CFL target when they differ by
+ * more than tolerance * dt_current, with refactorisation (update_dt_if_needed,
+ * timeKeeping.f90:171-183; factorize_operators); after it the target becomes
+ * CFL_C * cfl_based_DT capped at dt_max, and the run stops with
+ * CORAL_ENONFINITE below dt_min = 1e-9 (compare_dt_against_CFL, :78-89).  The
+ * timeseries objects are written every 20 steps and at the end to
+ * output_directory/Timeseries/ in the reference's files (time.dat,
+ * NAME_volAvg.dat, NAME_XYavg_zKKKKK.dat: raw float64, step k at offset 8(k-1);
+ * PL_IMEX_timestepping_output.f90:136-231); output_directory may be NULL.
+ * Synchronous: returns when the steps are done.
+ */
+int coral_run(coral_handle* h, int nsteps, const char* output_directory);
+
 #ifdef __cplusplus
 }
 #endif
