@@ -1,0 +1,81 @@
+"""Long run of the reference's benchmark 02 (rotating Rayleigh-Benard, Julien
+et al. 1996 no-slip case: Ra = 2.81e5, E^-1 = 707.1, Pr = 1, 96 x 96 x 48 modes,
+box 2 x 2 x 1, ARS_222, CFL-adaptive dt with CFL_C = 0.2, dt_max = 1e-3,
+tolerance 0.3) from its own input files (read unmodified), on the GPU, with
+the mean Nusselt number computed by the benchmark's rule
+(coral_b200.nusselt).  The reference publishes 4.76905 +- 0.00993
+(etc/benchmarks/02_RRBC_julien_JFM96/benchmark_02_RRBC_julien96.ipynb:97-98).
+
+The reference starts this case from its unseeded random initial condition;
+here the start is a seeded white-noise temperature perturbation (amplitude
+1e-2, times sin(pi z)) written as QuickSave files.  A spin-up phase of
+--spinup simulated time units is run without output; then the step index is
+reset to 1 and --record time units are recorded into <out>/Timeseries.
+
+usage: python -m coral_b200.benchmark02 --out DIR [--inputs DIR] [--spinup T] [--record T] [--seed S]
+"""
+import argparse
+import json
+import os
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", required=True)
+    ap.add_argument("--inputs", default=os.path.join(ROOT, "tests", "golden", "benchmark02"))
+    ap.add_argument("--spinup", type=float, default=0.5)
+    ap.add_argument("--record", type=float, default=1.0)
+    ap.add_argument("--seed", type=int, default=4)
+    ap.add_argument("--chunk", type=int, default=2000)
+    ap.add_argument("--max-seconds", type=float, default=1e9, help="wall-clock limit of the recorded phase")
+    a = ap.parse_args(argv)
+
+    from coral_b200 import initial_conditions as ic
+    from coral_b200 import nusselt
+    from coral_b200.solver import PlaneLayer
+
+    eq = os.path.join(a.inputs, "coral.equations.velocityPressure")
+    par = os.path.join(a.inputs, "coral.parameters.in")
+    pl = PlaneLayer.from_files(eq, par)
+    pl._check(pl._lib.coral_set_timeseries_from_file(pl._h, os.fsencode(os.path.join(a.inputs, "coral.timeseries"))))
+    os.makedirs(a.out, exist_ok=True)
+    qs = os.path.join(a.out, "Restart")
+    ic.white_noise_temperature(qs, pl.NX, pl.NY, pl.NZ, amplitude=1e-2, seed=a.seed)
+    pl.import_quicksave(qs)
+
+    def advance(t_end, outdir, wall_limit=1e9):
+        t0 = time.time()
+        steps = 0
+        while pl.get_time()["time"] < t_end and time.time() - t0 < wall_limit:
+            pl.run(a.chunk, outdir)
+            steps += a.chunk
+            st = pl.get_time()
+            print("t = %.5f  dt = %.3e  steps %d  refactorisations %d  %.0f steps/s" % (
+                st["time"], st["dt"], st["i_timestep"] - 1, st["refactorizations"], steps / (time.time() - t0)),
+                flush=True)
+        return steps, time.time() - t0
+
+    s1, w1 = advance(a.spinup, None)
+    st = pl.get_time()
+    pl.set_time(st["time"], st["dt"], 1)
+    s2, w2 = advance(st["time"] + a.record, a.out, a.max_seconds)
+    pl.synchronize()
+    m, s, q = nusselt.mean_nusselt(a.out, pl.NZAA)
+    res = dict(case="benchmark02 velocity-pressure 96x96x48", spinup_time=a.spinup, record_time=pl.get_time()["time"] - st["time"],
+               spinup_steps=s1, record_steps=s2, steps_per_s=(s1 + s2) / (w1 + w2), seed=a.seed,
+               nusselt_mean=m, nusselt_spread=s, quarters=q, published=[4.76905366624831, 0.009934859274015244],
+               refactorizations=pl.get_time()["refactorizations"])
+    print(json.dumps(res))
+    with open(os.path.join(a.out, "nusselt.json"), "w") as f:
+        json.dump(res, f, indent=1)
+    pl.close()
+
+
+if __name__ == "__main__":
+    main()

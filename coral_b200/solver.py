@@ -188,6 +188,32 @@ class PlaneLayer:
         self._check(self._lib.coral_profile_step(self._h, float(dt), _dptr(ms), len(ms)))
         return dict(zip(self.PHASES, ms.tolist()))
 
+    # --- timeseries and the time loop (plane_layer_main.f90:138-205)
+    def set_timeseries(self, text):
+        """coral.timeseries text (master_recipe%add_timeseries)."""
+        self._check(self._lib.coral_set_timeseries(self._h, text.encode()))
+        self.n_timeseries = text.count(">>Volume_average") + text.count(">>Horizontal_avg")
+
+    def timeseries(self):
+        """Values of the timeseries objects at the last step's first stage."""
+        out = np.zeros(16)
+        self._check(self._lib.coral_timeseries(self._h, _dptr(out), 16))
+        return out
+
+    def set_time(self, time, dt, i_timestep=1):
+        self._check(self._lib.coral_set_time(self._h, float(time), float(dt), int(i_timestep)))
+
+    def get_time(self):
+        out = np.zeros(4)
+        self._check(self._lib.coral_get_time(self._h, _dptr(out)))
+        return dict(time=float(out[0]), dt=float(out[1]), i_timestep=int(out[2]), refactorizations=int(out[3]))
+
+    def run(self, nsteps, output_directory=None):
+        """nsteps of the driver loop with CFL-adaptive dt; timeseries files under
+        output_directory/Timeseries when given."""
+        d = os.fsencode(output_directory) if output_directory else None
+        self._check(self._lib.coral_run(self._h, int(nsteps), d))
+
     def diagnostics(self):
         out = np.zeros(3)
         self._check(self._lib.coral_diagnostics(self._h, _dptr(out)))

@@ -914,6 +914,7 @@ class Solver:
         for i in range(self.nstages):
             fphys, qphys, qspec = self.compute_phys(aux, zaux)
             if i == 0:
+                self.stage0_phys = (fphys, qphys)
                 self.ke = None
                 names = [q[0] for q in r.quad_vars]
                 if all(n in names for n in ("uu", "vv", "ww")):
@@ -964,6 +965,47 @@ class Solver:
             f[~act] = 0.0
             self.field[isys] = f
         self.zfield = [z.copy() for z in zaux]
+
+    # ---------------- timeseries and the time loop ----------------
+    def timeseries_values(self, objects):
+        """output_global_quantities (PL_IMEX_timestepping_output.f90:5-127) on the
+        first stage's fields of the last step.  objects: [(name, zpos)] with zpos
+        None for a volume average, else the 1-based grid level of a horizontal
+        average; name a full or quadratic variable."""
+        fphys, qphys = self.stage0_phys
+        fnames = [f[0] for f in self.recipe.full_vars]
+        qnames = [q[0] for q in self.recipe.quad_vars]
+        out = []
+        for name, zpos in objects:
+            ph = fphys[fnames.index(name)] if name in fnames else qphys[qnames.index(name)]
+            if zpos is None:
+                out.append(self.volume_average(ph))
+            else:
+                out.append(float(ph[:, :, zpos - 1].sum() / self.g.NXAA / self.g.NYAA))
+        return out
+
+    def run(self, nsteps, objects=()):
+        """The time loop of plane_layer_main.f90:138-205 with the dt rules of
+        timeKeeping.f90:78-89,171-183 (parameters dt_max, tolerance, CFL_C of the
+        parameter file).  Returns [(step index, time, dt used, timeseries values)]."""
+        p = self.params
+        if not hasattr(self, "t_time"):
+            self.t_time, self.t_dt_current, self.t_dt, self.t_step = 0.0, p["dt_max"], p["dt_max"], 1
+        rows = []
+        for _ in range(nsteps):
+            if abs(self.t_dt - self.t_dt_current) > p["tolerance"] * self.t_dt_current:
+                self.t_dt_current = self.t_dt
+            self.step(self.t_dt_current)
+            rows.append((self.t_step, self.t_time, self.t_dt_current, self.timeseries_values(objects)))
+            dt = self.cfl_dt * p["CFL_C"]
+            if dt > p["dt_max"]:
+                dt = p["dt_max"]
+            if dt < 1e-9:
+                raise RuntimeError("minimal timestep reached")
+            self.t_dt = dt
+            self.t_time += self.t_dt_current
+            self.t_step += 1
+        return rows
 
     # ---------------- state in physical space (checkpoint / quicksave) ----------------
     def var_cheb(self, isys: int, v: int) -> np.ndarray:

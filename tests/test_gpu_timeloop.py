@@ -1,0 +1,152 @@
+"""The driver loop on the GPU against the oracle: timeseries objects
+(output_global_quantities), the CFL-adaptive time step with refactorisation
+(timeKeeping.f90), the Timeseries/*.dat files, and the reference's own
+benchmark-02 input files read unmodified through coral_create_from_files."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle import coral_oracle as co
+from tests.problems import equations
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+TS_TEXT = """>>Volume_average :: uu <<
+>>Volume_average :: vv <<
+>>Volume_average :: ww <<
+>>Horizontal_avg :: tFull ;; Position= 1 <<
+>>Horizontal_avg :: tFull ;; Position= 24 <<
+>>Horizontal_avg :: tFull ;; Position= 72 <<
+>>Horizontal_avg :: tFull ;; Position= 100 <<
+>>Volume_average :: tFull <<
+>>Horizontal_avg :: ww ;; Position= 5 <<
+>>EOF<<
+"""
+# the reference's buffer order: full variables (recipe order) first, then the
+# quadratic ones, each with its objects in file order; position 100 > NZAA is ignored
+TS_OBJECTS = [("tFull", 1), ("tFull", 24), ("tFull", 72), ("tFull", None),
+              ("uu", None), ("vv", None), ("ww", None), ("ww", 5)]
+TS_FILES = ["tFull_XYavg_z00001.dat", "tFull_XYavg_z00024.dat", "tFull_XYavg_z00072.dat", "tFull_volAvg.dat",
+            "uu_volAvg.dat", "vv_volAvg.dat", "ww_volAvg.dat", "ww_XYavg_z00005.dat"]
+
+
+def _params(NX, NY, NZ, dt_max, tol, cfl):
+    return """0
+{NX}
+{NY}
+{NZ}
+0
+6.283185307179586
+6.283185307179586
+1.d0
+0.5d0
+0
+{dt!r}
+{tol!r}
+{cfl!r}
+'ARS_222'
+0
+.True.
+0
+1.d9
+""".format(NX=NX, NY=NY, NZ=NZ, dt=dt_max, tol=tol, cfl=cfl)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _random_state(solver, pl, seed, amp):
+    rng = np.random.default_rng(seed)
+    for s, lay in enumerate(solver.lay):
+        f = amp * (rng.standard_normal((pl.NXH, pl.NYAA, lay.T)) + 1j * rng.standard_normal((pl.NXH, pl.NYAA, lay.T)))
+        solver.field[s] = f.copy()
+        pl.set_field(s, f)
+    for s, lay in enumerate(solver.zlay):
+        z = amp * rng.standard_normal(lay.T)
+        solver.zfield[s] = z.copy()
+        pl.set_mean_field(s, z)
+
+
+def test_timeseries_objects_match_oracle():
+    from coral_b200.solver import PlaneLayer
+    eq = equations("rbc_noslip_ra1e8", **{"1.d8": "1.d5"})
+    par = _params(16, 12, 48, 1e-5, 0.3, 1e30)
+    ref = co.Solver(eq, par)
+    pl = PlaneLayer(eq, par)
+    pl.set_timeseries(TS_TEXT)
+    _random_state(ref, pl, 31, amp=1e-2)
+    for _ in range(2):
+        ref.step(1e-5)
+    pl.march_forward(1e-5, 2)
+    got = pl.timeseries()[:len(TS_OBJECTS)]
+    want = np.array(ref.timeseries_values(TS_OBJECTS))
+    assert np.all(np.abs(got - want) <= 1e-11 * np.abs(want) + 1e-16), (got, want)
+    assert np.all(pl.timeseries()[len(TS_OBJECTS):] == 0.0)
+    pl.close()
+
+
+def test_adaptive_dt_loop_refactorises_and_matches_oracle():
+    """A state whose CFL time step is well below dt_max: the first step runs at
+    dt_max, then dt follows CFL_C * cfl_based_DT whenever it moves by more than
+    the tolerance, each change refactorising the operators; the dt sequence,
+    the times, the timeseries rows and the state match the oracle's loop."""
+    from coral_b200.solver import PlaneLayer
+    eq = equations("rbc_noslip_ra1e8", **{"1.d8": "1.d5"})
+    par = _params(16, 12, 48, 1e-3, 0.3, 0.01)
+    ref = co.Solver(eq, par)
+    pl = PlaneLayer(eq, par)
+    pl.set_timeseries(TS_TEXT)
+    _random_state(ref, pl, 32, amp=1e-2)
+    nsteps = 5
+    rows = ref.run(nsteps, TS_OBJECTS)
+    with tempfile.TemporaryDirectory() as d:
+        pl.run(nsteps, d)
+        tm = pl.get_time()
+        assert tm["i_timestep"] == nsteps + 1
+        assert tm["refactorizations"] >= 1
+        assert abs(tm["time"] - ref.t_time) <= 1e-12 * ref.t_time
+        assert abs(tm["dt"] - ref.t_dt_current) <= 1e-12 * ref.t_dt_current
+        dts = [r[2] for r in rows]
+        assert len(set(dts)) >= 2, dts  # the time step changed at least once
+        t = np.fromfile(os.path.join(d, "Timeseries", "time.dat"))
+        np.testing.assert_allclose(t, [r[1] for r in rows], rtol=1e-12, atol=0)
+        for k, fn in enumerate(TS_FILES):
+            v = np.fromfile(os.path.join(d, "Timeseries", fn))
+            want = np.array([r[3][k] for r in rows])
+            assert v.shape == want.shape, fn
+            assert np.all(np.abs(v - want) <= 1e-10 * np.abs(want) + 1e-15), (fn, v, want)
+    assert _rel(pl.get_field(0), ref.field[0]) < 1e-10
+    for s in range(len(ref.zlay)):
+        assert _rel(pl.get_mean_field(s), ref.zfield[s]) < 1e-10
+    pl.close()
+
+
+def test_reference_benchmark02_files_read_unmodified():
+    """coral.equations.velocityPressure, coral.parameters.in and coral.timeseries
+    of the reference's benchmark 02 (copied verbatim into tests/golden) create a
+    handle through the file-reading entry points; the systems have the sizes
+    of the oracle's reading of the same files, and a few steps of the loop match
+    the oracle."""
+    from coral_b200.solver import PlaneLayer
+    b = os.path.join(GOLDEN, "benchmark02")
+    eq = os.path.join(b, "coral.equations.velocityPressure")
+    par = os.path.join(b, "coral.parameters.in")
+    pl = PlaneLayer.from_files(eq, par)
+    pl._check(pl._lib.coral_set_timeseries_from_file(pl._h, os.fsencode(os.path.join(b, "coral.timeseries"))))
+    ref = co.Solver(open(eq).read(), open(par).read())
+    assert (pl.NX, pl.NY, pl.NZ) == (96, 96, 48)
+    assert pl.T == [l.T for l in ref.lay] and pl.Tz == [l.T for l in ref.zlay]
+    _random_state(ref, pl, 33, amp=1e-2)
+    objs = [("tFull", 1), ("tFull", 24), ("tFull", 48), ("tFull", 72), ("uu", None), ("vv", None), ("ww", None)]
+    rows = ref.run(3, objs)
+    pl.run(3)
+    got = pl.timeseries()[:len(objs)]
+    want = np.array(rows[-1][3])
+    assert np.all(np.abs(got - want) <= 1e-10 * np.abs(want) + 1e-15), (got, want)
+    assert _rel(pl.get_field(0), ref.field[0]) < 1e-10
+    pl.close()
