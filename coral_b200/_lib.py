@@ -49,6 +49,18 @@ SIGNATURES = {
     "coral_set_time": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_longlong]),
     "coral_get_time": (ctypes.c_int, [_P, _D]),
     "coral_run": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_char_p]),
+    "coral_set_z_transform": (ctypes.c_int, [_P, ctypes.c_int]),
+    "coral_var_positions": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_int)]),
+    "coral_ensemble_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
+                                             ctypes.POINTER(ctypes.c_char_p), ctypes.c_char_p, ctypes.c_int,
+                                             ctypes.POINTER(_P)]),
+    "coral_ensemble_destroy": (None, [_P]),
+    "coral_ensemble_last_error": (ctypes.c_char_p, [_P]),
+    "coral_ensemble_member": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_P)]),
+    "coral_ensemble_march": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int]),
+    "coral_ensemble_synchronize": (ctypes.c_int, [_P]),
+    "coral_ensemble_query": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]),
 }
 
 _lib = None

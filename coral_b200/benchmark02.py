@@ -6,9 +6,9 @@ the mean Nusselt number computed by the benchmark's rule
 (coral_b200.nusselt).  The reference publishes 4.76905 +- 0.00993
 (etc/benchmarks/02_RRBC_julien_JFM96/benchmark_02_RRBC_julien96.ipynb:97-98).
 
-The reference starts this case from its unseeded random initial condition;
-here the start is a seeded white-noise temperature perturbation (amplitude
-1e-2, times sin(pi z)) written as QuickSave files.  A spin-up phase of
+The reference starts this case from its default random initial condition
+(noisy_initial_conditions, amplitude 1e-16, unseeded); here the start is the
+seeded form of it (coral_b200.initial_conditions.noisy_modes).  A spin-up phase of
 --spinup simulated time units is run without output; then the step index is
 reset to 1 and --record time units are recorded into <out>/Timeseries.
 
@@ -34,6 +34,11 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=4)
     ap.add_argument("--chunk", type=int, default=2000)
     ap.add_argument("--max-seconds", type=float, default=1e9, help="wall-clock limit of the recorded phase")
+    ap.add_argument("--amp", type=float, default=1e-16,
+                    help="amplitude of the seeded form of the reference's default initial condition")
+    ap.add_argument("--white-noise", action="store_true",
+                    help="start from a white-noise temperature of amplitude --amp instead")
+    ap.add_argument("--cfl", type=float, default=None, help="override CFL_C of the parameter file")
     a = ap.parse_args(argv)
 
     from coral_b200 import initial_conditions as ic
@@ -42,12 +47,20 @@ def main(argv=None):
 
     eq = os.path.join(a.inputs, "coral.equations.velocityPressure")
     par = os.path.join(a.inputs, "coral.parameters.in")
-    pl = PlaneLayer.from_files(eq, par)
+    if a.cfl is None:
+        pl = PlaneLayer.from_files(eq, par)
+    else:
+        lines = open(par).read().splitlines(True)
+        lines[12] = "%r ! CFL_C (overridden)\n" % a.cfl
+        pl = PlaneLayer(open(eq).read(), "".join(lines))
     pl._check(pl._lib.coral_set_timeseries_from_file(pl._h, os.fsencode(os.path.join(a.inputs, "coral.timeseries"))))
     os.makedirs(a.out, exist_ok=True)
-    qs = os.path.join(a.out, "Restart")
-    ic.white_noise_temperature(qs, pl.NX, pl.NY, pl.NZ, amplitude=1e-2, seed=a.seed)
-    pl.import_quicksave(qs)
+    if a.white_noise:
+        qs = os.path.join(a.out, "Restart")
+        ic.white_noise_temperature(qs, pl.NX, pl.NY, pl.NZ, amplitude=a.amp, seed=a.seed)
+        pl.import_quicksave(qs)
+    else:
+        ic.noisy_modes(pl, 2.0, 2.0, amp=a.amp, amp0=a.amp, seed=a.seed)
 
     def advance(t_end, outdir, wall_limit=1e9):
         t0 = time.time()
@@ -56,13 +69,17 @@ def main(argv=None):
             pl.run(a.chunk, outdir)
             steps += a.chunk
             st = pl.get_time()
-            print("t = %.5f  dt = %.3e  steps %d  refactorisations %d  %.0f steps/s" % (
-                st["time"], st["dt"], st["i_timestep"] - 1, st["refactorizations"], steps / (time.time() - t0)),
-                flush=True)
+            dg = pl.diagnostics()
+            print("t = %.5f  dt = %.3e  steps %d  refactorisations %d  KE %.4e  cfl_dt %.3e  %.0f steps/s" % (
+                st["time"], st["dt"], st["i_timestep"] - 1, st["refactorizations"], dg["KE"], dg["cfl_dt"],
+                steps / (time.time() - t0)), flush=True)
         return steps, time.time() - t0
 
     s1, w1 = advance(a.spinup, None)
     st = pl.get_time()
+    if a.record <= 0:
+        pl.close()
+        return
     pl.set_time(st["time"], st["dt"], 1)
     s2, w2 = advance(st["time"] + a.record, a.out, a.max_seconds)
     pl.synchronize()

@@ -168,6 +168,14 @@ struct coral_handle {
   long long i_timestep = 1, refactorizations = 0;
   // timeseries rows not yet written: (i_timestep, time, values)
   std::vector<std::pair<long long, std::vector<double>>> ts_rows;
+  // z transforms: 0 = FP64 FFT (k_z_fused), 1 = int8-digit contractions on the
+  // tensor cores (zsplit.cu); form_last = the form of the last step (KE sums)
+  int zform = 0, zform_last = 0;
+  unsigned char *zmat_inv = nullptr, *zmat_fwd = nullptr;
+  double* ke_partial_split = nullptr;  // [forward CTAs][3]
+  size_t n_ke_split = 0;
+  double* ts_partial_split = nullptr;  // [inverse + forward CTAs][kMaxTs]
+  size_t ts_rows_split = 0, ts_inv_rows = 0;
 };
 
 namespace {
@@ -681,7 +689,94 @@ struct PhaseTimer {
   void end() { cudaEventRecord(ev.back().second.second, s); }
 };
 
-int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
+// Arguments of the stage-i kernels of coupled kxky system k.
+NLArgs make_nl_args(coral_handle* h, KSys& k, int i) {
+  NLArgs na{};
+  na.d = h->d;
+  na.T = k.T;
+  na.NL = k.NL;
+  na.qspec = h->qspec;
+  na.kx = h->d_kx;
+  na.ky = h->d_ky;
+  na.act_index = h->d_act_index;
+  na.Khat = k.Khat[i];
+  na.nq = h->nQ;
+  return na;
+}
+
+SolveArgs make_solve_args(coral_handle* h, KSys& k, int i, double dt) {
+  const int S = h->TB.stages;
+  const bool last = (i == S - 1);
+  SolveArgs sa{};
+  sa.d = h->d;
+  sa.T = k.T;
+  sa.kl = k.real ? k.kl_s : k.kl;
+  sa.ku = k.real ? k.ku_s : k.ku;
+  sa.ldab = k.real ? k.ldab_s : k.ldab;
+  sa.M = k.M;
+  sa.L = k.L;
+  sa.field = k.field;
+  sa.out = last ? k.field : k.aux;
+  sa.work = k.work;
+  sa.Kstd_out = last ? nullptr : k.Kstd[i];
+  sa.nprev = i;
+  for (int j = 0; j <= i; ++j) {
+    sa.Kstd[j] = k.Kstd[j];
+    sa.Khat[j] = k.Khat[j];
+    sa.ca[j] = (j < i) ? dt * h->TB.a(i, j) : 0.0;
+    sa.ch[j] = dt * h->TB.ahat(i + 1, j);
+  }
+  sa.ab = k.ab;
+  sa.dpiv = k.dpiv;
+  sa.act_index = h->d_act_index;
+  sa.act_list = h->d_act_list;
+  sa.nact = h->nact;
+  sa.last_stage = last ? 1 : 0;
+  sa.kx = h->d_kx;
+  sa.ky = h->d_ky;
+  sa.flags = h->flags;
+  sa.abr = k.abr;
+  sa.rowflip = k.rowflip;
+  sa.colflip = k.colflip;
+  sa.ncls = k.ncls;
+  sa.Tc = k.Tc;
+  sa.wst = k.wst;
+  sa.row_pos = k.row_pos;
+  sa.col_pos = k.col_pos;
+  sa.colflip_cls = k.colflip_cls;
+  sa.Lp = k.Lp;
+  sa.work2 = k.work2;
+  sa.nblk = k.ncls * h->nact;
+  sa.cls_col = k.cls_col;
+  sa.lmask = k.lmask;
+  sa.umask = k.umask;
+  sa.tile_win = k.tile_win;
+  sa.tile_lwin_max = k.tile_lwin_max;
+  sa.rhs_win = k.rhs_win;
+  sa.rhs_win_max = k.rhs_win_max;
+  sa.Mw = k.Mw;
+  sa.NLw = k.NLw;
+  sa.NLg = k.NLg;
+  // CORAL_GENERIC_TILES=1: the run-time forms of the tile kernels (tests cover
+  // them with the plane-layer recipes, whose layouts are otherwise compiled)
+  sa.generic_tiles = std::getenv("CORAL_GENERIC_TILES") != nullptr;
+  sa.Lw = k.Lw;
+  {
+    const int kv = sa.kl + sa.ku;
+    const int u_rows = (kv + 2) & ~1, l_rows = ((kv + 1 + sa.kl + 1) & ~1) - ((kv + 1) & ~1);
+    sa.ring_cols = k.ncls * std::max(u_rows, l_rows);
+  }
+  return sa;
+}
+
+// Stage i of one_step_beyond (marching.f90:9-28) in three phases, so that an
+// ensemble can run the band substitutions of all its members as one launch:
+//   pre   full variables -> physical space, products, forward transforms
+//         (compute_NL_terms_to_K_hat), and the right-hand side with the NL
+//         assembly (or, for complex factors, NL assembly + the whole solve);
+//   subst the band substitutions (backsolve_to_aux);
+//   post  K_std = L aux and the stage output (stif_aux_to_K_std), the mean systems.
+int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
   auto B = [&](int k) { if (pt) pt->begin(k); };
   auto E = [&]() { if (pt) pt->end(); };
   const Dims& d = h->d;
@@ -689,140 +784,163 @@ int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
   int nl = 0;
   const int S = h->TB.stages;
   const double scale = 1.0 / ((double)g.NXAA * (double)g.NYAA * (double)g.NZAA);
-  for (int i = 0; i < S; ++i) {
-    const bool last = (i == S - 1);
-    {
-      StateSet st = state_set(h, i == 0);
-      B(0); launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream); E();
-      B(1); launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream); E();
-      // the CFL maxima reported after a step are those of its last stage's fields
-      // (each stage's evaluation replaces them): only the last stage computes them
-      if (last) CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
-      nl += 2;
-    }
-    // z passes fused (inverse DCT, CFL maxima, products, KE, forward DCT); the
-    // quadratic variables overwrite Y2 in place, each CTA reading and writing only
-    // its own (y, x pair) columns
-    B(3);
-    {
-      // the first stage's fields also give the timeseries objects
-      QuadDesc q = h->quads;
-      q.ts_partial = (i == 0 && q.ts_n > 0) ? h->ts_partial : nullptr;
-      launch_z_fused(d, h->nF, q, h->Y2, h->Y2, h->pz, h->dct_tw, h->d_wz, h->d_wzinv,
-                     last ? h->cfl_bits : nullptr, i == 0 ? h->ke_partial : nullptr, h->stream);
-    }
-    E();
-    B(4); launch_fwd_x(d, h->nQ, h->Y2, h->Y1, h->px, h->stream); E();
-    B(5); launch_fwd_y(d, h->nQ, h->Y1, h->qspec, scale, h->py, h->stream); E();
-    nl += 3;
-    for (int q : h->zmean_quads) {
-      launch_remove_zmean(d, h->qspec + (size_t)q * d.NXH * d.NYA * d.NZ, h->stream);
-      ++nl;
-    }
-    for (auto& k : h->ks) {
-      NLArgs na{};
-      na.d = d;
-      na.T = k.T;
-      na.NL = k.NL;
-      na.qspec = h->qspec;
-      na.kx = h->d_kx;
-      na.ky = h->d_ky;
-      na.act_index = h->d_act_index;
-      na.Khat = k.Khat[i];
-      na.nq = h->nQ;
-      SolveArgs sa{};
-      sa.d = d;
-      sa.T = k.T;
-      sa.kl = k.real ? k.kl_s : k.kl;
-      sa.ku = k.real ? k.ku_s : k.ku;
-      sa.ldab = k.real ? k.ldab_s : k.ldab;
-      sa.M = k.M;
-      sa.L = k.L;
-      sa.field = k.field;
-      sa.out = last ? k.field : k.aux;
-      sa.work = k.work;
-      sa.Kstd_out = last ? nullptr : k.Kstd[i];
-      sa.nprev = i;
-      for (int j = 0; j <= i; ++j) {
-        sa.Kstd[j] = k.Kstd[j];
-        sa.Khat[j] = k.Khat[j];
-        sa.ca[j] = (j < i) ? dt * h->TB.a(i, j) : 0.0;
-        sa.ch[j] = dt * h->TB.ahat(i + 1, j);
-      }
-      sa.ab = k.ab;
-      sa.dpiv = k.dpiv;
-      sa.act_index = h->d_act_index;
-      sa.act_list = h->d_act_list;
-      sa.nact = h->nact;
-      sa.last_stage = last ? 1 : 0;
-      sa.kx = h->d_kx;
-      sa.ky = h->d_ky;
-      sa.flags = h->flags;
-      sa.abr = k.abr;
-      sa.rowflip = k.rowflip;
-      sa.colflip = k.colflip;
-      sa.ncls = k.ncls;
-      sa.Tc = k.Tc;
-      sa.wst = k.wst;
-      sa.row_pos = k.row_pos;
-      sa.col_pos = k.col_pos;
-      sa.colflip_cls = k.colflip_cls;
-      sa.Lp = k.Lp;
-      sa.work2 = k.work2;
-      sa.nblk = k.ncls * h->nact;
-      sa.cls_col = k.cls_col;
-      sa.lmask = k.lmask;
-      sa.umask = k.umask;
-      sa.tile_win = k.tile_win;
-      sa.tile_lwin_max = k.tile_lwin_max;
-      sa.rhs_win = k.rhs_win;
-      sa.rhs_win_max = k.rhs_win_max;
-      sa.Mw = k.Mw;
-      sa.NLw = k.NLw;
-      sa.NLg = k.NLg;
-      // CORAL_GENERIC_TILES=1: the run-time forms of the tile kernels (tests cover
-      // them with the plane-layer recipes, whose layouts are otherwise compiled)
-      sa.generic_tiles = std::getenv("CORAL_GENERIC_TILES") != nullptr;
-      sa.Lw = k.Lw;
-      {
-        const int kv = sa.kl + sa.ku;
-        const int u_rows = (kv + 2) & ~1, l_rows = ((kv + 1 + sa.kl + 1) & ~1) - ((kv + 1) & ~1);
-        sa.ring_cols = k.ncls * std::max(u_rows, l_rows);
-      }
-      if (k.real) {
-        B(7); launch_rhs_nl(sa, na, h->stream); E();
-        B(9); launch_subst(sa, h->stream); E();
-        B(10); launch_kstd_out(sa, h->stream); E();
-        nl += 3;
-      } else {
-        B(6); launch_nl(na, h->stream); E();
-        B(7); launch_solve(sa, h->stream); E();
-        nl += 2;
-      }
-    }
-    if (!h->zs.empty()) {
-      ZeroArgs za{};
-      za.nsys = (int)h->zs.size();
-      for (size_t s = 0; s < h->zs.size(); ++s) za.sys[s] = h->zs[s].dev;
-      za.qspec = h->qspec;
-      za.d = d;
-      za.stage = i;
-      for (int j = 0; j <= i; ++j) {
-        za.ca[j] = (j < i) ? dt * h->TB.a(i, j) : 0.0;
-        za.ch[j] = dt * h->TB.ahat(i + 1, j);
-      }
-      za.last_stage = last ? 1 : 0;
-      B(8); launch_zero_step(za, h->stream); E();
-      ++nl;
-    }
+  const bool last = (i == S - 1);
+  {
+    StateSet st = state_set(h, i == 0);
+    B(0); launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream); E();
+    B(1); launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream); E();
+    // the CFL maxima reported after a step are those of its last stage's fields
+    // (each stage's evaluation replaces them): only the last stage computes them
+    if (last) CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
+    nl += 2;
   }
-  if (h->quads.ts_n > 0) {
-    launch_ts_reduce(h->ts_partial, h->ts_ncta, h->quads.ts_n, 1.0 / ((double)g.NXAA * (double)g.NYAA), h->ts_out,
-                     h->stream);
+  // z passes fused (inverse DCT, CFL maxima, products, KE, forward DCT); the
+  // quadratic variables overwrite Y2 in place, each CTA reading and writing only
+  // its own (y, x pair) columns
+  B(3);
+  if (h->zform == 1) {
+    // the tensor-core form: inverse contraction into the physical fields,
+    // then products and the forward contraction back into Y2
+    QuadDesc q = h->quads;
+    q.ts_partial = nullptr;
+    const bool ts = (i == 0 && q.ts_n > 0);
+    launch_zsplit_inv(d, h->nF, q, h->Y2, h->fphys, h->zmat_inv, h->d_wz, h->d_wzinv,
+                      last ? h->cfl_bits : nullptr, ts ? h->ts_partial_split : nullptr, h->flags, h->stream);
+    launch_zsplit_fwd(d, h->nF, q, h->fphys, h->Y2, h->zmat_fwd, h->d_wz,
+                      i == 0 ? h->ke_partial_split : nullptr, ts ? h->ts_partial_split : nullptr,
+                      (long long)h->ts_inv_rows, h->flags, h->stream);
+    ++nl;
+  } else {
+    // the first stage's fields also give the timeseries objects
+    QuadDesc q = h->quads;
+    q.ts_partial = (i == 0 && q.ts_n > 0) ? h->ts_partial : nullptr;
+    launch_z_fused(d, h->nF, q, h->Y2, h->Y2, h->pz, h->dct_tw, h->d_wz, h->d_wzinv,
+                   last ? h->cfl_bits : nullptr, i == 0 ? h->ke_partial : nullptr, h->stream);
+  }
+  E();
+  B(4); launch_fwd_x(d, h->nQ, h->Y2, h->Y1, h->px, h->stream); E();
+  B(5); launch_fwd_y(d, h->nQ, h->Y1, h->qspec, scale, h->py, h->stream); E();
+  nl += 3;
+  for (int q : h->zmean_quads) {
+    launch_remove_zmean(d, h->qspec + (size_t)q * d.NXH * d.NYA * d.NZ, h->stream);
     ++nl;
   }
+  for (auto& k : h->ks) {
+    NLArgs na = make_nl_args(h, k, i);
+    SolveArgs sa = make_solve_args(h, k, i, dt);
+    if (k.real) {
+      B(7); launch_rhs_nl(sa, na, h->stream); E();
+      ++nl;
+    } else {
+      B(6); launch_nl(na, h->stream); E();
+      B(7); launch_solve(sa, h->stream); E();
+      nl += 2;
+    }
+  }
+  return nl;
+}
+
+int enqueue_stage_subst(coral_handle* h, int i, double dt, PhaseTimer* pt) {
+  int nl = 0;
+  for (auto& k : h->ks)
+    if (k.real) {
+      SolveArgs sa = make_solve_args(h, k, i, dt);
+      if (pt) pt->begin(9);
+      launch_subst(sa, h->stream);
+      if (pt) pt->end();
+      ++nl;
+    }
+  return nl;
+}
+
+int enqueue_stage_post(coral_handle* h, int i, double dt, PhaseTimer* pt) {
+  int nl = 0;
+  const int S = h->TB.stages;
+  const bool last = (i == S - 1);
+  for (auto& k : h->ks)
+    if (k.real) {
+      SolveArgs sa = make_solve_args(h, k, i, dt);
+      if (pt) pt->begin(10);
+      launch_kstd_out(sa, h->stream);
+      if (pt) pt->end();
+      ++nl;
+    }
+  if (!h->zs.empty()) {
+    ZeroArgs za{};
+    za.nsys = (int)h->zs.size();
+    for (size_t s = 0; s < h->zs.size(); ++s) za.sys[s] = h->zs[s].dev;
+    za.qspec = h->qspec;
+    za.d = h->d;
+    za.stage = i;
+    for (int j = 0; j <= i; ++j) {
+      za.ca[j] = (j < i) ? dt * h->TB.a(i, j) : 0.0;
+      za.ch[j] = dt * h->TB.ahat(i + 1, j);
+    }
+    za.last_stage = last ? 1 : 0;
+    if (pt) pt->begin(8);
+    launch_zero_step(za, h->stream);
+    if (pt) pt->end();
+    ++nl;
+  }
+  return nl;
+}
+
+// after the stages: the timeseries totals of the step
+int enqueue_step_end(coral_handle* h) {
+  const Geometry& g = *h->G;
+  int nl = 0;
+  if (h->quads.ts_n > 0) {
+    if (h->zform == 1)
+      launch_ts_reduce(h->ts_partial_split, h->ts_rows_split, h->quads.ts_n, 1.0 / ((double)g.NXAA * (double)g.NYAA),
+                       h->ts_out, h->stream);
+    else
+      launch_ts_reduce(h->ts_partial, h->ts_ncta, h->quads.ts_n, 1.0 / ((double)g.NXAA * (double)g.NYAA), h->ts_out,
+                       h->stream);
+    ++nl;
+  }
+  h->zform_last = h->zform;
   CK(cudaGetLastError());
   return nl;
+}
+
+int enqueue_step(coral_handle* h, double dt, PhaseTimer* pt = nullptr) {
+  int nl = 0;
+  for (int i = 0; i < h->TB.stages; ++i) {
+    nl += enqueue_stage_pre(h, i, dt, pt);
+    nl += enqueue_stage_subst(h, i, dt, pt);
+    nl += enqueue_stage_post(h, i, dt, pt);
+  }
+  return nl + enqueue_step_end(h);
+}
+
+// Select the z-transform form; the tensor-core form needs NZ and NZAA to be
+// multiples of 96 (its output tiles) and allocates its digit tables and
+// partial-sum arrays on first use.
+void set_z_transform(coral_handle* h, int form) {
+  if (form != 0 && form != 1) throw CoralError(CORAL_EBADARG, "z transform form must be 0 (FP64) or 1 (int8 digits)");
+  const Geometry& g = *h->G;
+  if (form == 1) {
+    if (!zsplit_supported(g.NZ, g.NZAA))
+      throw CoralError(CORAL_EUNSUPPORTED, "the tensor-core z transform needs NZ and 3 NZ / 2 to be multiples of 96");
+    if (!h->zmat_inv) {
+      h->zmat_inv = h->mem.upload(zsplit_matrix_digits(g.NZ, g.NZAA, false, g.NZAA));
+      h->zmat_fwd = h->mem.upload(zsplit_matrix_digits(g.NZAA, g.NZ, true, g.NZAA));
+      const long long ncol = (long long)g.NYAA * g.NXAA;
+      const size_t nfwd = zsplit_ctas(ncol, h->nQ);
+      h->ts_inv_rows = zsplit_ctas(ncol, h->nF);
+      h->ts_rows_split = h->ts_inv_rows + nfwd;
+      h->n_ke_split = nfwd * 3;
+      h->ke_partial_split = h->mem.get<double>(h->n_ke_split);
+      h->ts_partial_split = h->mem.get<double>(h->ts_rows_split * kMaxTs);
+      CK(cudaMemset(h->ke_partial_split, 0, h->n_ke_split * sizeof(double)));
+      CK(cudaMemset(h->ts_partial_split, 0, h->ts_rows_split * kMaxTs * sizeof(double)));
+    }
+  }
+  h->zform = form;
+  if (h->graph) {
+    cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+  }
 }
 
 void factorize(coral_handle* h, double dt) {
@@ -1366,6 +1484,7 @@ int coral_synchronize(coral_handle* h) {
     CK(cudaStreamSynchronize(h->stream));
     unsigned int f = 0;
     CK(cudaMemcpy(&f, h->flags, sizeof(f), cudaMemcpyDeviceToHost));
+    if (f & 2u) throw CoralError(CORAL_ECUDA, "a tensor-core wait of the z transform timed out");
     if (f & 1u) throw CoralError(CORAL_ENONFINITE, "non-finite value in the state");
   });
 }
@@ -1559,7 +1678,8 @@ int coral_diagnostics(coral_handle* h, double* out3) {
     out3[0] = cfl_dt_of(h, bits);
     // the partial sums are totalled on the device: 8 bytes come back, not the
     // per-CTA array
-    launch_ke_sum(h->ke_partial, h->n_ke_partial, h->ke_total, h->stream);
+    if (h->zform_last == 1) launch_ke_sum(h->ke_partial_split, h->n_ke_split, h->ke_total, h->stream);
+    else launch_ke_sum(h->ke_partial, h->n_ke_partial, h->ke_total, h->stream);
     ++h->launches;
     double ke = 0.0;
     CK(cudaMemcpyAsync(&ke, h->ke_total, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -1617,8 +1737,264 @@ int coral_get_time(coral_handle* h, double* out4) {
   });
 }
 
+int coral_var_positions(coral_handle* h, int isys, int ivar, int* positions, int n, int* size) {
+  return guarded(h, [&] {
+    check_sys(h, isys, false);
+    const SystemOps& o = h->ks[isys].ops;
+    if (ivar < 0 || ivar >= o.nV) throw CoralError(CORAL_EBADARG, "variable index out of range");
+    const auto& vp = o.var_pos[ivar];
+    if (size) *size = (int)vp.size();
+    if (!positions) return;
+    if (n < (int)vp.size()) throw CoralError(CORAL_EBADARG, "buffer smaller than the variable");
+    for (size_t i = 0; i < vp.size(); ++i) positions[i] = vp[i];
+  });
+}
+
+int coral_set_z_transform(coral_handle* h, int form) {
+  return guarded(h, [&] { set_z_transform(h, form); });
+}
+
 int coral_run(coral_handle* h, int nsteps, const char* output_directory) {
   return guarded(h, [&] { run_loop(h, nsteps, output_directory); });
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Ensembles: many independent plane-layer runs (different grids, parameters
+// and recipes) advanced together on one stream, one CUDA graph per step.  Per
+// stage every member's transforms and right-hand sides are queued, then the
+// band substitutions of all members run as one persistent launch
+// (k_subst_tpb_multi), then every member's K_std and mean systems.  The
+// reference solves its systems one (kx, ky) at a time in a loop
+// (src/plane_layer/PL_algebra_z_3D.f90:197-214) and runs one problem per job.
+// ---------------------------------------------------------------------------
+struct coral_ensemble {
+  std::string err;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<coral_handle*> mem;
+  cudaGraphExec_t graph = nullptr;
+  double graph_dt = -1.0;
+  bool batched = false;                       // all members' substitutions in one launch
+  std::vector<SolveArgs*> d_args;             // per stage: SolveArgs of every (member, system)
+  std::vector<long long*> d_prefix;           // per stage: first block of each (member, system)
+  std::vector<int> nsub;                      // per stage: (member, system) entries
+  std::vector<long long> total;               // per stage: blocks in all
+  long long launches = 0;
+  int launches_per_step = 0;
+};
+
+namespace {
+
+void ens_free_args(coral_ensemble* e) {
+  for (auto* p : e->d_args) cudaFree(p);
+  for (auto* p : e->d_prefix) cudaFree(p);
+  e->d_args.clear();
+  e->d_prefix.clear();
+  e->nsub.clear();
+  e->total.clear();
+}
+
+// the per-stage argument tables of the batched substitution (for dt)
+void ens_build_args(coral_ensemble* e, double dt) {
+  ens_free_args(e);
+  const int S = e->mem[0]->TB.stages;
+  e->batched = true;
+  for (int i = 0; i < S && e->batched; ++i) {
+    std::vector<SolveArgs> args;
+    std::vector<long long> prefix(1, 0);
+    for (coral_handle* h : e->mem)
+      for (auto& k : h->ks) {
+        if (!k.real) { e->batched = false; break; }
+        SolveArgs sa = make_solve_args(h, k, i, dt);
+        if (!subst_multi_supported(sa)) { e->batched = false; break; }
+        args.push_back(sa);
+        prefix.push_back(prefix.back() + sa.nblk);
+      }
+    if (!e->batched) break;
+    SolveArgs* da = nullptr;
+    long long* dp = nullptr;
+    CK(cudaMalloc(&da, args.size() * sizeof(SolveArgs)));
+    e->d_args.push_back(da);
+    CK(cudaMalloc(&dp, prefix.size() * sizeof(long long)));
+    e->d_prefix.push_back(dp);
+    CK(cudaMemcpy(da, args.data(), args.size() * sizeof(SolveArgs), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dp, prefix.data(), prefix.size() * sizeof(long long), cudaMemcpyHostToDevice));
+    e->nsub.push_back((int)args.size());
+    e->total.push_back(prefix.back());
+  }
+  if (!e->batched) ens_free_args(e);
+}
+
+int ens_enqueue(coral_ensemble* e, double dt) {
+  int nl = 0;
+  const int S = e->mem[0]->TB.stages;
+  for (int i = 0; i < S; ++i) {
+    for (coral_handle* h : e->mem) nl += enqueue_stage_pre(h, i, dt, nullptr);
+    if (e->batched) {
+      launch_subst_multi(e->d_args[i], e->d_prefix[i], e->nsub[i], e->total[i], e->stream);
+      ++nl;
+    } else {
+      for (coral_handle* h : e->mem) nl += enqueue_stage_subst(h, i, dt, nullptr);
+    }
+    for (coral_handle* h : e->mem) nl += enqueue_stage_post(h, i, dt, nullptr);
+  }
+  for (coral_handle* h : e->mem) nl += enqueue_step_end(h);
+  CK(cudaGetLastError());
+  return nl;
+}
+
+void ens_march(coral_ensemble* e, double dt, int nsteps) {
+  if (!(dt > 0.0) || nsteps < 0) throw CoralError(CORAL_EBADARG, "march: dt must be > 0 and nsteps >= 0");
+  CK(cudaSetDevice(e->device));
+  bool refactored = false;
+  for (coral_handle* h : e->mem)
+    if (h->dt_factored != dt) {
+      factorize(h, dt);
+      refactored = true;
+    }
+  int done = 0;
+  if (!e->graph || e->graph_dt != dt || refactored) {
+    if (nsteps == 0) return;
+    ens_build_args(e, dt);
+    e->launches_per_step = ens_enqueue(e, dt);  // eager step (kernel attributes)
+    e->launches += e->launches_per_step;
+    done = 1;
+    if (e->graph) {
+      cudaGraphExecDestroy(e->graph);
+      e->graph = nullptr;
+    }
+    cudaGraph_t gr;
+    CK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      ens_enqueue(e, dt);
+    } catch (...) {
+      cudaStreamEndCapture(e->stream, &gr);
+      throw;
+    }
+    CK(cudaStreamEndCapture(e->stream, &gr));
+    CK(cudaGraphInstantiate(&e->graph, gr, 0));
+    cudaGraphDestroy(gr);
+    e->graph_dt = dt;
+  }
+  for (int s = done; s < nsteps; ++s) {
+    CK(cudaGraphLaunch(e->graph, e->stream));
+    e->launches += e->launches_per_step;
+  }
+}
+
+template <typename F>
+int ens_guarded(coral_ensemble* e, F&& f) {
+  if (!e) return CORAL_EBADARG;
+  try {
+    CK(cudaSetDevice(e->device));
+    f();
+    return CORAL_OK;
+  } catch (const CoralError& x) {
+    e->err = x.what();
+    return x.code;
+  } catch (const std::exception& x) {
+    e->err = x.what();
+    return CORAL_EBADARG;
+  }
+}
+
+void ens_destroy(coral_ensemble* e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  ens_free_args(e);
+  for (coral_handle* h : e->mem) {
+    if (h->stream == e->stream) h->stream = nullptr;  // the ensemble's stream, destroyed below
+    coral_destroy(h);
+  }
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+}  // namespace
+
+extern "C" {
+
+int coral_ensemble_create(int n, const char* const* equations_texts, const char* const* parameters_texts,
+                          const char* scheme, int device, coral_ensemble** out) {
+  if (!out || n <= 0 || !equations_texts || !parameters_texts) {
+    g_create_error = "coral_ensemble_create: bad arguments";
+    return CORAL_EBADARG;
+  }
+  *out = nullptr;
+  auto* e = new coral_ensemble();
+  e->device = device;
+  for (int i = 0; i < n; ++i) {
+    coral_handle* h = nullptr;
+    const int rc = coral_create(equations_texts[i], parameters_texts[i], scheme, device, &h);
+    if (rc != CORAL_OK) {
+      const std::string msg = "member " + std::to_string(i) + ": " + g_create_error;
+      ens_destroy(e);
+      g_create_error = msg;
+      return rc;
+    }
+    e->mem.push_back(h);
+    if (h->TB.stages != e->mem[0]->TB.stages) {
+      ens_destroy(e);
+      g_create_error = "coral_ensemble_create: members use IMEX schemes with different stage counts";
+      return CORAL_EBADARG;
+    }
+  }
+  // one stream for all members
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    ens_destroy(e);
+    g_create_error = "coral_ensemble_create: stream creation failed";
+    return CORAL_ECUDA;
+  }
+  for (coral_handle* h : e->mem) {
+    cudaStreamSynchronize(h->stream);
+    cudaStreamDestroy(h->stream);
+    h->stream = e->stream;
+  }
+  *out = e;
+  return CORAL_OK;
+}
+
+void coral_ensemble_destroy(coral_ensemble* e) { ens_destroy(e); }
+
+const char* coral_ensemble_last_error(const coral_ensemble* e) { return e ? e->err.c_str() : g_create_error.c_str(); }
+
+int coral_ensemble_member(coral_ensemble* e, int i, coral_handle** member) {
+  return ens_guarded(e, [&] {
+    if (!member || i < 0 || i >= (int)e->mem.size()) throw CoralError(CORAL_EBADARG, "member index out of range");
+    *member = e->mem[i];
+  });
+}
+
+int coral_ensemble_march(coral_ensemble* e, double dt, int nsteps) {
+  return ens_guarded(e, [&] { ens_march(e, dt, nsteps); });
+}
+
+int coral_ensemble_synchronize(coral_ensemble* e) {
+  return ens_guarded(e, [&] {
+    CK(cudaStreamSynchronize(e->stream));
+    for (size_t i = 0; i < e->mem.size(); ++i) {
+      unsigned int f = 0;
+      CK(cudaMemcpy(&f, e->mem[i]->flags, sizeof(f), cudaMemcpyDeviceToHost));
+      if (f & 1u) throw CoralError(CORAL_ENONFINITE, "non-finite value in the state of member " + std::to_string(i));
+    }
+  });
+}
+
+int coral_ensemble_query(coral_ensemble* e, int what, long long* value) {
+  return ens_guarded(e, [&] {
+    if (!value) throw CoralError(CORAL_EBADARG, "null pointer");
+    switch (what) {
+      case 0: *value = (long long)e->mem.size(); break;                 // members
+      case 1: *value = e->launches; break;                              // kernels launched so far
+      case 2: *value = e->batched ? 1 : 0; break;                       // substitutions batched
+      case 3: *value = e->launches_per_step; break;                     // kernels per ensemble step
+      default: throw CoralError(CORAL_EBADARG, "unknown ensemble query");
+    }
+  });
 }
 
 }  // extern "C"

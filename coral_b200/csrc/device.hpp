@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <vector>
 
 #include "fft.cuh"
 
@@ -112,6 +113,23 @@ void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const Ff
 void launch_fwd_y(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
                   cudaStream_t s);
 void launch_remove_zmean(const Dims& d, double2* qspec_q, cudaStream_t s);
+// ---- split-precision z transforms on the tensor cores (zsplit.cu) ----
+// int8 digits of the REDFT01 (fwd = false: NZAA x NZ) or REDFT10 (fwd = true:
+// NZ x NZAA) matrix in the kernels' streaming order
+std::vector<unsigned char> zsplit_matrix_digits(int K, int NOUT, bool fwd, int NZAA);
+bool zsplit_supported(int NZ, int NZAA);
+size_t zsplit_ctas(long long ncol, int nvar);
+// inverse: Y2 [f][col][NZ] -> phys [f][col][NZAA], CFL maxima (cfl_bits non-null)
+// and the full-variable timeseries objects (ts_partial non-null, rows 0..)
+void launch_zsplit_inv(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* phys,
+                       const unsigned char* mat, const double* wz, const double* wzinv, unsigned long long* cfl_bits,
+                       double* ts_partial, unsigned* flags, cudaStream_t s);
+// forward: products of phys -> Q2 [q][col][NZ], KE partials [cta][3] and the
+// quadratic-variable timeseries objects (rows ts_row0..)
+void launch_zsplit_fwd(const Dims& d, int nf, const QuadDesc& q, const double* phys, double* Q2,
+                       const unsigned char* mat, const double* wz, double* ke_partial, double* ts_partial,
+                       long long ts_row0, unsigned* flags, cudaStream_t s);
+
 // CTAs of launch_z_fused (rows of its KE and timeseries partial sums)
 size_t z_fused_ctas(const Dims& d);
 // total of the n KE partial sums (one CTA, fixed order) into *out
@@ -210,6 +228,13 @@ void launch_solve_real(const SolveArgs& a, const NLArgs& n, cudaStream_t s);
 void launch_rhs_nl(const SolveArgs& a, const NLArgs& n, cudaStream_t s);
 void launch_subst(const SolveArgs& a, cudaStream_t s);
 void launch_kstd_out(const SolveArgs& a, cudaStream_t s);
+// the substitutions of several systems in one persistent launch (ensembles):
+// d_args[m] the SolveArgs of member m, d_prefix[m] its first block in the
+// concatenated range (d_prefix[nmem] = total); every member must pass
+// subst_multi_supported (thread-per-block layout, band (9, 23), ldab 34)
+bool subst_multi_supported(const SolveArgs& a);
+void launch_subst_multi(const SolveArgs* d_args, const long long* d_prefix, int nmem, long long total,
+                        cudaStream_t s);
 
 struct FactorArgs {
   Dims d;

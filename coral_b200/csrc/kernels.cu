@@ -1476,15 +1476,14 @@ __global__ void k_mask_rows(FactorArgs a) {
 // Band entries outside the matrix are stored zeros, so the forward sweep runs
 // unpredicated (it only touches dead window slots near the end); the backward
 // rows within KV of the last column take the guarded loop.
+// The substitution of block b of the system described by a; win is this
+// thread's band-window column in shared memory (slot stride kTpbThreads).
 template <int KL, int KV, int LD>
-__global__ void __launch_bounds__(kTpbThreads) k_subst_tpb(SolveArgs a) {
+__device__ __forceinline__ void subst_tpb_block(const SolveArgs& a, int b, double2* win) {
   constexpr int W1 = (KL + 2 <= 16) ? 16 : 32;  // power of 2 >= KL + 2
   constexpr int W2 = KV + 1;
   constexpr int S = kTpbThreads;                // slot stride
   constexpr size_t CS = (size_t)LD * 32;        // column stride (doubles)
-  extern __shared__ double2 swin[];
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= a.nblk) return;  // no warp-collective operations below
   const int T = a.Tc;
   const int cls = b % a.ncls;
   const size_t gb = (size_t)(b >> 5) * T;
@@ -1495,7 +1494,6 @@ __global__ void __launch_bounds__(kTpbThreads) k_subst_tpb(SolveArgs a) {
   const int* ccol = a.cls_col + (size_t)cls * T;
   double2* out = a.out + (size_t)a.act_list[b / a.ncls] * a.T;  // this system's stage output
   bool bad = false;
-  double2* win = swin + threadIdx.x;
   // ---- forward: positions j..j+KL in slots p mod W1 ----
   for (int p = 0; p <= KL && p < T; ++p) win[(p & (W1 - 1)) * S] = X[(size_t)p * 32];
   // L rows / U entries that are zero in every block are not loaded
@@ -1615,6 +1613,34 @@ __global__ void __launch_bounds__(kTpbThreads) k_subst_tpb(SolveArgs a) {
   }
   // non-finite check (no warp-collective operation: lanes of a partial warp returned early)
   if (bad) atomicOr(a.flags, 1u);
+}
+
+template <int KL, int KV, int LD>
+__global__ void __launch_bounds__(kTpbThreads) k_subst_tpb(SolveArgs a) {
+  extern __shared__ double2 swin[];
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.nblk) return;  // no warp-collective operations below
+  subst_tpb_block<KL, KV, LD>(a, b, swin + threadIdx.x);
+}
+
+// The substitutions of many systems (the members of an ensemble) in one
+// persistent launch: thread slots walk the concatenated block range of all
+// members (member m owns blocks [prefix[m], prefix[m+1])) with a grid stride;
+// each block runs exactly the arithmetic of k_subst_tpb.
+template <int KL, int KV, int LD>
+__global__ void __launch_bounds__(kTpbThreads) k_subst_tpb_multi(const SolveArgs* args, const long long* prefix,
+                                                                 int nmem, long long total) {
+  extern __shared__ double2 swin[];
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nmem - 1;  // member m with prefix[m] <= g < prefix[m+1]
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (prefix[mid] <= g) lo = mid;
+      else hi = mid - 1;
+    }
+    subst_tpb_block<KL, KV, LD>(args[lo], (int)(g - prefix[lo]), swin + threadIdx.x);
+  }
 }
 
 // The same solve for any band within (KL, KV) = (15, 31), kl and ku read at run time.
@@ -2601,6 +2627,20 @@ void launch_subst(const SolveArgs& a, cudaStream_t s) {
   const size_t sm = (size_t)kWPBr * kNBUF * kCW * a.ring_cols * sizeof(double);
   set_smem(k_subst_real<32>, sm);
   k_subst_real<32><<<(a.nact + kWPBr - 1) / kWPBr, kWPBr * 32, sm, s>>>(a);
+}
+bool subst_multi_supported(const SolveArgs& a) {
+  return a.work2 && a.nblk > 0 && a.kl == 9 && a.kl + a.ku == 23 && a.ldab == 34;
+}
+void launch_subst_multi(const SolveArgs* d_args, const long long* d_prefix, int nmem, long long total,
+                        cudaStream_t s) {
+  if (total <= 0) return;
+  const size_t sm = (size_t)kTpbThreads * 24 * sizeof(double2);
+  set_smem(k_subst_tpb_multi<9, 23, 34>, sm);
+  static int nct = 0;
+  if (!nct) nct = persistent_ctas(k_subst_tpb_multi<9, 23, 34>, kTpbThreads, sm);
+  const long long need = (total + kTpbThreads - 1) / kTpbThreads;
+  k_subst_tpb_multi<9, 23, 34><<<(int)std::min<long long>(nct, need), kTpbThreads, sm, s>>>(d_args, d_prefix, nmem,
+                                                                                          total);
 }
 void launch_kstd_out(const SolveArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;

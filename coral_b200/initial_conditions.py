@@ -69,3 +69,38 @@ def fourier_modes_temperature(directory, NX, NY, NZ, Lx, Ly, center=0.5, gap=1.0
     theta = plane[:, :, None] * np.sin(math.pi * zp)[None, None, :]
     _write(directory, NXAA, NYAA, NZAA, theta, dt)
     return theta
+
+
+def noisy_modes(pl, Lx, Ly, amp=1e-16, amp0=1e-16, seed=0):
+    """A seeded form of the reference's default initial condition
+    (noisy_initial_conditions, src/plane_layer/PL_IMEX_timestepping.f90:425-483),
+    written straight into the coupled-system states of a PlaneLayer: every
+    coefficient t of every kxky system at (kx, ky) gets
+        amp [exp(-(n - 3.5)^2 / 8) exp(-(|k| - 6 kx_box)^2 / 8) e^{i phi1}
+             + 3 exp(-(n - 1.5)^2 / 8) exp(-(|k| - 3 kx_box)^2 / 32) e^{i phi2}],
+    with phi1, phi2 uniform in [0, 2 pi) (PCG64 seed) and n = t // (coupled
+    variables) the Chebyshev degree of the coefficient in the interleaved
+    layout; every mean-system coefficient t gets amp0 exp(-(n - 1.5)^2 / 8) cos(t + 1).
+    The reference draws its phases from an unseeded generator and uses amplitude
+    1e-16 by default (its --noises-amplitude option changes it)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    kxb, kyb = 2 * math.pi / Lx, 2 * math.pi / Ly
+    kx = np.arange(pl.NXH) * kxb
+    iy = np.arange(pl.NYAA)
+    ky = np.where(iy <= pl.NYAA // 2, iy, iy - pl.NYAA) * kyb
+    kk = np.sqrt(kx[:, None] ** 2 + ky[None, :] ** 2)
+    for s in range(pl.n_kxky):
+        T = pl.T[s]
+        nv = pl.query(300 + s)
+        n = (np.arange(T) // nv).astype(np.float64)
+        e1 = np.exp(-(n - 3.5) ** 2 / 8.0)[None, None, :] * np.exp(-(kk - 6 * kxb) ** 2 / 8.0)[:, :, None]
+        e2 = np.exp(-(n - 1.5) ** 2 / 8.0)[None, None, :] * np.exp(-(kk - 3 * kxb) ** 2 / 32.0)[:, :, None]
+        p1 = rng.uniform(0.0, 2 * math.pi, size=(pl.NXH, pl.NYAA, T))
+        p2 = rng.uniform(0.0, 2 * math.pi, size=(pl.NXH, pl.NYAA, T))
+        pl.set_field(s, amp * (e1 * np.exp(1j * p1) + 3.0 * e2 * np.exp(1j * p2)))
+    for s in range(pl.n_zero):
+        T = pl.Tz[s]
+        nv = pl.query(400 + s)
+        t = np.arange(T)
+        n = (t // nv).astype(np.float64)
+        pl.set_mean_field(s, amp0 * np.exp(-(n - 1.5) ** 2 / 8.0) * np.cos(t + 1.0))

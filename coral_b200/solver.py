@@ -45,6 +45,10 @@ class PlaneLayer:
         if rc != 0:
             raise CoralError(rc, self._lib.coral_last_error(None).decode())
         self._h = h
+        self._owner = None
+        self._init_sizes()
+
+    def _init_sizes(self):
         q = self.query
         self.NX, self.NY, self.NZ = q(Q["NX"]), q(Q["NY"]), q(Q["NZ"])
         self.NXAA, self.NYAA, self.NZAA = q(Q["NXAA"]), q(Q["NYAA"]), q(Q["NZAA"])
@@ -56,6 +60,17 @@ class PlaneLayer:
         self.stages = q(Q["STAGES"])
         self.T = [q(100 + i) for i in range(self.n_kxky)]
         self.Tz = [q(200 + i) for i in range(self.n_zero)]
+
+    @classmethod
+    def _wrap(cls, handle, owner):
+        """A view of a handle owned by someone else (an ensemble member): same
+        procedures, but close() leaves the handle alone."""
+        self = cls.__new__(cls)
+        self._lib = _lib.load()
+        self._h = handle
+        self._owner = owner
+        self._init_sizes()
+        return self
 
     @classmethod
     def from_files(cls, equations_path, parameters_path, scheme=None, device=0):
@@ -77,7 +92,8 @@ class PlaneLayer:
 
     def close(self):
         if getattr(self, "_h", None):
-            self._lib.coral_destroy(self._h)
+            if getattr(self, "_owner", None) is None:
+                self._lib.coral_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -213,6 +229,19 @@ class PlaneLayer:
         output_directory/Timeseries when given."""
         d = os.fsencode(output_directory) if output_directory else None
         self._check(self._lib.coral_run(self._h, int(nsteps), d))
+
+    def var_positions(self, isys, ivar):
+        """Positions within T of the Galerkin coefficients of coupled variable
+        ivar of kxky system isys (the interleaved layout)."""
+        n = ctypes.c_int()
+        self._check(self._lib.coral_var_positions(self._h, int(isys), int(ivar), None, 0, ctypes.byref(n)))
+        buf = (ctypes.c_int * max(n.value, 1))()
+        self._check(self._lib.coral_var_positions(self._h, int(isys), int(ivar), buf, n.value, ctypes.byref(n)))
+        return np.frombuffer(buf, dtype=np.int32)[:n.value].copy()
+
+    def set_z_transform(self, form):
+        """0: FP64 FFT z transforms; 1: int8-digit tensor-core contractions."""
+        self._check(self._lib.coral_set_z_transform(self._h, int(form)))
 
     def diagnostics(self):
         out = np.zeros(3)

@@ -244,6 +244,55 @@ int coral_get_time(coral_handle* h, double* out4);
  */
 int coral_run(coral_handle* h, int nsteps, const char* output_directory);
 
+/*
+ * Positions (0-based, within T) of the Galerkin coefficients of coupled variable
+ * ivar of kxky system isys in the interleaved state layout
+ * (src/plane_layer/PL_IMEX_timestepping.f90:1344-1414).  *size receives the
+ * variable's coefficient count; positions (may be NULL) needs n >= that count.
+ */
+int coral_var_positions(coral_handle* h, int isys, int ivar, int* positions, int n, int* size);
+
+/*
+ * The form of the z (Chebyshev) transforms inside the time step:
+ *   0  FP64 FFT-based transforms fused with the products (default);
+ *   1  split precision: the transforms as dense contractions on the tensor
+ *      cores (tcgen05.mma kind::i8) with both operands in five int8 digits
+ *      (a shared exponent per data column), exact INT32 accumulation and one
+ *      rounding to FP64 -- about 39 significant bits relative to a column's
+ *      largest value; the x / y FFTs, the band solves and the stage sums stay
+ *      FP64.  Needs NZ and 3 NZ / 2 to be multiples of 96 (CORAL_EUNSUPPORTED
+ *      otherwise).
+ * The reference does these transforms with FFTW r2r in FP64
+ * (src/slabs.fftw3mpi/transforms.f90:216-249); form 1 has no counterpart there.
+ */
+int coral_set_z_transform(coral_handle* h, int form);
+
+/*
+ * Ensembles: n independent runs (each its own coral.equations /
+ * coral.parameters.in text: grid, parameters and recipe may differ; the IMEX
+ * scheme's stage count may not) advanced together on one CUDA stream with one
+ * CUDA graph per step.  Per stage the band substitutions of every member's
+ * (kx, ky) systems run as one persistent launch when every member's systems
+ * use the split thread-per-block layout with the plane-layer band (9, 23)
+ * (coral_ensemble_query(e, 2) = 1); otherwise member by member.  The
+ * reference runs one problem per job and solves its systems one at a time
+ * (src/plane_layer/PL_algebra_z_3D.f90:197-214); each member here computes
+ * exactly what a single handle of the same problem computes.
+ * coral_ensemble_member returns a member's handle (owned by the ensemble; do
+ * not destroy it) for the state, QuickSave, diagnostics and transform calls.
+ * coral_ensemble_query: what = 0 members, 1 kernels launched so far,
+ * 2 substitutions batched (0/1), 3 kernels per ensemble step.
+ */
+typedef struct coral_ensemble coral_ensemble;
+int coral_ensemble_create(int n, const char* const* equations_texts, const char* const* parameters_texts,
+                          const char* scheme, int device, coral_ensemble** out);
+void coral_ensemble_destroy(coral_ensemble* e);
+const char* coral_ensemble_last_error(const coral_ensemble* e);
+int coral_ensemble_member(coral_ensemble* e, int i, coral_handle** member);
+int coral_ensemble_march(coral_ensemble* e, double dt, int nsteps);
+int coral_ensemble_synchronize(coral_ensemble* e);
+int coral_ensemble_query(coral_ensemble* e, int what, long long* value);
+
 #ifdef __cplusplus
 }
 #endif

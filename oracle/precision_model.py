@@ -96,6 +96,42 @@ def gemm_int8(A, B, k):
     return acc * (sa / 127.0) * (sb / 127.0)
 
 
+def balanced_digits(a, ndig):
+    """Signed base-256 digits of the int64 array a, most significant first:
+    a = sum_s d_s 256^(ndig-1-s) with every d_s in [-128, 127] (each lower digit
+    the centred residue (a + 128) mod 256 - 128; the top digit what is left)."""
+    out = []
+    r = a.copy()
+    for _ in range(ndig - 1):
+        d = ((r + 128) & 255) - 128
+        out.append(d)
+        r = (r - d) >> 8
+    out.append(r)
+    return out[::-1]
+
+
+def gemm_digits256(M, cols, ndig=5):
+    """M @ cols in the integer-digit scheme of the tensor-core z kernels
+    (coral_b200/csrc/zsplit.cu), restated exactly: per data column an exponent
+    e with max|col| < 2^e, m = rint(col 2^(38-e)); matrix entries (|c| <= 2)
+    mc = rint(c 2^36); both written in ndig signed base-256 digits (centred,
+    so the dropped low-order products carry random signs instead of a bias);
+    the digit products with i + j <= ndig - 1 summed exactly per anti-diagonal
+    d; S = sum_d D_d 2^(8(ndig-1-d)) in 64-bit integers; one rounding to FP64:
+    S 2^(e - 74 + 8(ndig-1))."""
+    mx = np.abs(cols).max(axis=0)
+    e = np.where(mx > 0, np.frexp(np.where(mx > 0, mx, 1.0))[1], 0)
+    m = np.rint(cols * np.exp2(38 - e)[None, :]).astype(np.int64)
+    mc = np.rint(M * 2.0 ** 36).astype(np.int64)
+    top = 8 * (ndig - 1)
+    dm, dx = balanced_digits(mc, ndig), balanced_digits(m, ndig)
+    S = np.zeros((M.shape[0], cols.shape[1]), dtype=np.int64)
+    for i in range(ndig):
+        for j in range(ndig - i):
+            S += (dm[i] @ dx[j]) << (top - 8 * (i + j))
+    return S.astype(np.float64) * np.exp2(e - 74 + top)[None, :]
+
+
 _MATS = {}
 
 
@@ -121,9 +157,12 @@ def make_transforms(k, fp32_acc=True, fp32_fft=True):
     rd = np.float32 if fp32_fft else np.float64
 
     def zgemm(M, cols):
+        if k == "digits256":
+            return gemm_digits256(M, cols)
         if k < 0:
             return gemm_int8(M, cols, -k)
         return gemm_sliced(M, cols, k, fp32_acc) if k else M @ cols
+
 
     def spec_to_phys(spec, g):
         b = sfft.ifft(spec.astype(cd), axis=1, norm="forward")
@@ -171,6 +210,7 @@ VARIANTS = [  # (label, slices, FP32 accumulation, FP32 FFTs)
     ("4 int8 slices, INT32 acc, FP64 FFTs", -4, False, False),
     ("5 int8 slices, INT32 acc, FP64 FFTs", -5, False, False),
     ("6 int8 slices, INT32 acc, FP64 FFTs", -6, False, False),
+    ("5 base-256 digits (zsplit.cu), FP64 FFTs", "digits256", False, False),
 ]
 
 
