@@ -40,7 +40,7 @@ CONFIGS = {
     "rrbc_192x192x96": dict(eq="rrbc_stressfree_ek1e-4_ra5e7.equations", par="rrbc_stressfree_192x192x96.parameters.in",
                             NX=192, NY=192, NZ=96, dt=5e-6, seed=1, Ra=5e7),
 }
-METRIC = "timesteps/s at 384^2x192 (FP64 path)"
+METRIC = "timesteps/s at 384\u00b2\u00d7192 (FP64 vs split-prec TC) at stated err vs FP64 oracle"
 PHASES = ("inv_y", "inv_x", "inv_z", "z_products", "fwd_x", "fwd_y", "nl_assembly", "rhs_nl", "mean_systems",
           "substitution", "kstd_out")
 
@@ -216,6 +216,93 @@ def phase_launches(stages, ncls):
     return n
 
 
+def save_state(pl):
+    return ([pl.get_field(s) for s in range(pl.n_kxky)], [pl.get_mean_field(s) for s in range(pl.n_zero)])
+
+
+def load_state(pl, st):
+    for s, f in enumerate(st[0]):
+        pl.set_field(s, f)
+    for s, z in enumerate(st[1]):
+        pl.set_mean_field(s, z)
+
+
+def field_errors(pl, got, ref):
+    """Relative L2 difference per coupled variable (kxky system 0) and per mean system."""
+    out = {}
+    names = ("u", "v", "w", "p", "t", "chi")
+    for v in range(pl.query(300)):
+        pos = pl.var_positions(0, v)
+        a, b = got[0][0][..., pos], ref[0][0][..., pos]
+        out[names[v] if v < len(names) else "var%d" % v] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    for s in range(len(ref[1])):
+        out["mean_system%d" % s] = float(np.linalg.norm(got[1][s] - ref[1][s]) / max(np.linalg.norm(ref[1][s]), 1e-300))
+    return out
+
+
+def measure_int8_peak(dev):
+    """Dense int8 tensor-core throughput of this GPU, measured with the library
+    int8 GEMM (torch._int_mm, 8192^3, best of 5); None if unavailable."""
+    import torch
+    try:
+        n = 8192
+        a = torch.randint(-100, 100, (n, n), dtype=torch.int8, device=dev)
+        b = torch.randint(-100, 100, (n, n), dtype=torch.int8, device=dev)
+        for _ in range(2):
+            torch._int_mm(a, b)
+        best = None
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch._int_mm(a, b)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            t = e0.elapsed_time(e1) / 1e3
+            best = t if best is None else min(best, t)
+        del a, b
+        return 2.0 * n ** 3 / best / 1e12
+    except Exception:
+        return None
+
+
+def split_leg(pl, dt, args, dev, stream, s0, nerr=100):
+    """The split-precision form (int8-digit tensor-core z transforms) on the same
+    handle: timed steps, per-phase times, and the per-field error against the
+    FP64 form after nerr steps from the same initial state (the FP64 form
+    matches the oracle to 1e-10 after 100 steps; tests/test_gpu_parity*.py)."""
+    import torch
+    load_state(pl, s0)
+    pl.set_z_transform(1)
+    pl.march_forward(dt, args.warmup)
+    pl.synchronize()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    pl.march_forward(dt, args.steps)
+    e1.record(stream)
+    pl.synchronize()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / args.steps
+    prof = {k: 0.0 for k in PHASES}
+    for _ in range(2):
+        p = pl.profile_step(dt)
+        for k in PHASES:
+            prof[k] += p[k] / 2
+    # error after nerr steps from s0: FP64 form, then split form
+    pl.set_z_transform(0)
+    load_state(pl, s0)
+    pl.march_forward(dt, nerr)
+    ref = save_state(pl)
+    pl.set_z_transform(1)
+    load_state(pl, s0)
+    pl.march_forward(dt, nerr)
+    got = save_state(pl)
+    pl.synchronize()
+    errs = field_errors(pl, got, ref)
+    pl.set_z_transform(0)
+    return ms, prof, errs
+
+
 def run_ours(args, cfg):
     import torch
     import torch.distributed as dist
@@ -233,6 +320,7 @@ def run_ours(args, cfg):
     pl = PlaneLayer(eq, par, device=dev)
     make_ic(cfg, pl)
     dt = cfg["dt"]
+    s0 = save_state(pl)
     t0 = time.perf_counter()
     pl.factorize_operators(dt)
     pl.synchronize()
@@ -302,6 +390,35 @@ def run_ours(args, cfg):
            "h2d_bytes_per_step": state_bytes / args.steps,
            "d2h_bytes_per_step": state_bytes / args.steps + diag_bytes}
 
+    # the split-precision form on the same handle and initial state
+    split = None
+    if not args.no_split:
+        try:
+            sms, sprof, serr = split_leg(pl, dt, args, dev, stream, s0)
+        except Exception as ex:  # e.g. a grid the tensor-core form does not support
+            split = {"unavailable": str(ex)}
+        else:
+            ncol = pl.NXAA * pl.NYAA
+            nF_, nQ_ = pl.query(8), pl.query(9)
+            macs = 15 * (nF_ + nQ_) * pl.NZ * pl.NZAA * ncol * pl.stages  # executed int8 MACs per step
+            zms = sprof["z_products"]
+            i8 = measure_int8_peak(dev)
+            split = {"form": "z transforms as tcgen05.mma kind::i8 contractions, 5 signed base-256 digits per operand "
+                             "(15 digit products), exact INT32 accumulation, one FP64 rounding; x/y FFTs, band "
+                             "solves and stage sums FP64",
+                     "value": world * 1e3 / sms, "unit": "timesteps/s", "ms_per_step": sms,
+                     "ratio_vs_fp64": ms_per_step / sms,
+                     "err_vs_fp64_form_after_100_steps": serr,
+                     "max_err": max(serr.values()),
+                     "phase_ms_per_step": {k: round(v, 4) for k, v in sprof.items()},
+                     "tensor_roofline": {"bound": "tensor", "kernels": "k_zsplit<false> + k_zsplit<true>",
+                                         "executed_int8_ops_per_step": 2 * macs,
+                                         "algorithmic_flops_per_step": 2 * (nF_ + nQ_) * pl.NZ * pl.NZAA * ncol * pl.stages,
+                                         "z_phase_ms_per_step": zms,
+                                         "achieved_tops": 2 * macs / (zms / 1e3) / 1e12 if zms > 0 else None,
+                                         "peak_tops": i8, "peak_source": "measured (torch._int_mm, int8 dense 8192^3)",
+                                         "frac": (2 * macs / (zms / 1e3) / 1e12) / i8 if (i8 and zms > 0) else None}}
+
     # roofline of every phase; the headline one is the phase with the largest time
     T = pl.T[0]
     nsys = pl.NXH * pl.NYAA
@@ -330,21 +447,18 @@ def run_ours(args, cfg):
     traffic = read_traffic(PHASE_KERNELS[top])
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(cfg, eq, par, max_seconds=args.cpu_seconds)
+        cpu = cpu_baseline(cfg, eq, par, pl=pl)
     clocks = clk.summary()
     line = {
         "metric": METRIC, "value": value, "unit": "timesteps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded white-noise temperature IC, PCG64 seed %d)" % cfg["seed"],
-        "config": {"workload": "%s: RBC no-slip Ra=%g Pr=1, %dx%dx%d modes, grid %dx%dx%d, ARS_222, dt=%g, FP64"
-                               % (args.config, cfg["Ra"], pl.NX, pl.NY, pl.NZ, pl.NXAA, pl.NYAA, pl.NZAA, dt),
-                   "grid_points": pl.NXAA * pl.NYAA * pl.NZAA, "systems": nsys, "active_systems": nact, "T": T,
-                   "band": [pl.query(500), pl.query(600)], "blocks": ncls, "block_T": Tc, "block_band": [kl_c, ku_c],
-                   "l2": "inputs larger than L2 (state %.2f GB, LU factors %.1f GB)"
-                   % (field.nbytes / 1e9, nact * ncls * Tc * (2 * kl_c + ku_c + 1) * fbytes / 1e9),
+        "config": workload_config(args, cfg, pl.NX, pl.NY, pl.NZ, world),
+        "layout": {"systems": nsys, "active_systems": nact, "T": T, "band": [pl.query(500), pl.query(600)],
+                   "blocks": ncls, "block_T": Tc, "block_band": [kl_c, ku_c],
                    "lu_factors": ("real-scaled" if fbytes == 8 else "complex")
                                  + (", split into %d independent blocks per system" % ncls if ncls > 1 else ""),
-                   "parallelism": "replicas x%d" % world},
+                   "lu_factor_gb": nact * ncls * Tc * (2 * kl_c + ku_c + 1) * fbytes / 1e9},
         "grid_point_steps_per_s": value * pl.NXAA * pl.NYAA * pl.NZAA,
         "e2e": e2e,
         "gpu_launches": gpu_launches,
@@ -357,6 +471,7 @@ def run_ours(args, cfg):
         "cpu_baseline": cpu,
         "clocks": clocks,
         "state_ok": not diag["nonfinite"],
+        "split": split,
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -383,21 +498,6 @@ def read_traffic(kernels):
     return None
 
 
-def _solve_worker(job):
-    """Repeated zgbtrs on the sampled factors for about `seconds`; returns the
-    number of solves (runs in a spawned process of the CPU baseline)."""
-    facs, kl, ku, b, seconds = job
-    import time as _t
-    import scipy.linalg.lapack as _lapack
-    n = 0
-    t0 = _t.perf_counter()
-    while _t.perf_counter() - t0 < seconds:
-        for lu, piv in facs:
-            _lapack.zgbtrs(lu, kl, ku, b, piv)
-        n += len(facs)
-    return n
-
-
 def host_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -405,124 +505,222 @@ def host_threads():
         return os.cpu_count() or 1
 
 
-def cpu_baseline(cfg, eq, par, max_seconds=20.0, processes=None):
-    """The oracle (CPU restatement, FP64) timed on a bounded sample of the same
-    workload with `processes` host threads (default: all): one inverse and one
-    forward 3-D transform at full size (scipy.fft workers), the band LU solves
-    of a sample of (kx,ky) systems and the operator applications of a sample of
-    kx slabs (a spawned process pool for the solves, a thread pool for the
-    sparse products), as throughput; the step time is extrapolated to the full
-    step.""" 
-    from concurrent.futures import ThreadPoolExecutor
+def cpu_baseline(cfg, eq, par, pl=None):
+    """The oracle timed on one bounded sample of the workload (OracleSample),
+    and, as the checker of the GPU's FP64 transforms, the oracle's transforms
+    compared with the GPU's on the same random input at full size."""
     from oracle import coral_oracle as co
     import scipy.fft as sfft
-    import scipy.linalg.lapack as lapack
-    processes = processes or host_threads()
-    t_start = time.perf_counter()
-    s = co.Solver.__new__(co.Solver)
-    s.recipe = co.parse_equations(eq)
-    p = co.read_parameters_text(par)
-    s.params = p
-    g = co.Geometry(p["NX"], p["NY"], p["NZ"], p["Lx"], p["Ly"], p["gap"], p["center"])
-    s.g = g
-    s.scheme = p["scheme"]
-    s.nstages, s.A, s.Ah = co.ars_tableau(s.scheme)
-    # operators of the kxky system (reduced to a few kx slabs for the timing sample)
-    rec = s.recipe.kxky[0]
-    lay = co.SystemLayout(g.NZ, rec)
-    cache = {}
-    mass = [(pc, co.build_piece_matrix(g.NZ, g.center, g.gap, lay, rec, pc, cache)) for pc in rec.mass]
-    stif = [(pc, co.build_piece_matrix(g.NZ, g.center, g.gap, lay, rec, pc, cache)) for pc in rec.stif]
-    T = lay.T
-    nF, nQ = len(s.recipe.full_vars), len(s.recipe.quad_vars)
-    rng = np.random.default_rng(0)
-    # (a) transforms at full size
-    spec = rng.standard_normal((g.NXH, g.NYAA, g.NZ)) + 1j * rng.standard_normal((g.NXH, g.NYAA, g.NZ))
-    with sfft.set_workers(processes):
+    procs = host_threads()
+    t0 = time.perf_counter()
+    smp = OracleSample(cfg, eq, par, procs)
+    sec, desc = smp.step_seconds()
+    check = None
+    if pl is not None:
+        g = smp.g
+        rng = np.random.default_rng(5)
+        spec = rng.standard_normal((g.NXH, g.NYAA, g.NZ)) + 1j * rng.standard_normal((g.NXH, g.NYAA, g.NZ))
+        with sfft.set_workers(procs):
+            ph = co.spec_to_phys(spec, g)
+            sp2 = co.phys_to_spec(ph * ph, g)
+        gp = pl.spec_to_phys(spec)
+        gs = pl.phys_to_spec(ph * ph)
+        check = {"spec_to_phys_max_err_over_max": float(np.abs(gp - ph).max() / np.abs(ph).max()),
+                 "phys_to_spec_max_err_over_max": float(np.abs(gs - sp2).max() / np.abs(sp2).max())}
+    return {"value": 1.0 / sec, "unit": "timesteps/s", "cores": procs, "kind": "port", "sample": desc,
+            "seconds_per_step": sec, "sample_wall_s": time.perf_counter() - t0,
+            "fp64_transforms_vs_oracle": check}
+
+
+class OracleSample:
+    """The oracle (the CPU restatement of the reference's timestep, numpy/scipy
+    FP64) timed on the workload, for the reference arm and the CPU baseline.
+
+    Small workloads (all (kx,ky) systems solvable in seconds) run whole oracle
+    steps.  At larger sizes a step is measured component by component on a
+    bounded sample -- every phase of one_step_beyond
+    (src/plane_layer/PL_IMEX_timestepping_marching.f90:3-48) is timed, none is
+    left out -- and the step time is the sum of the phases scaled by how often
+    each occurs in a step:
+      inverse 3-D transforms (nF per stage) and forward transforms with the
+      pointwise products (nQ per stage), at full size (scipy workers);
+      NL assembly (every NL term's truncated I^Iz M^mz contraction and
+      Fourier factors), stage right-hand sides (M field + the stage sums of
+      K_std and K_hat), K_std = L aux and the band solves (zgbtrs) on a sample
+      of kx slabs / systems of at least 1% of the systems, scaled to all."""
+
+    def __init__(self, cfg, eq, par, processes, seed=0):
+        from oracle import coral_oracle as co
+        import scipy.linalg.lapack as lapack
+        self.co = co
+        self.processes = processes
+        self.cfg = cfg
         t0 = time.perf_counter()
-        ph = co.spec_to_phys(spec, g)
-        t_inv = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        co.phys_to_spec(ph * ph, g)
-        t_fwd = time.perf_counter() - t0
-    del ph, spec
-    # (b) band LU solve per system: factor a handful, time zgbtrs on them
-    kl = ku = 0
-    for _, B in mass + stif:
-        c = B.tocoo()
-        kl = max(kl, int((c.row - c.col).max()))
-        ku = max(ku, int((c.col - c.row).max()))
-    nsample = 16
-    facs = []
-    for k in range(nsample):
-        ix, iy = 1 + (k % max(g.NXH - 1, 1)), 1 + 7 * k % (g.NY // 2)
-        M = sum((pc.dsca * co.complex_pow(complex(g.py[iy]), pc.ky) * co.complex_pow(complex(g.px[ix]), pc.kx)) * B
-                for pc, B in mass)
-        L = sum((pc.dsca * co.complex_pow(complex(g.py[iy]), pc.ky) * co.complex_pow(complex(g.px[ix]), pc.kx)) * B
-                for pc, B in stif)
-        E = (M - cfg["dt"] * s.A[0, 0] * L).tocoo()
-        ab = np.zeros((2 * kl + ku + 1, T), dtype=np.complex128)
-        ab[kl + ku + E.row - E.col, E.col] = E.data
-        lu, piv, info = lapack.zgbtrf(ab, kl, ku)
-        facs.append((lu, piv))
-    b = rng.standard_normal(T) + 1j * rng.standard_normal(T)
+        p = co.read_parameters_text(par)
+        g = co.Geometry(p["NX"], p["NY"], p["NZ"], p["Lx"], p["Ly"], p["gap"], p["center"])
+        self.g = g
+        self.whole = g.NXH * g.NYAA <= 4096
+        if self.whole:
+            self.solver = co.Solver(eq, par)
+            self.solver.factorize(cfg["dt"])
+            rng = np.random.default_rng(seed)
+            for sidx, lay in enumerate(self.solver.lay):
+                self.solver.field[sidx] = 1e-3 * (rng.standard_normal(self.solver.field[sidx].shape)
+                                                  + 1j * rng.standard_normal(self.solver.field[sidx].shape))
+            self.setup_s = time.perf_counter() - t0
+            return
+        s = co.Solver.__new__(co.Solver)
+        s.recipe = co.parse_equations(eq)
+        s.params = p
+        s.g = g
+        s.scheme = p["scheme"]
+        s.nstages, s.A, s.Ah = co.ars_tableau(s.scheme)
+        self.s = s
+        rec = s.recipe.kxky[0]
+        lay = co.SystemLayout(g.NZ, rec)
+        self.lay, self.rec = lay, rec
+        cache = {}
+        self.mass = [(pc, co.build_piece_matrix(g.NZ, g.center, g.gap, lay, rec, pc, cache)) for pc in rec.mass]
+        self.stif = [(pc, co.build_piece_matrix(g.NZ, g.center, g.gap, lay, rec, pc, cache)) for pc in rec.stif]
+        self.nF, self.nQ = len(s.recipe.full_vars), len(s.recipe.quad_vars)
+        self.T = lay.T
+        kl = ku = 0
+        for _, B in self.mass + self.stif:
+            c = B.tocoo()
+            kl = max(kl, int((c.row - c.col).max()))
+            ku = max(ku, int((c.col - c.row).max()))
+        self.kl, self.ku = kl, ku
+        self.nsys = g.NXH * g.NYAA
+        self.nact = int(g.active.sum())
+        # sample of >= 1% of the active systems, factorised once (the factorisation
+        # is not part of a step)
+        act = np.argwhere(g.active)
+        nsample = max(1, int(math.ceil(0.01 * self.nact)))
+        pick = act[np.linspace(0, len(act) - 1, nsample).astype(int)]
+        self.facs = []
+        for ix, iy in pick:
+            M = sum((pc.dsca * co.complex_pow(complex(g.py[iy]), pc.ky) * co.complex_pow(complex(g.px[ix]), pc.kx)) * B
+                    for pc, B in self.mass)
+            L = sum((pc.dsca * co.complex_pow(complex(g.py[iy]), pc.ky) * co.complex_pow(complex(g.px[ix]), pc.kx)) * B
+                    for pc, B in self.stif)
+            E = (M - cfg["dt"] * s.A[0, 0] * L).tocoo()
+            ab = np.zeros((2 * kl + ku + 1, self.T), dtype=np.complex128)
+            ab[kl + ku + E.row - E.col, E.col] = E.data
+            lu, piv, info = lapack.zgbtrf(ab, kl, ku)
+            self.facs.append((lu, piv))
+        # kx slabs of the operator sample: >= 1% of the systems
+        self.nslab = max(1, int(math.ceil(0.01 * g.NXH)))
+        self.im = {}
+        for t in rec.nl:
+            key = (t.Iz, t.mz)
+            if key not in self.im:
+                self.im[key] = co.cheb_IM(g.NZ, g.center, g.gap, t.Iz, t.mz)
+        self.setup_s = time.perf_counter() - t0
 
-    X = (rng.standard_normal((g.NYAA, T)) + 1j * rng.standard_normal((g.NYAA, T)))
-
-    def mv_slab(_):
-        for _, B in mass + stif:
-            (B @ X.T)
-
-    if processes > 1:
-        # band solves in a spawned process pool (the LAPACK wrapper holds the
-        # interpreter lock): total solves of all workers over the wall time
-        import multiprocessing as mp
-        with mp.get_context("spawn").Pool(processes) as pp:
-            pp.map(_solve_worker, [(facs[:1], kl, ku, b, 0.0)] * processes)  # start the workers
+    def step_seconds(self):
+        """One sample; returns (seconds per step, description)."""
+        co, g = self.co, self.g
+        if self.whole:
             t0 = time.perf_counter()
-            counts = pp.map(_solve_worker, [(facs, kl, ku, b, 2.0)] * processes)
-            t_solve = (time.perf_counter() - t0) / sum(counts)
-    else:
-        t_solve = 2.0 / _solve_worker((facs, kl, ku, b, 2.0))
-    with ThreadPoolExecutor(processes) as pool:
-        # (c) mass / stiffness applications, one kx slab per task
+            self.solver.step(self.cfg["dt"])
+            dt = time.perf_counter() - t0
+            return dt, ("whole oracle timesteps (numpy/scipy FP64) at %dx%dx%d: all %d (kx,ky) systems, every phase"
+                        % (g.NX, g.NY, g.NZ, g.NXH * g.NYAA))
+        import scipy.fft as sfft
+        import scipy.linalg.lapack as lapack
+        rng = np.random.default_rng(1)
+        s, lay = self.s, self.lay
+        # (1) transforms and products at full size
+        spec = rng.standard_normal((g.NXH, g.NYAA, g.NZ)) + 1j * rng.standard_normal((g.NXH, g.NYAA, g.NZ))
+        with sfft.set_workers(self.processes):
+            t0 = time.perf_counter()
+            ph = co.spec_to_phys(spec, g)
+            t_inv = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            q = ph * ph
+            co.phys_to_spec(q, g)
+            t_fwd = time.perf_counter() - t0
+        del ph, q
+        # (2) NL assembly, stage right-hand side, K_std on nslab kx slabs
+        ns = self.nslab
+        qspec = spec[:ns]
+        state = (rng.standard_normal((ns, g.NYAA, self.T)) + 1j * rng.standard_normal((ns, g.NYAA, self.T)))
+        Ks = [state.copy() for _ in range(2)]
         t0 = time.perf_counter()
-        list(pool.map(mv_slab, range(processes)))
-        t_mv = (time.perf_counter() - t0) / (processes * g.NYAA)
-    nsys = g.NXH * g.NYAA
-    nact = int(g.active.sum())
-    step = s.nstages * (nF * t_inv + nQ * t_fwd + nact * t_solve + nsys * t_mv)
-    return {"value": 1.0 / step, "unit": "timesteps/s", "cores": processes, "kind": "port",
-            "sample": ("oracle (numpy/scipy FP64, %d host threads) timed on: 1 inverse + 1 forward 3-D transform at "
-                       "%dx%dx%d, zgbtrs on %d of the %d (kx,ky) systems (T=%d, kl=%d, ku=%d), M/L applications "
-                       "on one kx slab; extrapolated to %d stages x (%d inverse + %d forward transforms + %d solves "
-                       "+ %d operator applications); sample took %.1f s"
-                       % (processes, g.NXAA, g.NYAA, g.NZAA, nsample, nact, T, kl, ku, s.nstages, nF, nQ, nact,
-                          nsys, time.perf_counter() - t_start)),
-            "seconds_per_step_extrapolated": step}
+        K = np.zeros_like(state)
+        for t in self.rec.nl:
+            fx = np.array([co.complex_pow(complex(p_), t.dx) for p_ in g.px[:ns]])
+            fy = np.array([co.complex_pow(complex(p_), t.dy) for p_ in g.py])
+            buf = (t.dsca * fx[:, None] * fy[None, :])[:, :, None] * qspec
+            trunc = self.im[(t.Iz, t.mz)][self.rec.orders[t.eqn]:, :]
+            K[:, :, lay.eq_pos[t.eqn]] += buf @ trunc.T
+        t_nl = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        X = state.reshape(-1, self.T)
+        rhs = np.zeros_like(X)
+        for pc, B in self.mass:
+            rhs += (B @ X.T).T
+        rhs += 0.5 * Ks[0].reshape(-1, self.T) + 0.5 * Ks[1].reshape(-1, self.T) + 0.5 * K.reshape(-1, self.T)
+        t_rhs = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        Y = np.zeros_like(X)
+        for pc, B in self.stif:
+            Y += (B @ X.T).T
+        t_kstd = time.perf_counter() - t0
+        # (3) band solves on the factorised sample
+        b = rng.standard_normal(self.T) + 1j * rng.standard_normal(self.T)
+        t0 = time.perf_counter()
+        for lu, piv in self.facs:
+            lapack.zgbtrs(lu, self.kl, self.ku, b, piv)
+        t_solve = (time.perf_counter() - t0) / len(self.facs)
+        per_slab = (t_nl + t_rhs + t_kstd) / ns
+        stage = self.nF * t_inv + self.nQ * t_fwd + g.NXH * per_slab + self.nact * t_solve
+        step = s.nstages * stage
+        desc = ("oracle (numpy/scipy FP64, %d host threads for the FFTs) at %dx%dx%d, every phase of a step timed: "
+                "1 inverse + 1 forward transform with a product at full size (x %d / %d per stage), NL assembly "
+                "(%d terms), stage right-hand side and K_std on %d of %d kx slabs (%.1f%% of the systems), zgbtrs on "
+                "%d of %d active systems (%.1f%%); scaled to %d stages"
+                % (self.processes, g.NX, g.NY, g.NZ, self.nF, self.nQ, len(self.rec.nl), ns, g.NXH,
+                   100.0 * ns / g.NXH, len(self.facs), self.nact, 100.0 * len(self.facs) / self.nact, s.nstages))
+        return step, desc
+
+
+def workload_config(args, cfg, NX, NY, NZ, world):
+    """The workload description shared by both arms."""
+    return {"workload": "%s: RBC no-slip Ra=%g Pr=1, %dx%dx%d modes, grid %dx%dx%d, ARS_222, dt=%g, FP64 state"
+                        % (args.config, cfg["Ra"], NX, NY, NZ, 3 * NX // 2, 3 * NY // 2, 3 * NZ // 2, cfg["dt"]),
+            "grid_points": (3 * NX // 2) * (3 * NY // 2) * (3 * NZ // 2),
+            "l2": "inputs larger than L2 at 384^2x192 (state 2.02 GB, LU factors 22.2 GB)",
+            "parallelism": "replicas x%d" % world}
 
 
 def run_reference(args, cfg):
     """The reference arm: the reference itself cannot be built here (Fortran
     2003 + MPI + FFTW3 + MKL, none installed), so its CPU restatement (the
-    oracle) is timed on the host cores, one bounded sample per step."""
+    oracle) is timed on the host cores (OracleSample: whole steps where they
+    take seconds, otherwise every phase of a step on a bounded sample)."""
     rank, world, local = dist_env()
     if rank != 0:
         return
     from coral_b200 import CONFIG_DIR
     eq = open(os.path.join(CONFIG_DIR, cfg["eq"])).read()
     par = open(os.path.join(CONFIG_DIR, cfg["par"])).read()
+    procs = host_threads()
+    smp = OracleSample(cfg, eq, par, procs)
     vals = []
+    desc = ""
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(cfg, eq, par)
+        t, desc = smp.step_seconds()
         if i >= args.warmup:
-            vals.append(r["value"])
-    v = statistics.median(vals)
-    r["value"] = v
+            vals.append(t)
+    sec = statistics.median(vals)
+    v = 1.0 / sec
+    r = {"value": v, "unit": "timesteps/s", "cores": procs, "kind": "port", "sample": desc,
+         "seconds_per_step": sec, "setup_s": smp.setup_s}
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "timesteps/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.config}, "cpu_baseline": r,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(args, cfg, cfg["NX"], cfg["NY"], cfg["NZ"], world), "cpu_baseline": r,
             "e2e": {"value": v, "unit": "timesteps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -536,6 +734,7 @@ def main():
     ap.add_argument("--config", default="rbc_384x384x192", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-split", action="store_true", help="skip the split-precision leg")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -50,6 +50,7 @@ SIGNATURES = {
     "coral_get_time": (ctypes.c_int, [_P, _D]),
     "coral_run": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_char_p]),
     "coral_set_z_transform": (ctypes.c_int, [_P, ctypes.c_int]),
+    "coral_set_hermitian_kx0": (ctypes.c_int, [_P, ctypes.c_int]),
     "coral_var_positions": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_int)]),
     "coral_ensemble_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
@@ -61,6 +62,21 @@ SIGNATURES = {
     "coral_ensemble_march": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int]),
     "coral_ensemble_synchronize": (ctypes.c_int, [_P]),
     "coral_ensemble_query": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]),
+    "coral_closure_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_ulonglong, ctypes.POINTER(_P)]),
+    "coral_closure_destroy": (None, [_P]),
+    "coral_closure_last_error": (ctypes.c_char_p, [_P]),
+    "coral_closure_param_count": (ctypes.c_int, []),
+    "coral_closure_set_scales": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)]),
+    "coral_closure_get_params": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
+    "coral_closure_set_params": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
+    "coral_closure_get_gradient": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
+    "coral_closure_zero_gradient": (ctypes.c_int, [_P]),
+    "coral_closure_train": (ctypes.c_int, [_P, _P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P,
+                                           ctypes.c_longlong, ctypes.c_float, ctypes.c_int,
+                                           ctypes.POINTER(ctypes.c_double)]),
+    "coral_closure_infer": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P]),
+    "coral_closure_attach": (ctypes.c_int, [_P, _P]),
+    "coral_autotune": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
 }
 
 _lib = None

@@ -19,6 +19,10 @@
 
 using namespace coral;
 
+namespace coral {
+ClosureImpl* closure_impl(coral_closure* c);  // closure.cu
+}
+
 namespace {
 
 thread_local std::string g_create_error;
@@ -171,6 +175,17 @@ struct coral_handle {
   // z transforms: 0 = FP64 FFT (k_z_fused), 1 = int8-digit contractions on the
   // tensor cores (zsplit.cu); form_last = the form of the last step (KE sums)
   int zform = 0, zform_last = 0;
+  bool hermitian_kx0 = false;  // project the kx = 0 line onto its Hermitian part after each step
+  // kernel variants chosen by coral_autotune (defaults: the choices measured best at 384^2 x 192)
+  struct Tune {
+    int x_plan = 1;         // x passes: 1 two-pass FFT plans, 0 three-pass
+    int fwd_y_grid = 0;     // forward y pass: 0 persistent pipelined, 1 one CTA per tile
+    int generic_tiles = 0;  // operator tile kernels: 0 compiled group layouts, 1 run-time forms
+    int subst_rt = 0;       // band substitution: 0 compiled band, 1 run-time band
+  } tune;
+  // learned closure (not owned) and its output [9][y][x][z]
+  coral_closure* closure = nullptr;
+  double* tau = nullptr;
   unsigned char *zmat_inv = nullptr, *zmat_fwd = nullptr;
   double* ke_partial_split = nullptr;  // [forward CTAs][3]
   size_t n_ke_split = 0;
@@ -759,7 +774,8 @@ SolveArgs make_solve_args(coral_handle* h, KSys& k, int i, double dt) {
   sa.NLg = k.NLg;
   // CORAL_GENERIC_TILES=1: the run-time forms of the tile kernels (tests cover
   // them with the plane-layer recipes, whose layouts are otherwise compiled)
-  sa.generic_tiles = std::getenv("CORAL_GENERIC_TILES") != nullptr;
+  sa.generic_tiles = std::getenv("CORAL_GENERIC_TILES") != nullptr || h->tune.generic_tiles;
+  sa.subst_rt = h->tune.subst_rt;
   sa.Lw = k.Lw;
   {
     const int kv = sa.kl + sa.ku;
@@ -788,7 +804,7 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
   {
     StateSet st = state_set(h, i == 0);
     B(0); launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream); E();
-    B(1); launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream); E();
+    B(1); launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream, h->tune.x_plan); E();
     // the CFL maxima reported after a step are those of its last stage's fields
     // (each stage's evaluation replaces them): only the last stage computes them
     if (last) CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
@@ -798,7 +814,18 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
   // quadratic variables overwrite Y2 in place, each CTA reading and writing only
   // its own (y, x pair) columns
   B(3);
-  if (h->zform == 1) {
+  if (h->closure) {
+    // unfused z passes around the network: physical fields to HBM, the
+    // network's subgrid parts, then the products (plus those parts) forward
+    launch_inv_z(d, h->nF, h->Y2, h->fphys, h->pz, h->dct_tw, h->d_wz, last ? h->cfl_bits : nullptr, h->stream);
+    closure_infer(closure_impl(h->closure), h->fphys, d.NYA, d.NXA, d.NZA, h->tau, h->stream);
+    QuadDesc q = h->quads;
+    q.ts_partial = nullptr;
+    q.tau = h->tau;
+    launch_fwd_z(d, h->nF, q, h->fphys, h->Y2, h->pz, h->dct_tw, h->d_wz, i == 0 ? h->ke_partial : nullptr,
+                 h->stream);
+    nl += 2;
+  } else if (h->zform == 1) {
     // the tensor-core form: inverse contraction into the physical fields,
     // then products and the forward contraction back into Y2
     QuadDesc q = h->quads;
@@ -818,8 +845,8 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
                    last ? h->cfl_bits : nullptr, i == 0 ? h->ke_partial : nullptr, h->stream);
   }
   E();
-  B(4); launch_fwd_x(d, h->nQ, h->Y2, h->Y1, h->px, h->stream); E();
-  B(5); launch_fwd_y(d, h->nQ, h->Y1, h->qspec, scale, h->py, h->stream); E();
+  B(4); launch_fwd_x(d, h->nQ, h->Y2, h->Y1, h->px, h->stream, h->tune.x_plan); E();
+  B(5); launch_fwd_y(d, h->nQ, h->Y1, h->qspec, scale, h->py, h->stream, h->tune.fwd_y_grid); E();
   nl += 3;
   for (int q : h->zmean_quads) {
     launch_remove_zmean(d, h->qspec + (size_t)q * d.NXH * d.NYA * d.NZ, h->stream);
@@ -885,10 +912,16 @@ int enqueue_stage_post(coral_handle* h, int i, double dt, PhaseTimer* pt) {
   return nl;
 }
 
-// after the stages: the timeseries totals of the step
+// after the stages: the kx = 0 projection (when enabled) and the timeseries
+// totals of the step
 int enqueue_step_end(coral_handle* h) {
   const Geometry& g = *h->G;
   int nl = 0;
+  if (h->hermitian_kx0)
+    for (auto& k : h->ks) {
+      launch_hermitian_kx0(k.field, h->d.NYA, k.T, h->stream);
+      ++nl;
+    }
   if (h->quads.ts_n > 0) {
     if (h->zform == 1)
       launch_ts_reduce(h->ts_partial_split, h->ts_rows_split, h->quads.ts_n, 1.0 / ((double)g.NXAA * (double)g.NYAA),
@@ -1747,6 +1780,110 @@ int coral_var_positions(coral_handle* h, int isys, int ivar, int* positions, int
     if (!positions) return;
     if (n < (int)vp.size()) throw CoralError(CORAL_EBADARG, "buffer smaller than the variable");
     for (size_t i = 0; i < vp.size(); ++i) positions[i] = vp[i];
+  });
+}
+
+int coral_autotune(coral_handle* h, double dt, int repeats, char* report, int n) {
+  return guarded(h, [&] {
+    if (!(dt > 0.0) || repeats < 1) throw CoralError(CORAL_EBADARG, "autotune: dt > 0 and repeats >= 1");
+    if (h->dt_factored != dt) factorize(h, dt);
+    // the tuning steps advance a copy of the state: save it, restore it after
+    std::vector<void*> saved;
+    for (auto& k : h->ks) {
+      void* p = nullptr;
+      const size_t b = (size_t)h->d.NXH * h->d.NYA * k.T * sizeof(double2);
+      CK(cudaMalloc(&p, b));
+      CK(cudaMemcpyAsync(p, k.field, b, cudaMemcpyDeviceToDevice, h->stream));
+      saved.push_back(p);
+    }
+    std::vector<std::vector<double>> zsaved;
+    for (auto& z : h->zs) {
+      std::vector<double> v(z.dev.T);
+      CK(cudaMemcpy(v.data(), z.dev.field, z.dev.T * sizeof(double), cudaMemcpyDeviceToHost));
+      zsaved.push_back(v);
+    }
+    auto time_phases = [&](std::initializer_list<int> phases) {
+      double best = 1e300;
+      for (int r = 0; r < repeats + 1; ++r) {  // the first step sets attributes and warms the caches
+        PhaseTimer pt{h->stream, {}};
+        enqueue_step(h, dt, &pt);
+        CK(cudaStreamSynchronize(h->stream));
+        double t = 0.0;
+        for (auto& e : pt.ev) {
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, e.second.first, e.second.second);
+          for (int ph : phases)
+            if (e.first == ph) t += ms;
+          cudaEventDestroy(e.second.first);
+          cudaEventDestroy(e.second.second);
+        }
+        if (r > 0) best = std::min(best, t);
+      }
+      return best;
+    };
+    struct Knob { const char* name; int* var; int a, b; const char* na; const char* nb; std::vector<int> phases; };
+    std::vector<Knob> knobs = {
+        {"x_fft_plan", &h->tune.x_plan, 1, 0, "two-pass", "three-pass", {1, 4}},
+        {"fwd_y_pass", &h->tune.fwd_y_grid, 0, 1, "persistent-pipelined", "one-CTA-per-tile", {5}},
+        {"operator_tiles", &h->tune.generic_tiles, 0, 1, "compiled-groups", "run-time-forms", {7, 10}},
+        {"band_substitution", &h->tune.subst_rt, 0, 1, "compiled-band", "run-time-band", {9}}};
+    std::string rep;
+    for (auto& kb : knobs) {
+      double ta = 0, tb = 0;
+      *kb.var = kb.a;
+      if (kb.phases.size() == 2) ta = time_phases({kb.phases[0], kb.phases[1]});
+      else ta = time_phases({kb.phases[0]});
+      *kb.var = kb.b;
+      if (kb.phases.size() == 2) tb = time_phases({kb.phases[0], kb.phases[1]});
+      else tb = time_phases({kb.phases[0]});
+      *kb.var = (tb < ta) ? kb.b : kb.a;
+      char buf[256];
+      std::snprintf(buf, sizeof(buf), "%s%s: %s %.4f ms, %s %.4f ms -> %s", rep.empty() ? "" : "; ", kb.name, kb.na, ta,
+                    kb.nb, tb, (tb < ta) ? kb.nb : kb.na);
+      rep += buf;
+    }
+    for (size_t i = 0; i < h->ks.size(); ++i) {
+      const size_t b = (size_t)h->d.NXH * h->d.NYA * h->ks[i].T * sizeof(double2);
+      CK(cudaMemcpyAsync(h->ks[i].field, saved[i], b, cudaMemcpyDeviceToDevice, h->stream));
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    for (void* p : saved) cudaFree(p);
+    for (size_t i = 0; i < h->zs.size(); ++i)
+      CK(cudaMemcpy(h->zs[i].dev.field, zsaved[i].data(), zsaved[i].size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (h->graph) {
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
+    if (report && n > 0) {
+      std::strncpy(report, rep.c_str(), (size_t)n - 1);
+      report[n - 1] = 0;
+    }
+  });
+}
+
+int coral_closure_attach(coral_handle* h, coral_closure* c) {
+  return guarded(h, [&] {
+    if (c) {
+      if (h->nF != 4 || h->nQ != 9)
+        throw CoralError(CORAL_EUNSUPPORTED, "the closure needs 4 full variables (u, v, w, T) and 9 quadratic ones");
+      if (h->zform != 0) throw CoralError(CORAL_EUNSUPPORTED, "the closure runs with the FP64 z transforms");
+      if (!h->tau) h->tau = h->mem.get<double>((size_t)9 * h->d.NYA * h->d.NXA * h->d.NZA);
+    }
+    h->closure = c;
+    if (h->graph) {
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
+  });
+}
+
+int coral_set_hermitian_kx0(coral_handle* h, int on) {
+  return guarded(h, [&] {
+    h->hermitian_kx0 = on != 0;
+    if (h->graph) {
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
   });
 }
 

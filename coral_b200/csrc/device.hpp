@@ -86,6 +86,9 @@ struct QuadDesc {
   int ts_n;
   int ts_src[kMaxTs], ts_z[kMaxTs];
   double* ts_partial;
+  // learned closure: tau[q][y][x][z] added to quadratic variable q after its
+  // product (and after its KE contribution) in the unfused forward z pass; null: none
+  const double* tau;
 };
 
 struct Dims {
@@ -96,7 +99,8 @@ struct Dims {
 // inverse transform of nf scalars: spectral build (or a plain spec input) + y-FFT
 void launch_inv_y(const Dims& d, int nf, const FullVarDev* fv, StateSet st, const double2* plain_spec,
                   const double* kx, const double* ky, double2* Y1, const FftPlan& py, cudaStream_t s);
-void launch_inv_x(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s);
+// pv: FFT plan of the compiled lengths, 1 = two passes (576 = 24 x 24, 288 = 18 x 16), 0 = three passes
+void launch_inv_x(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s, int pv = 1);
 // z DCT-III; cfl: maxima of |u|, |v|, |w|/wz written (as uint64 bit patterns) to cfl_bits when non-null
 void launch_inv_z(const Dims& d, int nf, const double* Y2, double* phys, const FftPlan& pz,
                   const double2* dct_tw, const double* wz, unsigned long long* cfl_bits, cudaStream_t s);
@@ -109,9 +113,10 @@ void launch_fwd_z(const Dims& d, int nf, const QuadDesc& q, const double* phys, 
 void launch_z_fused(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* Q2, const FftPlan& pz,
                     const double2* dct_tw, const double* wz, const double* wzinv, unsigned long long* cfl_bits,
                     double* ke_partial, cudaStream_t s);
-void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s);
+void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s, int pv = 1);
+// grid_variant = 1: one CTA per tile instead of the persistent pipelined kernel
 void launch_fwd_y(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
-                  cudaStream_t s);
+                  cudaStream_t s, int grid_variant = 0);
 void launch_remove_zmean(const Dims& d, double2* qspec_q, cudaStream_t s);
 // ---- split-precision z transforms on the tensor cores (zsplit.cu) ----
 // int8 digits of the REDFT01 (fwd = false: NZAA x NZ) or REDFT10 (fwd = true:
@@ -129,6 +134,15 @@ void launch_zsplit_inv(const Dims& d, int nf, const QuadDesc& q, const double* Y
 void launch_zsplit_fwd(const Dims& d, int nf, const QuadDesc& q, const double* phys, double* Q2,
                        const unsigned char* mat, const double* wz, double* ke_partial, double* ts_partial,
                        long long ts_row0, unsigned* flags, cudaStream_t s);
+
+// learned closure (closure.cu): inference on a whole grid, 4 full variables
+// [f][y][x][z] -> tau [9][y][x][z]
+struct ClosureImpl;
+void closure_infer(ClosureImpl* c, const double* fields, int NYA, int NXA, int NZA, double* tau, cudaStream_t s);
+
+// the kx = 0 line (the first NYA x T entries) of a coupled state onto its
+// Hermitian part (timeseries.cu)
+void launch_hermitian_kx0(double2* field, int NYA, int T, cudaStream_t s);
 
 // CTAs of launch_z_fused (rows of its KE and timeseries partial sums)
 size_t z_fused_ctas(const Dims& d);
@@ -214,6 +228,7 @@ struct SolveArgs {
   DevEll Mw, NLw;
   DevGEll NLg;           // NLw in grouped form (valid = 0: none)
   int generic_tiles;     // 1: the tile kernels' run-time forms only (no compiled group layouts)
+  int subst_rt;          // 1: the run-time-band substitution kernel even for the compiled band
   // band entries that are zero in every block are not loaded (FactorArgs::lmask,
   // umask; null: load all)
   const unsigned* lmask;

@@ -51,7 +51,7 @@ __host__ __device__ constexpr int xy_threads(int N, int nl, int pv) {
   for (int i = 0; i < p.nst; ++i) m = (nl * N / p.r[i] > m) ? nl * N / p.r[i] : m;
   return (m + 31) / 32 * 32;
 }
-#define kThreadsX xy_threads(NF, kNB2 / 2, kPlanHot)
+#define kThreadsX xy_threads(NF, kNB2 / 2, PV)
 #define kThreadsY xy_threads(NF, 4, kPlanY)
 // the pipelined forward y pass reads its first-pass inputs from shared memory:
 // plan and threads of its own
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(kThreadsY, kMinBlocksY) k_inv_y(Dims d, const 
 // inverse transform, pass 2: x c2r with zero padding NX/2 -> NXAA (transforms.f90:197-210)
 // two real output lines per complex FFT
 // ------------------------------------------------------------------------------
-template <int NF>
+template <int NF, int PV>
 __global__ void __launch_bounds__(kThreadsX, hot_min_blocks(kThreadsX)) k_inv_x(Dims d, const double2* Y1, double* Y2, FftPlan px) {
   extern __shared__ double2 sm[];
   const int f = blockIdx.x, n0 = blockIdx.y * kNB2, y = blockIdx.z;
@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(kThreadsX, hot_min_blocks(kThreadsX)) k_inv_x(
     return lo ? make_double2(a.x - b.y, a.y + b.x)    // a + i b
               : make_double2(a.x + b.y, b.x - a.y);   // conj(a) + i conj(b)
   };
-  const double2* R = fft_lines_ld<NF, true, kThreadsX, kNB2 / 2, true, kPlanHot>(A, B, NP, LS, px, ld);
+  const double2* R = fft_lines_ld<NF, true, kThreadsX, kNB2 / 2, true, PV>(A, B, NP, LS, px, ld);
   for (int idx = threadIdx.x; idx < NP * NXA; idx += blockDim.x) {
     const int m = idx % NP, x = idx / NP, na = n0 + 2 * m;
     double2 z = R[m * LS + x];
@@ -333,11 +333,16 @@ __global__ void __launch_bounds__(kThreads, kMinBlocksZ) k_fwd_z(Dims d, int nf,
         pa = P[(v1 * 2) * N + m] * P[(v2 * 2) * N + m];
         pb = P[(v1 * 2 + 1) * N + m] * P[(v2 * 2 + 1) * N + m];
       }
-      A[qi * N + m] = make_double2(pa, pb);
       if (ke_partial) {
         for (int j = 0; j < 3; ++j)
           if (q.ke_q[j] == qg) ke[j] += wz[z] * (pa + ((x0 + 1 < d.NXA) ? pb : 0.0));
       }
+      if (q.tau) {  // learned subgrid part of this quadratic variable
+        const double* tq = q.tau + (((size_t)qg * d.NYA + y) * d.NXA + x0) * N + z;
+        pa += tq[0];
+        if (x0 + 1 < d.NXA) pb += tq[N];
+      }
+      A[qi * N + m] = make_double2(pa, pb);
     }
     __syncthreads();
     const double2* R = fft_lines_n<NF, false, kThreads, kQC>(A, B, nc, N, pz);
@@ -609,7 +614,7 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
 // ------------------------------------------------------------------------------
 // forward transform, pass 2: x r2c, keep kx < NX/2 (transforms.f90:255-267)
 // ------------------------------------------------------------------------------
-template <int NF>
+template <int NF, int PV>
 __global__ void __launch_bounds__(kThreadsX, hot_min_blocks(kThreadsX)) k_fwd_x(Dims d, const double* Q2, double2* Q1, FftPlan px) {
   extern __shared__ double2 sm[];
   const int qi = blockIdx.x, n0 = blockIdx.y * kNB2, y = blockIdx.z;
@@ -624,7 +629,7 @@ __global__ void __launch_bounds__(kThreadsX, hot_min_blocks(kThreadsX)) k_fwd_x(
     const double* src = src0 + (size_t)x * d.NZ;
     return make_double2(na < d.NZ ? src[na] : 0.0, na + 1 < d.NZ ? src[na + 1] : 0.0);
   };
-  const double2* R = fft_lines_ld<NF, false, kThreadsX, kNB2 / 2, true, kPlanHot>(A, B, NP, LS, px, ld);
+  const double2* R = fft_lines_ld<NF, false, kThreadsX, kNB2 / 2, true, PV>(A, B, NP, LS, px, ld);
   for (int idx = threadIdx.x; idx < NP * d.NXH; idx += blockDim.x) {
     const int m = idx % NP, kx = idx / NP, na = n0 + 2 * m;
     const double2 Z = R[m * LS + kx];
@@ -2433,11 +2438,16 @@ struct InvY {
 };
 template <int NF>
 struct InvX {
-  static void run(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s) {
+  template <int PV>
+  static void go(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s) {
     size_t sm = (NF ? 1 : 2) * (kNB2 / 2) * (size_t)(d.NXA + kPadXY) * sizeof(double2);
-    set_smem(k_inv_x<NF>, sm);
+    set_smem(k_inv_x<NF, PV>, sm);
     dim3 g(nf, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
-    k_inv_x<NF><<<g, kThreadsX, sm, s>>>(d, Y1, Y2, px);
+    k_inv_x<NF, PV><<<g, kThreadsX, sm, s>>>(d, Y1, Y2, px);
+  }
+  static void run(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, int pv, cudaStream_t s) {
+    if (pv) go<1>(d, nf, Y1, Y2, px, s);
+    else go<0>(d, nf, Y1, Y2, px, s);
   }
 };
 template <int NF>
@@ -2479,18 +2489,24 @@ struct ZFused {
 };
 template <int NF>
 struct FwdX {
-  static void run(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s) {
+  template <int PV>
+  static void go(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s) {
     size_t sm = (NF ? 1 : 2) * (kNB2 / 2) * (size_t)(d.NXA + kPadXY) * sizeof(double2);
-    set_smem(k_fwd_x<NF>, sm);
+    set_smem(k_fwd_x<NF, PV>, sm);
     dim3 g(nq, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
-    k_fwd_x<NF><<<g, kThreadsX, sm, s>>>(d, Q2, Q1, px);
+    k_fwd_x<NF, PV><<<g, kThreadsX, sm, s>>>(d, Q2, Q1, px);
+  }
+  static void run(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, int pv, cudaStream_t s) {
+    if (pv) go<1>(d, nq, Q2, Q1, px, s);
+    else go<0>(d, nq, Q2, Q1, px, s);
   }
 };
 template <int NF>
 struct FwdY {
   static void run(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
-                  cudaStream_t s) {
+                  int grid_variant, cudaStream_t s) {
     if constexpr (NF != 0) {
+      if (!grid_variant) {
       // persistent pipelined kernel: as many CTAs as fit on the device at once
       const size_t sm = (kNB1 * (size_t)(NF + kPadY) + (size_t)NF * kNB1) * sizeof(double2);
       set_smem(k_fwd_y_pipe<NF>, sm);
@@ -2499,6 +2515,7 @@ struct FwdY {
       const int ntiles = nq * ((d.NZ + kNB1 - 1) / kNB1) * d.NXH;
       k_fwd_y_pipe<NF><<<std::min(nct, ntiles), kThreadsYF, sm, s>>>(d, nq, Q1, qspec, scale, py);
       return;
+    }
     }
     size_t sm = (NF ? 1 : 2) * kNB1 * (size_t)(d.NYA + kPadY) * sizeof(double2);
     set_smem(k_fwd_y<NF>, sm);
@@ -2516,8 +2533,8 @@ void launch_z_fused(const Dims& d, int nf, const QuadDesc& q, const double* Y2, 
                     double* ke_partial, cudaStream_t s) {
   dispatch_len<ZFused>(d.NZA, d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, s);
 }
-void launch_inv_x(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s) {
-  dispatch_len<InvX>(d.NXA, d, nf, Y1, Y2, px, s);
+void launch_inv_x(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s, int pv) {
+  dispatch_len<InvX>(d.NXA, d, nf, Y1, Y2, px, pv, s);
 }
 void launch_inv_z(const Dims& d, int nf, const double* Y2, double* phys, const FftPlan& pz,
                   const double2* dct_tw, const double* wz, unsigned long long* cfl_bits, cudaStream_t s) {
@@ -2527,12 +2544,12 @@ void launch_fwd_z(const Dims& d, int nf, const QuadDesc& q, const double* phys, 
                   const double2* dct_tw, const double* wz, double* ke_partial, cudaStream_t s) {
   dispatch_len<FwdZ>(d.NZA, d, nf, q, phys, Q2, pz, dct_tw, wz, ke_partial, s);
 }
-void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s) {
-  dispatch_len<FwdX>(d.NXA, d, nq, Q2, Q1, px, s);
+void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s, int pv) {
+  dispatch_len<FwdX>(d.NXA, d, nq, Q2, Q1, px, pv, s);
 }
 void launch_fwd_y(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
-                  cudaStream_t s) {
-  dispatch_len<FwdY>(d.NYA, d, nq, Q1, qspec, scale, py, s);
+                  cudaStream_t s, int grid_variant) {
+  dispatch_len<FwdY>(d.NYA, d, nq, Q1, qspec, scale, py, grid_variant, s);
 }
 // total of the KE partial sums written by the z kernels: one CTA, each thread a
 // strided sum, then a fixed-order tree
@@ -2607,19 +2624,15 @@ void launch_subst(const SolveArgs& a, cudaStream_t s) {
       const int kv = a.kl + a.ku, grid = (a.nblk + kTpbThreads - 1) / kTpbThreads;
       // band (kl, kl+ku) = (9, 23) of the plane-layer recipes compiled, any other
       // band within (15, 31) through the run-time-band kernel
-#define CORAL_TPB_CASE(KL_, KV_)                                                     \
-  if (a.kl == KL_ && kv == KV_ && a.ldab == ((KL_ + KV_ + 2) & ~1)) {                 \
-    constexpr int LD_ = (KL_ + KV_ + 2) & ~1;                                         \
-    const size_t sm = (size_t)kTpbThreads * (KV_ + 1 > 16 ? KV_ + 1 : 16) * sizeof(double2); \
-    set_smem(k_subst_tpb<KL_, KV_, LD_>, sm);                                         \
-    k_subst_tpb<KL_, KV_, LD_><<<grid, kTpbThreads, sm, s>>>(a);                     \
-  } else
-      CORAL_TPB_CASE(9, 23) {
+      if (!a.subst_rt && a.kl == 9 && kv == 23 && a.ldab == 34) {
+        const size_t sm = (size_t)kTpbThreads * 24 * sizeof(double2);
+        set_smem(k_subst_tpb<9, 23, 34>, sm);
+        k_subst_tpb<9, 23, 34><<<grid, kTpbThreads, sm, s>>>(a);
+      } else {
         const size_t sm = (size_t)kTpbThreads * 32 * sizeof(double2);
         set_smem(k_subst_tpb_rt<15, 31>, sm);
         k_subst_tpb_rt<15, 31><<<grid, kTpbThreads, sm, s>>>(a);
       }
-#undef CORAL_TPB_CASE
     }
     return;
   }

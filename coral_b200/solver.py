@@ -239,6 +239,17 @@ class PlaneLayer:
         self._check(self._lib.coral_var_positions(self._h, int(isys), int(ivar), buf, n.value, ctypes.byref(n)))
         return np.frombuffer(buf, dtype=np.int32)[:n.value].copy()
 
+    def autotune(self, dt, repeats=2):
+        """Time the kernel variants of the step and keep the fastest; returns the report."""
+        buf = ctypes.create_string_buffer(2048)
+        self._check(self._lib.coral_autotune(self._h, float(dt), int(repeats), buf, 2048))
+        return buf.value.decode()
+
+    def set_hermitian_kx0(self, on=True):
+        """Project the kx = 0 line onto its Hermitian part after every step
+        (removes the invisible anti-Hermitian part; off by default)."""
+        self._check(self._lib.coral_set_hermitian_kx0(self._h, 1 if on else 0))
+
     def set_z_transform(self, form):
         """0: FP64 FFT z transforms; 1: int8-digit tensor-core contractions."""
         self._check(self._lib.coral_set_z_transform(self._h, int(form)))

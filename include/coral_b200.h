@@ -245,6 +245,19 @@ int coral_get_time(coral_handle* h, double* out4);
 int coral_run(coral_handle* h, int nsteps, const char* output_directory);
 
 /*
+ * on != 0: after every step, replace the kx = 0 line of every coupled state by
+ * its Hermitian part (f(0,ky) + conj f(0,-ky)) / 2.  Off by default, which
+ * reproduces the reference's arithmetic.  Every physical value is unchanged:
+ * the inverse transform keeps only the real part of the kx = 0 coefficient
+ * (src/slabs.fftw3mpi/transforms.f90:197-210), so the anti-Hermitian part of
+ * that line is invisible, receives no nonlinear feedback and, where the
+ * (kx = 0, ky) operators are unstable, grows exponentially from round-off
+ * until it contaminates the fields (seen in the rotating convection benchmark
+ * after ~0.2 diffusive times).  Has no counterpart in the reference.
+ */
+int coral_set_hermitian_kx0(coral_handle* h, int on);
+
+/*
  * Positions (0-based, within T) of the Galerkin coefficients of coupled variable
  * ivar of kxky system isys in the interleaved state layout
  * (src/plane_layer/PL_IMEX_timestepping.f90:1344-1414).  *size receives the
@@ -292,6 +305,55 @@ int coral_ensemble_member(coral_ensemble* e, int i, coral_handle** member);
 int coral_ensemble_march(coral_ensemble* e, double dt, int nsteps);
 int coral_ensemble_synchronize(coral_ensemble* e);
 int coral_ensemble_query(coral_ensemble* e, int what, long long* value);
+
+/*
+ * Autotuner (no counterpart in the reference): times the kernel variants of the
+ * step on this handle's problem at dt -- the FFT plans of the x passes (two or
+ * three passes), the forward y pass (persistent pipelined or one CTA per tile),
+ * the operator tile kernels (compiled group layouts or run-time forms) and the
+ * band substitution (compiled or run-time band) -- each over `repeats` eager
+ * steps (CUDA events on the handle's stream, best time of the phases it
+ * affects), keeps the fastest of each, and restores the state (the tuning steps
+ * leave it unchanged).  All variants compute the same arithmetic.  report (may
+ * be NULL) receives the timings and choices, at most n bytes.
+ */
+int coral_autotune(coral_handle* h, double dt, int repeats, char* report, int n);
+
+/*
+ * Learned subgrid closure (no counterpart in the reference).  A stencil network
+ * (5 inputs -- u, v, w, T scaled by in_scale and z' -- at the 27 points of a
+ * 3 x 3 x 3 stencil, three tanh layers of 64, 9 outputs) predicts, on a coarse
+ * grid, the subgrid part tau_q of every quadratic variable; with a network
+ * attached to a handle (coral_closure_attach) every stage adds tau_q to the
+ * products before their forward transform, so the subgrid fluxes reach K_hat
+ * through the recipe's own NL terms (src/plane_layer/PL_IMEX_timestepping_marching.f90:279-352
+ * has only the products).  Weights BF16 with FP32 master copies, FP32
+ * accumulation; forward, backward and Adam are CUDA kernels.
+ *   train: inputs [nsnap][4][NYAA][NXAA][NZAA] and targets [nsnap][9][...] (float,
+ *   device), points (device) = snapshot * NYAA NXAA NZAA + linear grid index;
+ *   accumulates the gradient of the mean squared error (targets divided by
+ *   out_scale) over the points and, with apply != 0, takes one Adam step
+ *   (lr; beta1 = 0.9, beta2 = 0.999, eps = 1e-8) and clears the gradient.
+ *   infer: fields = 4 full variables [f][NYAA][NXAA][NZAA] (double, device) ->
+ *   tau [9][NYAA][NXAA][NZAA] (double, device), queued on stream.
+ */
+typedef struct coral_closure coral_closure;
+int coral_closure_create(int device, unsigned long long seed, coral_closure** out);
+void coral_closure_destroy(coral_closure* c);
+const char* coral_closure_last_error(const coral_closure* c);
+int coral_closure_param_count(void);
+int coral_closure_set_scales(coral_closure* c, const float* in_scale4, const float* out_scale9);
+int coral_closure_get_params(coral_closure* c, float* params, int n);
+int coral_closure_set_params(coral_closure* c, const float* params, int n);
+int coral_closure_get_gradient(coral_closure* c, float* grad, int n);
+int coral_closure_zero_gradient(coral_closure* c);
+int coral_closure_train(coral_closure* c, const float* inputs, const float* targets, int nsnap, int NXAA, int NYAA,
+                        int NZAA, const long long* points, long long npts, float lr, int apply, double* loss);
+int coral_closure_infer(coral_closure* c, const double* fields, int NXAA, int NYAA, int NZAA, double* tau,
+                        void* stream);
+/* Attach a network to a handle (NULL detaches): the full variables must be u, v,
+ * w, T (4) and the quadratic variables 9.  The handle does not own the network. */
+int coral_closure_attach(coral_handle* h, coral_closure* c);
 
 #ifdef __cplusplus
 }

@@ -10,7 +10,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def test_library_exports_every_header_symbol():
     lib = _lib.load()
     hdr = open(os.path.join(ROOT, "include", "coral_b200.h")).read()
-    names = set(re.findall(r"\b(coral_[a-z_]+)\s*\(", hdr))
+    names = set(re.findall(r"\b(coral_[a-z0-9_]+)\s*\(", hdr))
     assert names, "no declarations found"
     assert names == set(_lib.SIGNATURES), names ^ set(_lib.SIGNATURES)
     for n in names:

@@ -150,3 +150,62 @@ def test_reference_benchmark02_files_read_unmodified():
     assert np.all(np.abs(got - want) <= 1e-10 * np.abs(want) + 1e-15), (got, want)
     assert _rel(pl.get_field(0), ref.field[0]) < 1e-10
     pl.close()
+
+
+def _project_kx0(f):
+    """numpy form of the Hermitian projection of the kx = 0 line."""
+    g = f.copy()
+    NYA = f.shape[1]
+    for iy in range(1, (NYA + 1) // 2):
+        h = 0.5 * (f[0, iy] + np.conj(f[0, NYA - iy]))
+        g[0, iy] = h
+        g[0, NYA - iy] = np.conj(h)
+    g[0, 0] = g[0, 0].real
+    if NYA % 2 == 0:
+        g[0, NYA // 2] = g[0, NYA // 2].real
+    return g
+
+
+def test_hermitian_kx0_projection_matches_projected_oracle():
+    """With the projection on, the state after n steps is the oracle's state
+    after n steps with its kx = 0 line projected (the anti-Hermitian part
+    evolves on its own and never reaches the physical fields)."""
+    from coral_b200.solver import PlaneLayer
+    eq = equations("rbc_noslip_ra1e8", **{"1.d8": "1.d5"})
+    par = _params(16, 12, 48, 1e-5, 0.3, 1e30)
+    ref = co.Solver(eq, par)
+    pl = PlaneLayer(eq, par)
+    pl.set_hermitian_kx0(True)
+    _random_state(ref, pl, 34, amp=1e-2)
+    for _ in range(3):
+        ref.step(1e-5)
+    pl.march_forward(1e-5, 3)
+    got = pl.get_field(0)
+    want = _project_kx0(ref.field[0])
+    assert _rel(got, want) < 1e-10
+    assert np.array_equal(got, _project_kx0(got))
+    for s in range(len(ref.zlay)):
+        assert _rel(pl.get_mean_field(s), ref.zfield[s]) < 1e-10
+    pl.close()
+
+
+def test_autotune_keeps_the_state_and_the_results():
+    """The autotuner times every kernel variant, leaves the state as it was, and
+    the step with its choices gives the default step's results to round-off."""
+    from coral_b200.solver import PlaneLayer
+    eq = equations("rbc_noslip_ra1e8", **{"1.d8": "1.d5"})
+    par = _params(16, 12, 48, 1e-5, 0.3, 1e30)
+    a, b = PlaneLayer(eq, par), PlaneLayer(eq, par)
+    rng = np.random.default_rng(35)
+    f = 1e-2 * (rng.standard_normal((a.NXH, a.NYAA, a.T[0])) + 1j * rng.standard_normal((a.NXH, a.NYAA, a.T[0])))
+    for pl in (a, b):
+        pl.set_field(0, f)
+    rep = b.autotune(1e-5, repeats=1)
+    for knob in ("x_fft_plan", "fwd_y_pass", "operator_tiles", "band_substitution"):
+        assert knob in rep, rep
+    assert np.array_equal(b.get_field(0), f)
+    a.march_forward(1e-5, 2)
+    b.march_forward(1e-5, 2)
+    assert _rel(b.get_field(0), a.get_field(0)) < 1e-12
+    a.close()
+    b.close()
