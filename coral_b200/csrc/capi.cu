@@ -1328,6 +1328,7 @@ void flush_timeseries(coral_handle* h, const std::string& dir) {
 // (buffer_length, PL_IMEX_timestepping.f90:159) and at the end.
 void run_loop(coral_handle* h, int nsteps, const char* outdir) {
   if (nsteps < 0) throw CoralError(CORAL_EBADARG, "coral_run: nsteps must be >= 0");
+  if (outdir && !*outdir) outdir = nullptr;  // an empty string (a Fortran c_null_char) means no output
   const Parameters& P = h->P;
   const double dt_min = 1e-9;
   const int n = h->quads.ts_n;

@@ -239,7 +239,7 @@ int coral_get_time(coral_handle* h, double* out4);
  * timeseries objects are written every 20 steps and at the end to
  * output_directory/Timeseries/ in the reference's files (time.dat,
  * NAME_volAvg.dat, NAME_XYavg_zKKKKK.dat: raw float64, step k at offset 8(k-1);
- * PL_IMEX_timestepping_output.f90:136-231); output_directory may be NULL.
+ * PL_IMEX_timestepping_output.f90:136-231); output_directory may be NULL or empty (no files).
  * Synchronous: returns when the steps are done.
  */
 int coral_run(coral_handle* h, int nsteps, const char* output_directory);

@@ -29,3 +29,34 @@ def test_create_without_gpu_fails_loudly():
         assert e.code == -9
     else:
         raise AssertionError("expected CORAL_ENODEV")
+
+
+def _build_harness(out_dir):
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    assert gcc, "gcc not found"
+    lib_dir = os.path.join(ROOT, "coral_b200")
+    exe = os.path.join(out_dir, "harness")
+    subprocess.run([gcc, "-O2", "-std=c99", "-Wall", "-Werror", "-I" + os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c_harness", "harness.c"), "-L" + lib_dir, "-lcoral_b200",
+                    "-L/usr/local/cuda/lib64", "-lcudart", "-lm", "-Wl,-rpath," + lib_dir, "-o", exe], check=True)
+    return exe
+
+
+def test_plain_c_caller_compiles_and_links():
+    """The header is plain C: a C99 driver (tests/c_harness/harness.c) compiles
+    without warnings and links against the library."""
+    import tempfile
+    with tempfile.TemporaryDirectory() as d:
+        assert os.path.exists(_build_harness(d))
+
+
+def test_fortran_module_binds_every_entry_point():
+    """include/coral_b200.f90 declares a bind(C) interface for every function of
+    the C header, under the same C name."""
+    hdr = open(os.path.join(ROOT, "include", "coral_b200.h")).read()
+    names = set(re.findall(r"\b(coral_[a-z0-9_]+)\s*\(", hdr))
+    f90 = open(os.path.join(ROOT, "include", "coral_b200.f90")).read()
+    bound = set(re.findall(r'bind\(C, name="(coral_[a-z0-9_]+)"\)', f90))
+    assert names == bound, names ^ bound

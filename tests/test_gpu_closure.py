@@ -107,27 +107,30 @@ def test_closure_in_the_time_step():
 
 def test_trained_closure_gains_over_plain_coarse_products():
     """Subgrid data from the solver itself: a fine 48 x 48 x 24 no-slip run
-    (Ra 1e6) truncated to 16 x 16 x 12; the network trained on 6 snapshots cuts
+    (Ra 1e6, CFL-adaptive) truncated to 16 x 16 x 12; the network trained on 6 snapshots cuts
     the error of the coarse quadratic variables against the filtered fine ones
     on 2 held-out snapshots (a-priori gain = 1 - error with / error without)."""
     import torch
     from coral_b200.closure import Closure, subgrid_snapshot
     from coral_b200.solver import PlaneLayer
-    eqf = equations(**{">>Param :: Rayleigh := 1.d5 <<": ">>Param :: Rayleigh := 1.d6 <<"})
-    fine = PlaneLayer(eqf, params(48, 48, 24, dt=2e-5))
-    coarse = PlaneLayer(eqf, params(16, 16, 12, dt=2e-5))
+    from coral_b200.closure_demo import texts
     from coral_b200.initial_conditions import noisy_modes
+    eqf, parf = texts(1e6, (48, 48, 24), dt_max=1e-4, cfl=0.3)
+    _, parc = texts(1e6, (16, 16, 12), dt_max=1e-4, cfl=0.3)
+    fine = PlaneLayer(eqf, parf)
+    coarse = PlaneLayer(eqf, parc)
     noisy_modes(fine, 2 * np.pi, 2 * np.pi, amp=1.0, amp0=0.0, seed=10)
     fine.set_hermitian_kx0(True)
-    fine.march_forward(2e-5, 300)
+    fine.run(300)  # CFL-adaptive time loop
     xs, ys = [], []
     for _ in range(8):
-        fine.march_forward(2e-5, 10)
+        fine.run(10)
         x, y = subgrid_snapshot(fine, coarse)
         xs.append(x)
         ys.append(y)
     x = np.stack(xs).astype(np.float32)
     y = np.stack(ys).astype(np.float32)
+    assert np.all(np.isfinite(x)) and np.all(np.isfinite(y))
     ins = 1.0 / (x[:6].std(axis=(0, 2, 3, 4)) + 1e-30)
     outs = y[:6].std(axis=(0, 2, 3, 4)) + 1e-30
     net = Closure(seed=4)

@@ -44,13 +44,20 @@ def _bench_case(d):
 
 
 def _field_errors(pl, field, zfields, lay):
+    """Relative L2 error per spectral field.  A field whose norm is below 1e-9 of
+    the coupled state's (the mean horizontal flow of no-slip convection, which
+    carries no net momentum: ~1e-12 of the state here) has no significant digits
+    at the 1e-9 level in any finite-precision transform; its error is measured
+    against 1e-9 of the state norm instead."""
     f = pl.get_field(0)
+    scale = 1e-9 * np.linalg.norm(field)
     errs = {}
     for v in range(lay.nV):
         idx = lay.var_pos[v]
-        errs["kxky%d" % v] = _rel(f[..., idx], field[..., idx])
+        b = field[..., idx]
+        errs["kxky%d" % v] = float(np.linalg.norm(f[..., idx] - b) / max(np.linalg.norm(b), scale))
     for s, z in enumerate(zfields):
-        errs["mean%d" % s] = _rel(pl.get_mean_field(s), z)
+        errs["mean%d" % s] = float(np.linalg.norm(pl.get_mean_field(s) - z) / max(np.linalg.norm(z), scale))
     return errs
 
 
