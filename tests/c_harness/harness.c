@@ -57,7 +57,7 @@ int main(int argc, char** argv) {
   }
   double diag[3];
   CHECK(coral_diagnostics(h, diag));
-  printf("steps %d rel_change %.6e cfl_dt %.6e KE %.6e nonfinite %d\n", nsteps, sqrt(num / den), diag[0], diag[1],
+  printf("steps %d rel_change %.17e cfl_dt %.17e KE %.17e nonfinite %d\n", nsteps, sqrt(num / den), diag[0], diag[1],
          (int)diag[2]);
   free(f0);
   free(f1);
