@@ -33,6 +33,8 @@ CONFIGS = {
                          NX=64, NY=64, NZ=48, dt=1e-4, seed=0, Ra=1e5),
     "rbc_96x96x192": dict(eq="rbc_noslip_ra1e8.equations", par="rbc_noslip_ra1e8_96x96x192.parameters.in",
                           NX=96, NY=96, NZ=192, dt=1e-6, seed=2, Ra=1e8),
+    "rbc_128x128x192": dict(eq="rbc_noslip_ra1e8.equations", par="rbc_noslip_ra1e8_128x128x192.parameters.in",
+                            NX=128, NY=128, NZ=192, dt=1e-6, seed=2, Ra=1e8),
     "rbc_192x192x192": dict(eq="rbc_noslip_ra1e8.equations", par="rbc_noslip_ra1e8_192x192x192.parameters.in",
                             NX=192, NY=192, NZ=192, dt=1e-6, seed=2, Ra=1e8),
     "rbc_32x32x192": dict(eq="rbc_noslip_ra1e8.equations", par="rbc_noslip_ra1e8_32x32x192.parameters.in",
@@ -318,6 +320,9 @@ def run_ours(args, cfg):
     eq = open(os.path.join(CONFIG_DIR, cfg["eq"])).read()
     par = open(os.path.join(CONFIG_DIR, cfg["par"])).read()
     pl = PlaneLayer(eq, par, device=dev)
+    for v in args.variant:
+        knob, val = v.split("=")
+        pl.set_variant(knob, int(val))
     make_ic(cfg, pl)
     dt = cfg["dt"]
     s0 = save_state(pl)
@@ -388,7 +393,11 @@ def run_ours(args, cfg):
     diag_bytes = 3 * 8 + 8 + 4  # CFL maxima, KE total, non-finite flag
     e2e = {"value": world * args.steps / e2e_s, "unit": "timesteps/s",
            "h2d_bytes_per_step": state_bytes / args.steps,
-           "d2h_bytes_per_step": state_bytes / args.steps + diag_bytes}
+           "d2h_bytes_per_step": state_bytes / args.steps + diag_bytes,
+           "copies": ("the state (%.2f GB) host->device from page-locked memory before the first step and "
+                      "device->host after the last, amortised over the %d steps (a driver that keeps the state "
+                      "resident, as Coral's does); the CFL/KE diagnostics (%d bytes) device->host every step"
+                      % (state_bytes / 1e9, args.steps, diag_bytes))}
 
     # the split-precision form on the same handle and initial state
     split = None
@@ -471,6 +480,7 @@ def run_ours(args, cfg):
         "cpu_baseline": cpu,
         "clocks": clocks,
         "state_ok": not diag["nonfinite"],
+        "variants": dict(v.split("=") for v in args.variant),
         "split": split,
     }
     if rank == 0:
@@ -772,6 +782,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-split", action="store_true", help="skip the split-precision leg")
+    ap.add_argument("--variant", action="append", default=[], metavar="KNOB=0|1",
+                    help="pin a kernel variant of the autotuner (coral_set_variant); repeatable")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

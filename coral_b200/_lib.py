@@ -77,6 +77,7 @@ SIGNATURES = {
     "coral_closure_infer": (ctypes.c_int, [_P, _P, ctypes.c_int, ctypes.c_int, ctypes.c_int, _P, _P]),
     "coral_closure_attach": (ctypes.c_int, [_P, _P]),
     "coral_autotune": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
+    "coral_set_variant": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_int]),
 }
 
 _lib = None

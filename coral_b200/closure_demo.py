@@ -8,7 +8,9 @@ Ra = 1e7, Pr = 1, no-slip, box 2 pi x 2 pi x 1, trained on snapshots of a
 256^2 x 128 run truncated to the coarse modes (coral_b200.closure.subgrid_snapshot).
 
   1. fine run: seeded form of the reference's default initial condition
-     (amplitude --amp), CFL-adaptive time loop (CFL_C 0.3, dt_max 1e-4), the
+     (amplitude --amp, small: the instability grows it; large random states of
+     all six variables are far from balance and blow up), CFL-adaptive time
+     loop (CFL_C 0.3, dt_max 1e-4), the
      kx = 0 line kept Hermitian; after --spinup time units one snapshot every
      --every steps;
   2. training: the first 80% of the snapshots, Adam, random batches of points;
@@ -91,7 +93,7 @@ def main(argv=None):
     ap.add_argument("--fine", type=int, nargs=3, default=(256, 256, 128))
     ap.add_argument("--coarse", type=int, nargs=3, default=(64, 64, 48))
     ap.add_argument("--ra", type=float, default=1e7)
-    ap.add_argument("--amp", type=float, default=1.0)
+    ap.add_argument("--amp", type=float, default=1e-6)
     ap.add_argument("--spinup", type=float, default=0.02)
     ap.add_argument("--snapshots", type=int, default=40)
     ap.add_argument("--every", type=int, default=40)

@@ -182,6 +182,9 @@ struct coral_handle {
     int fwd_y_grid = 0;     // forward y pass: 0 persistent pipelined, 1 one CTA per tile
     int generic_tiles = 0;  // operator tile kernels: 0 compiled group layouts, 1 run-time forms
     int subst_rt = 0;       // band substitution: 0 compiled band, 1 run-time band
+    int z_batch6 = 1;       // fused z pass: 1 forward batches of 6 lines (3 CTAs per SM), 0 of 9 lines
+    int inv_x_tiles = 1;    // inverse x pass: 1 one CTA per tile, 0 persistent pipelined
+    int factor_window = 1;  // band factorisation: 1 shared-memory window, 0 in place in global memory
   } tune;
   // learned closure (not owned) and its output [9][y][x][z]
   coral_closure* closure = nullptr;
@@ -804,7 +807,7 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
   {
     StateSet st = state_set(h, i == 0);
     B(0); launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream); E();
-    B(1); launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream, h->tune.x_plan); E();
+    B(1); launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream, h->tune.x_plan, h->tune.inv_x_tiles); E();
     // the CFL maxima reported after a step are those of its last stage's fields
     // (each stage's evaluation replaces them): only the last stage computes them
     if (last) CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
@@ -842,7 +845,7 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
     QuadDesc q = h->quads;
     q.ts_partial = (i == 0 && q.ts_n > 0) ? h->ts_partial : nullptr;
     launch_z_fused(d, h->nF, q, h->Y2, h->Y2, h->pz, h->dct_tw, h->d_wz, h->d_wzinv,
-                   last ? h->cfl_bits : nullptr, i == 0 ? h->ke_partial : nullptr, h->stream);
+                   last ? h->cfl_bits : nullptr, i == 0 ? h->ke_partial : nullptr, h->stream, h->tune.z_batch6);
   }
   E();
   B(4); launch_fwd_x(d, h->nQ, h->Y2, h->Y1, h->px, h->stream, h->tune.x_plan); E();
@@ -991,6 +994,7 @@ void factorize(coral_handle* h, double dt) {
     fa.cls_row = k.cls_row;
     fa.col_pos = k.col_pos;
     fa.tpb = k.work2 != nullptr;
+    fa.window = h->tune.factor_window;
     fa.cmask = k.cmask;
     fa.lmask = k.lmask;
     fa.umask = k.umask;
@@ -1784,6 +1788,40 @@ int coral_var_positions(coral_handle* h, int isys, int ivar, int* positions, int
   });
 }
 
+namespace {
+// the kernel variants of the step: name, the handle's switch, its default (a)
+// and alternative (b) values with their names, and the timed phases they affect
+struct Knob { const char* name; int* var; int a, b; const char* na; const char* nb; std::vector<int> phases; };
+std::vector<Knob> knobs_of(coral_handle* h) {
+  return {{"x_fft_plan", &h->tune.x_plan, 1, 0, "two-pass", "three-pass", {1, 4}},
+          {"fwd_y_pass", &h->tune.fwd_y_grid, 0, 1, "persistent-pipelined", "one-CTA-per-tile", {5}},
+          {"operator_tiles", &h->tune.generic_tiles, 0, 1, "compiled-groups", "run-time-forms", {7, 10}},
+          {"band_substitution", &h->tune.subst_rt, 0, 1, "compiled-band", "run-time-band", {9}},
+          {"z_pass", &h->tune.z_batch6, 1, 0, "6-line-batches", "9-line-batches", {3}},
+          {"inv_x_pass", &h->tune.inv_x_tiles, 1, 0, "one-CTA-per-tile", "persistent-pipelined", {1}},
+          // not timed by the autotuner (a factorisation, not a step phase)
+          {"band_factor", &h->tune.factor_window, 1, 0, "shared-memory-window", "in-place", {}}};
+}
+}  // namespace
+
+int coral_set_variant(coral_handle* h, const char* knob, int value) {
+  return guarded(h, [&] {
+    if (!knob) throw CoralError(CORAL_EBADARG, "set_variant: knob name is NULL");
+    for (auto& kb : knobs_of(h)) {
+      if (std::strcmp(kb.name, knob) != 0) continue;
+      if (value != 0 && value != 1) throw CoralError(CORAL_EBADARG, "set_variant: value is 0 (default) or 1 (alternative)");
+      *kb.var = value ? kb.b : kb.a;
+      if (kb.var == &h->tune.factor_window && h->dt_factored >= 0.0) factorize(h, h->dt_factored);
+      if (h->graph) {
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+      }
+      return;
+    }
+    throw CoralError(CORAL_EBADARG, std::string("set_variant: unknown knob ") + knob);
+  });
+}
+
 int coral_autotune(coral_handle* h, double dt, int repeats, char* report, int n) {
   return guarded(h, [&] {
     if (!(dt > 0.0) || repeats < 1) throw CoralError(CORAL_EBADARG, "autotune: dt > 0 and repeats >= 1");
@@ -1822,14 +1860,10 @@ int coral_autotune(coral_handle* h, double dt, int repeats, char* report, int n)
       }
       return best;
     };
-    struct Knob { const char* name; int* var; int a, b; const char* na; const char* nb; std::vector<int> phases; };
-    std::vector<Knob> knobs = {
-        {"x_fft_plan", &h->tune.x_plan, 1, 0, "two-pass", "three-pass", {1, 4}},
-        {"fwd_y_pass", &h->tune.fwd_y_grid, 0, 1, "persistent-pipelined", "one-CTA-per-tile", {5}},
-        {"operator_tiles", &h->tune.generic_tiles, 0, 1, "compiled-groups", "run-time-forms", {7, 10}},
-        {"band_substitution", &h->tune.subst_rt, 0, 1, "compiled-band", "run-time-band", {9}}};
+    std::vector<Knob> knobs = knobs_of(h);
     std::string rep;
     for (auto& kb : knobs) {
+      if (kb.phases.empty()) continue;
       double ta = 0, tb = 0;
       *kb.var = kb.a;
       if (kb.phases.size() == 2) ta = time_phases({kb.phases[0], kb.phases[1]});

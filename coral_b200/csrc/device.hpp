@@ -100,7 +100,10 @@ struct Dims {
 void launch_inv_y(const Dims& d, int nf, const FullVarDev* fv, StateSet st, const double2* plain_spec,
                   const double* kx, const double* ky, double2* Y1, const FftPlan& py, cudaStream_t s);
 // pv: FFT plan of the compiled lengths, 1 = two passes (576 = 24 x 24, 288 = 18 x 16), 0 = three passes
-void launch_inv_x(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s, int pv = 1);
+// tiles = 1: one CTA per tile; 0: the persistent pipelined kernel (compiled
+// lengths with a two-pass plan and pv = 1; others fall back to one CTA per tile)
+void launch_inv_x(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s, int pv = 1,
+                  int tiles = 1);
 // z DCT-III; cfl: maxima of |u|, |v|, |w|/wz written (as uint64 bit patterns) to cfl_bits when non-null
 void launch_inv_z(const Dims& d, int nf, const double* Y2, double* phys, const FftPlan& pz,
                   const double2* dct_tw, const double* wz, unsigned long long* cfl_bits, cudaStream_t s);
@@ -112,7 +115,7 @@ void launch_fwd_z(const Dims& d, int nf, const QuadDesc& q, const double* phys, 
 // wzinv[z] = 1 / wz[z]
 void launch_z_fused(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* Q2, const FftPlan& pz,
                     const double2* dct_tw, const double* wz, const double* wzinv, unsigned long long* cfl_bits,
-                    double* ke_partial, cudaStream_t s);
+                    double* ke_partial, cudaStream_t s, int batch6 = 0);
 void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s, int pv = 1);
 // grid_variant = 1: one CTA per tile instead of the persistent pipelined kernel
 void launch_fwd_y(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
@@ -270,6 +273,7 @@ struct FactorArgs {
   const int* cls_row;    // [ncls*Tc] equation row of a class position, -1 = identity padding
   const int* col_pos;    // [T] class position of a variable column
   int tpb;               // 1: interleaved thread-per-block factor layout (see SolveArgs::work2)
+  int window;            // thread-per-block layout: 1 shared-memory band window, 0 in place in global memory
   // thread-per-block layout: per class column j, the band rows nonzero in any
   // block (cmask, bit r = band row r), and derived from it the L rows
   // (lmask[j], bit i = row kl+ku+1+i of column j) and the U entries of row j

@@ -315,9 +315,30 @@ __device__ __forceinline__ void dft(double2 (&x)[R]) {
   }
 }
 
+// Twiddles of the second pass of a two-pass plan N = R0 x R1, laid out [k][r - 1]
+// (k < R0, 1 <= r < R1): t[k (R1 - 1) + r - 1] = exp(-2 pi i r k / N).  For a
+// fixed r, consecutive k are R1 - 1 16-byte words apart, an odd number for the
+// even R1 of the two-pass plans, so the 16-byte reads of 8 consecutive k fall in
+// 8 distinct bank groups (the N-entry table read at r k conflicts up to 8-way).
+template <int N, int PV>
+__host__ __device__ constexpr int tw_pass2_len() {
+  return plan_of(N, PV).nst == 2 ? plan_of(N, PV).r[0] * (plan_of(N, PV).r[1] - 1) : 0;
+}
+template <int N, int PV>
+__device__ __forceinline__ void build_tw_pass2(double2* t, const double2* tw) {
+  constexpr PlanR P = plan_of(N, PV);
+  static_assert(P.nst == 2 && (P.r[1] % 2) == 0, "two-pass plan with an even second radix");
+  constexpr int R0 = P.r[0], R1 = P.r[1];
+  for (int i = threadIdx.x; i < R0 * (R1 - 1); i += blockDim.x) {
+    const int k = i / (R1 - 1), r = i - k * (R1 - 1) + 1;
+    t[i] = tw[r * k];  // N = R0 R1: the pass's twiddle stride is 1
+  }
+}
+
 // One in-place pass of radix R over nl lines (line stride LS) by NT threads;
 // NLMAX bounds nl (registers hold ceil(NLMAX N / (R NT)) butterflies per thread).
-template <int N, int R, int Ns, bool INV, int NT, int NLMAX>
+// TWL: tw is the [k][r - 1] table of build_tw_pass2 (second pass of a two-pass plan).
+template <int N, int R, int Ns, bool INV, int NT, int NLMAX, bool TWL = false>
 __device__ __forceinline__ void fft_pass(double2* A, int nl, int LS, const double2* __restrict__ tw) {
   constexpr int NB = N / R;               // butterflies per line
   constexpr int TS = N / (Ns * R);        // twiddle stride
@@ -336,7 +357,7 @@ __device__ __forceinline__ void fft_pass(double2* A, int nl, int LS, const doubl
         const int k = j % Ns;
 #pragma unroll
         for (int r = 1; r < R; ++r) {
-          double2 w = tw[r * k * TS];
+          double2 w = TWL ? tw[k * (R - 1) + r - 1] : tw[r * k * TS];
           if (INV) w = cconj(w);
           v[i][r] = cmul(v[i][r], w);
         }
@@ -388,13 +409,14 @@ __device__ __forceinline__ void fft_pass_first(double2* A, int nl, int LS, Load&
   __syncthreads();
 }
 
-template <int N, int S, int Ns, bool INV, int NT, int NLMAX, int PV = 0>
+template <int N, int S, int Ns, bool INV, int NT, int NLMAX, int PV = 0, bool TWL = false>
 __device__ __forceinline__ void fft_passes(double2* A, int nl, int LS, const double2* tw) {
   constexpr PlanR P = plan_of(N, PV);
+  static_assert(!TWL || P.nst == 2, "the pass-2 twiddle table belongs to two-pass plans");
   if constexpr (S < P.nst) {
     constexpr int R = P.r[S];
-    fft_pass<N, R, Ns, INV, NT, NLMAX>(A, nl, LS, tw);
-    fft_passes<N, S + 1, Ns * R, INV, NT, NLMAX, PV>(A, nl, LS, tw);
+    fft_pass<N, R, Ns, INV, NT, NLMAX, TWL>(A, nl, LS, tw);
+    fft_passes<N, S + 1, Ns * R, INV, NT, NLMAX, PV, TWL>(A, nl, LS, tw);
   }
 }
 
@@ -404,7 +426,8 @@ __device__ __forceinline__ void fft_passes(double2* A, int nl, int LS, const dou
 // before (inputs written) and may read the result directly after.
 // The same with the inputs produced by ld(line, k) (see fft_pass_first); the
 // caller need not synchronise before.  Runtime plans stage the inputs in A first.
-template <int NC, bool INV, int NT, int NLMAX, bool LINE_FAST = false, int PV = 0, class Load>
+// TWL: p.tw is the table of build_tw_pass2 (compiled two-pass plans only).
+template <int NC, bool INV, int NT, int NLMAX, bool LINE_FAST = false, int PV = 0, bool TWL = false, class Load>
 __device__ __forceinline__ double2* fft_lines_ld(double2* A, double2* B, int nl, int LS, const FftPlan& p,
                                                  Load&& ld) {
   if constexpr (NC == 0) {
@@ -418,7 +441,7 @@ __device__ __forceinline__ double2* fft_lines_ld(double2* A, double2* B, int nl,
     constexpr PlanR P = plan_of(NC, PV);
     static_assert(P.nst > 0, "transform length must be 2^a 3^b");
     fft_pass_first<NC, P.r[0], INV, NT, NLMAX, LINE_FAST>(A, nl, LS, ld);
-    fft_passes<NC, 1, P.r[0], INV, NT, NLMAX, PV>(A, nl, LS, p.tw);
+    fft_passes<NC, 1, P.r[0], INV, NT, NLMAX, PV, TWL>(A, nl, LS, p.tw);
     return A;
   }
 }

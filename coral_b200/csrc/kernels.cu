@@ -227,6 +227,80 @@ __global__ void __launch_bounds__(kThreadsX, hot_min_blocks(kThreadsX)) k_inv_x(
   }
 }
 
+// The same pass for compiled lengths with the two-pass plan, as a persistent
+// kernel: each CTA walks the tiles (full variable, block of kNB2 Chebyshev rows,
+// y) with a stride of the grid size; the next tile's input rows (kx < NX/2,
+// kNB2 coefficients each) are copied into a staging buffer with cp.async while
+// the current tile's second FFT pass and stores run (the first pass reads the
+// staging buffer and frees it).  Staging rows are kNB2 + 1 16-byte words apart,
+// so that the first pass's reads (4 lines x 2 positions a quarter warp) fall in
+// distinct bank groups; the second pass reads its twiddles from the
+// conflict-free table of build_tw_pass2.  Shared memory (line buffer, staging,
+// table) admits 3 CTAs per SM at NXAA = 576: registers are sized for 3.
+constexpr int kStgX = kNB2 + 1;
+#define kThreadsXP xy_threads(NF, kNB2 / 2, 1)
+template <int NF>
+__global__ void __launch_bounds__(kThreadsXP, 3) k_inv_x_pipe(Dims d, int nf, const double2* Y1,
+                                                                                      double* Y2, FftPlan px) {
+  constexpr int NT = kThreadsXP, NXA = NF, NP = kNB2 / 2;
+  constexpr PlanR P = plan_of(NF, 1);
+  constexpr int kTw2 = tw_pass2_len<NF, 1>();
+  static_assert(kTw2 > 0, "two-pass plan");
+  extern __shared__ double2 sm[];
+  __shared__ double2 s_tw[kTw2];
+  const int LS = NXA + kPadXY;
+  double2* A = sm;               // NP lines, stride LS
+  double2* stg = A + NP * LS;    // staged input [kx][kStgX]
+  const int NXH = d.NXH, NZ = d.NZ;
+  const int nnb = (NZ + kNB2 - 1) / kNB2;
+  const int ntiles = nf * nnb * d.NYA;
+  build_tw_pass2<NF, 1>(s_tw, px.tw);  // read after the loop's first barrier
+  auto issue = [&](int tile) {
+    if (tile < ntiles) {
+      const int f = tile % nf, r = tile / nf, nb = r % nnb, y = r / nnb, n0 = nb * kNB2;
+      const double2* src = Y1 + ((size_t)f * d.NYA + y) * NXH * NZ + n0;
+      for (int e = threadIdx.x; e < NXH * kNB2; e += NT) {
+        const int kx = e / kNB2, ln = e - kx * kNB2;
+        const bool ok = n0 + ln < NZ;
+        cp_async16z(stg + kx * kStgX + ln, ok ? src + (size_t)kx * NZ + ln : Y1, ok);
+      }
+    }
+    cp_async_commit();
+  };
+  issue(blockIdx.x);
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int f = tile % nf, r = tile / nf, nb = r % nnb, y = r / nnb, n0 = nb * kNB2;
+    cp_async_wait<0>();
+    __syncthreads();
+    // position p of line m (Chebyshev pair 2m, 2m+1 of the block): as in k_inv_x
+    auto ld = [&](int m, int p) -> double2 {
+      const bool lo = p < NXH, hi = p > NXA - NXH;
+      if (!lo && !hi) return zero2();
+      const int kx = lo ? p : NXA - p;
+      const double2 a = stg[kx * kStgX + 2 * m], b = stg[kx * kStgX + 2 * m + 1];
+      if (p == 0) return make_double2(a.x, b.x);
+      return lo ? make_double2(a.x - b.y, a.y + b.x) : make_double2(a.x + b.y, b.x - a.y);
+    };
+    fft_pass_first<NF, P.r[0], true, NT, NP, true>(A, NP, LS, ld);  // ends with a barrier
+    issue(tile + gridDim.x);
+    fft_passes<NF, 1, P.r[0], true, NT, NP, 1, true>(A, NP, LS, s_tw);
+    double* dst0 = Y2 + ((size_t)f * d.NYA + y) * NXA * NZ;
+    for (int idx = threadIdx.x; idx < NP * NXA; idx += NT) {
+      const int m = idx % NP, x = idx / NP, na = n0 + 2 * m;
+      const double2 z = A[m * LS + x];
+      double* dst = dst0 + (size_t)x * NZ + na;
+      if (na + 1 < NZ && (NZ & 1) == 0) {
+        *reinterpret_cast<double2*>(dst) = z;  // na and NZ even: 16-byte aligned
+      } else {
+        if (na < NZ) dst[0] = z.x;
+        if (na + 1 < NZ) dst[1] = z.y;
+      }
+    }
+    __syncthreads();  // A is rewritten by the next tile's first pass
+  }
+  cp_async_wait<0>();
+}
+
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long* addr, double v) {
   atomicMax(addr, (unsigned long long)__double_as_longlong(v));
 }
@@ -403,14 +477,20 @@ __host__ __device__ constexpr int z_threads(int N, int nl) {
 }
 constexpr int kZPairs = 2;               // x-column pairs per CTA
 constexpr int kZLines = 4 * kZPairs;     // lines per inverse FFT batch (4 full variables x 2 pairs)
-constexpr int kZFwd = 9;                 // lines per forward FFT batch ((quadratic variable, pair) lines)
-__host__ __device__ constexpr int z_threads_fused(int N) {
-  return z_threads(N, kZLines) > z_threads(N, kZFwd) ? z_threads(N, kZLines) : z_threads(N, kZFwd);
+// lines per forward FFT batch ((quadratic variable, pair) lines), the kernel's
+// FB: 9 (two batches for 9 quadratic variables; 2 CTAs per SM at NZAA = 288) or
+// 6 (three batches; shared memory and registers for 3 CTAs per SM)
+constexpr int kZFwd = 9;
+__host__ __device__ constexpr int z_threads_fused(int N, int fb) {
+  return z_threads(N, kZLines) > z_threads(N, fb) ? z_threads(N, kZLines) : z_threads(N, fb);
 }
-#define kThreadsZF z_threads_fused(NF)
+__host__ __device__ constexpr int z_min_blocks(int N, int fb) {
+  return fb < kZFwd ? 3 : hot_min_blocks(z_threads_fused(N, fb));
+}
+#define kThreadsZF z_threads_fused(NF, FB)
 
-template <int NF>
-__global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fused(Dims d, int nf, QuadDesc q, const double* Y2,
+template <int NF, int FB>
+__global__ void __launch_bounds__(kThreadsZF, z_min_blocks(NF, FB)) k_z_fused(Dims d, int nf, QuadDesc q, const double* Y2,
                                                                        double* Q2, FftPlan pz, const double2* dct_tw,
                                                                        const double* wz, const double* wzinv,
                                                                        unsigned long long* cfl_bits, double* ke_partial) {
@@ -428,15 +508,20 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
     qv[0][threadIdx.x] = q.v1[threadIdx.x];
     qv[1][threadIdx.x] = q.v2[threadIdx.x];
   }
-  // compiled lengths: the FFT and DCT twiddles in shared memory
-  __shared__ double2 s_tw[NF ? NF : 1], s_dtw[NF ? NF : 1];
+  // compiled lengths: the FFT and DCT twiddles in shared memory; with a
+  // two-pass plan the FFT twiddles as the bank-conflict-free pass-2 table
+  constexpr int kTw2 = NF ? tw_pass2_len<NF, kPlanHot>() : 0;
+  constexpr bool kTwl = kTw2 > 0;
+  __shared__ double2 s_tw[kTwl ? kTw2 : (NF ? NF : 1)], s_dtw[NF ? NF : 1];
   FftPlan pzl = pz;
   const double2* dtw = dct_tw;
   if constexpr (NF != 0) {
-    for (int i = threadIdx.x; i < NF; i += blockDim.x) {
-      s_tw[i] = pz.tw[i];
-      s_dtw[i] = dct_tw[i];
+    if constexpr (kTwl) {
+      build_tw_pass2<NF, kPlanHot>(s_tw, pz.tw);
+    } else {
+      for (int i = threadIdx.x; i < NF; i += blockDim.x) s_tw[i] = pz.tw[i];
     }
+    for (int i = threadIdx.x; i < NF; i += blockDim.x) s_dtw[i] = dct_tw[i];
     pzl.tw = s_tw;
     dtw = s_dtw;
   }
@@ -444,8 +529,8 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
   // x0 + 2p (re) and x0 + 2p + 1 (im))
   auto col_ok = [&](int c) { return x0 + c < d.NXA; };
   double2* Fv = sm;                   // nf * kZPairs lines of the full variables
-  double2* A = Fv + nf * kZPairs * N; // kZFwd lines of quadratic variables
-  double2* B = A + kZFwd * N;         // runtime plan only (max(kZLines, kZFwd) lines)
+  double2* A = Fv + nf * kZPairs * N; // FB lines of quadratic variables
+  double2* B = A + FB * N;            // runtime plan only (max(kZLines, FB) lines)
   // ---- inverse: X_n and X_{N-n} of both columns, twiddled, packed as va + i vb,
   //      produced inside the first FFT pass ----
   __syncthreads();  // qv
@@ -464,7 +549,7 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
       const double2 vb = cmul(w, make_double2(b0, -b1));
       return make_double2(va.x - vb.y, va.y + vb.x);
     };
-    const double2* R = fft_lines_ld<NF, true, NT, kZLines, false, kPlanHot>(Fv + l0 * N, B, nl, N, pzl, ld);
+    const double2* R = fft_lines_ld<NF, true, NT, kZLines, false, kPlanHot, kTwl>(Fv + l0 * N, B, nl, N, pzl, ld);
     if (R != Fv + l0 * N) {  // runtime plan with the result in the scratch lines
       for (int idx = threadIdx.x; idx < nl * N; idx += blockDim.x) Fv[l0 * N + idx] = R[idx];
       __syncthreads();
@@ -574,9 +659,9 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
       }
     }
   }
-  // ---- products and forward transforms, kZFwd (quadratic variable, pair) lines a batch ----
-  for (int l0 = 0; l0 < nq * kZPairs; l0 += kZFwd) {
-    const int nc = min(kZFwd, nq * kZPairs - l0);
+  // ---- products and forward transforms, FB (quadratic variable, pair) lines a batch ----
+  for (int l0 = 0; l0 < nq * kZPairs; l0 += FB) {
+    const int nc = min(FB, nq * kZPairs - l0);
     // products formed inside the first FFT pass
     auto ld = [&](int line, int m) -> double2 {
       const int lg = l0 + line, qg = lg / kZPairs, pr = lg - qg * kZPairs;
@@ -593,19 +678,29 @@ __global__ void __launch_bounds__(kThreadsZF, hot_min_blocks(kThreadsZF)) k_z_fu
       }
       return make_double2(pa, pb);
     };
-    const double2* R = fft_lines_ld<NF, false, NT, kZFwd, false, kPlanHot>(A, B, nc, N, pzl, ld);
-    for (int idx = threadIdx.x; idx < nc * NZ; idx += blockDim.x) {
-      const int li = idx / NZ, n = idx - li * NZ;
+    const double2* R = fft_lines_ld<NF, false, NT, FB, false, kPlanHot, kTwl>(A, B, nc, N, pzl, ld);
+    // coefficient n of the two packed columns from Z = R[n] and conj(R[N - n]);
+    // coefficients n and N - n share those two loads: items n = 0 .. N/2 write
+    // n (< NZ) and, for 0 < n < N/2, N - n when it is < NZ
+    const int NH = N / 2 + 1;
+    for (int idx = threadIdx.x; idx < nc * NH; idx += blockDim.x) {
+      const int li = idx / NH, n = idx - li * NH;
       const int lg = l0 + li, qg = lg / kZPairs, pr = lg - qg * kZPairs;
-      const double2 Z = R[li * N + n];
-      const double2 Zc = cconj(R[li * N + (n == 0 ? 0 : N - n)]);
-      const double2 va = make_double2(0.5 * (Z.x + Zc.x), 0.5 * (Z.y + Zc.y));
-      const double2 dd = csub(Z, Zc);
-      const double2 vb = make_double2(0.5 * dd.y, -0.5 * dd.x);  // (Z - Zc) / 2i
-      const double2 w = dtw[n];                                   // exp(-i pi n / 2N)
+      const int n2 = (n == 0) ? 0 : N - n;
+      const double2 Z = R[li * N + n], W = R[li * N + n2];
       double* dst = Q2 + qg * vstride + col0 + (size_t)(2 * pr) * NZ;
-      if (col_ok(2 * pr)) dst[n] = 2.0 * (w.x * va.x - w.y * va.y);
-      if (col_ok(2 * pr + 1)) dst[NZ + n] = 2.0 * (w.x * vb.x - w.y * vb.y);
+      const bool oa = col_ok(2 * pr), ob = col_ok(2 * pr + 1);
+      auto out = [&](int k, double2 P, double2 Pm) {  // coefficient k from R[k] = P, R[N - k] = Pm
+        const double2 Pc = cconj(Pm);
+        const double2 va = make_double2(0.5 * (P.x + Pc.x), 0.5 * (P.y + Pc.y));
+        const double2 dd = csub(P, Pc);
+        const double2 vb = make_double2(0.5 * dd.y, -0.5 * dd.x);  // (P - Pc) / 2i
+        const double2 w = dtw[k];                                   // exp(-i pi k / 2N)
+        if (oa) dst[k] = 2.0 * (w.x * va.x - w.y * va.y);
+        if (ob) dst[NZ + k] = 2.0 * (w.x * vb.x - w.y * vb.y);
+      };
+      if (n < NZ) out(n, Z, W);
+      if (n > 0 && n2 != n && n2 < NZ) out(n2, W, Z);
     }
     __syncthreads();  // A is refilled by the next batch
   }
@@ -1363,9 +1458,10 @@ constexpr int kTpbThreads = 128;
 
 // DGBTF2 on one block, in the interleaved layout: the algorithm, pivot choice
 // and update order of k_factor_real.
-__global__ void __launch_bounds__(kTpbThreads) k_factor_tpb(FactorArgs a) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= a.ncls * a.nact) return;
+// Assembly of block b (system b / ncls, class b % ncls) of M - dt a(0,0) L into
+// its interleaved band storage: zero fill, then every operator entry added in
+// row order (M before L, slots in order).
+__device__ void assemble_tpb(const FactorArgs& a, int b) {
   const int sys = b / a.ncls, cls = b - sys * a.ncls;
   const int T = a.Tc, kl = a.kl, ku = a.ku, kv = kl + ku, ldab = a.ldab;
   const int sid = a.act_list[sys];
@@ -1405,6 +1501,21 @@ __global__ void __launch_bounds__(kTpbThreads) k_factor_tpb(FactorArgs a) {
       }
     }
   }
+}
+
+__global__ void __launch_bounds__(kTpbThreads) k_assemble_tpb(FactorArgs a) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b < a.ncls * a.nact) assemble_tpb(a, b);
+}
+
+__global__ void __launch_bounds__(kTpbThreads) k_factor_tpb(FactorArgs a) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= a.ncls * a.nact) return;
+  assemble_tpb(a, b);
+  const int sys = b / a.ncls;
+  const int T = a.Tc, kl = a.kl, ku = a.ku, kv = kl + ku, ldab = a.ldab;
+  double* F = a.abr + (size_t)(b >> 5) * T * ldab * 32 + (b & 31);
+  auto at = [&](int j, int r) -> double& { return F[((size_t)j * ldab + r) * 32]; };
   unsigned char* P = a.dpiv + (size_t)(b >> 5) * T * 32 + (b & 31);
   int ju = 0, info = 0;
   for (int j = 0; j < T; ++j) {
@@ -1440,6 +1551,107 @@ __global__ void __launch_bounds__(kTpbThreads) k_factor_tpb(FactorArgs a) {
     }
     at(j, kv) = r;
   }
+  if (info) atomicMax(a.info + sys, info);
+}
+
+// DGBTF2 on one block (after k_assemble_tpb) with its active band columns in
+// shared memory: the algorithm, pivot choice and update order of k_factor_tpb
+// (the same factors bit for bit), but every factor entry is read from and
+// written to global memory once instead of being updated there up to kl times.
+// At step j the window holds columns j .. j + W - 1 (W = kl + ku + 1: a step
+// touches columns j .. ju, and ju <= j + ku + kl) and column j + W is in
+// flight (cp.async, issued one step ahead into the slot column j - 1 left): a
+// circular buffer of W + 1 slots.  Column j, final after step j, is written
+// back in place.  Each thread's slots are (W + 1) ldab doubles in its own column
+// of shared memory (slot stride blockDim.x <= 32), so the warp's accesses are
+// conflict-free and its global accesses the 256-byte rows of the interleaved
+// layout.  A step's multipliers and each updated column segment are staged in
+// registers (kl <= kFacKl), so that its shared-memory loads issue together.
+constexpr int kFacKl = 16;
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__global__ void __launch_bounds__(32) k_factor_win(FactorArgs a) {
+  extern __shared__ double fwin[];
+  const int NT = blockDim.x;
+  const int b = blockIdx.x * NT + threadIdx.x;
+  if (b >= a.ncls * a.nact) return;  // no barriers below
+  const int sys = b / a.ncls;
+  const int T = a.Tc, kl = a.kl, ku = a.ku, kv = kl + ku, ldab = a.ldab, W = kl + ku + 1, W1 = W + 1;
+  double* F = a.abr + (size_t)(b >> 5) * T * ldab * 32 + (b & 31);
+  double* wz = fwin + threadIdx.x;
+  int j0 = 0, s0 = 0;  // the window's first column and its slot
+  auto slot = [&](int c) { const int q = s0 + (c - j0); return q >= W1 ? q - W1 : q; };
+  auto at = [&](int c, int r) -> double& { return wz[(slot(c) * ldab + r) * NT]; };
+  auto fetch = [&](int c, int sl) {  // column c of the block into slot sl
+    if (c < T) {
+      const double* src = F + (size_t)c * ldab * 32;
+      double* dst = wz + (size_t)sl * ldab * NT;
+      for (int r = 0; r < ldab; ++r) cp_async8(dst + r * NT, src + (size_t)r * 32);
+    }
+  };
+  for (int c = 0; c < W; ++c) fetch(c, c);
+  cp_async_commit();
+  unsigned char* P = a.dpiv + (size_t)(b >> 5) * T * 32 + (b & 31);
+  int ju = 0, info = 0;
+  for (int j = 0; j < T; ++j) {
+    j0 = j;
+    fetch(j + W, s0 == 0 ? W1 - 1 : s0 - 1);  // the slot column j - 1 left (the spare at j = 0)
+    cp_async_commit();
+    cp_async_wait<1>();  // columns up to j + W - 1 have landed
+    const int km = min(kl, T - 1 - j);
+    int jp = 0;
+    double mag = fabs(at(j, kv));
+    for (int i = 1; i <= km; ++i) {
+      const double m2 = fabs(at(j, kv + i));
+      if (m2 > mag) { mag = m2; jp = i; }  // first maximum
+    }
+    P[(size_t)j * 32] = (unsigned char)jp;
+    if (at(j, kv + jp) == 0.0) {
+      if (info == 0) info = j + 1;
+    } else {
+      ju = max(ju, min(j + ku + jp, T - 1));
+      if (jp != 0) {
+        for (int c = j; c <= ju; ++c) {
+          double& p1 = at(c, kv + j + jp - c);
+          double& p0 = at(c, kv + j - c);
+          const double t0 = p0, t1 = p1;
+          p0 = t1;
+          p1 = t0;
+        }
+      }
+      const double r = 1.0 / at(j, kv);
+      if (km > 0) {
+        double m[kFacKl];
+        double* cj = wz + ((size_t)s0 * ldab + kv + 1) * NT;
+#pragma unroll
+        for (int i = 0; i < kFacKl; ++i) m[i] = (i < km) ? cj[i * NT] : 0.0;
+#pragma unroll
+        for (int i = 0; i < kFacKl; ++i)
+          if (i < km) {
+            m[i] *= r;
+            cj[i * NT] = m[i];
+          }
+        for (int c = j + 1; c <= ju; ++c) {
+          double* col = wz + ((size_t)slot(c) * ldab + kv + j - c) * NT;
+          double x[kFacKl + 1];
+#pragma unroll
+          for (int i = 0; i <= kFacKl; ++i) x[i] = (i <= km) ? col[i * NT] : 0.0;
+#pragma unroll
+          for (int i = 0; i < kFacKl; ++i)
+            if (i < km) col[(1 + i) * NT] = x[1 + i] - m[i] * x[0];
+        }
+      }
+      at(j, kv) = r;
+    }
+    // column j is final
+    const double* cw = wz + (size_t)s0 * ldab * NT;
+    double* dst = F + (size_t)j * ldab * 32;
+    for (int q = 0; q < ldab; ++q) dst[(size_t)q * 32] = cw[q * NT];
+    s0 = (s0 + 1 == W1) ? 0 : s0 + 1;
+  }
+  cp_async_wait<0>();
   if (info) atomicMax(a.info + sys, info);
 }
 
@@ -2445,7 +2657,20 @@ struct InvX {
     dim3 g(nf, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
     k_inv_x<NF, PV><<<g, kThreadsX, sm, s>>>(d, Y1, Y2, px);
   }
-  static void run(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, int pv, cudaStream_t s) {
+  static void run(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, int pv, int tiles,
+                  cudaStream_t s) {
+    if constexpr (NF != 0 && tw_pass2_len<NF, 1>() > 0) {
+      if (pv && !tiles) {
+        // persistent pipelined kernel: as many CTAs as fit on the device at once
+        const size_t sm = ((kNB2 / 2) * (size_t)(NF + kPadXY) + (size_t)d.NXH * kStgX) * sizeof(double2);
+        set_smem(k_inv_x_pipe<NF>, sm);
+        static int nct = 0;
+        if (!nct) nct = persistent_ctas(k_inv_x_pipe<NF>, kThreadsXP, sm);
+        const int ntiles = nf * ((d.NZ + kNB2 - 1) / kNB2) * d.NYA;
+        k_inv_x_pipe<NF><<<std::min(nct, ntiles), kThreadsXP, sm, s>>>(d, nf, Y1, Y2, px);
+        return;
+      }
+    }
     if (pv) go<1>(d, nf, Y1, Y2, px, s);
     else go<0>(d, nf, Y1, Y2, px, s);
   }
@@ -2472,19 +2697,26 @@ struct FwdZ {
 };
 template <int NF>
 struct ZFused {
+  template <int FB>
+  static void go(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* Q2, const FftPlan& pz,
+                 const double2* dct_tw, const double* wz, const double* wzinv, unsigned long long* cfl_bits,
+                 double* ke_partial, cudaStream_t s) {
+    const size_t lines = (size_t)nf * kZPairs + FB + (NF ? 0 : std::max(kZLines, FB));
+    const size_t sm = lines * d.NZA * sizeof(double2);
+    set_smem(k_z_fused<NF, FB>, sm);
+    dim3 g((d.NXA + 2 * kZPairs - 1) / (2 * kZPairs), d.NYA);
+    k_z_fused<NF, FB><<<g, z_threads_fused(NF, FB), sm, s>>>(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits,
+                                                               ke_partial);
+  }
   static void run(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* Q2, const FftPlan& pz,
                   const double2* dct_tw, const double* wz, const double* wzinv, unsigned long long* cfl_bits,
-                  double* ke_partial, cudaStream_t s) {
+                  double* ke_partial, int batch6, cudaStream_t s) {
     if (NF != 0 && 3 * d.NZ != 2 * NF) {  // compiled lengths assume NZAA = 3 NZ / 2
-      ZFused<0>::run(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, s);
+      ZFused<0>::run(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, batch6, s);
       return;
     }
-    const size_t lines = (size_t)nf * kZPairs + kZFwd + (NF ? 0 : std::max(kZLines, kZFwd));
-    const size_t sm = lines * d.NZA * sizeof(double2);
-    set_smem(k_z_fused<NF>, sm);
-    dim3 g((d.NXA + 2 * kZPairs - 1) / (2 * kZPairs), d.NYA);
-    k_z_fused<NF><<<g, z_threads_fused(NF), sm, s>>>(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits,
-                                                       ke_partial);
+    if (batch6 && nf <= 4) go<6>(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, s);
+    else go<kZFwd>(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, s);
   }
 };
 template <int NF>
@@ -2530,11 +2762,12 @@ void launch_inv_y(const Dims& d, int nf, const FullVarDev* fv, StateSet st, cons
 }
 void launch_z_fused(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* Q2, const FftPlan& pz,
                     const double2* dct_tw, const double* wz, const double* wzinv, unsigned long long* cfl_bits,
-                    double* ke_partial, cudaStream_t s) {
-  dispatch_len<ZFused>(d.NZA, d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, s);
+                    double* ke_partial, cudaStream_t s, int batch6) {
+  dispatch_len<ZFused>(d.NZA, d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, batch6, s);
 }
-void launch_inv_x(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s, int pv) {
-  dispatch_len<InvX>(d.NXA, d, nf, Y1, Y2, px, pv, s);
+void launch_inv_x(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s, int pv,
+                  int tiles) {
+  dispatch_len<InvX>(d.NXA, d, nf, Y1, Y2, px, pv, tiles, s);
 }
 void launch_inv_z(const Dims& d, int nf, const double* Y2, double* phys, const FftPlan& pz,
                   const double2* dct_tw, const double* wz, unsigned long long* cfl_bits, cudaStream_t s) {
@@ -2687,7 +2920,20 @@ void launch_factor_real(const FactorArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;
   if (a.tpb) {
     const int nb = a.ncls * a.nact;
-    k_factor_tpb<<<(nb + kTpbThreads - 1) / kTpbThreads, kTpbThreads, 0, s>>>(a);
+    // the shared-memory window kernel when a warp's (or at least one thread's)
+    // windows fit in a CTA's shared memory, else the in-place kernel
+    int dev = 0, smax = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smax, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t wbytes = (size_t)(a.kl + a.ku + 2) * a.ldab * sizeof(double);
+    const int nt = (int)std::min<size_t>(32, (size_t)smax / wbytes);
+    if (a.window && a.kl <= kFacKl && nt >= 1) {
+      k_assemble_tpb<<<(nb + kTpbThreads - 1) / kTpbThreads, kTpbThreads, 0, s>>>(a);
+      set_smem(k_factor_win, (size_t)nt * wbytes);
+      k_factor_win<<<(nb + nt - 1) / nt, nt, (size_t)nt * wbytes, s>>>(a);
+    } else {
+      k_factor_tpb<<<(nb + kTpbThreads - 1) / kTpbThreads, kTpbThreads, 0, s>>>(a);
+    }
     if (a.cmask && a.ldab <= 64 && a.kl + a.ku <= 32 && a.kl <= 32) {
       cudaMemsetAsync(a.cmask, 0, (size_t)a.Tc * sizeof(unsigned long long), s);
       k_mask_cols<<<dim3((nb + 31) / 32, (a.Tc + 7) / 8), 256, 0, s>>>(a);

@@ -245,6 +245,10 @@ class PlaneLayer:
         self._check(self._lib.coral_autotune(self._h, float(dt), int(repeats), buf, 2048))
         return buf.value.decode()
 
+    def set_variant(self, knob, value):
+        """Pin one kernel variant of the autotuner (0 default, 1 alternative)."""
+        self._check(self._lib.coral_set_variant(self._h, knob.encode(), int(value)))
+
     def set_hermitian_kx0(self, on=True):
         """Project the kx = 0 line onto its Hermitian part after every step
         (removes the invisible anti-Hermitian part; off by default)."""

@@ -137,6 +137,12 @@ module coral_b200_c
       integer(c_int), value :: repeats, n
       character(kind=c_char), dimension(*) :: report
     end function
+    integer(c_int) function coral_set_variant(h, knob, value) bind(C, name="coral_set_variant")
+      import :: c_int, c_ptr, c_char
+      type(c_ptr), value :: h
+      character(kind=c_char), dimension(*) :: knob
+      integer(c_int), value :: value
+    end function
     ! ---- state, transforms, QuickSave and checkpoints -----------------------------------
     integer(c_int) function coral_get_field(h, isys, field) bind(C, name="coral_get_field")
       import :: c_int, c_ptr, c_double_complex

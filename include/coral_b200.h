@@ -310,14 +310,27 @@ int coral_ensemble_query(coral_ensemble* e, int what, long long* value);
  * Autotuner (no counterpart in the reference): times the kernel variants of the
  * step on this handle's problem at dt -- the FFT plans of the x passes (two or
  * three passes), the forward y pass (persistent pipelined or one CTA per tile),
- * the operator tile kernels (compiled group layouts or run-time forms) and the
- * band substitution (compiled or run-time band) -- each over `repeats` eager
+ * the operator tile kernels (compiled group layouts or run-time forms), the
+ * band substitution (compiled or run-time band), the fused z pass (forward
+ * batches of 9 or 6 lines) and the inverse x pass (persistent pipelined or one
+ * CTA per tile) -- each over `repeats` eager
  * steps (CUDA events on the handle's stream, best time of the phases it
  * affects), keeps the fastest of each, and restores the state (the tuning steps
  * leave it unchanged).  All variants compute the same arithmetic.  report (may
  * be NULL) receives the timings and choices, at most n bytes.
  */
 int coral_autotune(coral_handle* h, double dt, int repeats, char* report, int n);
+
+/*
+ * Sets one kernel variant of the autotuner by its knob name ("x_fft_plan",
+ * "fwd_y_pass", "operator_tiles", "band_substitution", "z_pass",
+ * "inv_x_pass"), or of the band factorisation ("band_factor": shared-memory
+ * window or in place; refactorises at once when factors exist): value 0 the
+ * default, 1 the alternative named in the autotuner's report -- to re-apply an
+ * earlier tuning without timing it again.  The variants compute the same
+ * arithmetic.  CORAL_EBADARG for an unknown knob or a value other than 0 or 1.
+ */
+int coral_set_variant(coral_handle* h, const char* knob, int value);
 
 /*
  * Learned subgrid closure (no counterpart in the reference).  A stencil network

@@ -201,7 +201,7 @@ def test_autotune_keeps_the_state_and_the_results():
     for pl in (a, b):
         pl.set_field(0, f)
     rep = b.autotune(1e-5, repeats=1)
-    for knob in ("x_fft_plan", "fwd_y_pass", "operator_tiles", "band_substitution"):
+    for knob in ("x_fft_plan", "fwd_y_pass", "operator_tiles", "band_substitution", "z_pass", "inv_x_pass"):
         assert knob in rep, rep
     assert np.array_equal(b.get_field(0), f)
     a.march_forward(1e-5, 2)
@@ -209,3 +209,66 @@ def test_autotune_keeps_the_state_and_the_results():
     assert _rel(b.get_field(0), a.get_field(0)) < 1e-12
     a.close()
     b.close()
+
+
+KNOBS = ("z_pass", "inv_x_pass", "band_factor", "x_fft_plan", "fwd_y_pass", "operator_tiles", "band_substitution")
+EXACT = ("z_pass", "inv_x_pass", "band_factor")  # same arithmetic in the same order: bit for bit
+
+
+def _variants_match(make, steps, dt):
+    ref = make()
+    ref.march_forward(dt, steps)
+    want = ref.get_field(0)
+    for knob in KNOBS:
+        pl = make()
+        pl.set_variant(knob, 1)
+        pl.march_forward(dt, steps)
+        got = pl.get_field(0)
+        if knob in EXACT:
+            assert np.array_equal(got, want), knob
+        else:
+            assert _rel(got, want) < 1e-12, knob
+        pl.close()
+    return ref
+
+
+def test_variants_compute_the_same_step():
+    """Every kernel variant the autotuner chooses between gives the default
+    step's state: bit for bit for the fused z pass (9- or 6-line forward
+    batches), the inverse x pass (pipelined or one CTA per tile) and the band
+    factorisation (shared-memory window or in place), to round-off for the FFT
+    plans, bands and operator tiles.  At the benchmark's
+    z length (32 x 32 x 192: z pass of length 288) and x length (384 x 384 x
+    48: x passes of length 576); unknown knobs and values are refused."""
+    from coral_b200 import initial_conditions as ic
+    from coral_b200.solver import CoralError, PlaneLayer
+    from coral_b200 import CONFIG_DIR
+    eq = open(os.path.join(CONFIG_DIR, "rbc_noslip_ra1e8.equations")).read()
+    par = open(os.path.join(CONFIG_DIR, "rbc_noslip_ra1e8_32x32x192.parameters.in")).read()
+    with tempfile.TemporaryDirectory() as d:
+        ic.white_noise_temperature(d, 32, 32, 192, seed=2)
+
+        def make():
+            pl = PlaneLayer(eq, par)
+            pl.import_quicksave(d)
+            return pl
+        ref = _variants_match(make, 2, 1e-6)
+    with pytest.raises(CoralError):
+        ref.set_variant("no_such_knob", 1)
+    with pytest.raises(CoralError):
+        ref.set_variant("z_pass", 2)
+    ref.close()
+    eq5 = equations("rbc_noslip_ra1e8", **{"1.d8": "1.d5"})
+    par5 = _params(384, 384, 48, 1e-5, 0.3, 1e30)
+    rng = np.random.default_rng(36)
+    f = None
+
+    def make5():
+        nonlocal f
+        pl = PlaneLayer(eq5, par5)
+        if f is None:
+            f = 1e-2 * (rng.standard_normal((pl.NXH, pl.NYAA, pl.T[0])) +
+                        1j * rng.standard_normal((pl.NXH, pl.NYAA, pl.T[0])))
+        pl.set_field(0, f)
+        return pl
+    _variants_match(make5, 1, 1e-5).close()
