@@ -497,9 +497,10 @@ def iy_dealiased(iy, NY, NYAA):
 
 
 def read_traffic(kernels):
-    """DRAM bytes (read + write) per launch of the phase's kernels at 384^2 x 192,
-    from the ncu launch list summarised in profiles/, or None."""
-    p = os.path.join(ROOT, "profiles", "dram_traffic_rbc_384x384x192.txt")
+    """DRAM bytes (read + write) per launch of the phase's kernel at 384^2 x 192,
+    from the one-kernel ncu captures at 128^2 x 192 summarised in profiles/
+    (scaled by the units processed), or None."""
+    p = os.path.join(ROOT, "profiles", "dram_traffic_rbc_128x128x192.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
