@@ -125,10 +125,16 @@ namespace coral {
 void set_global_error(const std::string& msg) { g_create_error = msg; }
 }  // namespace coral
 
+// side streams of the y-chunked pipeline of a stage (inverse x, fused z and
+// forward x passes per band of y rows, bands round-robin over the streams)
+constexpr int kYStreams = 3;
+
 struct coral_handle {
   std::string err;
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaStream_t ystream[kYStreams] = {};
+  cudaEvent_t yfork = nullptr, yjoin[kYStreams] = {};
   Parameters P;
   Recipe R;
   std::unique_ptr<Geometry> G;
@@ -185,6 +191,8 @@ struct coral_handle {
     int z_batch6 = 1;       // fused z pass: 1 forward batches of 6 lines (3 CTAs per SM), 0 of 9 lines
     int inv_x_tiles = 1;    // inverse x pass: 1 one CTA per tile, 0 persistent pipelined
     int factor_window = 1;  // band factorisation: 1 shared-memory window, 0 in place in global memory
+    int y_chunks = 1;       // stage passes inverse x -> z -> forward x in this many bands of y rows on
+                            // kYStreams streams (grids of at least 288 x 288 points); 1: whole passes
   } tune;
   // learned closure (not owned) and its output [9][y][x][z]
   coral_closure* closure = nullptr;
@@ -330,6 +338,11 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
   h->device = device;
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  for (int k = 0; k < kYStreams; ++k) {
+    CK(cudaStreamCreateWithFlags(&h->ystream[k], cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->yjoin[k], cudaEventDisableTiming));
+  }
+  CK(cudaEventCreateWithFlags(&h->yfork, cudaEventDisableTiming));
   h->P = parse_parameters(pars);
   h->R = parse_equations(eqs);
   h->TB = ars_tableau(scheme && *scheme ? std::string(scheme) : h->P.scheme);
@@ -804,53 +817,84 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
   const int S = h->TB.stages;
   const double scale = 1.0 / ((double)g.NXAA * (double)g.NYAA * (double)g.NZAA);
   const bool last = (i == S - 1);
-  {
+  // the y-chunked pipeline (eager phase timing keeps whole passes, one kernel per phase)
+  const bool chunked = !pt && h->tune.y_chunks > 1 && !h->closure && h->zform == 0 && h->tune.inv_x_tiles == 1 &&
+                       (size_t)d.NXA * d.NYA >= (size_t)288 * 288;
+  if (chunked) {
     StateSet st = state_set(h, i == 0);
-    B(0); launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream); E();
-    B(1); launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream, h->tune.x_plan, h->tune.inv_x_tiles); E();
-    // the CFL maxima reported after a step are those of its last stage's fields
-    // (each stage's evaluation replaces them): only the last stage computes them
+    launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream);
     if (last) CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
-    nl += 2;
-  }
-  // z passes fused (inverse DCT, CFL maxima, products, KE, forward DCT); the
-  // quadratic variables overwrite Y2 in place, each CTA reading and writing only
-  // its own (y, x pair) columns
-  B(3);
-  if (h->closure) {
-    // unfused z passes around the network: physical fields to HBM, the
-    // network's subgrid parts, then the products (plus those parts) forward
-    launch_inv_z(d, h->nF, h->Y2, h->fphys, h->pz, h->dct_tw, h->d_wz, last ? h->cfl_bits : nullptr, h->stream);
-    closure_infer(closure_impl(h->closure), h->fphys, d.NYA, d.NXA, d.NZA, h->tau, h->stream);
-    QuadDesc q = h->quads;
-    q.ts_partial = nullptr;
-    q.tau = h->tau;
-    launch_fwd_z(d, h->nF, q, h->fphys, h->Y2, h->pz, h->dct_tw, h->d_wz, i == 0 ? h->ke_partial : nullptr,
-                 h->stream);
-    nl += 2;
-  } else if (h->zform == 1) {
-    // the tensor-core form: inverse contraction into the physical fields,
-    // then products and the forward contraction back into Y2
-    QuadDesc q = h->quads;
-    q.ts_partial = nullptr;
-    const bool ts = (i == 0 && q.ts_n > 0);
-    launch_zsplit_inv(d, h->nF, q, h->Y2, h->fphys, h->zmat_inv, h->d_wz, h->d_wzinv,
-                      last ? h->cfl_bits : nullptr, ts ? h->ts_partial_split : nullptr, h->flags, h->stream);
-    launch_zsplit_fwd(d, h->nF, q, h->fphys, h->Y2, h->zmat_fwd, h->d_wz,
-                      i == 0 ? h->ke_partial_split : nullptr, ts ? h->ts_partial_split : nullptr,
-                      (long long)h->ts_inv_rows, h->flags, h->stream);
-    ++nl;
-  } else {
-    // the first stage's fields also give the timeseries objects
     QuadDesc q = h->quads;
     q.ts_partial = (i == 0 && q.ts_n > 0) ? h->ts_partial : nullptr;
-    launch_z_fused(d, h->nF, q, h->Y2, h->Y2, h->pz, h->dct_tw, h->d_wz, h->d_wzinv,
-                   last ? h->cfl_bits : nullptr, i == 0 ? h->ke_partial : nullptr, h->stream, h->tune.z_batch6);
+    // a band of y rows needs only its own rows through the three passes: Y1 rows
+    // -> Y2 rows (x c2r), Y2 rows in place (z), Y2 rows -> Y1 rows (x r2c)
+    const int nch = std::min(h->tune.y_chunks, d.NYA);
+    CK(cudaEventRecord(h->yfork, h->stream));
+    for (int k = 0; k < kYStreams; ++k) CK(cudaStreamWaitEvent(h->ystream[k], h->yfork, 0));
+    for (int c = 0; c < nch; ++c) {
+      const int y0 = (int)((long long)d.NYA * c / nch), y1 = (int)((long long)d.NYA * (c + 1) / nch);
+      cudaStream_t ss = h->ystream[c % kYStreams];
+      launch_inv_x_rows(d, h->nF, h->Y1, h->Y2, h->px, h->tune.x_plan, y0, y1 - y0, ss);
+      launch_z_fused(d, h->nF, q, h->Y2, h->Y2, h->pz, h->dct_tw, h->d_wz, h->d_wzinv, last ? h->cfl_bits : nullptr,
+                     i == 0 ? h->ke_partial : nullptr, ss, h->tune.z_batch6, y0, y1 - y0);
+      launch_fwd_x(d, h->nQ, h->Y2, h->Y1, h->px, ss, h->tune.x_plan, y0, y1 - y0);
+    }
+    for (int k = 0; k < kYStreams; ++k) {
+      CK(cudaEventRecord(h->yjoin[k], h->ystream[k]));
+      CK(cudaStreamWaitEvent(h->stream, h->yjoin[k], 0));
+    }
+    launch_fwd_y(d, h->nQ, h->Y1, h->qspec, scale, h->py, h->stream, h->tune.fwd_y_grid);
+    nl += 2 + 3 * nch;
   }
-  E();
-  B(4); launch_fwd_x(d, h->nQ, h->Y2, h->Y1, h->px, h->stream, h->tune.x_plan); E();
-  B(5); launch_fwd_y(d, h->nQ, h->Y1, h->qspec, scale, h->py, h->stream, h->tune.fwd_y_grid); E();
-  nl += 3;
+  if (!chunked) {
+    {
+      StateSet st = state_set(h, i == 0);
+      B(0); launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream); E();
+      B(1); launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream, h->tune.x_plan, h->tune.inv_x_tiles); E();
+      // the CFL maxima reported after a step are those of its last stage's fields
+      // (each stage's evaluation replaces them): only the last stage computes them
+      if (last) CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
+      nl += 2;
+    }
+    // z passes fused (inverse DCT, CFL maxima, products, KE, forward DCT); the
+    // quadratic variables overwrite Y2 in place, each CTA reading and writing only
+    // its own (y, x pair) columns
+    B(3);
+    if (h->closure) {
+      // unfused z passes around the network: physical fields to HBM, the
+      // network's subgrid parts, then the products (plus those parts) forward
+      launch_inv_z(d, h->nF, h->Y2, h->fphys, h->pz, h->dct_tw, h->d_wz, last ? h->cfl_bits : nullptr, h->stream);
+      closure_infer(closure_impl(h->closure), h->fphys, d.NYA, d.NXA, d.NZA, h->tau, h->stream);
+      QuadDesc q = h->quads;
+      q.ts_partial = nullptr;
+      q.tau = h->tau;
+      launch_fwd_z(d, h->nF, q, h->fphys, h->Y2, h->pz, h->dct_tw, h->d_wz, i == 0 ? h->ke_partial : nullptr,
+                   h->stream);
+      nl += 2;
+    } else if (h->zform == 1) {
+      // the tensor-core form: inverse contraction into the physical fields,
+      // then products and the forward contraction back into Y2
+      QuadDesc q = h->quads;
+      q.ts_partial = nullptr;
+      const bool ts = (i == 0 && q.ts_n > 0);
+      launch_zsplit_inv(d, h->nF, q, h->Y2, h->fphys, h->zmat_inv, h->d_wz, h->d_wzinv,
+                        last ? h->cfl_bits : nullptr, ts ? h->ts_partial_split : nullptr, h->flags, h->stream);
+      launch_zsplit_fwd(d, h->nF, q, h->fphys, h->Y2, h->zmat_fwd, h->d_wz,
+                        i == 0 ? h->ke_partial_split : nullptr, ts ? h->ts_partial_split : nullptr,
+                        (long long)h->ts_inv_rows, h->flags, h->stream);
+      ++nl;
+    } else {
+      // the first stage's fields also give the timeseries objects
+      QuadDesc q = h->quads;
+      q.ts_partial = (i == 0 && q.ts_n > 0) ? h->ts_partial : nullptr;
+      launch_z_fused(d, h->nF, q, h->Y2, h->Y2, h->pz, h->dct_tw, h->d_wz, h->d_wzinv,
+                     last ? h->cfl_bits : nullptr, i == 0 ? h->ke_partial : nullptr, h->stream, h->tune.z_batch6);
+    }
+    E();
+    B(4); launch_fwd_x(d, h->nQ, h->Y2, h->Y1, h->px, h->stream, h->tune.x_plan); E();
+    B(5); launch_fwd_y(d, h->nQ, h->Y1, h->qspec, scale, h->py, h->stream, h->tune.fwd_y_grid); E();
+    nl += 3;
+  }
   for (int q : h->zmean_quads) {
     launch_remove_zmean(d, h->qspec + (size_t)q * d.NXH * d.NYA * d.NZ, h->stream);
     ++nl;
@@ -1400,6 +1444,21 @@ std::string slurp(const char* path) {
 
 extern "C" {
 
+namespace {
+void release_streams(coral_handle* h) {
+  for (int k = 0; k < kYStreams; ++k) {
+    if (h->ystream[k]) cudaStreamDestroy(h->ystream[k]);
+    if (h->yjoin[k]) cudaEventDestroy(h->yjoin[k]);
+    h->ystream[k] = nullptr;
+    h->yjoin[k] = nullptr;
+  }
+  if (h->yfork) cudaEventDestroy(h->yfork);
+  h->yfork = nullptr;
+  if (h->stream) cudaStreamDestroy(h->stream);
+  h->stream = nullptr;
+}
+}  // namespace
+
 int coral_create(const char* equations_text, const char* parameters_text, const char* scheme, int device,
                  coral_handle** out) {
   if (!out || !equations_text || !parameters_text) {
@@ -1414,14 +1473,14 @@ int coral_create(const char* equations_text, const char* parameters_text, const 
     g_create_error = e.what();
     h->mem.free_all();
     if (h->h_pin) cudaFreeHost(h->h_pin);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    release_streams(h);
     delete h;
     return e.code;
   } catch (const std::exception& e) {
     g_create_error = e.what();
     h->mem.free_all();
     if (h->h_pin) cudaFreeHost(h->h_pin);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    release_streams(h);
     delete h;
     return CORAL_EBADARG;
   }
@@ -1453,7 +1512,7 @@ void coral_destroy(coral_handle* h) {
   if (h->graph) cudaGraphExecDestroy(h->graph);
   h->mem.free_all();
   if (h->h_pin) cudaFreeHost(h->h_pin);
-  if (h->stream) cudaStreamDestroy(h->stream);
+  release_streams(h);
   delete h;
 }
 
@@ -1799,6 +1858,8 @@ std::vector<Knob> knobs_of(coral_handle* h) {
           {"band_substitution", &h->tune.subst_rt, 0, 1, "compiled-band", "run-time-band", {9}},
           {"z_pass", &h->tune.z_batch6, 1, 0, "6-line-batches", "9-line-batches", {3}},
           {"inv_x_pass", &h->tune.inv_x_tiles, 1, 0, "one-CTA-per-tile", "persistent-pipelined", {1}},
+          // timed over whole steps (its passes overlap across streams)
+          {"y_pipeline", &h->tune.y_chunks, 1, 8, "whole-passes", "8-row-bands-3-streams", {-1}},
           // not timed by the autotuner (a factorisation, not a step phase)
           {"band_factor", &h->tune.factor_window, 1, 0, "shared-memory-window", "in-place", {}}};
 }
@@ -1860,17 +1921,37 @@ int coral_autotune(coral_handle* h, double dt, int repeats, char* report, int n)
       }
       return best;
     };
+    auto time_steps = [&]() {  // whole eager steps, CUDA events on the handle's stream
+      double best = 1e300;
+      cudaEvent_t a = nullptr, b = nullptr;
+      CK(cudaEventCreate(&a));
+      CK(cudaEventCreate(&b));
+      for (int r = 0; r < repeats + 1; ++r) {
+        CK(cudaEventRecord(a, h->stream));
+        enqueue_step(h, dt, nullptr);
+        CK(cudaEventRecord(b, h->stream));
+        CK(cudaEventSynchronize(b));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (r > 0) best = std::min(best, (double)ms);
+      }
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+      return best;
+    };
     std::vector<Knob> knobs = knobs_of(h);
     std::string rep;
     for (auto& kb : knobs) {
       if (kb.phases.empty()) continue;
-      double ta = 0, tb = 0;
+      auto timed = [&]() {
+        if (kb.phases[0] < 0) return time_steps();
+        if (kb.phases.size() == 2) return time_phases({kb.phases[0], kb.phases[1]});
+        return time_phases({kb.phases[0]});
+      };
       *kb.var = kb.a;
-      if (kb.phases.size() == 2) ta = time_phases({kb.phases[0], kb.phases[1]});
-      else ta = time_phases({kb.phases[0]});
+      const double ta = timed();
       *kb.var = kb.b;
-      if (kb.phases.size() == 2) tb = time_phases({kb.phases[0], kb.phases[1]});
-      else tb = time_phases({kb.phases[0]});
+      const double tb = timed();
       *kb.var = (tb < ta) ? kb.b : kb.a;
       char buf[256];
       std::snprintf(buf, sizeof(buf), "%s%s: %s %.4f ms, %s %.4f ms -> %s", rep.empty() ? "" : "; ", kb.name, kb.na, ta,

@@ -115,8 +115,14 @@ void launch_fwd_z(const Dims& d, int nf, const QuadDesc& q, const double* phys, 
 // wzinv[z] = 1 / wz[z]
 void launch_z_fused(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* Q2, const FftPlan& pz,
                     const double2* dct_tw, const double* wz, const double* wzinv, unsigned long long* cfl_bits,
-                    double* ke_partial, cudaStream_t s, int batch6 = 0);
-void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s, int pv = 1);
+                    double* ke_partial, cudaStream_t s, int batch6 = 0, int y0 = 0, int ny = -1);
+void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s, int pv = 1,
+                  int y0 = 0, int ny = -1);
+// the inverse x pass (one CTA per tile) over the y rows y0 .. y0 + ny - 1 only; with
+// launch_z_fused and launch_fwd_x over the same rows, the three passes of a band
+// of y rows depend on no other rows (the y-chunked pipeline of a stage)
+void launch_inv_x_rows(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, int pv, int y0, int ny,
+                       cudaStream_t s);
 // grid_variant = 1: one CTA per tile instead of the persistent pipelined kernel
 void launch_fwd_y(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
                   cudaStream_t s, int grid_variant = 0);

@@ -195,9 +195,10 @@ __global__ void __launch_bounds__(kThreadsY, kMinBlocksY) k_inv_y(Dims d, const 
 // two real output lines per complex FFT
 // ------------------------------------------------------------------------------
 template <int NF, int PV>
-__global__ void __launch_bounds__(kThreadsX, hot_min_blocks(kThreadsX)) k_inv_x(Dims d, const double2* Y1, double* Y2, FftPlan px) {
+__global__ void __launch_bounds__(kThreadsX, hot_min_blocks(kThreadsX)) k_inv_x(Dims d, const double2* Y1, double* Y2, FftPlan px,
+                                                                               int y0) {
   extern __shared__ double2 sm[];
-  const int f = blockIdx.x, n0 = blockIdx.y * kNB2, y = blockIdx.z;
+  const int f = blockIdx.x, n0 = blockIdx.y * kNB2, y = y0 + blockIdx.z;
   const int NXA = NF ? NF : d.NXA, NP = kNB2 / 2, LS = NXA + kPadXY;
   double2* A = sm;
   double2* B = sm + NP * LS;  // runtime plan only
@@ -493,12 +494,14 @@ template <int NF, int FB>
 __global__ void __launch_bounds__(kThreadsZF, z_min_blocks(NF, FB)) k_z_fused(Dims d, int nf, QuadDesc q, const double* Y2,
                                                                        double* Q2, FftPlan pz, const double2* dct_tw,
                                                                        const double* wz, const double* wzinv,
-                                                                       unsigned long long* cfl_bits, double* ke_partial) {
+                                                                       unsigned long long* cfl_bits, double* ke_partial,
+                                                                       int y0) {
   constexpr int NT = kThreadsZF;
   extern __shared__ double2 sm[];
   __shared__ double red[3][(NT + 31) / 32];
   __shared__ int qv[2][kMaxQuad];
-  const int x0 = blockIdx.x * 2 * kZPairs, y = blockIdx.y;
+  const int x0 = blockIdx.x * 2 * kZPairs, y = y0 + blockIdx.y;
+  const size_t cta = (size_t)y * gridDim.x + blockIdx.x;  // row of the KE and timeseries partial sums
   // compiled lengths: NZAA = 3 NZ / 2 (the launcher checks it)
   const int N = NF ? NF : d.NZA, NZ = NF ? 2 * NF / 3 : d.NZ;
   const int nq = q.nq;
@@ -619,13 +622,12 @@ __global__ void __launch_bounds__(kThreadsZF, z_min_blocks(NF, FB)) k_z_fused(Di
       if (threadIdx.x < 3) {
         double s = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
-        ke_partial[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 3 + threadIdx.x] = s;
+        ke_partial[cta * 3 + threadIdx.x] = s;
       }
       __syncthreads();
     }
     // timeseries objects, one at a time (one accumulator register)
     if (ke_partial && q.ts_partial) {
-      const size_t cta = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
       for (int o = 0; o < q.ts_n; ++o) {
         const int src = q.ts_src[o], zsel = q.ts_z[o];
         const int fa = src >= 0 ? src : qv[0][-1 - src], fb = src >= 0 ? -1 : qv[1][-1 - src];
@@ -710,9 +712,10 @@ __global__ void __launch_bounds__(kThreadsZF, z_min_blocks(NF, FB)) k_z_fused(Di
 // forward transform, pass 2: x r2c, keep kx < NX/2 (transforms.f90:255-267)
 // ------------------------------------------------------------------------------
 template <int NF, int PV>
-__global__ void __launch_bounds__(kThreadsX, hot_min_blocks(kThreadsX)) k_fwd_x(Dims d, const double* Q2, double2* Q1, FftPlan px) {
+__global__ void __launch_bounds__(kThreadsX, hot_min_blocks(kThreadsX)) k_fwd_x(Dims d, const double* Q2, double2* Q1, FftPlan px,
+                                                                               int y0) {
   extern __shared__ double2 sm[];
-  const int qi = blockIdx.x, n0 = blockIdx.y * kNB2, y = blockIdx.z;
+  const int qi = blockIdx.x, n0 = blockIdx.y * kNB2, y = y0 + blockIdx.z;
   const int NXA = NF ? NF : d.NXA, NP = kNB2 / 2, LS = NXA + kPadXY;
   double2* A = sm;
   double2* B = sm + NP * LS;  // runtime plan only
@@ -2652,10 +2655,20 @@ template <int NF>
 struct InvX {
   template <int PV>
   static void go(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s) {
+    go<PV>(d, nf, Y1, Y2, px, 0, d.NYA, s);
+  }
+  template <int PV>
+  static void go(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, int y0, int ny,
+                 cudaStream_t s) {
     size_t sm = (NF ? 1 : 2) * (kNB2 / 2) * (size_t)(d.NXA + kPadXY) * sizeof(double2);
     set_smem(k_inv_x<NF, PV>, sm);
-    dim3 g(nf, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
-    k_inv_x<NF, PV><<<g, kThreadsX, sm, s>>>(d, Y1, Y2, px);
+    dim3 g(nf, (d.NZ + kNB2 - 1) / kNB2, ny);
+    k_inv_x<NF, PV><<<g, kThreadsX, sm, s>>>(d, Y1, Y2, px, y0);
+  }
+  static void rows(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, int pv, int y0, int ny,
+                   cudaStream_t s) {
+    if (pv) go<1>(d, nf, Y1, Y2, px, y0, ny, s);
+    else go<0>(d, nf, Y1, Y2, px, y0, ny, s);
   }
   static void run(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, int pv, int tiles,
                   cudaStream_t s) {
@@ -2700,37 +2713,39 @@ struct ZFused {
   template <int FB>
   static void go(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* Q2, const FftPlan& pz,
                  const double2* dct_tw, const double* wz, const double* wzinv, unsigned long long* cfl_bits,
-                 double* ke_partial, cudaStream_t s) {
+                 double* ke_partial, int y0, int ny, cudaStream_t s) {
     const size_t lines = (size_t)nf * kZPairs + FB + (NF ? 0 : std::max(kZLines, FB));
     const size_t sm = lines * d.NZA * sizeof(double2);
     set_smem(k_z_fused<NF, FB>, sm);
-    dim3 g((d.NXA + 2 * kZPairs - 1) / (2 * kZPairs), d.NYA);
+    dim3 g((d.NXA + 2 * kZPairs - 1) / (2 * kZPairs), ny);
     k_z_fused<NF, FB><<<g, z_threads_fused(NF, FB), sm, s>>>(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits,
-                                                               ke_partial);
+                                                               ke_partial, y0);
   }
   static void run(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* Q2, const FftPlan& pz,
                   const double2* dct_tw, const double* wz, const double* wzinv, unsigned long long* cfl_bits,
-                  double* ke_partial, int batch6, cudaStream_t s) {
+                  double* ke_partial, int batch6, int y0, int ny, cudaStream_t s) {
     if (NF != 0 && 3 * d.NZ != 2 * NF) {  // compiled lengths assume NZAA = 3 NZ / 2
-      ZFused<0>::run(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, batch6, s);
+      ZFused<0>::run(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, batch6, y0, ny, s);
       return;
     }
-    if (batch6 && nf <= 4) go<6>(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, s);
-    else go<kZFwd>(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, s);
+    if (batch6 && nf <= 4) go<6>(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, y0, ny, s);
+    else go<kZFwd>(d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, y0, ny, s);
   }
 };
 template <int NF>
 struct FwdX {
   template <int PV>
-  static void go(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s) {
+  static void go(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, int y0, int ny,
+                 cudaStream_t s) {
     size_t sm = (NF ? 1 : 2) * (kNB2 / 2) * (size_t)(d.NXA + kPadXY) * sizeof(double2);
     set_smem(k_fwd_x<NF, PV>, sm);
-    dim3 g(nq, (d.NZ + kNB2 - 1) / kNB2, d.NYA);
-    k_fwd_x<NF, PV><<<g, kThreadsX, sm, s>>>(d, Q2, Q1, px);
+    dim3 g(nq, (d.NZ + kNB2 - 1) / kNB2, ny);
+    k_fwd_x<NF, PV><<<g, kThreadsX, sm, s>>>(d, Q2, Q1, px, y0);
   }
-  static void run(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, int pv, cudaStream_t s) {
-    if (pv) go<1>(d, nq, Q2, Q1, px, s);
-    else go<0>(d, nq, Q2, Q1, px, s);
+  static void run(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, int pv, int y0, int ny,
+                  cudaStream_t s) {
+    if (pv) go<1>(d, nq, Q2, Q1, px, y0, ny, s);
+    else go<0>(d, nq, Q2, Q1, px, y0, ny, s);
   }
 };
 template <int NF>
@@ -2762,8 +2777,20 @@ void launch_inv_y(const Dims& d, int nf, const FullVarDev* fv, StateSet st, cons
 }
 void launch_z_fused(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* Q2, const FftPlan& pz,
                     const double2* dct_tw, const double* wz, const double* wzinv, unsigned long long* cfl_bits,
-                    double* ke_partial, cudaStream_t s, int batch6) {
-  dispatch_len<ZFused>(d.NZA, d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, batch6, s);
+                    double* ke_partial, cudaStream_t s, int batch6, int y0, int ny) {
+  if (ny < 0) ny = d.NYA - y0;
+  dispatch_len<ZFused>(d.NZA, d, nf, q, Y2, Q2, pz, dct_tw, wz, wzinv, cfl_bits, ke_partial, batch6, y0, ny, s);
+}
+template <int NF>
+struct InvXRows {
+  static void run(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, int pv, int y0, int ny,
+                  cudaStream_t s) {
+    InvX<NF>::rows(d, nf, Y1, Y2, px, pv, y0, ny, s);
+  }
+};
+void launch_inv_x_rows(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, int pv, int y0, int ny,
+                       cudaStream_t s) {
+  dispatch_len<InvXRows>(d.NXA, d, nf, Y1, Y2, px, pv, y0, ny, s);
 }
 void launch_inv_x(const Dims& d, int nf, const double2* Y1, double* Y2, const FftPlan& px, cudaStream_t s, int pv,
                   int tiles) {
@@ -2777,8 +2804,10 @@ void launch_fwd_z(const Dims& d, int nf, const QuadDesc& q, const double* phys, 
                   const double2* dct_tw, const double* wz, double* ke_partial, cudaStream_t s) {
   dispatch_len<FwdZ>(d.NZA, d, nf, q, phys, Q2, pz, dct_tw, wz, ke_partial, s);
 }
-void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s, int pv) {
-  dispatch_len<FwdX>(d.NXA, d, nq, Q2, Q1, px, pv, s);
+void launch_fwd_x(const Dims& d, int nq, const double* Q2, double2* Q1, const FftPlan& px, cudaStream_t s, int pv,
+                  int y0, int ny) {
+  if (ny < 0) ny = d.NYA - y0;
+  dispatch_len<FwdX>(d.NXA, d, nq, Q2, Q1, px, pv, y0, ny, s);
 }
 void launch_fwd_y(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
                   cudaStream_t s, int grid_variant) {

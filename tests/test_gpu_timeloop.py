@@ -201,7 +201,8 @@ def test_autotune_keeps_the_state_and_the_results():
     for pl in (a, b):
         pl.set_field(0, f)
     rep = b.autotune(1e-5, repeats=1)
-    for knob in ("x_fft_plan", "fwd_y_pass", "operator_tiles", "band_substitution", "z_pass", "inv_x_pass"):
+    for knob in ("x_fft_plan", "fwd_y_pass", "operator_tiles", "band_substitution", "z_pass", "inv_x_pass",
+                 "y_pipeline"):
         assert knob in rep, rep
     assert np.array_equal(b.get_field(0), f)
     a.march_forward(1e-5, 2)
@@ -211,8 +212,10 @@ def test_autotune_keeps_the_state_and_the_results():
     b.close()
 
 
-KNOBS = ("z_pass", "inv_x_pass", "band_factor", "x_fft_plan", "fwd_y_pass", "operator_tiles", "band_substitution")
-EXACT = ("z_pass", "inv_x_pass", "band_factor")  # same arithmetic in the same order: bit for bit
+KNOBS = ("z_pass", "inv_x_pass", "band_factor", "y_pipeline", "x_fft_plan", "fwd_y_pass", "operator_tiles",
+         "band_substitution")
+# same arithmetic in the same order: bit for bit
+EXACT = ("z_pass", "inv_x_pass", "band_factor", "y_pipeline")
 
 
 def _variants_match(make, steps, dt):
@@ -235,9 +238,10 @@ def _variants_match(make, steps, dt):
 def test_variants_compute_the_same_step():
     """Every kernel variant the autotuner chooses between gives the default
     step's state: bit for bit for the fused z pass (9- or 6-line forward
-    batches), the inverse x pass (pipelined or one CTA per tile) and the band
-    factorisation (shared-memory window or in place), to round-off for the FFT
-    plans, bands and operator tiles.  At the benchmark's
+    batches), the inverse x pass (pipelined or one CTA per tile), the band
+    factorisation (shared-memory window or in place) and the y-chunked
+    multi-stream pipeline (grids of 288 x 288 or more: here 576 x 576), to
+    round-off for the FFT plans, bands and operator tiles.  At the benchmark's
     z length (32 x 32 x 192: z pass of length 288) and x length (384 x 384 x
     48: x passes of length 576); unknown knobs and values are refused."""
     from coral_b200 import initial_conditions as ic
