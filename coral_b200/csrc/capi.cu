@@ -150,6 +150,7 @@ struct coral_handle {
   FftPlan py{}, px{}, pz{};
   double2* dct_tw = nullptr;
   FullVarDev* d_fv = nullptr;
+  bool fv_single = false;  // every full variable: mean terms, then exactly one kxky term
   QuadDesc quads{};
   std::vector<int> zmean_quads;
   double2 *Y1 = nullptr, *qspec = nullptr, *tmp_spec = nullptr;
@@ -191,6 +192,7 @@ struct coral_handle {
     int z_batch6 = 1;       // fused z pass: 1 forward batches of 6 lines (3 CTAs per SM), 0 of 9 lines
     int inv_x_tiles = 1;    // inverse x pass: 1 one CTA per tile, 0 persistent pipelined
     int factor_window = 1;  // band factorisation: 1 shared-memory window, 0 in place in global memory
+    int inv_y_loop = 0;     // inverse y pass: 0 single-term build where the recipe allows, 1 term loop
     int y_chunks = 1;       // stage passes inverse x -> z -> forward x in this many bands of y rows on
                             // kYStreams streams (grids of at least 288 x 288 points); 1: whole passes
   } tune;
@@ -646,6 +648,12 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
     }
   }
   h->d_fv = mem.upload(fv);
+  h->fv_single = h->nF > 0;
+  for (int f = 0; f < h->nF; ++f) {
+    int nk = 0;
+    for (int t = 0; t < fv[f].nterms; ++t) nk += fv[f].term[t].zero_kind ? 0 : 1;
+    if (nk != 1 || fv[f].term[fv[f].nterms - 1].zero_kind) h->fv_single = false;
+  }
   // quadratic variables
   h->quads.nq = h->nQ;
   h->quads.ke_q[0] = h->quads.ke_q[1] = h->quads.ke_q[2] = -1;
@@ -698,7 +706,8 @@ StateSet state_set(coral_handle* h, bool use_field) {
 // inverse transforms of all full variables built from field (stage 0) or aux
 int full_vars_to_phys(coral_handle* h, bool use_field, bool cfl) {
   const Dims& d = h->d;
-  launch_inv_y(d, h->nF, h->d_fv, state_set(h, use_field), nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream);
+  launch_inv_y(d, h->nF, h->d_fv, state_set(h, use_field), nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream,
+               h->fv_single && !h->tune.inv_y_loop);
   launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream);
   if (cfl) CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
   launch_inv_z(d, h->nF, h->Y2, h->fphys, h->pz, h->dct_tw, h->d_wz, cfl ? h->cfl_bits : nullptr, h->stream);
@@ -822,7 +831,7 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
                        (size_t)d.NXA * d.NYA >= (size_t)288 * 288;
   if (chunked) {
     StateSet st = state_set(h, i == 0);
-    launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream);
+    launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream, h->fv_single && !h->tune.inv_y_loop);
     if (last) CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
     QuadDesc q = h->quads;
     q.ts_partial = (i == 0 && q.ts_n > 0) ? h->ts_partial : nullptr;
@@ -849,7 +858,7 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
   if (!chunked) {
     {
       StateSet st = state_set(h, i == 0);
-      B(0); launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream); E();
+      B(0); launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream, h->fv_single && !h->tune.inv_y_loop); E();
       B(1); launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream, h->tune.x_plan, h->tune.inv_x_tiles); E();
       // the CFL maxima reported after a step are those of its last stage's fields
       // (each stage's evaluation replaces them): only the last stage computes them
@@ -1857,6 +1866,7 @@ std::vector<Knob> knobs_of(coral_handle* h) {
           {"operator_tiles", &h->tune.generic_tiles, 0, 1, "compiled-groups", "run-time-forms", {7, 10}},
           {"band_substitution", &h->tune.subst_rt, 0, 1, "compiled-band", "run-time-band", {9}},
           {"z_pass", &h->tune.z_batch6, 1, 0, "6-line-batches", "9-line-batches", {3}},
+          {"inv_y_pass", &h->tune.inv_y_loop, 0, 1, "single-term-build", "term-loop-build", {0}},
           {"inv_x_pass", &h->tune.inv_x_tiles, 1, 0, "one-CTA-per-tile", "persistent-pipelined", {1}},
           // timed over whole steps (its passes overlap across streams)
           {"y_pipeline", &h->tune.y_chunks, 1, 8, "whole-passes", "8-row-bands-3-streams", {-1}},

@@ -97,8 +97,11 @@ struct Dims {
 
 // ---- launchers (kernels.cu) -------------------------------------------------
 // inverse transform of nf scalars: spectral build (or a plain spec input) + y-FFT
+// single = 1: every full variable is mean terms followed by exactly one kxky term
+// (the single-term kernel); plain_spec: the transform of one given spectrum
 void launch_inv_y(const Dims& d, int nf, const FullVarDev* fv, StateSet st, const double2* plain_spec,
-                  const double* kx, const double* ky, double2* Y1, const FftPlan& py, cudaStream_t s);
+                  const double* kx, const double* ky, double2* Y1, const FftPlan& py, cudaStream_t s,
+                  int single = 0);
 // pv: FFT plan of the compiled lengths, 1 = two passes (576 = 24 x 24, 288 = 18 x 16), 0 = three passes
 // tiles = 1: one CTA per tile; 0: the persistent pipelined kernel (compiled
 // lengths with a two-pass plan and pv = 1; others fall back to one CTA per tile)

@@ -190,6 +190,86 @@ __global__ void __launch_bounds__(kThreadsY, kMinBlocksY) k_inv_y(Dims d, const 
   }
 }
 
+// The same pass for full variables whose terms are mean variables followed by
+// exactly one kxky variable (the u, v, w, T of the plane-layer recipes): the
+// mean terms reach only the (0,0) mode and are summed in the prologue, in term
+// order, so that a position's build is one unrolled stencil whose state loads
+// do not wait on a loop over terms, and all of a thread's loads in the first
+// pass can be in flight at once.  The same arithmetic in the same order as
+// k_inv_y (bit for bit).
+template <int NF>
+__global__ void __launch_bounds__(kThreadsY, kMinBlocksY) k_inv_y1(Dims d, const FullVarDev* fv, StateSet st,
+                                                      const double* kxv, const double* kyv, double2* Y1, FftPlan py) {
+  extern __shared__ double2 sm[];
+  const int f = blockIdx.x, n0 = blockIdx.y * kNB1, kx = blockIdx.z;
+  const int NYA = NF ? NF : d.NYA, LS = NYA + kPadY;
+  double2* A = sm;
+  double2* B = sm + kNB1 * LS;  // runtime plan only
+  __shared__ int s_tt[kNB1][kTabW];
+  __shared__ double s_tv[kNB1][kTabW];
+  __shared__ double2 s_zc[kNB1];  // per line, the mean terms' sum at (kx, ky) = (0, 0)
+  const int tk = fv[f].nterms - 1;  // the kxky term is the last
+  const FullTermDev& ft = fv[f].term[tk];
+  for (int e = threadIdx.x; e < kNB1 * kTabW; e += blockDim.x) {
+    const int ln = e / kTabW, k = e - ln * kTabW, n = n0 + ln;
+    s_tt[ln][k] = n < d.NZ ? ft.tab_t[n * kTabW + k] : -1;
+    s_tv[ln][k] = n < d.NZ ? ft.tab_v[n * kTabW + k] : 0.0;
+  }
+  if (threadIdx.x < kNB1) {
+    const int ln = threadIdx.x, n = n0 + ln;
+    double2 c = zero2();
+    if (kx == 0 && n < d.NZ) {
+      for (int t = 0; t < tk; ++t) {  // the mean terms, as k_inv_y's build at iy = 0
+        const FullTermDev& fz = fv[f].term[t];
+        const double* zs = st.z[fz.set];
+        double s = 0.0;
+        for (int k = 0; k < kTabW; ++k) {
+          const int tt = fz.tab_t[n * kTabW + k];
+          if (tt >= 0) s += fz.tab_v[n * kTabW + k] * zs[tt];
+        }
+        c.x += s * fz.dsca;
+      }
+    }
+    s_zc[ln] = c;
+  }
+  const int kt = st.kT[ft.set], dx = ft.dx, dy = ft.dy;
+  const double2* base = st.k[ft.set] + (size_t)kx * NYA * kt;
+  const double dsca = ft.dsca;
+  const double2 kxf = ipow(kxv[kx], dx);
+  __syncthreads();
+  auto ld = [&](int ln, int iy) -> double2 {
+    const int n = n0 + ln;
+    double2 c = zero2();
+    if (n < d.NZ) {
+      if (kx == 0 && iy == 0) c = s_zc[ln];
+      const double2* sv = base + (size_t)iy * kt;
+      double2 s = zero2();
+#pragma unroll
+      for (int k = 0; k < kTabW; ++k) {
+        const int tt = s_tt[ln][k];
+        if (tt >= 0) {
+          const double w = s_tv[ln][k];
+          const double2 x = sv[tt];
+          s.x += w * x.x;
+          s.y += w * x.y;
+        }
+      }
+      s = cscale(s, dsca);
+      if (dx || dy) s = cmul(cmul(s, kxf), ipow(kyv[iy], dy));
+      c = cadd(c, s);
+    }
+    return c;
+  };
+  const double2* R = fft_lines_ld<NF, true, kThreadsY, kNB1, true, kPlanY>(A, B, kNB1, LS, py, ld);
+  for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
+    const int ln = idx % kNB1, y = idx / kNB1, n = n0 + ln;
+    if (n < d.NZ) {
+      const double s = (n == 0) ? 1.0 : 0.5;  // (x2 on Chebyshev index 0) * (0.5 of the x padding)
+      Y1[(((size_t)f * NYA + y) * d.NXH + kx) * d.NZ + n] = cscale(R[ln * LS + y], s);
+    }
+  }
+}
+
 // ------------------------------------------------------------------------------
 // inverse transform, pass 2: x c2r with zero padding NX/2 -> NXAA (transforms.f90:197-210)
 // two real output lines per complex FFT
@@ -2644,10 +2724,15 @@ int persistent_ctas(K kernel, int threads, size_t smem) {
 template <int NF>
 struct InvY {
   static void run(const Dims& d, int nf, const FullVarDev* fv, StateSet st, const double2* plain_spec,
-                  const double* kx, const double* ky, double2* Y1, const FftPlan& py, cudaStream_t s) {
+                  const double* kx, const double* ky, double2* Y1, const FftPlan& py, int single, cudaStream_t s) {
     size_t sm = (NF ? 1 : 2) * kNB1 * (size_t)(d.NYA + kPadY) * sizeof(double2);
-    set_smem(k_inv_y<NF>, sm);
     dim3 g(nf, (d.NZ + kNB1 - 1) / kNB1, d.NXH);
+    if (single && !plain_spec) {
+      set_smem(k_inv_y1<NF>, sm);
+      k_inv_y1<NF><<<g, kThreadsY, sm, s>>>(d, fv, st, kx, ky, Y1, py);
+      return;
+    }
+    set_smem(k_inv_y<NF>, sm);
     k_inv_y<NF><<<g, kThreadsY, sm, s>>>(d, fv, st, plain_spec, kx, ky, Y1, py);
   }
 };
@@ -2772,8 +2857,8 @@ struct FwdY {
 };
 
 void launch_inv_y(const Dims& d, int nf, const FullVarDev* fv, StateSet st, const double2* plain_spec,
-                  const double* kx, const double* ky, double2* Y1, const FftPlan& py, cudaStream_t s) {
-  dispatch_len<InvY>(d.NYA, d, nf, fv, st, plain_spec, kx, ky, Y1, py, s);
+                  const double* kx, const double* ky, double2* Y1, const FftPlan& py, cudaStream_t s, int single) {
+  dispatch_len<InvY>(d.NYA, d, nf, fv, st, plain_spec, kx, ky, Y1, py, single, s);
 }
 void launch_z_fused(const Dims& d, int nf, const QuadDesc& q, const double* Y2, double* Q2, const FftPlan& pz,
                     const double2* dct_tw, const double* wz, const double* wzinv, unsigned long long* cfl_bits,

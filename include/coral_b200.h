@@ -313,7 +313,8 @@ int coral_ensemble_query(coral_ensemble* e, int what, long long* value);
  * the operator tile kernels (compiled group layouts or run-time forms), the
  * band substitution (compiled or run-time band), the fused z pass (forward
  * batches of 9 or 6 lines), the inverse x pass (persistent pipelined or one
- * CTA per tile) and the y-chunked pipeline of a stage's inverse x, z and
+ * CTA per tile), the inverse y pass (single-term build or term loop) and the
+ * y-chunked pipeline of a stage's inverse x, z and
  * forward x passes (bands of y rows on three streams, or whole passes; timed
  * over whole steps) -- each over `repeats` eager
  * steps (CUDA events on the handle's stream, best time of the phases it
@@ -326,7 +327,7 @@ int coral_autotune(coral_handle* h, double dt, int repeats, char* report, int n)
 /*
  * Sets one kernel variant of the autotuner by its knob name ("x_fft_plan",
  * "fwd_y_pass", "operator_tiles", "band_substitution", "z_pass",
- * "inv_x_pass", "y_pipeline"), or of the band factorisation ("band_factor": shared-memory
+ * "inv_x_pass", "inv_y_pass", "y_pipeline"), or of the band factorisation ("band_factor": shared-memory
  * window or in place; refactorises at once when factors exist): value 0 the
  * default, 1 the alternative named in the autotuner's report -- to re-apply an
  * earlier tuning without timing it again.  The variants compute the same

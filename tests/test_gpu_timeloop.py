@@ -202,7 +202,7 @@ def test_autotune_keeps_the_state_and_the_results():
         pl.set_field(0, f)
     rep = b.autotune(1e-5, repeats=1)
     for knob in ("x_fft_plan", "fwd_y_pass", "operator_tiles", "band_substitution", "z_pass", "inv_x_pass",
-                 "y_pipeline"):
+                 "inv_y_pass", "y_pipeline"):
         assert knob in rep, rep
     assert np.array_equal(b.get_field(0), f)
     a.march_forward(1e-5, 2)
@@ -212,10 +212,10 @@ def test_autotune_keeps_the_state_and_the_results():
     b.close()
 
 
-KNOBS = ("z_pass", "inv_x_pass", "band_factor", "y_pipeline", "x_fft_plan", "fwd_y_pass", "operator_tiles",
-         "band_substitution")
+KNOBS = ("z_pass", "inv_x_pass", "inv_y_pass", "band_factor", "y_pipeline", "x_fft_plan", "fwd_y_pass",
+         "operator_tiles", "band_substitution")
 # same arithmetic in the same order: bit for bit
-EXACT = ("z_pass", "inv_x_pass", "band_factor", "y_pipeline")
+EXACT = ("z_pass", "inv_x_pass", "inv_y_pass", "band_factor", "y_pipeline")
 
 
 def _variants_match(make, steps, dt):
@@ -238,7 +238,8 @@ def _variants_match(make, steps, dt):
 def test_variants_compute_the_same_step():
     """Every kernel variant the autotuner chooses between gives the default
     step's state: bit for bit for the fused z pass (9- or 6-line forward
-    batches), the inverse x pass (pipelined or one CTA per tile), the band
+    batches), the inverse x pass (pipelined or one CTA per tile), the inverse
+    y pass (single-term build or term loop), the band
     factorisation (shared-memory window or in place) and the y-chunked
     multi-stream pipeline (grids of 288 x 288 or more: here 576 x 576), to
     round-off for the FFT plans, bands and operator tiles.  At the benchmark's
