@@ -340,11 +340,6 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
   h->device = device;
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-  for (int k = 0; k < kYStreams; ++k) {
-    CK(cudaStreamCreateWithFlags(&h->ystream[k], cudaStreamNonBlocking));
-    CK(cudaEventCreateWithFlags(&h->yjoin[k], cudaEventDisableTiming));
-  }
-  CK(cudaEventCreateWithFlags(&h->yfork, cudaEventDisableTiming));
   h->P = parse_parameters(pars);
   h->R = parse_equations(eqs);
   h->TB = ars_tableau(scheme && *scheme ? std::string(scheme) : h->P.scheme);
@@ -827,8 +822,8 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
   const double scale = 1.0 / ((double)g.NXAA * (double)g.NYAA * (double)g.NZAA);
   const bool last = (i == S - 1);
   // the y-chunked pipeline (eager phase timing keeps whole passes, one kernel per phase)
-  const bool chunked = !pt && h->tune.y_chunks > 1 && !h->closure && h->zform == 0 && h->tune.inv_x_tiles == 1 &&
-                       (size_t)d.NXA * d.NYA >= (size_t)288 * 288;
+  const bool chunked = !pt && h->tune.y_chunks > 1 && h->yfork && !h->closure && h->zform == 0 &&
+                       h->tune.inv_x_tiles == 1 && (size_t)d.NXA * d.NYA >= (size_t)288 * 288;
   if (chunked) {
     StateSet st = state_set(h, i == 0);
     launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream, h->fv_single && !h->tune.inv_y_loop);
@@ -1454,6 +1449,16 @@ std::string slurp(const char* path) {
 extern "C" {
 
 namespace {
+// the y pipeline's side streams and events, created when the variant is first
+// selected (outside any stream capture)
+void ensure_ystreams(coral_handle* h) {
+  if (h->yfork) return;
+  for (int k = 0; k < kYStreams; ++k) {
+    CK(cudaStreamCreateWithFlags(&h->ystream[k], cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->yjoin[k], cudaEventDisableTiming));
+  }
+  CK(cudaEventCreateWithFlags(&h->yfork, cudaEventDisableTiming));
+}
 void release_streams(coral_handle* h) {
   for (int k = 0; k < kYStreams; ++k) {
     if (h->ystream[k]) cudaStreamDestroy(h->ystream[k]);
@@ -1881,6 +1886,7 @@ int coral_set_variant(coral_handle* h, const char* knob, int value) {
     for (auto& kb : knobs_of(h)) {
       if (std::strcmp(kb.name, knob) != 0) continue;
       if (value != 0 && value != 1) throw CoralError(CORAL_EBADARG, "set_variant: value is 0 (default) or 1 (alternative)");
+      if (kb.var == &h->tune.y_chunks) ensure_ystreams(h);
       *kb.var = value ? kb.b : kb.a;
       if (kb.var == &h->tune.factor_window && h->dt_factored >= 0.0) factorize(h, h->dt_factored);
       if (h->graph) {
@@ -1949,6 +1955,7 @@ int coral_autotune(coral_handle* h, double dt, int repeats, char* report, int n)
       cudaEventDestroy(b);
       return best;
     };
+    ensure_ystreams(h);
     std::vector<Knob> knobs = knobs_of(h);
     std::string rep;
     for (auto& kb : knobs) {
@@ -2046,9 +2053,42 @@ struct coral_ensemble {
   std::vector<long long> total;               // per stage: blocks in all
   long long launches = 0;
   int launches_per_step = 0;
+  // members' own phases run on these streams (member m on stream m mod kEnsStreams),
+  // forked from and joined back into `stream`: the step graph has one branch per stream
+  std::vector<cudaStream_t> mstream;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
 };
 
 namespace {
+
+constexpr int kEnsStreams = 8;
+
+// f(h) for every member, member m queued on member stream m mod kEnsStreams,
+// forked from and joined back into the ensemble's stream
+template <class F>
+int ens_fan(coral_ensemble* e, F&& f) {
+  int nl = 0;
+  const int K = (int)e->mstream.size();
+  CK(cudaEventRecord(e->fork, e->stream));
+  for (int k = 0; k < K; ++k) CK(cudaStreamWaitEvent(e->mstream[k], e->fork, 0));
+  for (size_t m = 0; m < e->mem.size(); ++m) {
+    coral_handle* h = e->mem[m];
+    h->stream = e->mstream[m % K];
+    try {
+      nl += f(h);
+    } catch (...) {
+      h->stream = e->stream;
+      throw;
+    }
+    h->stream = e->stream;
+  }
+  for (int k = 0; k < K; ++k) {
+    CK(cudaEventRecord(e->join[k], e->mstream[k]));
+    CK(cudaStreamWaitEvent(e->stream, e->join[k], 0));
+  }
+  return nl;
+}
 
 void ens_free_args(coral_ensemble* e) {
   for (auto* p : e->d_args) cudaFree(p);
@@ -2094,16 +2134,16 @@ int ens_enqueue(coral_ensemble* e, double dt) {
   int nl = 0;
   const int S = e->mem[0]->TB.stages;
   for (int i = 0; i < S; ++i) {
-    for (coral_handle* h : e->mem) nl += enqueue_stage_pre(h, i, dt, nullptr);
+    nl += ens_fan(e, [&](coral_handle* h) { return enqueue_stage_pre(h, i, dt, nullptr); });
     if (e->batched) {
       launch_subst_multi(e->d_args[i], e->d_prefix[i], e->nsub[i], e->total[i], e->stream);
       ++nl;
     } else {
-      for (coral_handle* h : e->mem) nl += enqueue_stage_subst(h, i, dt, nullptr);
+      nl += ens_fan(e, [&](coral_handle* h) { return enqueue_stage_subst(h, i, dt, nullptr); });
     }
-    for (coral_handle* h : e->mem) nl += enqueue_stage_post(h, i, dt, nullptr);
+    nl += ens_fan(e, [&](coral_handle* h) { return enqueue_stage_post(h, i, dt, nullptr); });
   }
-  for (coral_handle* h : e->mem) nl += enqueue_step_end(h);
+  nl += ens_fan(e, [&](coral_handle* h) { return enqueue_step_end(h); });
   CK(cudaGetLastError());
   return nl;
 }
@@ -2173,6 +2213,9 @@ void ens_destroy(coral_ensemble* e) {
     if (h->stream == e->stream) h->stream = nullptr;  // the ensemble's stream, destroyed below
     coral_destroy(h);
   }
+  for (cudaStream_t st : e->mstream) cudaStreamDestroy(st);
+  for (cudaEvent_t ev : e->join) cudaEventDestroy(ev);
+  if (e->fork) cudaEventDestroy(e->fork);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }
@@ -2206,8 +2249,19 @@ int coral_ensemble_create(int n, const char* const* equations_texts, const char*
       return CORAL_EBADARG;
     }
   }
-  // one stream for all members
-  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  // the ensemble's stream (the members' home stream) and the member streams
+  bool ok = cudaSetDevice(device) == cudaSuccess &&
+            cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming) == cudaSuccess;
+  for (int k = 0; ok && k < std::min(kEnsStreams, n); ++k) {
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev = nullptr;
+    ok = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess;
+    if (ok) e->mstream.push_back(st);
+    ok = ok && cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess;
+    if (ok) e->join.push_back(ev);
+  }
+  if (!ok) {
     ens_destroy(e);
     g_create_error = "coral_ensemble_create: stream creation failed";
     return CORAL_ECUDA;

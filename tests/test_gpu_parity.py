@@ -3,6 +3,7 @@
 Tolerances: FP64 everywhere; transforms agree to 1e-13 of the field's maximum;
 timesteps to a relative L2 error of 1e-10 per coupled variable (the bound the
 plain FP64 path must hold against the reference after 100 steps)."""
+import ctypes
 import math
 import os
 import tempfile
@@ -215,4 +216,65 @@ def test_diagnostics_match_oracle(scheme):
     assert ref.cfl_dt is not None and ref.ke is not None
     assert abs(d["cfl_dt"] - ref.cfl_dt) <= 1e-11 * abs(ref.cfl_dt)
     assert abs(d["KE"] - ref.ke) <= 1e-11 * abs(ref.ke)
+    pl.close()
+
+
+@pytest.mark.parametrize("N", [(12, 12, 36), (36, 24, 12)])
+def test_steps_with_runtime_plans_and_block_tails(N):
+    """The benchmark recipe (no-slip RBC) at sizes whose grid lengths have no
+    compiled FFT plan (x 18 and 54, y 18, z 54 and 18; y 36 is compiled) and
+    whose Chebyshev counts leave a partial block of 4 rows in the x passes'
+    8-row blocks (NZ mod 8 = 4): the run-time-plan kernels, their second
+    shared buffer and the tail guards, over three ARS_222 steps against the
+    oracle."""
+    NX, NY, NZ = N
+    eq = equations("rbc_noslip_ra1e8", **{"1.d8": "1.d5"})
+    par = params(NX, NY, NZ, dt=1e-5)
+    ref = co.Solver(eq, par)
+    pl = _pl(eq, par)
+    _random_state(ref, pl, 11, amp=1e-2)
+    for _ in range(3):
+        ref.step(1e-5)
+    pl.march_forward(1e-5, 3)
+    pl.synchronize()
+    for s in range(len(ref.lay)):
+        assert _rel(pl.get_field(s), ref.field[s]) < 1e-11
+    for s in range(len(ref.zlay)):
+        assert _rel(pl.get_mean_field(s), ref.zfield[s]) < 1e-11
+    d = pl.diagnostics()
+    assert d["nonfinite"] is False
+    pl.close()
+
+
+def test_invalid_inputs_are_refused_and_nonfinite_states_reported():
+    """The C-ABI's error behaviour (the reference prints and stops; here a
+    negative code and a message, the handle stays usable): sizes outside the
+    build (NX not a multiple of 4; a grid length 3 NZ / 2 = 30 that is not
+    2^a 3^b), unreadable parameter files, dt <= 0, a system index out of range;
+    a NaN in the state is reported after a step (CORAL_ENONFINITE from
+    coral_synchronize, and the diagnostics' flag)."""
+    from coral_b200.solver import CoralError
+    for bad, code in ((params(18, 16, 16), -8), (params(16, 16, 20), -8),
+                      (params(16, 16, 16).replace("1.d0        ! gap", "one   ! gap"), -6),
+                      ("\n".join(params(16, 16, 16).splitlines()[:10]), -6)):
+        with pytest.raises(CoralError) as e:
+            _pl(equations(), bad)
+        assert e.value.code == code, (e.value.code, str(e.value))
+    pl = _pl(equations(), params(16, 16, 16))
+    with pytest.raises(CoralError) as e:
+        pl.march_forward(0.0, 1)
+    assert e.value.code == -1
+    buf = np.zeros(8, dtype=np.complex128)
+    rc = pl._lib.coral_get_field(pl._h, 7, buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    assert rc == -1 and "out of range" in pl._lib.coral_last_error(pl._h).decode()
+    f = pl.get_field(0)
+    pl.march_forward(1e-4, 1)  # still usable after the refusals
+    pl.synchronize()
+    f[1, 2, 0] = np.nan  # an entry the step reads (the oracle's step spreads it to 10,472 of 16,896 entries)
+    pl.set_field(0, f)
+    pl.march_forward(1e-4, 1)
+    with pytest.raises(CoralError) as e:
+        pl.synchronize()
+    assert e.value.code == -5
+    assert pl.diagnostics()["nonfinite"] is True
     pl.close()
