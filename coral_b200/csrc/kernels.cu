@@ -303,8 +303,12 @@ __global__ void __launch_bounds__(kThreadsX, hot_min_blocks(kThreadsX)) k_inv_x(
     const int m = idx % NP, x = idx / NP, na = n0 + 2 * m;
     double2 z = R[m * LS + x];
     double* dst = Y2 + (((size_t)f * d.NYA + y) * NXA + x) * d.NZ;
-    if (na < d.NZ) dst[na] = z.x;
-    if (na + 1 < d.NZ) dst[na + 1] = z.y;
+    if (na + 1 < d.NZ && (d.NZ & 1) == 0) {
+      *reinterpret_cast<double2*>(dst + na) = z;  // na and NZ even: one 16-byte store
+    } else {
+      if (na < d.NZ) dst[na] = z.x;
+      if (na + 1 < d.NZ) dst[na + 1] = z.y;
+    }
   }
 }
 
@@ -805,6 +809,7 @@ __global__ void __launch_bounds__(kThreadsX, hot_min_blocks(kThreadsX)) k_fwd_x(
   auto ld = [&](int m, int x) -> double2 {
     const int na = n0 + 2 * m;
     const double* src = src0 + (size_t)x * d.NZ;
+    if (na + 1 < d.NZ && (d.NZ & 1) == 0) return *reinterpret_cast<const double2*>(src + na);  // 16-byte aligned
     return make_double2(na < d.NZ ? src[na] : 0.0, na + 1 < d.NZ ? src[na + 1] : 0.0);
   };
   const double2* R = fft_lines_ld<NF, false, kThreadsX, kNB2 / 2, true, PV>(A, B, NP, LS, px, ld);
