@@ -86,6 +86,14 @@ __device__ __forceinline__ void cp_async16z(void* smem, const void* gmem, bool v
 }
 
 
+// 32-byte global store of two adjacent complex values (256-bit vector access;
+// the address must be 32-byte aligned).  (The matching 32-byte load, tried for
+// the inverse x pass's packed rows, was slower than two 16-byte loads.)
+__device__ __forceinline__ void st32(double2* p, double2 a, double2 b) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(a.x), "d"(a.y), "d"(b.x), "d"(b.y) : "memory");
+}
+__device__ __forceinline__ bool aligned32(const void* p) { return ((size_t)p & 31) == 0; }
+
 __device__ __forceinline__ double2 ipow(double k, int e) {
   // (i k)^e by repeated multiplication, as Fortran's complex**integer
   double2 r = make_double2(1.0, 0.0);
@@ -261,11 +269,18 @@ __global__ void __launch_bounds__(kThreadsY, kMinBlocksY) k_inv_y1(Dims d, const
     return c;
   };
   const double2* R = fft_lines_ld<NF, true, kThreadsY, kNB1, true, kPlanY>(A, B, kNB1, LS, py, ld);
-  for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
-    const int ln = idx % kNB1, y = idx / kNB1, n = n0 + ln;
-    if (n < d.NZ) {
-      const double s = (n == 0) ? 1.0 : 0.5;  // (x2 on Chebyshev index 0) * (0.5 of the x padding)
-      Y1[(((size_t)f * NYA + y) * d.NXH + kx) * d.NZ + n] = cscale(R[ln * LS + y], s);
+  // two adjacent Chebyshev rows per thread: one 32-byte store
+  for (int idx = threadIdx.x; idx < (kNB1 / 2) * NYA; idx += blockDim.x) {
+    const int l0 = 2 * (idx % (kNB1 / 2)), y = idx / (kNB1 / 2), n = n0 + l0;
+    // (x2 on Chebyshev index 0) * (0.5 of the x padding)
+    const double2 v0 = cscale(R[l0 * LS + y], (n == 0) ? 1.0 : 0.5);
+    const double2 v1 = cscale(R[(l0 + 1) * LS + y], 0.5);
+    double2* dst = Y1 + (((size_t)f * NYA + y) * d.NXH + kx) * d.NZ + n;
+    if (n + 1 < d.NZ && aligned32(dst)) {
+      st32(dst, v0, v1);
+    } else {
+      if (n < d.NZ) dst[0] = v0;
+      if (n + 1 < d.NZ) dst[1] = v1;
     }
   }
 }
@@ -821,8 +836,12 @@ __global__ void __launch_bounds__(kThreadsX, hot_min_blocks(kThreadsX)) k_fwd_x(
     const double2 dd = csub(Z, Zc);
     const double2 b = make_double2(0.5 * dd.y, -0.5 * dd.x);
     double2* dst = Q1 + (((size_t)qi * d.NYA + y) * d.NXH + kx) * d.NZ;
-    if (na < d.NZ) dst[na] = a;
-    if (na + 1 < d.NZ) dst[na + 1] = b;
+    if (na + 1 < d.NZ && aligned32(dst + na)) {
+      st32(dst + na, a, b);  // rows na, na + 1: one 32-byte store
+    } else {
+      if (na < d.NZ) dst[na] = a;
+      if (na + 1 < d.NZ) dst[na + 1] = b;
+    }
   }
 }
 
@@ -896,9 +915,17 @@ __global__ void __launch_bounds__(kThreadsYF, kMinBlocksYF) k_fwd_y_pipe(Dims d,
     fft_pass_first<NF, P.r[0], false, kThreadsYF, kNB1, true>(A, kNB1, LS, ld);  // ends with a barrier
     issue(tile + gridDim.x);
     fft_passes<NF, 1, P.r[0], false, kThreadsYF, kNB1, kPlanYF>(A, kNB1, LS, py.tw);
-    for (int idx = threadIdx.x; idx < kNB1 * NYA; idx += blockDim.x) {
-      const int ln = idx % kNB1, ky = idx / kNB1, n = n0 + ln;
-      if (n < d.NZ) qspec[(((size_t)qi * d.NXH + kx) * NYA + ky) * d.NZ + n] = cscale(A[ln * LS + ky], scale);
+    // two adjacent Chebyshev rows per thread: one 32-byte store
+    for (int idx = threadIdx.x; idx < (kNB1 / 2) * NYA; idx += blockDim.x) {
+      const int l0 = 2 * (idx % (kNB1 / 2)), ky = idx / (kNB1 / 2), n = n0 + l0;
+      const double2 v0 = cscale(A[l0 * LS + ky], scale), v1 = cscale(A[(l0 + 1) * LS + ky], scale);
+      double2* dst = qspec + (((size_t)qi * d.NXH + kx) * NYA + ky) * d.NZ + n;
+      if (n + 1 < d.NZ && aligned32(dst)) {
+        st32(dst, v0, v1);
+      } else {
+        if (n < d.NZ) dst[0] = v0;
+        if (n + 1 < d.NZ) dst[1] = v1;
+      }
     }
     __syncthreads();  // A is rewritten by the next tile's first pass
   }
