@@ -45,6 +45,9 @@ SIGNATURES = {
     "coral_spec_to_phys_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, _D, _D, _P]),
     "coral_set_timeseries": (ctypes.c_int, [_P, ctypes.c_char_p]),
     "coral_set_timeseries_from_file": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "coral_set_usr_output": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "coral_set_usr_output_from_file": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "coral_export_usr_output": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.c_longlong]),
     "coral_timeseries": (ctypes.c_int, [_P, _D, ctypes.c_int]),
     "coral_set_time": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_longlong]),
     "coral_get_time": (ctypes.c_int, [_P, _D]),

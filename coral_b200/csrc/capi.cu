@@ -179,6 +179,13 @@ struct coral_handle {
   long long i_timestep = 1, refactorizations = 0;
   // timeseries rows not yet written: (i_timestep, time, values)
   std::vector<std::pair<long long, std::vector<double>>> ts_rows;
+  // user outputs (coral.usrOutput): kind 0 volume, 1 z slice, 2 y slice, 3 x slice,
+  // 4 weighted z sum, 5 profile; src >= 0 a full variable, -1 - q quadratic
+  // variable q; index 0-based; the reference's counters and time_integer
+  struct UsrOut { int kind, src, index; long long period, counter; };
+  std::vector<UsrOut> uo;
+  long long time_integer = 1;
+  double* uo_buf = nullptr;  // one physical field: an object's file contents before the copy back
   // z transforms: 0 = FP64 FFT (k_z_fused), 1 = int8-digit contractions on the
   // tensor cores (zsplit.cu); form_last = the form of the last step (KE sums)
   int zform = 0, zform_last = 0;
@@ -1369,6 +1376,160 @@ void flush_timeseries(coral_handle* h, const std::string& dir) {
   h->ts_rows.clear();
 }
 
+// initialise_bookkeeping_counters (PL_IMEX_timestepping_marching.f90:620-637)
+void usr_output_counters(coral_handle* h) {
+  h->time_integer = h->i_timestep;
+  for (auto& o : h->uo) o.counter = h->i_timestep % o.period;
+}
+
+// add_outputs (PL_equations.f90:322-427) with the line readers of
+// PL_string_to_data.f90:244-300: '>>Volume :: var ;; Period= N <<',
+// '>>XSlice ::' / '>>YSlice ::' / '>>ZSlice ::' with ';; Position= I' (ignored
+// beyond NXAA / NYAA / NZAA), '>>Zsummed::', '>>Profile::'; objects kept per
+// variable, full variables first, each in file order.
+void set_usr_output(coral_handle* h, const std::string& text) {
+  std::vector<std::vector<coral_handle::UsrOut>> per_full(h->nF), per_quad(h->nQ);
+  std::istringstream in(text);
+  std::string line;
+  const Geometry& g = *h->G;
+  while (std::getline(in, line)) {
+    if (line.size() >= 5 && line.compare(2, 3, "EOF") == 0) break;
+    if (trim(line).empty()) continue;
+    const std::string head = line.substr(0, std::min<size_t>(11, line.size()));
+    int kind = -1, limit = 0;
+    if (head == ">>Volume ::") kind = 0;
+    else if (head == ">>ZSlice ::") kind = 1, limit = g.NZAA;
+    else if (head == ">>YSlice ::") kind = 2, limit = g.NYAA;
+    else if (head == ">>XSlice ::") kind = 3, limit = g.NXAA;
+    else if (head == ">>Zsummed::") kind = 4;
+    else if (head == ">>Profile::") kind = 5;
+    else
+      throw CoralError(CORAL_EPARSE, "coral.usrOutput: lines must start with '>>Volume ::', '>>XSlice ::', "
+                                     "'>>YSlice ::', '>>ZSlice ::', '>>Profile::' or '>>Zsummed::' ('" + line + "')");
+    const size_t dc = line.find("::"), pp = line.find(";; Period="), end = line.find("<<");
+    const size_t ps = line.find(";; Position=");
+    const bool positioned = kind >= 1 && kind <= 3;
+    if (dc == std::string::npos || pp == std::string::npos || end == std::string::npos || pp < dc || end < pp ||
+        (positioned && (ps == std::string::npos || ps < pp || end < ps)))
+      throw CoralError(CORAL_EPARSE, "coral.usrOutput: cannot read line '" + line + "'");
+    const std::string name = trim(line.substr(dc + 2, pp - dc - 2));
+    const long long period = std::atoll(trim(line.substr(pp + 10, (positioned ? ps : end) - pp - 10)).c_str());
+    int pos = 0;
+    if (positioned) {
+      pos = std::atoi(trim(line.substr(ps + 12, end - ps - 12)).c_str());
+      if (pos > limit) continue;  // ignored, as by the reference
+      if (pos < 1) throw CoralError(CORAL_EPARSE, "coral.usrOutput: position must be >= 1 in '" + line + "'");
+    }
+    if (period < 1) throw CoralError(CORAL_EPARSE, "coral.usrOutput: period must be >= 1 in '" + line + "'");
+    for (int f = 0; f < h->nF; ++f)
+      if (h->R.full[f].name == name) per_full[f].push_back({kind, f, pos - 1, period, 0});
+    for (int q = 0; q < h->nQ; ++q)
+      if (h->R.quad[q].name == name) {
+        // output_slices_volumes_and_profiles has no vertically summed slice of a
+        // quadratic variable (it stops with an error there)
+        if (kind == 4) throw CoralError(CORAL_EUNSUPPORTED, "coral.usrOutput: no Zsummed output of a quadratic variable");
+        per_quad[q].push_back({kind, -1 - q, pos - 1, period, 0});
+      }
+  }
+  h->uo.clear();
+  for (auto& v : per_full) h->uo.insert(h->uo.end(), v.begin(), v.end());
+  for (auto& v : per_quad) h->uo.insert(h->uo.end(), v.begin(), v.end());
+  usr_output_counters(h);
+  if (!h->uo.empty() && !h->uo_buf) h->uo_buf = h->mem.get<double>((size_t)g.NYAA * g.NXAA * g.NZAA);
+}
+
+// The physical field of output source src from the current state; the full
+// variables must be in fphys (full_vars_to_phys).  A quadratic variable is the
+// product (compute_NL_terms_to_K_hat, marching.f90:279-291), with its vertical
+// mean removed through its spectrum when the recipe asks (:292-298).
+const double* usr_field(coral_handle* h, int src) {
+  const Dims& d = h->d;
+  const size_t np = (size_t)d.NYA * d.NXA * d.NZA;
+  if (src >= 0) return h->fphys + (size_t)src * np;
+  const QuadVar& Q = h->R.quad[-1 - src];
+  const double* a = h->fphys + (size_t)(Q.v1 < 0 ? Q.v2 : Q.v1) * np;
+  const double* b = (Q.v1 < 0 || Q.v2 < 0) ? nullptr : h->fphys + (size_t)Q.v2 * np;
+  launch_phys_product(np, a, b, h->tmp_phys, h->stream);
+  ++h->launches;
+  if (Q.remove_mean) {
+    phys_to_spec_dev(h, h->tmp_phys, h->tmp_spec);
+    launch_remove_zmean(d, h->tmp_spec, h->stream);
+    spec_to_phys_dev(h, h->tmp_spec, h->tmp_phys);
+    ++h->launches;
+  }
+  return h->tmp_phys;
+}
+
+// export_volume / export_slice / export_verticallyAvgedSlice / export_profile
+// (PL_IMEX_timestepping_output.f90:250-307,489-581,685-715): the file under dir,
+// raw float64 in the reference's order, replaced if it exists.
+void write_usr_object(coral_handle* h, const coral_handle::UsrOut& o, long long itime, const std::string& dir) {
+  const Dims& d = h->d;
+  const double* f = usr_field(h, o.src);
+  const bool lin = o.src >= 0;
+  const int iv = lin ? o.src + 1 : -o.src;
+  const char* pre = lin ? "linear" : "quadra";
+  char name[160];
+  const char* sub = "Slices";
+  size_t n = 0;
+  double* out = h->uo_buf;
+  switch (o.kind) {
+    case 0:
+      sub = "Volumes";
+      std::snprintf(name, sizeof(name), "%s_var%02d_time%08lld_full.dat", pre, iv, itime);
+      launch_transpose_xy(d, f, out, 1, h->stream);
+      n = (size_t)d.NXA * d.NYA * d.NZA;
+      break;
+    case 1: case 2: case 3: {
+      const char axis = o.kind == 1 ? 'z' : (o.kind == 2 ? 'y' : 'x');
+      std::snprintf(name, sizeof(name), "%s_var%02d_%c%05d_time%08lld_full.dat", pre, iv, axis, o.index + 1, itime);
+      launch_usr_slice(d, f, o.kind, o.index, h->d_wz, out, h->stream);
+      n = o.kind == 1 ? (size_t)d.NXA * d.NYA : (o.kind == 2 ? (size_t)d.NXA * d.NZA : (size_t)d.NYA * d.NZA);
+      break;
+    }
+    case 4:
+      std::snprintf(name, sizeof(name), "%s_var%02d_zAvged_time%08lld_full.dat", pre, iv, itime);
+      launch_usr_slice(d, f, 4, 0, h->d_wz, out, h->stream);
+      n = (size_t)d.NXA * d.NYA;
+      break;
+    default:
+      sub = "Profiles";
+      std::snprintf(name, sizeof(name), "%s_var%02d_time%08lld_full.dat", pre, iv, itime);
+      launch_usr_profile(d, f, out, h->stream);
+      n = d.NZA;
+  }
+  ++h->launches;
+  CK(cudaGetLastError());
+  std::vector<double> buf(n);
+  CK(cudaMemcpyAsync(buf.data(), out, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  const std::string sdir = dir + "/" + sub;
+  if (mkdir_p(sdir) != 0) throw CoralError(CORAL_EIO, "cannot create " + sdir);
+  const std::string fn = sdir + "/" + name;
+  FILE* fp = std::fopen(fn.c_str(), "wb");
+  if (!fp) throw CoralError(CORAL_EIO, "cannot open " + fn);
+  const size_t w = std::fwrite(buf.data(), sizeof(double), n, fp);
+  std::fclose(fp);
+  if (w != n) throw CoralError(CORAL_EIO, "short write in " + fn);
+}
+
+// output_slices_volumes_and_profiles (PL_IMEX_timestepping_marching.f90:639-697),
+// at the first stage of a step, i.e. from the state at its start: time_integer
+// and every object's counter advance, the objects whose counter reaches their
+// period are written (dir null: counters only).
+void usr_output_step(coral_handle* h, const char* dir) {
+  ++h->time_integer;
+  std::vector<const coral_handle::UsrOut*> due;
+  for (auto& o : h->uo)
+    if (++o.counter == o.period) {
+      o.counter = 0;
+      due.push_back(&o);
+    }
+  if (due.empty() || !dir) return;
+  h->launches += full_vars_to_phys(h, true, false);
+  for (auto* o : due) write_usr_object(h, *o, h->time_integer, dir);
+}
+
 // The time loop of plane_layer_main.f90:138-205 for nsteps steps, with the
 // dt rules of timeKeeping.f90: after each step dt = CFL_C * cfl_based_DT
 // capped at dt_max (compare_dt_against_CFL, :78-89; stop below dt_min = 1e-9);
@@ -1390,6 +1551,7 @@ void run_loop(coral_handle* h, int nsteps, const char* outdir) {
       h->dt_current = h->dt_target;
       ++h->refactorizations;
     }
+    if (!h->uo.empty()) usr_output_step(h, outdir);
     march(h, h->dt_current, 1);  // refactorises when dt_current changed
     CK(cudaMemcpyAsync(h->h_pin + kMaxTs, h->cfl_bits, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                        h->stream));
@@ -1816,6 +1978,29 @@ int coral_set_timeseries_from_file(coral_handle* h, const char* path) {
   });
 }
 
+int coral_set_usr_output(coral_handle* h, const char* usr_output_text) {
+  return guarded(h, [&] {
+    if (!usr_output_text) throw CoralError(CORAL_EBADARG, "null text");
+    set_usr_output(h, usr_output_text);
+  });
+}
+
+int coral_set_usr_output_from_file(coral_handle* h, const char* path) {
+  return guarded(h, [&] {
+    if (!path) throw CoralError(CORAL_EBADARG, "null path");
+    set_usr_output(h, slurp(path));
+  });
+}
+
+int coral_export_usr_output(coral_handle* h, const char* output_directory, long long time_integer) {
+  return guarded(h, [&] {
+    if (!output_directory || !*output_directory) throw CoralError(CORAL_EBADARG, "null directory");
+    if (h->uo.empty()) return;
+    h->launches += full_vars_to_phys(h, true, false);
+    for (auto& o : h->uo) write_usr_object(h, o, time_integer, output_directory);
+  });
+}
+
 int coral_timeseries(coral_handle* h, double* values, int n) {
   return guarded(h, [&] {
     const int m = h->quads.ts_n;
@@ -1835,6 +2020,7 @@ int coral_set_time(coral_handle* h, double time, double dt, long long i_timestep
     h->dt_current = h->dt_target = d;
     h->i_timestep = i_timestep;
     h->ts_rows.clear();
+    usr_output_counters(h);
   });
 }
 

@@ -320,6 +320,13 @@ void launch_zero_step(const ZeroArgs& a, cudaStream_t s);
 void launch_zero_factor(const ZeroArgs& a, cudaStream_t s);
 
 // QuickSave helpers
+// user outputs: a slice (kind 1 z, 2 y, 3 x at index k) or the weighted z sum
+// (kind 4) of phys[y][x][z] in the reference's file order; the horizontal-average
+// profile; the product of two fields (b null: a copy)
+void launch_usr_slice(const Dims& d, const double* phys, int kind, int k, const double* wz, double* out,
+                      cudaStream_t s);
+void launch_usr_profile(const Dims& d, const double* phys, double* out, cudaStream_t s);
+void launch_phys_product(size_t n, const double* a, const double* b, double* out, cudaStream_t s);
 void launch_transpose_xy(const Dims& d, const double* in, double* out, int to_file_order, cudaStream_t s);
 // project Chebyshev coefficients spec[kx][ky][n] onto the Galerkin basis of one
 // variable (lower-triangular square stencil) and add them into the state

@@ -2657,6 +2657,64 @@ __global__ void k_transpose_xy(Dims d, const double* in, double* out, int to_fil
   }
 }
 
+// ------------------------------------------------------------------------------
+// User outputs (coral.usrOutput, PL_equations.f90:322-427) of one physical field
+// phys[y][x][z], in the reference's file order (transforms.f90:53-105,772-866):
+//   kind 1 ZSlice at z index k:  out[x][y] = phys(z = k)
+//   kind 2 YSlice at y index k:  out[x][z] = phys(y = k)
+//   kind 3 XSlice at x index k:  out[y][z] = phys(x = k)
+//   kind 4 Zsummed:              out[x][y] = sum_z w(z) phys, z in grid order
+// (indices 0-based here).  Profiles: k_usr_profile.
+// ------------------------------------------------------------------------------
+__global__ void k_usr_slice(Dims d, const double* phys, int kind, int k, const double* wz, double* out) {
+  const size_t n = kind == 1 || kind == 4 ? (size_t)d.NXA * d.NYA
+                   : kind == 2          ? (size_t)d.NXA * d.NZA
+                                        : (size_t)d.NYA * d.NZA;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    double v;
+    if (kind == 1 || kind == 4) {
+      const int y = (int)(e % d.NYA), x = (int)(e / d.NYA);
+      const double* col = phys + ((size_t)y * d.NXA + x) * d.NZA;
+      if (kind == 1) {
+        v = col[k];
+      } else {
+        v = 0.0;
+        for (int z = 0; z < d.NZA; ++z) v += col[z] * wz[z];
+      }
+    } else if (kind == 2) {
+      const int z = (int)(e % d.NZA), x = (int)(e / d.NZA);
+      v = phys[((size_t)k * d.NXA + x) * d.NZA + z];
+    } else {
+      const int z = (int)(e % d.NZA), y = (int)(e / d.NZA);
+      v = phys[((size_t)y * d.NXA + k) * d.NZA + z];
+    }
+    out[e] = v;
+  }
+}
+
+// Horizontal average profile (export_Profile_fftw_mpi, PL_IMEX_timestepping_output.f90:
+// 489-581): one CTA per z level, sum over x and y, then / NXAA / NYAA.
+__global__ void __launch_bounds__(256) k_usr_profile(Dims d, const double* phys, double* out) {
+  __shared__ double red[8];
+  const int z = blockIdx.x;
+  double s = 0.0;
+  for (size_t e = threadIdx.x; e < (size_t)d.NXA * d.NYA; e += blockDim.x) s += phys[e * d.NZA + z];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += red[w];
+    out[z] = t / d.NXA / d.NYA;
+  }
+}
+
+// product of two physical fields (a quadratic variable), or a copy when b is null
+__global__ void k_phys_product(size_t n, const double* a, const double* b, double* out) {
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    out[e] = b ? a[e] * b[e] : a[e];
+}
+
 // Projection of Chebyshev coefficients onto one variable's Galerkin basis
 // (square-stencil solve of import_quicksave, PL_IMEX_timestepping_output.f90:343-355).
 // The square stencil is lower triangular, so a forward substitution solves it;
@@ -3099,6 +3157,16 @@ void launch_zero_step(const ZeroArgs& a, cudaStream_t s) {
 void launch_zero_factor(const ZeroArgs& a, cudaStream_t s) {
   if (a.nsys <= 0) return;
   k_zero_factor<<<a.nsys, 32, 0, s>>>(a);
+}
+void launch_usr_slice(const Dims& d, const double* phys, int kind, int k, const double* wz, double* out,
+                      cudaStream_t s) {
+  k_usr_slice<<<1024, 256, 0, s>>>(d, phys, kind, k, wz, out);
+}
+void launch_usr_profile(const Dims& d, const double* phys, double* out, cudaStream_t s) {
+  k_usr_profile<<<d.NZA, 256, 0, s>>>(d, phys, out);
+}
+void launch_phys_product(size_t n, const double* a, const double* b, double* out, cudaStream_t s) {
+  k_phys_product<<<1024, 256, 0, s>>>(n, a, b, out);
 }
 void launch_transpose_xy(const Dims& d, const double* in, double* out, int to_file, cudaStream_t s) {
   k_transpose_xy<<<1024, 256, 0, s>>>(d, in, out, to_file);

@@ -210,6 +210,15 @@ class PlaneLayer:
         self._check(self._lib.coral_set_timeseries(self._h, text.encode()))
         self.n_timeseries = text.count(">>Volume_average") + text.count(">>Horizontal_avg")
 
+    def set_usr_output(self, text):
+        """coral.usrOutput text (master_recipe%add_outputs): volumes, slices,
+        vertically summed slices and profiles that run() writes at their periods."""
+        self._check(self._lib.coral_set_usr_output(self._h, text.encode()))
+
+    def export_usr_output(self, directory, time_integer):
+        """Write every user-output object now from the current state."""
+        self._check(self._lib.coral_export_usr_output(self._h, str(directory).encode(), int(time_integer)))
+
     def timeseries(self):
         """Values of the timeseries objects at the last step's first stage."""
         out = np.zeros(16)

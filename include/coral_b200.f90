@@ -103,6 +103,22 @@ module coral_b200_c
       type(c_ptr), value :: h
       character(kind=c_char), dimension(*), intent(in) :: path
     end function
+    integer(c_int) function coral_set_usr_output(h, text) bind(C, name="coral_set_usr_output")
+      import :: c_int, c_ptr, c_char
+      type(c_ptr), value :: h
+      character(kind=c_char), dimension(*), intent(in) :: text
+    end function
+    integer(c_int) function coral_set_usr_output_from_file(h, path) bind(C, name="coral_set_usr_output_from_file")
+      import :: c_int, c_ptr, c_char
+      type(c_ptr), value :: h
+      character(kind=c_char), dimension(*), intent(in) :: path
+    end function
+    integer(c_int) function coral_export_usr_output(h, dir, time_integer) bind(C, name="coral_export_usr_output")
+      import :: c_int, c_ptr, c_char, c_long_long
+      type(c_ptr), value :: h
+      character(kind=c_char), dimension(*), intent(in) :: dir
+      integer(c_long_long), value :: time_integer
+    end function
     integer(c_int) function coral_timeseries(h, vals, n) bind(C, name="coral_timeseries")
       import :: c_int, c_ptr, c_double
       type(c_ptr), value :: h

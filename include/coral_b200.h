@@ -245,6 +245,35 @@ int coral_get_time(coral_handle* h, double* out4);
 int coral_run(coral_handle* h, int nsteps, const char* output_directory);
 
 /*
+ * User outputs: the text of coral.usrOutput (lines '>>Volume :: NAME ;; Period= P <<',
+ * '>>XSlice :: NAME ;; Period= P ;; Position= I <<' and likewise '>>YSlice ::',
+ * '>>ZSlice ::', '>>Zsummed:: NAME ;; Period= P <<', '>>Profile:: NAME ;; Period= P <<'
+ * up to '>>EOF<<'; NAME a full or quadratic variable, I a 1-based grid index,
+ * entries beyond the grid ignored).  Replaces master_recipe%add_outputs
+ * (src/plane_layer/PL_equations.f90:322-427).  coral_run then writes, at the
+ * first stage of each step (from the state at its start), the objects whose
+ * counter reaches their period (output_slices_volumes_and_profiles,
+ * PL_IMEX_timestepping_marching.f90:639-697; counters and the time index start
+ * from the step index, as initialise_bookkeeping_counters, :620-637, and
+ * restart with coral_set_time) into output_directory/Volumes, /Slices and
+ * /Profiles under the reference's names (linear_varVV_timeTTTTTTTT_full.dat,
+ * linear_varVV_zKKKKK_..., _yKKKKK_, _xKKKKK_, _zAvged_, quadra_varVV_...), raw
+ * float64 in its order: a volume x-major then y then z; a z slice and the
+ * weighted z sum x-major then y; a y slice x-major then z; an x slice y-major
+ * then z; a profile z (PL_IMEX_timestepping_output.f90:250-307,489-581,685-715;
+ * src/slabs.fftw3mpi/transforms.f90:53-105,772-866).  Quadratic variables are
+ * the products of their full variables, with the vertical mean removed where
+ * the recipe asks; a Zsummed object of a quadratic variable is refused
+ * (CORAL_EUNSUPPORTED: the reference stops there).
+ */
+int coral_set_usr_output(coral_handle* h, const char* usr_output_text);
+int coral_set_usr_output_from_file(coral_handle* h, const char* path);
+/* Write every user-output object now, from the current state, with time index
+ * time_integer (export_allPhys / export_allProfiles for a driver that steps
+ * with coral_march); the periods and counters are not used. */
+int coral_export_usr_output(coral_handle* h, const char* output_directory, long long time_integer);
+
+/*
  * on != 0: after every step, replace the kx = 0 line of every coupled state by
  * its Hermitian part (f(0,ky) + conj f(0,-ky)) / 2.  Off by default, which
  * reproduces the reference's arithmetic.  Every physical value is unchanged:

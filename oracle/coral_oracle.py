@@ -1079,3 +1079,94 @@ def zgbtrs_band(lu, piv, kl, ku, b):
     if info != 0:
         raise RuntimeError("zgbtrs info=%d" % info)
     return x
+
+
+# --------------------------------------------------------------------------------------
+# user outputs (coral.usrOutput): the parser of PL_equations.f90:322-427 with the line
+# readers of PL_string_to_data.f90:244-300, the counters of
+# PL_IMEX_timestepping_marching.f90:620-697, and the files of
+# PL_IMEX_timestepping_output.f90:250-307,489-581,685-715 and
+# slabs.fftw3mpi/transforms.f90:53-105,772-866 (P = 1)
+# --------------------------------------------------------------------------------------
+
+USR_KINDS = {">>Volume ::": "volume", ">>ZSlice ::": "zSlice", ">>YSlice ::": "ySlice",
+             ">>XSlice ::": "xSlice", ">>Zsummed::": "zAvged", ">>Profile::": "profil"}
+
+
+def parse_usr_output(text: str, recipe: Recipe, g: Geometry):
+    """Objects [(kind, is_quad, var_index0, period, position)] in output order:
+    the full variables' objects first (variable order, then file order), then the
+    quadratic variables'.  Positions beyond the grid are dropped, as the reference
+    does (with a message); position is 1-based (0 for kinds without one)."""
+    fnames = [f[0] for f in recipe.full_vars]
+    qnames = [q[0] for q in recipe.quad_vars]
+    per_f = [[] for _ in fnames]
+    per_q = [[] for _ in qnames]
+    limit = {"zSlice": g.NZAA, "ySlice": g.NYAA, "xSlice": g.NXAA}
+    for line in text.splitlines():
+        if line[2:5] == "EOF":
+            break
+        if not line.strip():
+            continue
+        kind = USR_KINDS.get(line[:11])
+        if kind is None:
+            raise ValueError("coral.usrOutput: bad line %r" % line)
+        dc, pp, end = line.index("::") + 2, line.index(";; Period="), line.index("<<")
+        name = line[dc:pp].strip()
+        if kind in limit:
+            ps = line.index(";; Position=")
+            period = int(line[pp + 10:ps])
+            pos = int(line[ps + 12:end])
+            if pos > limit[kind]:
+                continue
+        else:
+            period, pos = int(line[pp + 10:end]), 0
+        if name in fnames:
+            per_f[fnames.index(name)].append((kind, False, fnames.index(name), period, pos))
+        if name in qnames:
+            per_q[qnames.index(name)].append((kind, True, qnames.index(name), period, pos))
+    return [o for v in per_f for o in v] + [o for v in per_q for o in v]
+
+
+def usr_output_files(objs, fphys, qphys, g: Geometry, itime: int):
+    """{relative file name: float64 array in file order} of the objects, from the
+    full and quadratic variables' physical fields (phys[y][x][z])."""
+    out = {}
+    w = g.zweights()
+    for kind, is_q, iv, _, pos in objs:
+        ph = qphys[iv] if is_q else fphys[iv]
+        pre = "quadra" if is_q else "linear"
+        tag = "%s_var%02d" % (pre, iv + 1)
+        tr = ph.transpose(1, 0, 2)  # transposed_phys(z, y, x) in C order [x][y][z]
+        if kind == "volume":
+            out["Volumes/%s_time%08d_full.dat" % (tag, itime)] = tr.ravel()
+        elif kind == "zSlice":
+            out["Slices/%s_z%05d_time%08d_full.dat" % (tag, pos, itime)] = tr[:, :, pos - 1].ravel()
+        elif kind == "ySlice":
+            out["Slices/%s_y%05d_time%08d_full.dat" % (tag, pos, itime)] = tr[:, pos - 1, :].ravel()
+        elif kind == "xSlice":
+            out["Slices/%s_x%05d_time%08d_full.dat" % (tag, pos, itime)] = tr[pos - 1, :, :].ravel()
+        elif kind == "zAvged":
+            out["Slices/%s_zAvged_time%08d_full.dat" % (tag, itime)] = (tr * w[None, None, :]).sum(axis=2).ravel()
+        else:
+            out["Profiles/%s_time%08d_full.dat" % (tag, itime)] = ph.sum(axis=(0, 1)) / g.NXAA / g.NYAA
+    return out
+
+
+def usr_output_schedule(objs, i_timestep: int, nsteps: int):
+    """[(step number within the run, time_integer, [objects due])]: counters start
+    at i_timestep mod period and time_integer at i_timestep; every step's first
+    stage advances both and writes the objects whose counter reaches the period."""
+    counters = [i_timestep % o[3] for o in objs]
+    t = i_timestep
+    sched = []
+    for s in range(nsteps):
+        t += 1
+        due = []
+        for k, o in enumerate(objs):
+            counters[k] += 1
+            if counters[k] == o[3]:
+                counters[k] = 0
+                due.append(o)
+        sched.append((s, t, due))
+    return sched

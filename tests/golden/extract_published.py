@@ -9,7 +9,7 @@ Rayleigh-Benard growth rate quoted by benchmark 01
 (etc/benchmarks/01_Rayleigh_Benard_stressFree/benchmark_01_stressfree_rayleigh_benard.ipynb:68)
 is stored beside them, with benchmark 02's published mean Nusselt number and
 its standard deviation (velocity-pressure form) and a verbatim copy of that
-benchmark's three input files (tests/golden/benchmark02/).
+benchmark's four input files (tests/golden/benchmark02/).
 
 usage: python tests/golden/extract_published.py <path-to-coral-tree>
 """
@@ -44,7 +44,7 @@ def main(root):
         json.dump(out, f, indent=1)
     dst = os.path.join(here, "benchmark02")
     os.makedirs(dst, exist_ok=True)
-    for name in ("coral.equations.velocityPressure", "coral.parameters.in", "coral.timeseries"):
+    for name in ("coral.equations.velocityPressure", "coral.parameters.in", "coral.timeseries", "coral.usrOutput"):
         with open(os.path.join(root, "etc/benchmarks/02_RRBC_julien_JFM96", name), "rb") as f:
             data = f.read()
         with open(os.path.join(dst, name), "wb") as f:

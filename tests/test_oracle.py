@@ -108,3 +108,31 @@ def test_rbc_system_band_structure():
     assert s.lay[0].T == 6 * 48 - 8
     s.factorize(1e-4)
     assert s.kl_ku[0] == (16, 27)
+
+
+def test_usr_output_parser_on_the_reference_file():
+    """The oracle's coral.usrOutput reader on benchmark 02's own file: 17
+    objects, grouped per full variable in the recipe's order (uFull, vFull,
+    wFull, tFull) and in file order within one; the counters of
+    initialise_bookkeeping_counters / output_slices_volumes_and_profiles put
+    the first tFull profile (period 50, run started at step 1) at time index 50
+    and the first slices (period 1000) at 1000."""
+    import os
+    from oracle import coral_oracle as co
+    b02 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "benchmark02")
+    recipe = co.parse_equations(open(os.path.join(b02, "coral.equations.velocityPressure")).read())
+    p = co.read_parameters_text(open(os.path.join(b02, "coral.parameters.in")).read())
+    g = co.Geometry(p["NX"], p["NY"], p["NZ"], p["Lx"], p["Ly"], p["gap"], p["center"])
+    objs = co.parse_usr_output(open(os.path.join(b02, "coral.usrOutput")).read(), recipe, g)
+    assert len(objs) == 17
+    assert [o[2] for o in objs] == sorted(o[2] for o in objs)  # grouped by variable
+    assert objs[0] == ("volume", False, 0, 10000, 0)
+    t_objs = [o for o in objs if o[2] == 3]
+    assert [o[0] for o in t_objs] == ["volume", "zSlice", "zSlice", "zSlice", "zSlice", "xSlice", "ySlice", "profil"]
+    assert [o[4] for o in t_objs if o[0] == "zSlice"] == [1, 24, 48, 72]
+    sched = co.usr_output_schedule(objs, 1, 1000)
+    first = {}
+    for _, t, due in sched:
+        for o in due:
+            first.setdefault(o[0], t)
+    assert first["profil"] == 50 and first["zSlice"] == 1000 and "volume" not in first
