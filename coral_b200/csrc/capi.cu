@@ -151,6 +151,13 @@ struct coral_handle {
   double2* dct_tw = nullptr;
   FullVarDev* d_fv = nullptr;
   bool fv_single = false;  // every full variable: mean terms, then exactly one kxky term
+  int* d_tab_id_t = nullptr;
+  double* d_tab_id_v = nullptr;
+  // z derivatives in full-variable builds: each dz term is built by k_full_dz
+  // into its own spectral buffer, which the build reads as pseudo-system
+  // ks.size() + j through an identity stencil
+  struct DzJob { int set, T, order; const int* tab_t; const double* tab_v; double dsca; double2* out; };
+  std::vector<DzJob> dz_jobs;
   QuadDesc quads{};
   std::vector<int> zmean_quads;
   double2 *Y1 = nullptr, *qspec = nullptr, *tmp_spec = nullptr;
@@ -628,8 +635,9 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
     fv[f].nterms = (int)F.terms.size();
     for (size_t t = 0; t < F.terms.size(); ++t) {
       const FullTerm& ft = F.terms[t];
-      if (ft.dz != 0 || ft.mz != 0)
-        throw CoralError(CORAL_EUNSUPPORTED, "dz/mz in a full-variable build is not supported by this build");
+      if (ft.mz != 0 || (ft.dz != 0 && ft.zero_kind))
+        throw CoralError(CORAL_EUNSUPPORTED,
+                         "mz, and dz of a mean variable, in a full-variable build are not supported by this build");
       FullTermDev& o = fv[f].term[t];
       o.zero_kind = ft.zero_kind ? 1 : 0;
       o.dx = ft.dx;
@@ -646,6 +654,29 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
         o.set = it->second.first;
         o.tab_t = h->ks[it->second.first].d_tab_t[it->second.second];
         o.tab_v = h->ks[it->second.first].d_tab_v[it->second.second];
+        if (ft.dz != 0) {
+          // built by k_full_dz (dsca applied before the derivatives, as the
+          // reference does), read back through an identity stencil
+          if (h->ks.size() + h->dz_jobs.size() >= (size_t)kMaxSets)
+            throw CoralError(CORAL_EUNSUPPORTED, "too many z-derivative terms in the full-variable builds");
+          if (!h->d_tab_id_t) {
+            std::vector<int> tt((size_t)g.NZ * kTabW, -1);
+            std::vector<double> tv((size_t)g.NZ * kTabW, 0.0);
+            for (int n = 0; n < g.NZ; ++n) {
+              tt[(size_t)n * kTabW] = n;
+              tv[(size_t)n * kTabW] = 1.0;
+            }
+            h->d_tab_id_t = mem.upload(tt);
+            h->d_tab_id_v = mem.upload(tv);
+          }
+          coral_handle::DzJob j{o.set, h->ks[o.set].T, ft.dz, o.tab_t, o.tab_v, o.dsca,
+                                mem.get<double2>((size_t)g.NXH * g.NYAA * g.NZ)};
+          o.set = (int)(h->ks.size() + h->dz_jobs.size());
+          o.tab_t = h->d_tab_id_t;
+          o.tab_v = h->d_tab_id_v;
+          o.dsca = 1.0;
+          h->dz_jobs.push_back(j);
+        }
       }
     }
   }
@@ -701,19 +732,32 @@ StateSet state_set(coral_handle* h, bool use_field) {
     st.k[s] = use_field ? h->ks[s].field : h->ks[s].aux;
     st.kT[s] = h->ks[s].T;
   }
+  for (size_t j = 0; j < h->dz_jobs.size(); ++j) {  // the dz terms' buffers (pseudo-systems)
+    st.k[h->ks.size() + j] = h->dz_jobs[j].out;
+    st.kT[h->ks.size() + j] = h->d.NZ;
+  }
   for (size_t s = 0; s < h->zs.size(); ++s) st.z[s] = use_field ? h->zs[s].dev.field : h->zs[s].dev.aux;
   return st;
+}
+
+// the dz terms of the full-variable builds from the state set st (before the build)
+int launch_dz_jobs(coral_handle* h, const StateSet& st) {
+  for (auto& j : h->dz_jobs)
+    launch_full_dz(h->d, st.k[j.set], j.T, j.tab_t, j.tab_v, j.dsca, j.order, h->G->gap, j.out, h->stream);
+  return (int)h->dz_jobs.size();
 }
 
 // inverse transforms of all full variables built from field (stage 0) or aux
 int full_vars_to_phys(coral_handle* h, bool use_field, bool cfl) {
   const Dims& d = h->d;
-  launch_inv_y(d, h->nF, h->d_fv, state_set(h, use_field), nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream,
+  const StateSet st = state_set(h, use_field);
+  const int ndz = launch_dz_jobs(h, st);
+  launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream,
                h->fv_single && !h->tune.inv_y_loop);
   launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream);
   if (cfl) CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
   launch_inv_z(d, h->nF, h->Y2, h->fphys, h->pz, h->dct_tw, h->d_wz, cfl ? h->cfl_bits : nullptr, h->stream);
-  return 3;
+  return 3 + ndz;
 }
 
 constexpr int kProfileClasses = 11;  // coral_profile_step
@@ -833,6 +877,7 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
                        h->tune.inv_x_tiles == 1 && (size_t)d.NXA * d.NYA >= (size_t)288 * 288;
   if (chunked) {
     StateSet st = state_set(h, i == 0);
+    nl += launch_dz_jobs(h, st);
     launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream, h->fv_single && !h->tune.inv_y_loop);
     if (last) CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
     QuadDesc q = h->quads;
@@ -860,7 +905,8 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
   if (!chunked) {
     {
       StateSet st = state_set(h, i == 0);
-      B(0); launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream, h->fv_single && !h->tune.inv_y_loop); E();
+      B(0); nl += launch_dz_jobs(h, st);
+      launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream, h->fv_single && !h->tune.inv_y_loop); E();
       B(1); launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream, h->tune.x_plan, h->tune.inv_x_tiles); E();
       // the CFL maxima reported after a step are those of its last stage's fields
       // (each stage's evaluation replaces them): only the last stage computes them

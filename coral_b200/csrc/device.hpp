@@ -9,7 +9,7 @@
 
 namespace coral {
 
-constexpr int kMaxGroups = 8;   // monomial groups (i kx)^a (i ky)^b per operator
+constexpr int kMaxGroups = 16;  // monomial groups (i kx)^a (i ky)^b per operator
 constexpr int kMaxStages = 4;   // ARS_443 has 4 implicit stages
 constexpr int kMaxSets = 8;     // coupled systems of one kind
 constexpr int kMaxQuad = 16;    // quadratic variables
@@ -320,6 +320,11 @@ void launch_zero_step(const ZeroArgs& a, cudaStream_t s);
 void launch_zero_factor(const ZeroArgs& a, cudaStream_t s);
 
 // QuickSave helpers
+// the z derivatives (order) of dsca x one kxky variable's Chebyshev coefficients
+// (its stencil tab_t / tab_v applied to state, T entries per (kx, ky)) into
+// out[kx][ky][n]: the full-variable build's dz terms
+void launch_full_dz(const Dims& d, const double2* state, int T, const int* tab_t, const double* tab_v, double dsca,
+                    int order, double gap, double2* out, cudaStream_t s);
 // user outputs: a slice (kind 1 z, 2 y, 3 x at index k) or the weighted z sum
 // (kind 4) of phys[y][x][z] in the reference's file order; the horizontal-average
 // profile; the product of two fields (b null: a copy)

@@ -1576,14 +1576,16 @@ constexpr int kTpbThreads = 128;
 // Assembly of block b (system b / ncls, class b % ncls) of M - dt a(0,0) L into
 // its interleaved band storage: zero fill, then every operator entry added in
 // row order (M before L, slots in order).
+// G: the monomial groups the coefficient registers hold (>= the operators' ngroups)
+template <int G = kMaxGroups>
 __device__ void assemble_tpb(const FactorArgs& a, int b) {
   const int sys = b / a.ncls, cls = b - sys * a.ncls;
   const int T = a.Tc, kl = a.kl, ku = a.ku, kv = kl + ku, ldab = a.ldab;
   const int sid = a.act_list[sys];
   const int kx = sid / a.d.NYA, ky = sid - kx * a.d.NYA;
-  double2 cm[kMaxGroups], cl[kMaxGroups];
+  double2 cm[G], cl[G];
 #pragma unroll
-  for (int g = 0; g < kMaxGroups; ++g) {
+  for (int g = 0; g < G; ++g) {
     cm[g] = (g < a.M.ngroups) ? cmul(ipow(a.kx[kx], a.M.gkx[g]), ipow(a.ky[ky], a.M.gky[g])) : zero2();
     cl[g] = (g < a.L.ngroups) ? cmul(ipow(a.kx[kx], a.L.gkx[g]), ipow(a.ky[ky], a.L.gky[g])) : zero2();
   }
@@ -1607,7 +1609,7 @@ __device__ void assemble_tpb(const FactorArgs& a, int b) {
         const int jc = a.col_pos[c] - cls * T;  // column in the class
         double2 cv = zero2();
 #pragma unroll
-        for (int gg = 0; gg < kMaxGroups; ++gg)
+        for (int gg = 0; gg < G; ++gg)
           if (g == gg) cv = pass ? cl[gg] : cm[gg];
         double2 z = cscale(cv, v);
         if (pass) z = cscale(z, a.zsca);
@@ -1618,9 +1620,10 @@ __device__ void assemble_tpb(const FactorArgs& a, int b) {
   }
 }
 
+template <int G>
 __global__ void __launch_bounds__(kTpbThreads) k_assemble_tpb(FactorArgs a) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b < a.ncls * a.nact) assemble_tpb(a, b);
+  if (b < a.ncls * a.nact) assemble_tpb<G>(a, b);
 }
 
 __global__ void __launch_bounds__(kTpbThreads) k_factor_tpb(FactorArgs a) {
@@ -2715,6 +2718,57 @@ __global__ void k_phys_product(size_t n, const double* a, const double* b, doubl
     out[e] = b ? a[e] * b[e] : a[e];
 }
 
+// ------------------------------------------------------------------------------
+// z derivatives in full-variable builds (compute_full_variables_in_physical_space,
+// marching.f90:455-466, with differentiate_kxky, PL_IMEX_timestepping.f90:276-319):
+// per (kx, ky) column, the Chebyshev coefficients of one kxky variable (its
+// Galerkin stencil applied to the state) times dsca, differentiated `order`
+// times -- the coefficients shifted down by one and back-substituted against
+// the Chebyshev integration operator trunc(I)[rows 2..NZ, cols 1..NZ-1] (upper
+// triangular: diagonal gap/2 at n = 0, gap/(4(n+1)) beyond; second
+// super-diagonal -gap/(4(n+1)); prepare_chebyshev_integration, :488-505), the
+// last coefficient zero -- into out[kx][ky][n].  One thread per column; the
+// back substitution runs in place with the values it still needs in registers.
+// ------------------------------------------------------------------------------
+__global__ void k_full_dz(Dims d, const double2* state, int T, const int* tab_t, const double* tab_v, double dsca,
+                          int order, double gap, double2* out) {
+  const size_t ncol = (size_t)d.NXH * d.NYA;
+  const int NZ = d.NZ;
+  for (size_t col = (size_t)blockIdx.x * blockDim.x + threadIdx.x; col < ncol; col += (size_t)gridDim.x * blockDim.x) {
+    const double2* sv = state + col * T;
+    double2* o = out + col * NZ;
+    for (int n = 0; n < NZ; ++n) {
+      double2 c = zero2();
+      for (int k = 0; k < kTabW; ++k) {
+        const int tt = tab_t[n * kTabW + k];
+        if (tt >= 0) {
+          const double w = tab_v[n * kTabW + k];
+          const double2 x = sv[tt];
+          c.x += w * x.x;
+          c.y += w * x.y;
+        }
+      }
+      o[n] = cscale(c, dsca);
+    }
+    for (int r = 0; r < order; ++r) {
+      double2 chi = o[NZ - 1];                 // c(n + 1), not yet overwritten
+      double2 dp1 = zero2(), dp2 = zero2();    // d(n + 1), d(n + 2)
+      for (int n = NZ - 2; n >= 0; --n) {
+        const double2 cn = o[n];
+        const double diag = (n == 0) ? 0.5 * gap : gap / (4.0 * (n + 1));
+        const double sup = -gap / (4.0 * (n + 1));
+        const double2 v = (n + 2 <= NZ - 2) ? make_double2(chi.x - sup * dp2.x, chi.y - sup * dp2.y) : chi;
+        const double2 dn = make_double2(v.x / diag, v.y / diag);
+        o[n] = dn;
+        chi = cn;
+        dp2 = dp1;
+        dp1 = dn;
+      }
+      o[NZ - 1] = zero2();
+    }
+  }
+}
+
 // Projection of Chebyshev coefficients onto one variable's Galerkin basis
 // (square-stencil solve of import_quicksave, PL_IMEX_timestepping_output.f90:343-355).
 // The square stencil is lower triangular, so a forward substitution solves it;
@@ -3132,7 +3186,10 @@ void launch_factor_real(const FactorArgs& a, cudaStream_t s) {
     const size_t wbytes = (size_t)(a.kl + a.ku + 2) * a.ldab * sizeof(double);
     const int nt = (int)std::min<size_t>(32, (size_t)smax / wbytes);
     if (a.window && a.kl <= kFacKl && nt >= 1) {
-      k_assemble_tpb<<<(nb + kTpbThreads - 1) / kTpbThreads, kTpbThreads, 0, s>>>(a);
+      if (a.M.ngroups <= 8 && a.L.ngroups <= 8)
+        k_assemble_tpb<8><<<(nb + kTpbThreads - 1) / kTpbThreads, kTpbThreads, 0, s>>>(a);
+      else
+        k_assemble_tpb<kMaxGroups><<<(nb + kTpbThreads - 1) / kTpbThreads, kTpbThreads, 0, s>>>(a);
       set_smem(k_factor_win, (size_t)nt * wbytes);
       k_factor_win<<<(nb + nt - 1) / nt, nt, (size_t)nt * wbytes, s>>>(a);
     } else {
@@ -3157,6 +3214,10 @@ void launch_zero_step(const ZeroArgs& a, cudaStream_t s) {
 void launch_zero_factor(const ZeroArgs& a, cudaStream_t s) {
   if (a.nsys <= 0) return;
   k_zero_factor<<<a.nsys, 32, 0, s>>>(a);
+}
+void launch_full_dz(const Dims& d, const double2* state, int T, const int* tab_t, const double* tab_v, double dsca,
+                    int order, double gap, double2* out, cudaStream_t s) {
+  k_full_dz<<<grid1d((size_t)d.NXH * d.NYA, 128), 128, 0, s>>>(d, state, T, tab_t, tab_v, dsca, order, gap, out);
 }
 void launch_usr_slice(const Dims& d, const double* phys, int kind, int k, const double* wz, double* out,
                       cudaStream_t s) {

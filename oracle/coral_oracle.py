@@ -803,13 +803,13 @@ class Solver:
         for name, ext, terms in r.full_vars:
             spec = np.zeros((g.NXH, g.NYAA, g.NZ), dtype=np.complex128)
             for t in terms:
-                if t.dz != 0:
-                    raise NotImplementedError("dz in full-variable builds")
                 if t.kind == "kxky":
                     isys, pos = r.kxky_loc[r.kxky_vars[t.var]]
                     buf = self._stencil_extract(isys, pos, src_kxky[isys])
                     buf = t.dsca * buf
-                    if t.dx == 0 and t.dy == 0:
+                    if t.dz:
+                        buf = self.differentiate(buf, t.dz)
+                    if t.dx == 0 and t.dy == 0 and t.dz == 0:
                         spec = spec + buf
                     else:
                         fx = np.array([complex_pow(complex(p), t.dx) for p in g.px])
@@ -820,8 +820,35 @@ class Solver:
                     lay = self.zlay[isys]
                     S = stencil(g.NZ, r.zero[isys].bcs[pos])
                     buf = S @ src_zero[isys][lay.var_pos[pos]]
+                    if t.dz:
+                        buf = self.differentiate(buf, t.dz)
                     spec[0, 0, :] = spec[0, 0, :] + buf * t.dsca
             out.append(spec)
+        return out
+
+    def differentiate(self, c: np.ndarray, order: int) -> np.ndarray:
+        """differentiate_kxky / differentiate_zero (PL_IMEX_timestepping.f90:276-360)
+        along the last axis (Chebyshev coefficients 0..NZ-1), `order` times: the
+        coefficients shifted down by one (deriv(n) = c(n + 1)) solved against the
+        Chebyshev integration operator trunc(I)[rows 2..NZ, cols 1..NZ-1]
+        (prepare_chebyshev_integration, :488-505; padding 10), the last
+        coefficient set to zero."""
+        g = self.g
+        NZ = g.NZ
+        I, _ = cheb_elementary(NZ, g.center, g.gap, 10)
+        A = I[1:NZ, 0:NZ - 1]  # upper triangular: diagonal and second super-diagonal
+        out = np.array(c, dtype=np.result_type(c, np.float64), copy=True)
+        for _ in range(order):
+            rhs = out[..., 1:NZ].copy()
+            d = np.zeros_like(rhs)
+            # back substitution (the band LU of an upper-triangular band has no pivots)
+            for n in range(NZ - 2, -1, -1):
+                v = rhs[..., n]
+                if n + 2 <= NZ - 2:
+                    v = v - A[n, n + 2] * d[..., n + 2]
+                d[..., n] = v / A[n, n]
+            out[..., :NZ - 1] = d
+            out[..., NZ - 1] = 0.0
         return out
 
     def nl_terms(self, qspec: List[np.ndarray]):

@@ -277,3 +277,45 @@ def test_variants_compute_the_same_step():
         pl.set_field(0, f)
         return pl
     _variants_match(make5, 1, 1e-5).close()
+
+
+def test_toroidal_poloidal_benchmark02_recipe_matches_oracle():
+    """The toroidal-poloidal form of benchmark 02, the reference's own
+    coral.equations.toroidalPoloidal read unmodified: full variables built with
+    z derivatives (uFull = uMean + dy psi + dx dz phi, vFull = vMean - dx psi +
+    dz dy phi), phi with four boundary conditions (code 40), fourth-order
+    equations with up to ten (kx, ky) monomials per operator.  At the benchmark's
+    parameters on a 16 x 16 x 24 grid, three steps of the time loop against the
+    oracle (every coupled and mean field, the timeseries objects and the
+    physical full variables)."""
+    from coral_b200.solver import PlaneLayer
+    b = os.path.join(GOLDEN, "benchmark02")
+    eq = open(os.path.join(b, "coral.equations.toroidalPoloidal")).read()
+    par = open(os.path.join(b, "coral.parameters.in")).read().splitlines(True)
+    par[1], par[2], par[3] = "16\n", "16\n", "24\n"
+    par[10], par[12] = "1.d-4\n", "1.d30\n"  # dt fixed at 1e-4 (the CFL rule is tested above)
+    par = "".join(par)
+    ref = co.Solver(eq, par)
+    pl = PlaneLayer(eq, par)
+    assert pl.T == [l.T for l in ref.lay] and pl.Tz == [l.T for l in ref.zlay]
+    # a small random state: the fourth-order operators turn larger random
+    # coefficients into violent transients
+    _random_state(ref, pl, 44, amp=1e-8)
+    objs = [("tFull", 1), ("tFull", 12), ("uu", None), ("ww", None)]
+    pl.set_timeseries(">>Horizontal_avg :: tFull ;; Position= 1 <<\n>>Horizontal_avg :: tFull ;; Position= 12 <<\n"
+                      ">>Volume_average :: uu <<\n>>Volume_average :: ww <<\n>>EOF<<\n")
+    rows = ref.run(3, objs)
+    pl.run(3)
+    got = pl.timeseries()[:len(objs)]
+    want = np.array(rows[-1][3])
+    assert np.all(np.abs(got - want) <= 1e-10 * np.abs(want) + 1e-15), (got, want)
+    for s in range(len(ref.lay)):
+        assert _rel(pl.get_field(s), ref.field[s]) < 1e-10
+    for s in range(len(ref.zlay)):
+        assert _rel(pl.get_mean_field(s), ref.zfield[s]) < 1e-10
+    # the physical full variables (the z-derivative terms) at the final state
+    fphys, _ = ref.compute_phys(ref.field, ref.zfield)[:2]
+    for f in range(4):
+        g = pl.full_phys(f)
+        assert np.abs(g - fphys[f]).max() <= 1e-11 * max(np.abs(fphys[f]).max(), 1e-300), f
+    pl.close()
