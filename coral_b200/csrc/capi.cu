@@ -158,6 +158,10 @@ struct coral_handle {
   // ks.size() + j through an identity stencil
   struct DzJob { int set, T, order; const int* tab_t; const double* tab_v; double dsca; double2* out; };
   std::vector<DzJob> dz_jobs;
+  // the same for dz terms of mean variables: one profile each, read as mean
+  // pseudo-system zs.size() + j
+  struct ZDzJob { int set, order; const int* tab_t; const double* tab_v; double dsca; double* out; };
+  std::vector<ZDzJob> zdz_jobs;
   QuadDesc quads{};
   std::vector<int> zmean_quads;
   double2 *Y1 = nullptr, *qspec = nullptr, *tmp_spec = nullptr;
@@ -635,9 +639,8 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
     fv[f].nterms = (int)F.terms.size();
     for (size_t t = 0; t < F.terms.size(); ++t) {
       const FullTerm& ft = F.terms[t];
-      if (ft.mz != 0 || (ft.dz != 0 && ft.zero_kind))
-        throw CoralError(CORAL_EUNSUPPORTED,
-                         "mz, and dz of a mean variable, in a full-variable build are not supported by this build");
+      if (ft.mz != 0)  // compute_full_variables_in_physical_space applies no mz (marching.f90:436-503)
+        throw CoralError(CORAL_EUNSUPPORTED, "mz in a full-variable build is not supported");
       FullTermDev& o = fv[f].term[t];
       o.zero_kind = ft.zero_kind ? 1 : 0;
       o.dx = ft.dx;
@@ -648,6 +651,27 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
         o.set = loc.first;
         o.tab_t = h->zs[loc.first].d_tab_t[loc.second];
         o.tab_v = h->zs[loc.first].d_tab_v[loc.second];
+        if (ft.dz != 0) {  // built by k_zero_dz, read back through an identity stencil
+          if (h->zs.size() + h->zdz_jobs.size() >= (size_t)kMaxSets)
+            throw CoralError(CORAL_EUNSUPPORTED, "too many z-derivative terms in the full-variable builds");
+          if (!h->d_tab_id_t) {
+            std::vector<int> tt((size_t)g.NZ * kTabW, -1);
+            std::vector<double> tv((size_t)g.NZ * kTabW, 0.0);
+            for (int n = 0; n < g.NZ; ++n) {
+              tt[(size_t)n * kTabW] = n;
+              tv[(size_t)n * kTabW] = 1.0;
+            }
+            h->d_tab_id_t = mem.upload(tt);
+            h->d_tab_id_v = mem.upload(tv);
+          }
+          // (the reference scales a mean term by dsca after its derivatives: the
+          // build applies o.dsca to the differentiated profile)
+          coral_handle::ZDzJob j{o.set, ft.dz, o.tab_t, o.tab_v, 1.0, mem.get<double>(g.NZ)};
+          o.set = (int)(h->zs.size() + h->zdz_jobs.size());
+          o.tab_t = h->d_tab_id_t;
+          o.tab_v = h->d_tab_id_v;
+          h->zdz_jobs.push_back(j);
+        }
       } else {
         auto it = R.kxky_loc.find(R.kxky_vars[ft.var]);
         if (it == R.kxky_loc.end()) throw CoralError(CORAL_EPARSE, "kxky variable in no coupled system");
@@ -737,6 +761,7 @@ StateSet state_set(coral_handle* h, bool use_field) {
     st.kT[h->ks.size() + j] = h->d.NZ;
   }
   for (size_t s = 0; s < h->zs.size(); ++s) st.z[s] = use_field ? h->zs[s].dev.field : h->zs[s].dev.aux;
+  for (size_t j = 0; j < h->zdz_jobs.size(); ++j) st.z[h->zs.size() + j] = h->zdz_jobs[j].out;
   return st;
 }
 
@@ -744,7 +769,9 @@ StateSet state_set(coral_handle* h, bool use_field) {
 int launch_dz_jobs(coral_handle* h, const StateSet& st) {
   for (auto& j : h->dz_jobs)
     launch_full_dz(h->d, st.k[j.set], j.T, j.tab_t, j.tab_v, j.dsca, j.order, h->G->gap, j.out, h->stream);
-  return (int)h->dz_jobs.size();
+  for (auto& j : h->zdz_jobs)
+    launch_zero_dz(h->d.NZ, st.z[j.set], j.tab_t, j.tab_v, j.dsca, j.order, h->G->gap, j.out, h->stream);
+  return (int)(h->dz_jobs.size() + h->zdz_jobs.size());
 }
 
 // inverse transforms of all full variables built from field (stage 0) or aux

@@ -325,6 +325,9 @@ void launch_zero_factor(const ZeroArgs& a, cudaStream_t s);
 // out[kx][ky][n]: the full-variable build's dz terms
 void launch_full_dz(const Dims& d, const double2* state, int T, const int* tab_t, const double* tab_v, double dsca,
                     int order, double gap, double2* out, cudaStream_t s);
+// the same for one mean variable's profile (state: its system's vector)
+void launch_zero_dz(int NZ, const double* state, const int* tab_t, const double* tab_v, double dsca, int order,
+                    double gap, double* out, cudaStream_t s);
 // user outputs: a slice (kind 1 z, 2 y, 3 x at index k) or the weighted z sum
 // (kind 4) of phys[y][x][z] in the reference's file order; the horizontal-average
 // profile; the product of two fields (b null: a copy)

@@ -2769,6 +2769,36 @@ __global__ void k_full_dz(Dims d, const double2* state, int T, const int* tab_t,
   }
 }
 
+// The same for a mean variable (differentiate_zero, PL_IMEX_timestepping.f90:
+// 321-360): one real profile, one thread.
+__global__ void k_zero_dz(int NZ, const double* state, const int* tab_t, const double* tab_v, double dsca,
+                          int order, double gap, double* out) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int n = 0; n < NZ; ++n) {
+    double c = 0.0;
+    for (int k = 0; k < kTabW; ++k) {
+      const int tt = tab_t[n * kTabW + k];
+      if (tt >= 0) c += tab_v[n * kTabW + k] * state[tt];
+    }
+    out[n] = c * dsca;
+  }
+  for (int r = 0; r < order; ++r) {
+    double chi = out[NZ - 1], dp1 = 0.0, dp2 = 0.0;
+    for (int n = NZ - 2; n >= 0; --n) {
+      const double cn = out[n];
+      const double diag = (n == 0) ? 0.5 * gap : gap / (4.0 * (n + 1));
+      const double sup = -gap / (4.0 * (n + 1));
+      const double v = (n + 2 <= NZ - 2) ? chi - sup * dp2 : chi;
+      const double dn = v / diag;
+      out[n] = dn;
+      chi = cn;
+      dp2 = dp1;
+      dp1 = dn;
+    }
+    out[NZ - 1] = 0.0;
+  }
+}
+
 // Projection of Chebyshev coefficients onto one variable's Galerkin basis
 // (square-stencil solve of import_quicksave, PL_IMEX_timestepping_output.f90:343-355).
 // The square stencil is lower triangular, so a forward substitution solves it;
@@ -3218,6 +3248,10 @@ void launch_zero_factor(const ZeroArgs& a, cudaStream_t s) {
 void launch_full_dz(const Dims& d, const double2* state, int T, const int* tab_t, const double* tab_v, double dsca,
                     int order, double gap, double2* out, cudaStream_t s) {
   k_full_dz<<<grid1d((size_t)d.NXH * d.NYA, 128), 128, 0, s>>>(d, state, T, tab_t, tab_v, dsca, order, gap, out);
+}
+void launch_zero_dz(int NZ, const double* state, const int* tab_t, const double* tab_v, double dsca, int order,
+                    double gap, double* out, cudaStream_t s) {
+  k_zero_dz<<<1, 32, 0, s>>>(NZ, state, tab_t, tab_v, dsca, order, gap, out);
 }
 void launch_usr_slice(const Dims& d, const double* phys, int kind, int k, const double* wz, double* out,
                       cudaStream_t s) {

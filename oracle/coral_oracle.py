@@ -820,7 +820,7 @@ class Solver:
                     lay = self.zlay[isys]
                     S = stencil(g.NZ, r.zero[isys].bcs[pos])
                     buf = S @ src_zero[isys][lay.var_pos[pos]]
-                    if t.dz:
+                    if t.dz:  # differentiate_zero, then dsca (marching.f90:488-494)
                         buf = self.differentiate(buf, t.dz)
                     spec[0, 0, :] = spec[0, 0, :] + buf * t.dsca
             out.append(spec)

@@ -319,3 +319,33 @@ def test_toroidal_poloidal_benchmark02_recipe_matches_oracle():
         g = pl.full_phys(f)
         assert np.abs(g - fphys[f]).max() <= 1e-11 * max(np.abs(fphys[f]).max(), 1e-300), f
     pl.close()
+
+
+def test_z_derivatives_of_kxky_and_mean_variables_in_full_builds():
+    """A recipe whose extra full variables take first and second z derivatives
+    of a kxky and of a mean variable (tz = dz tMean + dz t, tzz = dz dz tMean
+    + dz dz t + dx dz w): their physical fields against the oracle's
+    (differentiate_kxky / differentiate_zero restated)."""
+    from coral_b200.solver import PlaneLayer
+    eq = equations("rbc_noslip_ra1e8", **{"1.d8": "1.d5"})
+    extra = (">>linear_variable_full       :: tz <<\n>>linear_variable_full_build :: + dz.tMean <<\n"
+             ">>linear_variable_full_build :: + dz.t <<\n>>====================================<<\n"
+             ">>linear_variable_full       :: tzz <<\n>>linear_variable_full_build :: + dz.dz.tMean <<\n"
+             ">>linear_variable_full_build :: + dz.dz.t <<\n>>linear_variable_full_build :: + dx.dz.w <<\n"
+             ">>====================================<<\n")
+    i = eq.index(">>quadratic_variable")
+    eq = eq[:i] + extra + eq[i:]
+    par = _params(16, 12, 24, 1e-5, 0.3, 1e30)
+    ref = co.Solver(eq, par)
+    pl = PlaneLayer(eq, par)
+    _random_state(ref, pl, 51, amp=1e-2)
+    fphys = ref.compute_phys(ref.field, ref.zfield)[0]
+    names = [f[0] for f in ref.recipe.full_vars]
+    for f in (names.index("tz"), names.index("tzz")):
+        g = pl.full_phys(f)
+        assert np.abs(g - fphys[f]).max() <= 1e-12 * np.abs(fphys[f]).max(), names[f]
+    pl.march_forward(1e-5, 2)
+    ref.step(1e-5)
+    ref.step(1e-5)
+    assert _rel(pl.get_field(0), ref.field[0]) < 1e-10
+    pl.close()
