@@ -1959,6 +1959,14 @@ int coral_export_checkpoint(coral_handle* h, const char* directory, int rolling)
         CK(cudaMemcpyAsync(buf.data(), h->fphys, np * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         write_file(qs_name(directory, "kxky", (int)s + 1, v + 1, rolling), buf);
+        // as export_checkpoints does (PL_IMEX_timestepping_output.f90:412-425), the
+        // variable's Galerkin coefficients are replaced by the projection of the
+        // field just written (phys -> spec, square-stencil solve, insertion): the
+        // state is then exactly what importing these files gives.  The other
+        // variables' slots are untouched, so the next extraction reads the
+        // original state; the mean systems are not re-projected (nor are they by
+        // the reference).
+        set_var_phys_dev(h, (int)s, v, h->tmp_phys);
       }
     }
     for (size_t s = 0; s < h->zs.size(); ++s)

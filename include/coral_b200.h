@@ -140,7 +140,10 @@ int coral_get_full_phys(coral_handle* h, int ivar, double* phys);
  * Read / write the QuickSave files of a directory (…/QuickSave.kxky.sysSSS.varVVV.rollingR,
  * …/QuickSave.zero.sysSSS.varVVV.rollingR; physical fields in z-fastest, y, x order).
  * Replace main%import_quickSave and main%export_checkpoints
- * (src/plane_layer/PL_IMEX_timestepping_output.f90:309-456).
+ * (src/plane_layer/PL_IMEX_timestepping_output.f90:309-456).  As the reference's
+ * export does, coral_export_checkpoint then replaces each coupled variable's
+ * state by the projection of the field it wrote (the state becomes what
+ * importing the files gives; a round-off change on the represented modes).
  */
 int coral_import_quicksave(coral_handle* h, const char* directory, int rolling);
 int coral_export_checkpoint(coral_handle* h, const char* directory, int rolling);
