@@ -154,7 +154,7 @@ def make_ic(cfg, pl):
 
 # kernels of each timed phase (names as ncu lists them)
 PHASE_KERNELS = {
-    "inv_y": "k_inv_y", "inv_x": "k_inv_x", "inv_z": "k_inv_z", "z_products": "k_z_fused",
+    "inv_y": "k_inv_y1", "inv_x": "k_inv_x", "inv_z": "k_inv_z", "z_products": "k_z_fused",
     "fwd_x": "k_fwd_x", "fwd_y": "k_fwd_y_pipe", "nl_assembly": "k_nl",
     "rhs_nl": "k_rhs_tiles", "mean_systems": "k_zero_step", "substitution": "k_subst_tpb", "kstd_out": "k_kstd_tiles",
 }
