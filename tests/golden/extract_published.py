@@ -9,7 +9,8 @@ Rayleigh-Benard growth rate quoted by benchmark 01
 (etc/benchmarks/01_Rayleigh_Benard_stressFree/benchmark_01_stressfree_rayleigh_benard.ipynb:68)
 is stored beside them, with benchmark 02's published mean Nusselt number and
 its standard deviation (velocity-pressure form) and a verbatim copy of that
-benchmark's input files (tests/golden/benchmark02/: both equation forms).
+benchmark's input files (tests/golden/benchmark02/: both equation forms), and
+benchmark 01's (tests/golden/benchmark01/).
 
 usage: python tests/golden/extract_published.py <path-to-coral-tree>
 """
@@ -51,6 +52,14 @@ def main(root):
     for name in ("coral.equations.velocityPressure", "coral.equations.toroidalPoloidal", "coral.parameters.in",
                  "coral.timeseries", "coral.usrOutput"):
         with open(os.path.join(root, "etc/benchmarks/02_RRBC_julien_JFM96", name), "rb") as f:
+            data = f.read()
+        with open(os.path.join(dst, name), "wb") as f:
+            f.write(data)
+    # benchmark 01's input files (stress-free Rayleigh-Benard, linear growth)
+    dst = os.path.join(here, "benchmark01")
+    os.makedirs(dst, exist_ok=True)
+    for name in ("coral.equations", "coral.parameters.in", "coral.timeseries"):
+        with open(os.path.join(root, "etc/benchmarks/01_Rayleigh_Benard_stressFree", name), "rb") as f:
             data = f.read()
         with open(os.path.join(dst, name), "wb") as f:
             f.write(data)
