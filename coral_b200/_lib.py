@@ -22,6 +22,8 @@ SIGNATURES = {
     "coral_create": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(_P)]),
     "coral_create_from_files": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
                                                ctypes.POINTER(_P)]),
+    "coral_create_with_args": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_int,
+                                              ctypes.c_char_p, ctypes.POINTER(_P)]),
     "coral_destroy": (None, [_P]),
     "coral_last_error": (ctypes.c_char_p, [_P]),
     "coral_query": (ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong)]),
@@ -53,6 +55,8 @@ SIGNATURES = {
     "coral_get_time": (ctypes.c_int, [_P, _D]),
     "coral_run": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_char_p]),
     "coral_set_z_transform": (ctypes.c_int, [_P, ctypes.c_int]),
+    "coral_set_source": (ctypes.c_int, [_P, ctypes.c_int, _D]),
+    "coral_set_penalisation_mask": (ctypes.c_int, [_P, _D]),
     "coral_set_hermitian_kx0": (ctypes.c_int, [_P, ctypes.c_int]),
     "coral_var_positions": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int,
                                            ctypes.POINTER(ctypes.c_int)]),

@@ -1,6 +1,7 @@
 // The C-ABI (include/coral_b200.h): a handle owns the parsed problem, the
 // device-resident state, operators, LU factors and transform buffers, one CUDA
 // stream and a CUDA graph of one timestep.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -184,7 +185,7 @@ struct coral_handle {
   double* ts_partial = nullptr;   // [z_fused_ctas][kMaxTs]
   size_t ts_ncta = 0;
   double* ts_out = nullptr;       // [kMaxTs], totals of the last step's first stage
-  double* h_pin = nullptr;        // page-locked readback: kMaxTs timeseries values, 3 CFL maxima, flags
+  double* h_pin = nullptr;        // page-locked readback: kMaxTs timeseries values, 4 CFL maxima
   // time keeping of the driver loop (src/misc/timeKeeping.f90:22-49)
   double time = 0.0, dt_current = 0.0, dt_target = 0.0;
   long long i_timestep = 1, refactorizations = 0;
@@ -201,6 +202,27 @@ struct coral_handle {
   // tensor cores (zsplit.cu); form_last = the form of the last step (KE sums)
   int zform = 0, zform_last = 0;
   bool hermitian_kx0 = false;  // project the kx = 0 line onto its Hermitian part after each step
+  // the reference's command-line switches (coral_create_with_args)
+  bool smagorinsky = false;        // --withHorizontalSmagorinsky
+  double smago_prefactor = 1.0;    // --smagorinsky-prefactor
+  double cfl_factor_z = 1.0;       // --cflFactor-along-z
+  // full variables that are not plain transforms: penalisation fields ([y][x][z]
+  // each), the Smagorinsky viscosity profile and the z operations of surface
+  // values and vertical decompositions (marching.f90:505-575)
+  std::vector<double*> penal_phys;  // per full variable, null unless penalised
+  int smago_var = -1;
+  std::vector<int> smago_src;       // full variables dxUfull, dyUfull, dxVfull, dyVfull present
+  double* smago_prof = nullptr;     // [NZAA], carried from stage to stage
+  double* smago_part = nullptr;     // [NYAA][NZAA] scratch
+  struct ZFilter { int var, extract, decomp; };
+  std::vector<ZFilter> zfilters;
+  double* d_zgrid = nullptr;        // Gauss-Chebyshev grid (PL_cheby_misc.f90:19-27)
+  // sources of the mean equations: physical profiles on the z grid by index
+  // (defaults: the reference's PL_user_sources_definitions.f90) and the constant
+  // K_hat terms per mean system on the device
+  std::map<int, std::vector<double>> src_phys;
+  std::vector<double*> d_src;
+  std::string src_missing;          // non-empty: a referenced source has no profile
   // kernel variants chosen by coral_autotune (defaults: the choices measured best at 384^2 x 192)
   struct Tune {
     int x_plan = 1;         // x passes: 1 two-pass FFT plans, 0 three-pass
@@ -351,6 +373,91 @@ void stencil_tab(const SystemOps& o, int v, int NZ, std::vector<int>& tt, std::v
   }
 }
 
+// The two sources of the reference's default PL_user_sources_definitions.f90 on
+// the Gauss-Chebyshev grid: source01 = HovEll exp(-z HovEll) / (1 - exp(-HovEll))
+// - 1 (HovEll a sourceParam; sourceParams gives 0 when the file has none, which
+// makes it NaN, and the reference stops when the file has others but not
+// HovEll: source01 then stays undefined), source02 = -1.
+void default_sources(coral_handle* h) {
+  const Geometry& g = *h->G;
+  const double pi = 4.0 * std::atan(1.0);
+  std::vector<double> z(g.NZAA);
+  for (int i = 1; i <= g.NZAA; ++i)
+    z[i - 1] = g.center + std::cos(pi * double(2 * i - 1) / double(2 * g.NZAA)) * 0.5 * g.gap;
+  h->src_phys[2] = std::vector<double>(g.NZAA, -1.0);
+  bool have = false;
+  double hov = 0.0;
+  for (auto& p : h->R.source_params)
+    if (p.first == "HovEll") { have = true; hov = p.second; break; }
+  if (!have && !h->R.source_params.empty()) return;
+  std::vector<double> s1(g.NZAA);
+  for (int i = 0; i < g.NZAA; ++i) s1[i] = hov * std::exp(-z[i] * hov) / (1.0 - std::exp(-hov)) - 1.0;
+  h->src_phys[1] = s1;
+}
+
+// Constant K_hat terms of the mean systems (marching.f90:398-415): each source's
+// Chebyshev coefficients (Compute_1dCheby_transform, marching.f90:845-866:
+// REDFT10 / N, coefficient 0 halved; the first NZ), times dsca, through the
+// truncated Cheb_IM(Iz, 0) rows of its equation.
+void update_sources(coral_handle* h) {
+  const Geometry& g = *h->G;
+  const Recipe& R = h->R;
+  h->src_missing.clear();
+  std::vector<std::vector<double>> K(R.zero.size());
+  for (const SourceTerm& t : R.sources) K[t.set].assign(h->zs[t.set].ops.T, 0.0);
+  const long double pi = 3.141592653589793238462643383279502884L;
+  for (const SourceTerm& t : R.sources) {
+    auto it = h->src_phys.find(t.index);
+    if (it == h->src_phys.end()) {
+      char b[96];
+      std::snprintf(b, sizeof(b), "source%02d is not defined (coral_set_source)", t.index);
+      h->src_missing = b;
+      continue;
+    }
+    const std::vector<double>& ph = it->second;
+    const int N = g.NZAA;
+    std::vector<double> c(g.NZ);
+    for (int k = 0; k < g.NZ; ++k) {
+      long double acc = 0.0L;
+      for (int j = 0; j < N; ++j) acc += (long double)ph[j] * cosl(pi * ((long double)j + 0.5L) * k / N);
+      c[k] = (double)(2.0L * acc) / N;
+    }
+    c[0] = c[0] * 0.5;
+    const SystemOps& o = h->zs[t.set].ops;
+    const Dense C = cheb_IM(g.NZ, g.center, g.gap, t.Iz, 0);
+    const int oe = R.zero[t.set].orders[t.eqn];
+    for (int rr = 0; rr < o.eq_size[t.eqn]; ++rr) {
+      double acc = 0.0;
+      for (int n = 0; n < g.NZ; ++n) acc += C[oe + rr][n] * (c[n] * t.dsca);
+      K[t.set][o.eq_pos[t.eqn][rr]] += acc;
+    }
+  }
+  // (the device vectors are made once, at creation, so captured graphs stay valid)
+  for (size_t s = 0; s < R.zero.size(); ++s) {
+    if (K[s].empty()) continue;
+    if (!h->d_src[s]) h->d_src[s] = h->mem.get<double>(K[s].size());
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(h->d_src[s], K[s].data(), K[s].size() * sizeof(double), cudaMemcpyHostToDevice));
+    h->zs[s].dev.src = h->d_src[s];
+  }
+}
+
+// every penalised variable's field from a mask on the device ([y][x][z])
+void penal_fields(coral_handle* h, const double* mask) {
+  const size_t n = (size_t)h->d.NYA * h->d.NXA * h->d.NZA;
+  for (int f = 0; f < h->nF; ++f)
+    if (h->penal_phys[f])
+      launch_penal_field(n, mask, h->R.full[f].penal_strength, h->R.full[f].penal_width, h->penal_phys[f], h->stream);
+  CK(cudaStreamSynchronize(h->stream));
+}
+
+// the z operations of surface values and vertical decompositions on Y2 rows
+int launch_zfilters(coral_handle* h, int y0, int ny, cudaStream_t s) {
+  const size_t vstride = (size_t)h->d.NYA * h->d.NXA * h->d.NZ;
+  for (auto& z : h->zfilters) launch_zfilter(h->d, h->Y2 + z.var * vstride, z.extract, z.decomp, y0, ny, s);
+  return (int)h->zfilters.size();
+}
+
 void setup(coral_handle* h, const std::string& eqs, const std::string& pars, const char* scheme, int device) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) throw CoralError(CORAL_ENODEV, "no CUDA device");
@@ -359,7 +466,7 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   h->P = parse_parameters(pars);
-  h->R = parse_equations(eqs);
+  h->R = parse_equations(eqs, h->smagorinsky);
   h->TB = ars_tableau(scheme && *scheme ? std::string(scheme) : h->P.scheme);
   if (h->TB.stages > kMaxStages) throw CoralError(CORAL_EUNSUPPORTED, "too many implicit stages");
   const Parameters& P = h->P;
@@ -619,6 +726,7 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
     }
     dz.ab = mem.get<double>((size_t)dz.T * dz.ldab);
     dz.dpiv = mem.get<unsigned char>(dz.T);
+    dz.src = nullptr;
     for (int v = 0; v < z.ops.nV; ++v) {
       std::vector<int> tt;
       std::vector<double> tv;
@@ -722,6 +830,46 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
     if (R.quad[q].name == "vv") h->quads.ke_q[1] = q;
     if (R.quad[q].name == "ww") h->quads.ke_q[2] = q;
   }
+  // full variables that are not plain transforms
+  {
+    std::vector<double> zg(g.NZAA);
+    const double pi = 4.0 * std::atan(1.0);
+    for (int i = 1; i <= g.NZAA; ++i)
+      zg[i - 1] = g.center + std::cos(pi * double(2 * i - 1) / double(2 * g.NZAA)) * 0.5 * g.gap;
+    h->d_zgrid = mem.upload(zg);
+    h->penal_phys.assign(h->nF, nullptr);
+    h->quads.st_n = 0;
+    for (int f = 0; f < h->nF; ++f) {
+      const FullVar& F = R.full[f];
+      if (F.penal || F.smago) {
+        if (h->quads.st_n >= kMaxStatic) throw CoralError(CORAL_EUNSUPPORTED, "too many penalised variables");
+        const int k = h->quads.st_n++;
+        h->quads.st_var[k] = f;
+        h->quads.st_prof[k] = F.smago ? 1 : 0;
+        if (F.smago) {
+          h->smago_var = f;
+          h->smago_prof = mem.get<double>(g.NZAA);
+          CK(cudaMemset(h->smago_prof, 0, g.NZAA * sizeof(double)));
+          h->smago_part = mem.get<double>((size_t)g.NYAA * g.NZAA);
+          h->quads.st_src[k] = h->smago_prof;
+          for (int j = 0; j < h->nF; ++j) {
+            const std::string& n = R.full[j].name;
+            if (n == "dxUfull" || n == "dyUfull" || n == "dxVfull" || n == "dyVfull") h->smago_src.push_back(j);
+          }
+        } else {
+          h->penal_phys[f] = mem.get<double>((size_t)g.NYAA * g.NXAA * g.NZAA);
+          h->quads.st_src[k] = h->penal_phys[f];
+        }
+      } else if (F.extract || F.decomp) {
+        h->zfilters.push_back({f, F.extract, F.decomp});
+      }
+    }
+  }
+  // sources of the mean equations: the reference's default definitions, then the
+  // constant K_hat terms
+  h->d_src.assign(R.zero.size(), nullptr);
+  default_sources(h);
+  update_sources(h);
   // transform buffers
   const int nmax = std::max(std::max(h->nF, h->nQ), 1);
   h->Y1 = mem.get<double2>((size_t)nmax * g.NYAA * g.NXH * g.NZ);
@@ -734,15 +882,22 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
   h->ke_partial = mem.get<double>(h->n_ke_partial);
   h->ke_total = mem.get<double>(1);
   CK(cudaMemset(h->ke_partial, 0, h->n_ke_partial * sizeof(double)));
-  h->cfl_bits = mem.get<unsigned long long>(3);
-  CK(cudaMemset(h->cfl_bits, 0, 3 * sizeof(unsigned long long)));
+  // |u|, |v|, |w| / wz and the Smagorinsky viscosity
+  h->cfl_bits = mem.get<unsigned long long>(4);
+  CK(cudaMemset(h->cfl_bits, 0, 4 * sizeof(unsigned long long)));
   h->flags = mem.get<unsigned int>(1);
   CK(cudaMemset(h->flags, 0, sizeof(unsigned int)));
   h->ts_ncta = z_fused_ctas(h->d);
   h->ts_partial = mem.get<double>(h->ts_ncta * kMaxTs);
   h->ts_out = mem.get<double>(kMaxTs);
   CK(cudaMemset(h->ts_out, 0, kMaxTs * sizeof(double)));
-  CK(cudaMallocHost(&h->h_pin, (kMaxTs + 4) * sizeof(double)));
+  CK(cudaMallocHost(&h->h_pin, (kMaxTs + 5) * sizeof(double)));
+  // penalisation fields from the reference's default mask (coral_set_penalisation_mask
+  // replaces it)
+  if (std::any_of(R.full.begin(), R.full.end(), [](const FullVar& F) { return F.penal; })) {
+    launch_penal_default(h->d, g.Lx, g.Ly, h->d_zgrid, h->tmp_phys, h->stream);
+    penal_fields(h, h->tmp_phys);
+  }
   // timings%init (timeKeeping.f90:57-70): dt_current = dt = dt_max, t = 0, step 1
   h->dt_current = h->dt_target = P.dt_max;
   h->time = 0.0;
@@ -782,9 +937,11 @@ int full_vars_to_phys(coral_handle* h, bool use_field, bool cfl) {
   launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream,
                h->fv_single && !h->tune.inv_y_loop);
   launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream);
-  if (cfl) CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
+  const int nzf = launch_zfilters(h, 0, d.NYA, h->stream);
+  if (cfl) CK(cudaMemsetAsync(h->cfl_bits, 0, 4 * sizeof(unsigned long long), h->stream));
   launch_inv_z(d, h->nF, h->Y2, h->fphys, h->pz, h->dct_tw, h->d_wz, cfl ? h->cfl_bits : nullptr, h->stream);
-  return 3 + ndz;
+  launch_static_phys(d, h->quads, h->fphys, h->stream);
+  return 3 + ndz + nzf + (h->quads.st_n > 0 ? 1 : 0);
 }
 
 constexpr int kProfileClasses = 11;  // coral_profile_step
@@ -900,13 +1057,13 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
   const double scale = 1.0 / ((double)g.NXAA * (double)g.NYAA * (double)g.NZAA);
   const bool last = (i == S - 1);
   // the y-chunked pipeline (eager phase timing keeps whole passes, one kernel per phase)
-  const bool chunked = !pt && h->tune.y_chunks > 1 && h->yfork && !h->closure && h->zform == 0 &&
+  const bool chunked = !pt && h->tune.y_chunks > 1 && h->yfork && !h->closure && h->zform == 0 && h->smago_var < 0 &&
                        h->tune.inv_x_tiles == 1 && (size_t)d.NXA * d.NYA >= (size_t)288 * 288;
   if (chunked) {
     StateSet st = state_set(h, i == 0);
     nl += launch_dz_jobs(h, st);
     launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream, h->fv_single && !h->tune.inv_y_loop);
-    if (last) CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
+    if (last) CK(cudaMemsetAsync(h->cfl_bits, 0, 4 * sizeof(unsigned long long), h->stream));
     QuadDesc q = h->quads;
     q.ts_partial = (i == 0 && q.ts_n > 0) ? h->ts_partial : nullptr;
     // a band of y rows needs only its own rows through the three passes: Y1 rows
@@ -918,6 +1075,7 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
       const int y0 = (int)((long long)d.NYA * c / nch), y1 = (int)((long long)d.NYA * (c + 1) / nch);
       cudaStream_t ss = h->ystream[c % kYStreams];
       launch_inv_x_rows(d, h->nF, h->Y1, h->Y2, h->px, h->tune.x_plan, y0, y1 - y0, ss);
+      nl += launch_zfilters(h, y0, y1 - y0, ss);
       launch_z_fused(d, h->nF, q, h->Y2, h->Y2, h->pz, h->dct_tw, h->d_wz, h->d_wzinv, last ? h->cfl_bits : nullptr,
                      i == 0 ? h->ke_partial : nullptr, ss, h->tune.z_batch6, y0, y1 - y0);
       launch_fwd_x(d, h->nQ, h->Y2, h->Y1, h->px, ss, h->tune.x_plan, y0, y1 - y0);
@@ -934,11 +1092,24 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
       StateSet st = state_set(h, i == 0);
       B(0); nl += launch_dz_jobs(h, st);
       launch_inv_y(d, h->nF, h->d_fv, st, nullptr, h->d_kx, h->d_ky, h->Y1, h->py, h->stream, h->fv_single && !h->tune.inv_y_loop); E();
-      B(1); launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream, h->tune.x_plan, h->tune.inv_x_tiles); E();
+      B(1); launch_inv_x(d, h->nF, h->Y1, h->Y2, h->px, h->stream, h->tune.x_plan, h->tune.inv_x_tiles);
+      nl += launch_zfilters(h, 0, d.NYA, h->stream); E();
       // the CFL maxima reported after a step are those of its last stage's fields
       // (each stage's evaluation replaces them): only the last stage computes them
-      if (last) CK(cudaMemsetAsync(h->cfl_bits, 0, 3 * sizeof(unsigned long long), h->stream));
+      if (last) CK(cudaMemsetAsync(h->cfl_bits, 0, 4 * sizeof(unsigned long long), h->stream));
       nl += 2;
+    }
+    // the Smagorinsky viscosity needs every column's physical fields first: the
+    // inverse z transforms to HBM, the profile, then the z passes with the
+    // profile in nuSmago's place (marching.f90:516-541)
+    const bool smago_now = h->smago_var >= 0 && !h->closure;
+    if (smago_now) {
+      B(3);
+      launch_inv_z(d, h->nF, h->Y2, h->fphys, h->pz, h->dct_tw, h->d_wz, nullptr, h->stream);
+      launch_smago(d, h->fphys, h->smago_src.data(), (int)h->smago_src.size(), h->smago_prefactor, h->smago_part,
+                   h->smago_prof, last ? h->cfl_bits + 3 : nullptr, h->stream);
+      E();
+      nl += 3;
     }
     // z passes fused (inverse DCT, CFL maxima, products, KE, forward DCT); the
     // quadratic variables overwrite Y2 in place, each CTA reading and writing only
@@ -948,6 +1119,15 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
       // unfused z passes around the network: physical fields to HBM, the
       // network's subgrid parts, then the products (plus those parts) forward
       launch_inv_z(d, h->nF, h->Y2, h->fphys, h->pz, h->dct_tw, h->d_wz, last ? h->cfl_bits : nullptr, h->stream);
+      if (h->smago_var >= 0) {
+        launch_smago(d, h->fphys, h->smago_src.data(), (int)h->smago_src.size(), h->smago_prefactor, h->smago_part,
+                     h->smago_prof, last ? h->cfl_bits + 3 : nullptr, h->stream);
+        nl += 2;
+      }
+      if (h->quads.st_n > 0) {
+        launch_static_phys(d, h->quads, h->fphys, h->stream);
+        ++nl;
+      }
       closure_infer(closure_impl(h->closure), h->fphys, d.NYA, d.NXA, d.NZA, h->tau, h->stream);
       QuadDesc q = h->quads;
       q.ts_partial = nullptr;
@@ -1084,6 +1264,8 @@ void set_z_transform(coral_handle* h, int form) {
   if (form != 0 && form != 1) throw CoralError(CORAL_EBADARG, "z transform form must be 0 (FP64) or 1 (int8 digits)");
   const Geometry& g = *h->G;
   if (form == 1) {
+    if (h->quads.st_n > 0)
+      throw CoralError(CORAL_EUNSUPPORTED, "the tensor-core z transform does not take penalised or Smagorinsky variables");
     if (!zsplit_supported(g.NZ, g.NZAA))
       throw CoralError(CORAL_EUNSUPPORTED, "the tensor-core z transform needs NZ and 3 NZ / 2 to be multiples of 96");
     if (!h->zmat_inv) {
@@ -1176,6 +1358,7 @@ void factorize(coral_handle* h, double dt) {
 
 void march(coral_handle* h, double dt, int nsteps) {
   if (!(dt > 0.0) || nsteps < 0) throw CoralError(CORAL_EBADARG, "march: dt must be > 0 and nsteps >= 0");
+  if (!h->src_missing.empty()) throw CoralError(CORAL_EBADARG, h->src_missing);
   CK(cudaSetDevice(h->device));
   if (h->dt_factored != dt) factorize(h, dt);
   int done = 0;
@@ -1338,15 +1521,25 @@ int mkdir_p(const std::string& path) {
 }
 
 // cargo%cfl_based_DT from the CFL maxima of the last step's last stage
-// (compute_cfl_based_timestep, marching.f90:219-238, cflFactor_along_z = 1)
-double cfl_dt_of(const coral_handle* h, const unsigned long long bits[3]) {
+// (compute_cfl_based_timestep, marching.f90:219-251): the w term scaled by
+// cflFactor_along_z (skipped at or below 1e-10), and with the Smagorinsky
+// viscosity the diffusive limit 0.95 / ((2 pi)^2 max(nuSmago) (dx^-2 + dy^-2)),
+// whose literals 0.95 and 3.141592 are single precision there
+double cfl_dt_of(const coral_handle* h, const unsigned long long bits[4]) {
   const Geometry& g = *h->G;
-  double mx[3];
-  for (int i = 0; i < 3; ++i) std::memcpy(&mx[i], &bits[i], sizeof(double));
+  double mx[4];
+  for (int i = 0; i < 4; ++i) std::memcpy(&mx[i], &bits[i], sizeof(double));
   const double u = mx[0] * g.NXAA / g.Lx, v = mx[1] * g.NYAA / g.Ly;
-  const double w = std::max(v, mx[2]);
+  const double w = h->cfl_factor_z > 1e-10 ? std::max(v, mx[2] * h->cfl_factor_z) : v;
   const double m = std::max(u, std::max(v, w));
-  return (h->nF >= 3 && m > 0.0) ? 1.0 / m : (h->nF >= 3 ? INFINITY : 1.0);
+  double cfl = (h->nF >= 3 && m > 0.0) ? 1.0 / m : (h->nF >= 3 ? INFINITY : 1.0);
+  if (h->smago_var >= 0) {
+    const float tp = 2.0f * 3.141592f;
+    const double den = (double)(tp * tp) * mx[3] *
+                       ((g.NXAA / g.Lx) * (g.NXAA / g.Lx) + (g.NYAA / g.Ly) * (g.NYAA / g.Ly));
+    if (den > 0.0) cfl = std::min(cfl, (double)0.95f / den);
+  }
+  return cfl;
 }
 
 std::string trim(const std::string& t) {
@@ -1626,7 +1819,7 @@ void run_loop(coral_handle* h, int nsteps, const char* outdir) {
     }
     if (!h->uo.empty()) usr_output_step(h, outdir);
     march(h, h->dt_current, 1);  // refactorises when dt_current changed
-    CK(cudaMemcpyAsync(h->h_pin + kMaxTs, h->cfl_bits, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+    CK(cudaMemcpyAsync(h->h_pin + kMaxTs, h->cfl_bits, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                        h->stream));
     if (n > 0)
       CK(cudaMemcpyAsync(h->h_pin, h->ts_out, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
@@ -1637,7 +1830,7 @@ void run_loop(coral_handle* h, int nsteps, const char* outdir) {
       for (int o = 0; o < n; ++o) row[o + 1] = h->h_pin[o];
       h->ts_rows.emplace_back(h->i_timestep, std::move(row));
     }
-    unsigned long long bits[3];
+    unsigned long long bits[4];
     std::memcpy(bits, h->h_pin + kMaxTs, sizeof(bits));
     const double cfl = cfl_dt_of(h, bits);
     // apply_cfl
@@ -1708,8 +1901,41 @@ void release_streams(coral_handle* h) {
 }
 }  // namespace
 
+namespace {
+// the reference's command-line switches this library takes (plane_layer_main.f90:82;
+// PL_IMEX_timestepping.f90:526-552); values are read as Fortran reals
+int parse_args(const char* args, coral_handle* h) {
+  if (!args) return CORAL_OK;
+  std::istringstream is(args);
+  std::vector<std::string> tok;
+  std::string t;
+  while (is >> t) tok.push_back(t);
+  for (size_t i = 0; i < tok.size(); ++i) {
+    auto value = [&](double* v) {
+      if (i + 1 >= tok.size()) throw CoralError(CORAL_EBADARG, tok[i] + " needs a value");
+      std::string x = tok[++i];
+      for (char& c : x)
+        if (c == 'd' || c == 'D') c = 'e';
+      char* end = nullptr;
+      *v = std::strtod(x.c_str(), &end);
+      if (end == x.c_str() || *end) throw CoralError(CORAL_EBADARG, "bad value for " + tok[i - 1] + ": " + tok[i]);
+    };
+    if (tok[i] == "--withHorizontalSmagorinsky") h->smagorinsky = true;
+    else if (tok[i] == "--smagorinsky-prefactor") value(&h->smago_prefactor);
+    else if (tok[i] == "--cflFactor-along-z") value(&h->cfl_factor_z);
+    else throw CoralError(CORAL_EBADARG, "unsupported argument: " + tok[i]);
+  }
+  return CORAL_OK;
+}
+}  // namespace
+
 int coral_create(const char* equations_text, const char* parameters_text, const char* scheme, int device,
                  coral_handle** out) {
+  return coral_create_with_args(equations_text, parameters_text, scheme, device, nullptr, out);
+}
+
+int coral_create_with_args(const char* equations_text, const char* parameters_text, const char* scheme, int device,
+                           const char* args, coral_handle** out) {
   if (!out || !equations_text || !parameters_text) {
     g_create_error = "coral_create: null argument";
     return CORAL_EBADARG;
@@ -1717,6 +1943,7 @@ int coral_create(const char* equations_text, const char* parameters_text, const 
   *out = nullptr;
   auto* h = new coral_handle();
   try {
+    parse_args(args, h);
     setup(h, equations_text, parameters_text, scheme, device);
   } catch (const CoralError& e) {
     g_create_error = e.what();
@@ -2027,7 +2254,7 @@ int coral_diagnostics(coral_handle* h, double* out3) {
     if (!out3) throw CoralError(CORAL_EBADARG, "null buffer");
     const Geometry& g = *h->G;
     CK(cudaStreamSynchronize(h->stream));
-    unsigned long long bits[3];
+    unsigned long long bits[4];
     CK(cudaMemcpy(bits, h->cfl_bits, sizeof(bits), cudaMemcpyDeviceToHost));
     out3[0] = cfl_dt_of(h, bits);
     // the partial sums are totalled on the device: 8 bytes come back, not the
@@ -2284,6 +2511,26 @@ int coral_set_hermitian_kx0(coral_handle* h, int on) {
       cudaGraphExecDestroy(h->graph);
       h->graph = nullptr;
     }
+  });
+}
+
+int coral_set_source(coral_handle* h, int index, const double* profile) {
+  return guarded(h, [&] {
+    if (!profile || index < 1 || index > 99) throw CoralError(CORAL_EBADARG, "source index must be 1..99");
+    h->src_phys[index].assign(profile, profile + h->G->NZAA);
+    update_sources(h);
+  });
+}
+
+int coral_set_penalisation_mask(coral_handle* h, const double* mask) {
+  return guarded(h, [&] {
+    if (!mask) throw CoralError(CORAL_EBADARG, "null mask");
+    if (std::none_of(h->R.full.begin(), h->R.full.end(), [](const FullVar& F) { return F.penal; }))
+      throw CoralError(CORAL_EBADARG, "the recipe has no penalised variable");
+    const size_t n = (size_t)h->d.NYA * h->d.NXA * h->d.NZA;
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(h->tmp_phys, mask, n * sizeof(double), cudaMemcpyHostToDevice));
+    penal_fields(h, h->tmp_phys);
   });
 }
 

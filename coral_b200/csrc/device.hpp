@@ -13,7 +13,8 @@ constexpr int kMaxGroups = 16;  // monomial groups (i kx)^a (i ky)^b per operato
 constexpr int kMaxStages = 4;   // ARS_443 has 4 implicit stages
 constexpr int kMaxSets = 8;     // coupled systems of one kind
 constexpr int kMaxQuad = 16;    // quadratic variables
-constexpr int kMaxFull = 8;     // full variables
+constexpr int kMaxFull = 16;    // full variables
+constexpr int kMaxStatic = 4;   // full variables whose physical field is given, not transformed
 constexpr int kMaxFullTerms = 8;
 constexpr int kTabW = 5;        // Galerkin -> Chebyshev entries per Chebyshev row
 constexpr int kTileRows = 128;  // rows per tile of the operator-stationary K_std kernel
@@ -89,6 +90,14 @@ struct QuadDesc {
   // learned closure: tau[q][y][x][z] added to quadratic variable q after its
   // product (and after its KE contribution) in the unfused forward z pass; null: none
   const double* tau;
+  // full variables whose physical values are given instead of transformed:
+  // penalisation fields (st_prof 0: st_src[y][x][z], marching.f90:515) and the
+  // Smagorinsky viscosity (st_prof 1: one value per z level, st_src[z],
+  // marching.f90:516-541); the fused z pass puts them in place of the inverse
+  // transform's output
+  int st_n;
+  int st_var[kMaxStatic], st_prof[kMaxStatic];
+  const double* st_src[kMaxStatic];
 };
 
 struct Dims {
@@ -130,6 +139,21 @@ void launch_inv_x_rows(const Dims& d, int nf, const double2* Y1, double* Y2, con
 void launch_fwd_y(const Dims& d, int nq, const double2* Q1, double2* qspec, double scale, const FftPlan& py,
                   cudaStream_t s, int grid_variant = 0);
 void launch_remove_zmean(const Dims& d, double2* qspec_q, cudaStream_t s);
+// z operations on one full variable's Chebyshev columns of Y2 (rows y0 .. y0 + ny - 1)
+// before its inverse z transform: extract 1 bottom / 2 top surface value, decomp 1
+// barotropic / 2 baroclinic (marching.f90:543-575)
+void launch_zfilter(const Dims& d, double* Y2_var, int extract, int decomp, int y0, int ny, cudaStream_t s);
+// the given physical fields of q.st_* written into phys[var][y][x][z]
+void launch_static_phys(const Dims& d, const QuadDesc& q, double* phys, cudaStream_t s);
+// Smagorinsky viscosity profile (marching.f90:516-541, 591-617): prof[z] = c sqrt(prof[z]
+// + horizontal mean of the squares of phys[vars[k]]), part: NYA x NZA scratch; the
+// maximum goes to cfl_max (when non-null) by an atomic maximum of non-negative doubles
+void launch_smago(const Dims& d, const double* phys, const int* vars, int nvars, double c, double* part, double* prof,
+                  unsigned long long* cfl_max, cudaStream_t s);
+// the reference's default penalisation mask (PL_user_penalisation_mask.f90) on the grid,
+// mask[y][x][z]; the penalisation field strength (1 + tanh(width mask)) / 2
+void launch_penal_default(const Dims& d, double Lx, double Ly, const double* zgrid, double* mask, cudaStream_t s);
+void launch_penal_field(size_t n, const double* mask, double strength, double width, double* out, cudaStream_t s);
 // ---- split-precision z transforms on the tensor cores (zsplit.cu) ----
 // int8 digits of the REDFT01 (fwd = false: NZAA x NZ) or REDFT10 (fwd = true:
 // NZ x NZAA) matrix in the kernels' streaming order
@@ -304,6 +328,7 @@ struct ZeroSysDev {
   double* Khat[kMaxStages];
   double* ab;
   unsigned char* dpiv;
+  const double* src;  // constant source terms of K_hat (marching.f90:398-415), null: none
 };
 struct ZeroArgs {
   int nsys;

@@ -59,6 +59,23 @@ struct FullTerm {   // a_linear_contribution_T
 struct FullVar {
   std::string name;
   std::vector<FullTerm> terms;
+  // z operations on the Chebyshev coefficients before the inverse transform
+  // (marching.f90:543-575): extract 0 nowhere, 1 BotSurf, 2 TopSurf (the surface
+  // value, PL_equations.f90:497-500); decomp 0 none, 1 barotropic, 2 baroclinic
+  // (vertical_decomposition, :502-503, 1052-1067)
+  int extract = 0, decomp = 0;
+  // enable_penalisation (:508-517): the physical field is strength (1 + tanh(width
+  // mask)) / 2 of the user's mask, never transformed
+  bool penal = false;
+  double penal_strength = 0.0, penal_width = 0.0;
+  // nuSmago (--withHorizontalSmagorinsky, :519-526): the horizontal Smagorinsky
+  // viscosity, formed in physical space (marching.f90:516-541)
+  bool smago = false;
+};
+struct SourceTerm {  // source_term_T (PL_equations.f90:37-45)
+  double dsca;
+  int Iz, index;     // Iz^Iz sourceNN (index NN >= 1)
+  int set, eqn;      // mean system and equation
 };
 struct QuadVar {
   std::string name;
@@ -79,8 +96,13 @@ struct Recipe {
   std::vector<QuadVar> quad;
   std::vector<CoupledSet> kxky, zero;
   std::map<std::string, std::pair<int, int>> kxky_loc, zero_loc;  // (set, position)
+  std::vector<std::pair<std::string, double>> source_params;      // sourceParam lines
+  std::vector<SourceTerm> sources;                                // add_rhs_source lines
+  bool smagorinsky = false;
 };
-Recipe parse_equations(const std::string& text);
+// smagorinsky: the reference's --withHorizontalSmagorinsky switch (the full
+// variable nuSmago goes in before the first quadratic variable)
+Recipe parse_equations(const std::string& text, bool smagorinsky = false);
 
 // ---------------------------------------------------------------------------
 // geometry  (src/plane_layer/PL_geometry.f90:80-236)

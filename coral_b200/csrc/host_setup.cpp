@@ -2,6 +2,7 @@
 // Chebyshev matrices, Galerkin stencils and the assembly of the coupled
 // systems' operators in the interleaved polynomial ordering.
 #include <algorithm>
+#include <cctype>
 #include <array>
 #include <cmath>
 #include <cstdlib>
@@ -114,9 +115,10 @@ static std::vector<Atom> atoms(const std::string& line, const char* dz) {
   return out;
 }
 
-Recipe parse_equations(const std::string& text) {
+Recipe parse_equations(const std::string& text, bool smagorinsky) {
   Recipe r;
-  bool zero_set = false;
+  r.smagorinsky = smagorinsky;
+  bool zero_set = false, smago_pending = smagorinsky;
   auto param_value = [&](const std::string& n, double* v) {
     for (auto& p : r.params)
       if (p.first == n) { *v = p.second; return true; }
@@ -136,6 +138,11 @@ Recipe parse_equations(const std::string& text) {
       size_t e = body.find(":=");
       if (e == std::string::npos) throw CoralError(CORAL_EPARSE, "Param without ':=': " + line);
       r.params.emplace_back(clean(body.substr(0, e)), fortran_float(clean(body.substr(e + 2))));
+    } else if (starts(key, "sourceParam")) {  // add_source_parameter (PL_equations.f90:985-996)
+      std::string body = payload(line);
+      size_t e = body.find(":=");
+      if (e == std::string::npos) throw CoralError(CORAL_EPARSE, "sourceParam without ':=': " + line);
+      r.source_params.emplace_back(clean(body.substr(0, e)), fortran_float(clean(body.substr(e + 2))));
     } else if (starts(key, "linear_variable_kxky")) {
       r.kxky_vars.push_back(clean(payload(line)));
     } else if (starts(key, "linear_variable_mean")) {
@@ -159,7 +166,31 @@ Recipe parse_equations(const std::string& text) {
       }
     } else if (starts(key, "linear_variable_full")) {
       r.full.push_back(FullVar{clean(payload(line)), {}});
+    } else if (starts(key, "linear_variable_bottom_boundary_value") ||
+               starts(key, "linear_variable_top_boundary_value")) {
+      r.full.push_back(FullVar{clean(payload(line)), {}});
+      r.full.back().extract = starts(key, "linear_variable_bottom") ? 1 : 2;
+    } else if (starts(key, "vertical_decomposition")) {
+      if (r.full.empty()) throw CoralError(CORAL_EPARSE, "vertical_decomposition before a full variable");
+      const std::string k = clean(payload(line));
+      if (k == "barotropic") r.full.back().decomp = 1;
+      else if (k == "baroclinic") r.full.back().decomp = 2;
+      else throw CoralError(CORAL_EPARSE, "vertical_decomposition should be baroclinic or barotropic");
+    } else if (starts(key, "enable_penalisation")) {
+      r.full.push_back(FullVar{clean(payload(line)), {}});
+      r.full.back().penal = true;
+    } else if (starts(key, "penalisation_strength") || starts(key, "penalisation_width")) {
+      if (r.full.empty() || !r.full.back().penal)
+        throw CoralError(CORAL_EPARSE, "penalisation parameter without enable_penalisation");
+      const double v = fortran_float(clean(payload(line)));
+      if (starts(key, "penalisation_strength")) r.full.back().penal_strength = v;
+      else r.full.back().penal_width = v;
     } else if (starts(key, "quadratic_variable") || starts(key, "zFiltered_quadratic_variable")) {
+      if (smago_pending) {
+        r.full.push_back(FullVar{"nuSmago", {}});
+        r.full.back().smago = true;
+        smago_pending = false;
+      }
       std::string body = payload(line);
       size_t e = body.find(":=");
       std::string q = clean(body.substr(0, e)), rhs = clean(body.substr(e + 2));
@@ -227,12 +258,30 @@ Recipe parse_equations(const std::string& text) {
           (mass ? s.mass : s.stif).push_back(p);
         }
       }
-    } else if (starts(key, "linear_variable_bottom_boundary_value") ||
-               starts(key, "linear_variable_top_boundary_value") ||
-               starts(key, "vertical_decomposition") || starts(key, "enable_penalisation") ||
-               starts(key, "penalisation_") || starts(key, "sourceParam") ||
-               starts(key, "add_rhs_source")) {
-      throw CoralError(CORAL_EUNSUPPORTED, "equation feature not supported by this build: " + line.substr(0, 60));
+    } else if (starts(key, "add_rhs_source")) {
+      // build_zero_sources_in_full_recipe (PL_equations.f90:1156-1230): mean systems only
+      if (!zero_set || r.zero.empty()) throw CoralError(CORAL_EPARSE, "add_rhs_source outside a set of mean equations");
+      CoupledSet& s = r.zero.back();
+      for (auto& a : atoms(line, "Iz")) {
+        if (a.dx || a.dy) throw CoralError(CORAL_EPARSE, "x/y-derivative in a source term");
+        SourceTerm t{a.dsca, a.Iz, 0, int(r.zero.size()) - 1, int(s.orders.size()) - 1};
+        for (auto& st : a.unsorted) {
+          // a string of 8 characters 'sourceNN' names the source and ends the atom's
+          // strings; any other is a parameter
+          if (st.size() == 8 && starts(st, "source")) {
+            if (!std::isdigit((unsigned char)st[6]) || !std::isdigit((unsigned char)st[7]))
+              throw CoralError(CORAL_EPARSE, "Source terms must be of the form sourceNN: " + st);
+            t.index = std::atoi(st.substr(6).c_str());
+            break;
+          }
+          double v;
+          if (param_value(st, &v)) t.dsca = v * t.dsca;
+          else throw CoralError(CORAL_EPARSE, "unknown string in equations: " + st);
+        }
+        if (t.index == 0) throw CoralError(CORAL_EPARSE, "invalid source_index");
+        if (t.eqn < 0) throw CoralError(CORAL_EPARSE, "source term before new_equation");
+        r.sources.push_back(t);
+      }
     } else {
       throw CoralError(CORAL_EPARSE, "the line could not be read: " + line.substr(0, 78));
     }

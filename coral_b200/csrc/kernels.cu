@@ -657,6 +657,27 @@ __global__ void __launch_bounds__(kThreadsZF, z_min_blocks(NF, FB)) k_z_fused(Di
       __syncthreads();
     }
   }
+  // full variables with given physical values replace their transforms
+  if (q.st_n > 0) {
+    for (int k = 0; k < q.st_n; ++k) {
+      const double* src = q.st_src[k];
+      const int f = q.st_var[k], prof = q.st_prof[k];
+      for (int idx = threadIdx.x; idx < kZPairs * N; idx += blockDim.x) {
+        const int pr = idx / N, m = idx - pr * N;
+        const int z = (m < N / 2) ? 2 * m : 2 * (N - 1 - m) + 1;
+        double a = 0.0, b = 0.0;
+        if (prof) {
+          a = b = src[z];
+        } else {
+          const size_t at = ((size_t)y * d.NXA + x0 + 2 * pr) * N + z;
+          if (col_ok(2 * pr)) a = src[at];
+          if (col_ok(2 * pr + 1)) b = src[at + N];
+        }
+        Fv[(f * kZPairs + pr) * N + m] = make_double2(a, b);
+      }
+    }
+    __syncthreads();
+  }
   // ---- CFL maxima of |u|, |v|, |w| / wz and the KE sums (z-weighted products
   //      of the quadratic variables uu, vv, ww) over all columns, from the
   //      physical values (Makhoul order: position m is grid point z) ----
@@ -2550,6 +2571,7 @@ __global__ void k_zero_step(ZeroArgs a) {
       const int qv = c / a.d.NZ, n = c - qv * a.d.NZ;
       acc += z.NL.v(t, k) * a.qspec[(size_t)qv * a.d.NXH * a.d.NYA * a.d.NZ + n].x;
     }
+    if (z.src) acc += z.src[t];
     kh[t] = acc;
   }
   __syncwarp();
@@ -3093,6 +3115,164 @@ void launch_ke_sum(const double* part, size_t n, double* out, cudaStream_t s) {
 }
 void launch_remove_zmean(const Dims& d, double2* qspec_q, cudaStream_t s) {
   k_remove_zmean<<<grid1d((size_t)d.NXH * d.NYA, 128), 128, 0, s>>>(d, qspec_q);
+}
+
+// ------------------------------------------------------------------------------
+// full variables that are not plain transforms (marching.f90:505-575)
+// ------------------------------------------------------------------------------
+namespace {
+
+// z operations of one CTA on kZfCols consecutive x columns of one y row, whose
+// Chebyshev coefficients are contiguous in Y2: the tile is staged in shared
+// memory and each column runs the reference's loops in its order.  Y2 holds
+// c_0 and c_n / 2 (n >= 1; the inverse y pass folds the x padding's 0.5 and
+// the REDFT01 convention in), so every c_n (n >= 1) read into c_0 is 2 Y2[n]
+// (exact).
+constexpr int kZfCols = 16;
+__global__ void k_zfilter(Dims d, double* Y2v, int extract, int decomp, int y0) {
+  extern __shared__ double tile[];
+  const int NZ = d.NZ, y = y0 + blockIdx.y, xc0 = blockIdx.x * kZfCols;
+  const int nc = min(kZfCols, d.NXA - xc0);
+  double* base = Y2v + ((size_t)y * d.NXA + xc0) * NZ;
+  for (int i = threadIdx.x; i < nc * NZ; i += blockDim.x) tile[i] = base[i];
+  __syncthreads();
+  if ((int)threadIdx.x < nc) {
+    double* c = tile + threadIdx.x * NZ;
+    if (extract == 1) {  // bottom surface: T_n(-1) = (-1)^n
+      for (int iz = 2; iz <= NZ; ++iz) {
+        c[0] = c[0] - (2.0 * c[iz - 1]) * ((iz & 1) ? -1.0 : 1.0);
+        c[iz - 1] = 0.0;
+      }
+    } else if (extract == 2) {  // top surface: T_n(1) = 1
+      for (int iz = 2; iz <= NZ; ++iz) {
+        c[0] = c[0] + 2.0 * c[iz - 1];
+        c[iz - 1] = 0.0;
+      }
+    }
+    if (decomp == 2) {  // baroclinic: the vertical mean removed (PL_IMEX_timestepping.f90:238-250)
+      c[0] = 0.0;
+      for (int q = 1; q < NZ / 2; ++q)
+        c[0] = c[0] - (2.0 * c[2 * q]) * (0.5 / (2.0 * q + 1.0) - 0.5 / (2.0 * q - 1.0));
+    } else if (decomp == 1) {  // barotropic: the vertical fluctuations removed (:252-274)
+      for (int q = 1; q < NZ / 2; ++q) {
+        c[0] = c[0] + (2.0 * c[2 * q]) * (0.5 / (2.0 * q + 1.0) - 0.5 / (2.0 * q - 1.0));
+        c[2 * q - 1] = 0.0;
+        c[2 * q] = 0.0;
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nc * NZ; i += blockDim.x) base[i] = tile[i];
+}
+
+__global__ void k_static_phys(Dims d, QuadDesc q, double* phys) {
+  const size_t n = (size_t)d.NYA * d.NXA * d.NZA;
+  for (int k = 0; k < q.st_n; ++k) {
+    double* dst = phys + (size_t)q.st_var[k] * n;
+    const double* src = q.st_src[k];
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+      dst[i] = q.st_prof[k] ? src[i % d.NZA] : src[i];
+  }
+}
+
+struct SmagoVars {
+  int n;
+  int v[4];
+};
+// part[y][z]: the sum over x of the squares of the variables at (y, z); one CTA
+// per y row, threads along z (contiguous in phys)
+__global__ void k_smago_rows(Dims d, const double* phys, SmagoVars sv, double* part) {
+  const int y = blockIdx.x;
+  const size_t n = (size_t)d.NYA * d.NXA * d.NZA;
+  for (int z = threadIdx.x; z < d.NZA; z += blockDim.x) {
+    double acc = 0.0;
+    for (int x = 0; x < d.NXA; ++x) {
+      const size_t at = ((size_t)y * d.NXA + x) * d.NZA + z;
+      double s = 0.0;
+      for (int k = 0; k < sv.n; ++k) {
+        const double v = phys[(size_t)sv.v[k] * n + at];
+        s += v * v;
+      }
+      acc += s;
+    }
+    part[(size_t)y * d.NZA + z] = acc;
+  }
+}
+// prof[z] = c sqrt(prof[z] + sum_y part[y][z] / NXA / NYA); the maximum to cfl_max
+__global__ void k_smago_final(Dims d, const double* part, double c, double* prof, unsigned long long* cfl_max) {
+  __shared__ double red[32];
+  double mx = 0.0;
+  for (int z = threadIdx.x; z < d.NZA; z += blockDim.x) {
+    double s = 0.0;
+    for (int y = 0; y < d.NYA; ++y) s += part[(size_t)y * d.NZA + z];
+    const double p = c * sqrt(prof[z] + s / d.NXA / d.NYA);
+    prof[z] = p;
+    mx = fmax(mx, p);
+  }
+  if (!cfl_max) return;
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m2 = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m2 = fmax(m2, red[w]);
+    atomic_max_nonneg(cfl_max, m2);
+  }
+}
+
+// PL_user_penalisation_mask.f90 as the reference ships it: two masks, the
+// larger taken; grid labels x = (i + 2) Lx / NXAA, y = (j + 2) Ly / NYAA
+// (PL_geometry.f90:138-145 with phys_iStart = 1); pi, 0.9 and 0.1 are
+// single-precision literals there
+__global__ void k_penal_default(Dims d, double Lx, double Ly, const double* zgrid, double* mask) {
+  const size_t n = (size_t)d.NYA * d.NXA * d.NZA;
+  const double pi = (double)3.14159265358979311599796346854f, c09 = (double)0.9f, c01 = (double)0.1f;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(i % d.NZA);
+    const size_t r = i / d.NZA;
+    const int ix = (int)(r % d.NXA), iy = (int)(r / d.NXA);
+    const double x = (double)(ix + 2) * Lx / d.NXA, y = (double)(iy + 2) * Ly / d.NYA, z = zgrid[k];
+    const double m1 = z - (c09 + c01 * cos(5.0 * (x + y) * 2.0 * pi / Lx));
+    const double cx = 6.0 + cos(2.0 * pi * x / Lx);
+    const double m2 = (0.4 * exp(-(cx * cx)) / exp(-25.0)) - z;
+    mask[i] = fmax(m1, m2);
+  }
+}
+// init_penalisation (marching.f90:812-816)
+__global__ void k_penal_field(size_t n, const double* mask, double strength, double width, double* out) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double pm = tanh(width * mask[i]);
+    pm = (1.0 + pm) / 2.0;
+    out[i] = strength * pm;
+  }
+}
+
+}  // namespace
+
+void launch_zfilter(const Dims& d, double* Y2_var, int extract, int decomp, int y0, int ny, cudaStream_t s) {
+  if (ny <= 0 || (!extract && !decomp)) return;
+  const size_t sm = (size_t)kZfCols * d.NZ * sizeof(double);
+  set_smem(k_zfilter, sm);
+  k_zfilter<<<dim3((d.NXA + kZfCols - 1) / kZfCols, ny), 128, sm, s>>>(d, Y2_var, extract, decomp, y0);
+}
+void launch_static_phys(const Dims& d, const QuadDesc& q, double* phys, cudaStream_t s) {
+  if (q.st_n <= 0) return;
+  k_static_phys<<<4 * 148, 256, 0, s>>>(d, q, phys);
+}
+void launch_smago(const Dims& d, const double* phys, const int* vars, int nvars, double c, double* part, double* prof,
+                  unsigned long long* cfl_max, cudaStream_t s) {
+  SmagoVars sv{};
+  sv.n = nvars < 4 ? nvars : 4;
+  for (int k = 0; k < sv.n; ++k) sv.v[k] = vars[k];
+  const int bz = d.NZA < 128 ? 128 : (d.NZA >= 512 ? 512 : (d.NZA + 31) / 32 * 32);
+  k_smago_rows<<<d.NYA, bz, 0, s>>>(d, phys, sv, part);
+  k_smago_final<<<1, bz, 0, s>>>(d, part, c, prof, cfl_max);
+}
+void launch_penal_default(const Dims& d, double Lx, double Ly, const double* zgrid, double* mask, cudaStream_t s) {
+  k_penal_default<<<4 * 148, 256, 0, s>>>(d, Lx, Ly, zgrid, mask);
+}
+void launch_penal_field(size_t n, const double* mask, double strength, double width, double* out, cudaStream_t s) {
+  k_penal_field<<<4 * 148, 256, 0, s>>>(n, mask, strength, width, out);
 }
 void launch_nl(const NLArgs& a, cudaStream_t s) {
   const int nsys = a.d.NXH * a.d.NYA;

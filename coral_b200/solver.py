@@ -37,11 +37,14 @@ def _dptr(a):
 
 
 class PlaneLayer:
-    def __init__(self, equations_text, parameters_text, scheme=None, device=0):
+    def __init__(self, equations_text, parameters_text, scheme=None, device=0, args=None):
+        """args: the reference's command-line switches, e.g.
+        "--withHorizontalSmagorinsky --smagorinsky-prefactor 0.1" (coral_create_with_args)."""
         self._lib = _lib.load()
         h = ctypes.c_void_p()
-        rc = self._lib.coral_create(equations_text.encode(), parameters_text.encode(),
-                                    scheme.encode() if scheme else None, int(device), ctypes.byref(h))
+        rc = self._lib.coral_create_with_args(equations_text.encode(), parameters_text.encode(),
+                                              scheme.encode() if scheme else None, int(device),
+                                              args.encode() if args else None, ctypes.byref(h))
         if rc != 0:
             raise CoralError(rc, self._lib.coral_last_error(None).decode())
         self._h = h
@@ -73,12 +76,12 @@ class PlaneLayer:
         return self
 
     @classmethod
-    def from_files(cls, equations_path, parameters_path, scheme=None, device=0):
+    def from_files(cls, equations_path, parameters_path, scheme=None, device=0, args=None):
         with open(equations_path) as f:
             e = f.read()
         with open(parameters_path) as f:
             p = f.read()
-        return cls(e, p, scheme, device)
+        return cls(e, p, scheme, device, args)
 
     # --- plumbing
     def _check(self, rc):
@@ -262,6 +265,20 @@ class PlaneLayer:
         """Project the kx = 0 line onto its Hermitian part after every step
         (removes the invisible anti-Hermitian part; off by default)."""
         self._check(self._lib.coral_set_hermitian_kx0(self._h, 1 if on else 0))
+
+    def set_source(self, index, profile):
+        """sourceNN's physical values on the Gauss-Chebyshev grid (NZAA)."""
+        a = np.ascontiguousarray(profile, dtype=np.float64)
+        if a.shape != (self.NZAA,):
+            raise ValueError("profile must have NZAA values")
+        self._check(self._lib.coral_set_source(self._h, int(index), _dptr(a)))
+
+    def set_penalisation_mask(self, mask):
+        """the penalisation mask on the grid, (NYAA, NXAA, NZAA)."""
+        a = np.ascontiguousarray(mask, dtype=np.float64)
+        if a.shape != (self.NYAA, self.NXAA, self.NZAA):
+            raise ValueError("mask must be (NYAA, NXAA, NZAA)")
+        self._check(self._lib.coral_set_penalisation_mask(self._h, _dptr(a)))
 
     def set_z_transform(self, form):
         """0: FP64 FFT z transforms; 1: int8-digit tensor-core contractions."""

@@ -32,6 +32,13 @@ module coral_b200_c
       integer(c_int), value :: device
       type(c_ptr), intent(out) :: h
     end function
+    integer(c_int) function coral_create_with_args(eqs_text, pars_text, scheme, device, args, h) &
+        bind(C, name="coral_create_with_args")
+      import :: c_int, c_char, c_ptr
+      character(kind=c_char), dimension(*), intent(in) :: eqs_text, pars_text, scheme, args
+      integer(c_int), value :: device
+      type(c_ptr), intent(out) :: h
+    end function
     subroutine coral_destroy(h) bind(C, name="coral_destroy")
       import :: c_ptr
       type(c_ptr), value :: h
@@ -145,6 +152,17 @@ module coral_b200_c
       import :: c_int, c_ptr
       type(c_ptr), value :: h
       integer(c_int), value :: form
+    end function
+    integer(c_int) function coral_set_source(h, idx, profile) bind(C, name="coral_set_source")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      integer(c_int), value :: idx
+      real(c_double), dimension(*), intent(in) :: profile
+    end function
+    integer(c_int) function coral_set_penalisation_mask(h, mask) bind(C, name="coral_set_penalisation_mask")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: h
+      real(c_double), dimension(*), intent(in) :: mask
     end function
     integer(c_int) function coral_autotune(h, dt, repeats, report, n) bind(C, name="coral_autotune")
       import :: c_int, c_ptr, c_double, c_char

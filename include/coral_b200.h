@@ -89,6 +89,19 @@ int coral_create(const char* equations_text, const char* parameters_text, const 
 /* Same, reading the two files. */
 int coral_create_from_files(const char* equations_path, const char* parameters_path,
                             const char* scheme, int device, coral_handle** out);
+/*
+ * coral_create with the reference's command-line switches that change the
+ * solver, space-separated in args (NULL or "" for none):
+ *   --withHorizontalSmagorinsky      the full variable nuSmago, the horizontal
+ *                                    Smagorinsky viscosity (plane_layer_main.f90:82,
+ *                                    PL_equations.f90:519-526, marching.f90:516-541)
+ *   --smagorinsky-prefactor X        its prefactor (default 1)
+ *   --cflFactor-along-z X            the factor of the vertical CFL term (default 1;
+ *                                    at or below 1e-10 the term is left out)
+ * (PL_IMEX_timestepping.f90:526-552).  Any other word is CORAL_EBADARG.
+ */
+int coral_create_with_args(const char* equations_text, const char* parameters_text, const char* scheme,
+                           int device, const char* args, coral_handle** out);
 void coral_destroy(coral_handle* h);
 /* Text of the last error of h (or of the last failed create when h is NULL). */
 const char* coral_last_error(const coral_handle* h);
@@ -311,6 +324,26 @@ int coral_var_positions(coral_handle* h, int isys, int ivar, int* positions, int
  * (src/slabs.fftw3mpi/transforms.f90:216-249); form 1 has no counterpart there.
  */
 int coral_set_z_transform(coral_handle* h, int form);
+
+/*
+ * Source NN of the mean equations' 'add_rhs_source :: ... sourceNN' terms
+ * (marching.f90:398-415): its physical values on the Gauss-Chebyshev grid,
+ * NZAA doubles, z(i) = center + cos(pi (2i - 1) / (2 NZAA)) gap / 2.  Replaces
+ * the reference's compiled-in PL_user_sources_definitions.f90; without a call,
+ * source01 and source02 are that file's defaults (source01 from sourceParam
+ * HovEll, source02 = -1) and a step with any other source referenced fails
+ * with CORAL_EBADARG.
+ */
+int coral_set_source(coral_handle* h, int index, const double* profile);
+/*
+ * The penalisation mask (the maximum over the user's masks) on the physical
+ * grid, NYAA x NXAA x NZAA doubles, z fastest (phys(NZAA, NXAA, NYAA) of the
+ * reference).  Every 'enable_penalisation' variable's field becomes
+ * strength (1 + tanh(width mask)) / 2 (init_penalisation, marching.f90:778-822).
+ * Replaces the compiled-in PL_user_penalisation_mask.f90, whose two example
+ * masks are the default.
+ */
+int coral_set_penalisation_mask(coral_handle* h, const double* mask);
 
 /*
  * Ensembles: n independent runs (each its own coral.equations /

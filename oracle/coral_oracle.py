@@ -24,6 +24,12 @@ What it restates (file:line citations are into the Coral v1.3 sources):
 * one timestep ..................... src/plane_layer/PL_IMEX_timestepping_marching.f90:3-588
 * QuickSave import / export ........ src/plane_layer/PL_IMEX_timestepping_output.f90:309-456
 * Gauss-Chebyshev grid and weights . src/plane_layer/PL_cheby_misc.f90:8-55
+* sources, penalisation, Smagorinsky, surface values, vertical decompositions
+                                     src/plane_layer/PL_IMEX_timestepping_marching.f90:
+                                     398-415,505-575,711-866,
+                                     PL_IMEX_timestepping.f90:238-274 and the shipped
+                                     PL_user_sources_definitions.f90 /
+                                     PL_user_penalisation_mask.f90
 
 Third-party arithmetic the reference delegates to libraries is restated with
 the same published algorithms: FFTW's unnormalised c2c / c2r / r2c and
@@ -114,6 +120,17 @@ class FullTerm:
 
 
 @dataclasses.dataclass
+class SourceTerm:
+    """source_term_T (PL_equations.f90:37-45): dsca * Iz^Iz * sourceNN in equation
+    eqn of mean system sys."""
+    dsca: float
+    Iz: int
+    index: int
+    sys: int
+    eqn: int
+
+
+@dataclasses.dataclass
 class CoupledSystem:
     vars: List[str]
     bcs: List[int]
@@ -134,6 +151,12 @@ class Recipe:
     zero: List[CoupledSystem]
     kxky_loc: Dict[str, Tuple[int, int]]
     zero_loc: Dict[str, Tuple[int, int]]
+    # per full variable: extract ('nowhere' | 'BotSurf' | 'TopSurf'), decomp (None |
+    # 'barotropic' | 'baroclinic'), penal (None | [strength, width]), smago (bool)
+    full_opts: List[dict] = dataclasses.field(default_factory=list)
+    source_params: List[Tuple[str, float]] = dataclasses.field(default_factory=list)
+    sources: List[SourceTerm] = dataclasses.field(default_factory=list)
+    smagorinsky: bool = False
 
 
 def _clean(s: str) -> str:
@@ -181,9 +204,19 @@ def _payload(line: str) -> str:
     return line[i:j]
 
 
-def parse_equations(text: str) -> Recipe:
-    """build_full_recipe_from_text_file (PL_equations.f90:435-593)."""
+def parse_equations(text: str, smagorinsky: bool = False) -> Recipe:
+    """build_full_recipe_from_text_file (PL_equations.f90:435-593).  smagorinsky:
+    the --withHorizontalSmagorinsky switch, which adds the full variable nuSmago
+    before the first quadratic variable (:519-526)."""
     params: List[Tuple[str, float]] = []
+    source_params: List[Tuple[str, float]] = []
+    sources: List[SourceTerm] = []
+    full_opts: List[dict] = []
+    smago_pending = smagorinsky
+
+    def new_full(name, extract="nowhere", penal=None, smago=False):
+        full_vars.append((name, extract, []))
+        full_opts.append(dict(extract=extract, decomp=None, penal=penal, smago=smago))
     kxky_vars: List[str] = []
     zero_vars: List[str] = []
     full_vars: List[Tuple[str, str, List[FullTerm]]] = []
@@ -214,6 +247,10 @@ def parse_equations(text: str) -> Recipe:
             body = line[line.index("::") + 2: line.index("<<")]
             name, val = body.split(":=")
             params.append((_clean(name), _fortran_float(val)))
+        elif key.startswith("sourceParam"):   # add_source_parameter (:985-996)
+            body = line[line.index("::") + 2: line.index("<<")]
+            name, val = body.split(":=")
+            source_params.append((_clean(name), _fortran_float(val)))
         elif key.startswith("linear_variable_kxky"):
             kxky_vars.append(_clean(_payload(line)))
         elif key.startswith("linear_variable_mean"):
@@ -237,8 +274,26 @@ def parse_equations(text: str) -> Recipe:
                     raise ValueError("invalid full variable def.")
                 terms.append(t)
         elif key.startswith("linear_variable_full"):
-            full_vars.append((_clean(_payload(line)), "nowhere", []))
+            new_full(_clean(_payload(line)))
+        elif key.startswith("linear_variable_bottom_boundary_value"):
+            new_full(_clean(_payload(line)), "BotSurf")
+        elif key.startswith("linear_variable_top_boundary_value"):
+            new_full(_clean(_payload(line)), "TopSurf")
+        elif key.startswith("vertical_decomposition"):  # filter_linear_variable_full (:1052-1067)
+            kind = _payload(line).strip()
+            if kind not in ("baroclinic", "barotropic"):
+                raise ValueError("vertical_decomposition should be baroclinic or barotropic")
+            full_opts[-1]["decomp"] = kind
+        elif key.startswith("enable_penalisation"):     # :508-511, 1035-1050
+            new_full(_clean(_payload(line)), penal=[0.0, 0.0])
+        elif key.startswith("penalisation_strength"):
+            full_opts[-1]["penal"][0] = _fortran_float(_payload(line))
+        elif key.startswith("penalisation_width"):
+            full_opts[-1]["penal"][1] = _fortran_float(_payload(line))
         elif key.startswith("quadratic_variable") or key.startswith("zFiltered_quadratic_variable"):
+            if smago_pending:
+                new_full("nuSmago", smago=True)
+            smago_pending = False
             body = line[line.index("::") + 2: line.index("<<")]
             qname, rhs = body.split(":=")
             v1, v2 = [_clean(x) for x in rhs.split(".", 1)]
@@ -305,9 +360,31 @@ def parse_equations(text: str) -> Recipe:
                 if q < 0:
                     raise ValueError("invalid quad_var_index")
                 s.nl.append(NLTerm(dsca, a["dx"], a["dy"], a["Iz"], a["mz"], q, len(s.orders) - 1))
+        elif key.startswith("add_rhs_source"):
+            # build_zero_sources_in_full_recipe (PL_equations.f90:1156-1230): mean systems only
+            if current != "zero":
+                raise ValueError("add_rhs_source outside a set of mean equations")
+            for a in _atoms(line, "Iz"):
+                if a["dx"] or a["dy"]:
+                    raise ValueError("x/y-derivative in a source term")
+                t = SourceTerm(a["dsca"], a["Iz"], 0, len(zero) - 1, len(zero[-1].orders) - 1)
+                for st in a["unsorted"]:
+                    if len(st) == 8 and st.startswith("source"):
+                        if not st[6:].isdigit():
+                            raise ValueError("Source terms must be of the form sourceNN")
+                        t.index = int(st[6:])
+                        break
+                    v = param_value(st)
+                    if v is None:
+                        raise ValueError("unknown string in equations: " + st)
+                    t.dsca = v * t.dsca
+                if t.index == 0:
+                    raise ValueError("invalid source_index")
+                sources.append(t)
         else:
             raise ValueError("the line could not be read: " + line[:78])
-    return Recipe(params, kxky_vars, zero_vars, full_vars, quad_vars, kxky, zero, kxky_loc, zero_loc)
+    return Recipe(params, kxky_vars, zero_vars, full_vars, quad_vars, kxky, zero, kxky_loc, zero_loc,
+                  full_opts, source_params, sources, smagorinsky)
 
 
 # --------------------------------------------------------------------------------------
@@ -643,6 +720,94 @@ def r2r_backward(arr: np.ndarray) -> np.ndarray:
 
 
 # --------------------------------------------------------------------------------------
+# sources, penalisation, surface values and vertical decompositions
+# --------------------------------------------------------------------------------------
+
+
+def z_filter(spec: np.ndarray, extract: str, decomp: Optional[str]) -> np.ndarray:
+    """The z operations on a full variable's Chebyshev coefficients (last axis, NZ)
+    before its inverse transform (marching.f90:543-575): the value at the bottom
+    or top surface (T_n(-1) = (-1)^n, T_n(1) = 1) in coefficient 0, the rest
+    zeroed; then the vertical mean removed (baroclinic,
+    PL_IMEX_timestepping.f90:238-250) or the vertical fluctuations removed
+    (barotropic, :252-274), sequentially as the reference loops."""
+    spec = spec.copy()
+    NZ = spec.shape[-1]
+    if extract == "BotSurf":
+        for iz in range(2, NZ + 1):
+            spec[..., 0] = spec[..., 0] - spec[..., iz - 1] * (-1) ** iz
+            spec[..., iz - 1] = 0.0
+    elif extract == "TopSurf":
+        for iz in range(2, NZ + 1):
+            spec[..., 0] = spec[..., 0] + spec[..., iz - 1]
+            spec[..., iz - 1] = 0.0
+    if decomp == "baroclinic":
+        spec[..., 0] = 0.0
+        for q in range(1, NZ // 2):
+            spec[..., 0] = spec[..., 0] - spec[..., 2 * q] * (0.5 / (2.0 * q + 1.0) - 0.5 / (2.0 * q - 1.0))
+    elif decomp == "barotropic":
+        for q in range(1, NZ // 2):
+            spec[..., 0] = spec[..., 0] + spec[..., 2 * q] * (0.5 / (2.0 * q + 1.0) - 0.5 / (2.0 * q - 1.0))
+            spec[..., 2 * q - 1] = 0.0
+            spec[..., 2 * q] = 0.0
+    return spec
+
+
+def source_spectrum(phys: np.ndarray) -> np.ndarray:
+    """Compute_1dCheby_transform (marching.f90:845-866): REDFT10 / N, coefficient 0
+    halved."""
+    c = sfft.dct(np.asarray(phys, dtype=np.float64), type=2) / len(phys)
+    c[0] = c[0] * 0.5
+    return c
+
+
+def default_sources(r: Recipe, g: Geometry) -> Dict[int, np.ndarray]:
+    """The two sources of the reference's default PL_user_sources_definitions.f90:
+    source01 = HovEll exp(-z HovEll) / (1 - exp(-HovEll)) - 1 (HovEll a
+    sourceParam; 0 when the file has none, as sourceParams returns, which makes it
+    NaN), source02 = -1, on the Gauss-Chebyshev grid."""
+    z = g.zgrid()
+    hov = None
+    for n, v in r.source_params:
+        if n == "HovEll":
+            hov = v
+            break
+    out = {2: -np.ones(g.NZAA)}
+    if hov is None and r.source_params:
+        return out   # the reference stops here (an unknown sourceParams name)
+    h = 0.0 if hov is None else hov
+    with np.errstate(invalid="ignore", divide="ignore"):
+        out[1] = h * np.exp(-z * h) / (1.0 - np.exp(-h)) - 1.0
+    return out
+
+
+def default_penalisation_mask(g: Geometry) -> np.ndarray:
+    """max of the two masks of the reference's default PL_user_penalisation_mask.f90
+    on the grid, (NYAA, NXAA, NZAA): z - (0.9 + 0.1 cos(5 (x + y) 2 pi / Lx)) and
+    0.4 exp(-(6 + cos(2 pi x / Lx))^2) / exp(-25) - z, at the reference's grid
+    labels x = (i + 2) Lx / NXAA, y = (j + 2) Ly / NYAA (PL_geometry.f90:138-145,
+    phys_iStart = 1), with its single-precision literals pi, 0.9 and 0.1."""
+    pi = float(np.float32(3.14159265358979311599796346854))
+    c09, c01 = float(np.float32(0.9)), float(np.float32(0.1))
+    x = (np.arange(g.NXAA) + 2) * 1.0 * g.Lx / g.NXAA
+    y = (np.arange(g.NYAA) + 2) * 1.0 * g.Ly / g.NYAA
+    z = g.zgrid()
+    X = x[None, :, None]
+    Y = y[:, None, None]
+    Z = z[None, None, :]
+    m1 = Z - (c09 + c01 * np.cos(5 * (X + Y) * 2 * pi / g.Lx))
+    m2 = (0.4 * np.exp(-((6.0 + np.cos(2 * pi * X / g.Lx)) ** 2)) / np.exp(-25.0)) - Z
+    return np.maximum(m1, m2)
+
+
+def penalisation_field(mask: np.ndarray, strength: float, width: float) -> np.ndarray:
+    """init_penalisation (marching.f90:778-822): strength (1 + tanh(width mask)) / 2."""
+    pm = np.tanh(width * mask)
+    pm = (1.0 + pm) / 2.0
+    return strength * pm
+
+
+# --------------------------------------------------------------------------------------
 # the solver
 # --------------------------------------------------------------------------------------
 
@@ -650,8 +815,9 @@ def r2r_backward(arr: np.ndarray) -> np.ndarray:
 class Solver:
     """State and operators of one plane-layer problem on one rank (world_size = 1)."""
 
-    def __init__(self, equations_text: str, parameters_text: str, scheme: Optional[str] = None):
-        self.recipe = parse_equations(equations_text)
+    def __init__(self, equations_text: str, parameters_text: str, scheme: Optional[str] = None,
+                 smagorinsky: bool = False, smagorinsky_prefactor: float = 1.0, cfl_factor_z: float = 1.0):
+        self.recipe = parse_equations(equations_text, smagorinsky)
         p = read_parameters_text(parameters_text)
         self.params = p
         self.g = Geometry(p["NX"], p["NY"], p["NZ"], p["Lx"], p["Ly"], p["gap"], p["center"])
@@ -659,6 +825,29 @@ class Solver:
         self.nstages, self.A, self.Ah = ars_tableau(self.scheme)
         self._build()
         self.dt_factored = None
+        self.smagorinsky_prefactor = smagorinsky_prefactor
+        self.cfl_factor_z = cfl_factor_z
+        self.smago_profile = np.zeros(self.g.NZAA)   # nuSmago's physical values (one per z)
+        self.sources = default_sources(self.recipe, self.g)
+        self.penal_mask = default_penalisation_mask(self.g)
+        self.penal_phys = {}
+        for i, o in enumerate(self.recipe.full_opts):
+            if o["penal"] is not None:
+                self.penal_phys[i] = penalisation_field(self.penal_mask, *o["penal"])
+
+    def set_source(self, index: int, profile: np.ndarray):
+        """A user source sourceNN from its values on the Gauss-Chebyshev grid (the
+        reference's PL_user_sources_definitions.f90 include)."""
+        self.sources[index] = np.asarray(profile, dtype=np.float64).copy()
+
+    def set_penalisation_mask(self, mask: np.ndarray):
+        """max over the user's masks on the grid, (NYAA, NXAA, NZAA) (the reference's
+        PL_user_penalisation_mask.f90 include); every penalised variable's field is
+        remade from it."""
+        self.penal_mask = np.asarray(mask, dtype=np.float64).copy()
+        for i, o in enumerate(self.recipe.full_opts):
+            if o["penal"] is not None:
+                self.penal_phys[i] = penalisation_field(self.penal_mask, *o["penal"])
 
     # ---------------- setup ----------------
     def _build(self):
@@ -823,6 +1012,9 @@ class Solver:
                     if t.dz:  # differentiate_zero, then dsca (marching.f90:488-494)
                         buf = self.differentiate(buf, t.dz)
                     spec[0, 0, :] = spec[0, 0, :] + buf * t.dsca
+            o = r.full_opts[len(out)] if r.full_opts else None
+            if o is not None and o["penal"] is None and not o["smago"]:
+                spec = z_filter(spec, o["extract"], o["decomp"])
             out.append(spec)
         return out
 
@@ -881,6 +1073,18 @@ class Solver:
                     self._im_cache[key] = cheb_IM(g.NZ, g.center, g.gap, t.Iz, t.mz)
                 trunc = self._im_cache[key][s.orders[t.eqn]:, :]
                 K[lay.eq_pos[t.eqn]] += trunc @ buf
+            # sources (marching.f90:398-415): constant terms of the mean equations
+            for t in r.sources:
+                if t.sys != isys:
+                    continue
+                if t.index not in self.sources:
+                    raise ValueError("source%02d is not defined" % t.index)
+                buf = source_spectrum(self.sources[t.index])[:g.NZ] * t.dsca
+                key = (t.Iz, 0)
+                if key not in self._im_cache:
+                    self._im_cache[key] = cheb_IM(g.NZ, g.center, g.gap, t.Iz, 0)
+                trunc = self._im_cache[key][s.orders[t.eqn]:, :]
+                K[lay.eq_pos[t.eqn]] += trunc @ buf
             zk.append(K)
         return khat, zk
 
@@ -888,7 +1092,24 @@ class Solver:
         """Full variables in physical space plus the quadratic variables' spectra."""
         g, r = self.g, self.recipe
         fspec = self.full_var_spec(src_kxky, src_zero)
-        fphys = [spec_to_phys(s, g) for s in fspec]
+        fphys = []
+        for i, sp_ in enumerate(fspec):
+            o = r.full_opts[i] if r.full_opts else None
+            if o is not None and o["penal"] is not None:
+                # a penalised variable is its mask field, never transformed (marching.f90:515)
+                fphys.append(self.penal_phys[i])
+            elif o is not None and o["smago"]:
+                # nuSmago (marching.f90:516-541): the previous values plus the squares of
+                # dxUfull, dyUfull, dxVfull, dyVfull, averaged horizontally, prefactor * sqrt
+                acc = np.broadcast_to(self.smago_profile, (g.NYAA, g.NXAA, g.NZAA)).copy()
+                for j, (nm, _, _) in enumerate(r.full_vars[:i]):
+                    if nm in ("dxUfull", "dyUfull", "dxVfull", "dyVfull"):
+                        acc = acc + fphys[j] ** 2
+                prof = acc.sum(axis=0).sum(axis=0) / g.NXAA / g.NYAA
+                self.smago_profile = self.smagorinsky_prefactor * np.sqrt(prof)
+                fphys.append(np.broadcast_to(self.smago_profile, (g.NYAA, g.NXAA, g.NZAA)).copy())
+            else:
+                fphys.append(spec_to_phys(sp_, g))
         self._cfl(fphys)
         qphys, qspec = [], []
         for name, i1, i2, rm in r.quad_vars:
@@ -909,7 +1130,8 @@ class Solver:
         return fphys, qphys, qspec
 
     def _cfl(self, fphys):
-        """compute_cfl_based_timestep (marching.f90:200-254), cflFactor_along_z = 1."""
+        """compute_cfl_based_timestep (marching.f90:200-254): the w term scaled by
+        cflFactor_along_z and left out at or below 1e-10."""
         g = self.g
         if len(fphys) < 3:
             self.cfl_dt = None
@@ -917,9 +1139,15 @@ class Solver:
         w = g.zweights()
         u = np.abs(fphys[0]).max() * g.NXAA / g.Lx
         v = np.abs(fphys[1]).max() * g.NYAA / g.Ly
-        wz = max(v, (np.abs(fphys[2]) / w[None, None, :]).max())
+        f = getattr(self, "cfl_factor_z", 1.0)
+        wz = max(v, (np.abs(fphys[2]) / w[None, None, :] * f).max()) if f > 1e-10 else v
         m = max(u, v, wz)
         self.cfl_dt = 1.0 / m if m > 0 else float('inf')
+        if self.recipe.smagorinsky:
+            # marching.f90:241-251, with the single-precision literals 0.95 and 3.141592
+            c = float(np.float32(np.float32(2) * np.float32(3.141592)) ** np.float32(2))
+            den = c * float(np.max(fphys[-1])) * ((g.NXAA / g.Lx) ** 2 + (g.NYAA / g.Ly) ** 2)
+            self.cfl_dt = min(self.cfl_dt, float(np.float32(0.95)) / den if den > 0 else float('inf'))
 
     def volume_average(self, phys: np.ndarray) -> float:
         """output_global_quantities 'volume' object (PL_IMEX_timestepping_output.f90:38-52)."""

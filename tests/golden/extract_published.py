@@ -9,8 +9,10 @@ Rayleigh-Benard growth rate quoted by benchmark 01
 (etc/benchmarks/01_Rayleigh_Benard_stressFree/benchmark_01_stressfree_rayleigh_benard.ipynb:68)
 is stored beside them, with benchmark 02's published mean Nusselt number and
 its standard deviation (velocity-pressure form) and a verbatim copy of that
-benchmark's input files (tests/golden/benchmark02/: both equation forms), and
-benchmark 01's (tests/golden/benchmark01/).
+benchmark's input files (tests/golden/benchmark02/: both equation forms),
+benchmark 01's (tests/golden/benchmark01/) and the equation files of the
+examples with sources, penalisation and the stratified channel
+(tests/golden/examples/).
 
 usage: python tests/golden/extract_published.py <path-to-coral-tree>
 """
@@ -54,6 +56,19 @@ def main(root):
         with open(os.path.join(root, "etc/benchmarks/02_RRBC_julien_JFM96", name), "rb") as f:
             data = f.read()
         with open(os.path.join(dst, name), "wb") as f:
+            f.write(data)
+    # equation files of the reference's examples that use sources, penalisation and
+    # the stratified channel (tests/golden/examples/, names kept)
+    dst = os.path.join(here, "examples")
+    os.makedirs(dst, exist_ok=True)
+    for rel, name in (("etc/coral_equations_examples/coral.equations.RBC_penalised", None),
+                      ("etc/coral_equations_examples/coral.equations.radiative_heating_potentials", None),
+                      ("etc/benchmarks/coral.equations.stratifiedChannel.velocityPressure", None),
+                      ("etc/benchmarks/coral.equations.stratifiedChannel.toroidalPoloidal", None),
+                      ("etc/baroclinic_turbulence/coral.equations", "coral.equations.baroclinic_turbulence")):
+        with open(os.path.join(root, rel), "rb") as f:
+            data = f.read()
+        with open(os.path.join(dst, name or os.path.basename(rel)), "wb") as f:
             f.write(data)
     # benchmark 01's input files (stress-free Rayleigh-Benard, linear growth)
     dst = os.path.join(here, "benchmark01")

@@ -136,3 +136,76 @@ def test_usr_output_parser_on_the_reference_file():
         for o in due:
             first.setdefault(o[0], t)
     assert first["profil"] == 50 and first["zSlice"] == 1000 and "volume" not in first
+
+
+EXAMPLES = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "examples")
+
+
+def test_example_recipes_with_sources_and_penalisation_parse():
+    """The reference's example equation files read unmodified: sources with their
+    parameters, a penalised variable with strength and width."""
+    def rd(n):
+        with open(os.path.join(EXAMPLES, n)) as f:
+            return co.parse_equations(f.read())
+    r = rd("coral.equations.RBC_penalised")
+    assert [f[0] for f in r.full_vars] == ["uFull", "vFull", "wFull", "tFull", "GAMMA"]
+    assert r.full_opts[4]["penal"] == [1e3, 1e2] and len(r.quad_vars) == 12
+    r = rd("coral.equations.radiative_heating_potentials")
+    assert r.source_params == [("HovEll", 41.66666)]
+    assert [(t.index, t.dsca, t.Iz) for t in r.sources] == [(1, 1.0, 2), (2, 1.0, 2)]
+    r = rd("coral.equations.stratifiedChannel.velocityPressure")
+    assert [(t.index, t.dsca, t.Iz, t.sys) for t in r.sources] == [(2, -1.0, 2, 0)]
+    r = rd("coral.equations.baroclinic_turbulence")
+    assert sorted(t.index for t in r.sources) == [3, 4, 5]
+    assert co.parse_equations(open(os.path.join(EXAMPLES, "coral.equations.RBC_penalised")).read(),
+                              smagorinsky=True).full_vars[-1][0] == "nuSmago"
+
+
+def test_surface_values_and_vertical_decompositions():
+    """z_filter on Chebyshev series: surface values are the series at -1 / +1;
+    baroclinic leaves zero vertical mean, barotropic leaves only the mean (the
+    reference keeps coefficient NZ - 1, zero here)."""
+    rng = np.random.default_rng(0)
+    NZ = 16
+    c = rng.standard_normal((3, NZ))
+    c[:, NZ - 1] = 0.0
+    bot = co.z_filter(c, "BotSurf", None)
+    top = co.z_filter(c, "TopSurf", None)
+    assert np.allclose(bot[:, 0], np.polynomial.chebyshev.chebval(-1.0, c.T), rtol=0, atol=1e-13)
+    assert np.allclose(top[:, 0], np.polynomial.chebyshev.chebval(1.0, c.T), rtol=0, atol=1e-13)
+    assert not bot[:, 1:].any() and not top[:, 1:].any()
+
+    def mean(s):  # (1/2) integral over [-1, 1] of the series
+        C = np.polynomial.chebyshev
+        return np.array([C.chebval(1.0, C.chebint(x, lbnd=-1)) / 2.0 for x in s])
+    bc = co.z_filter(c, "nowhere", "baroclinic")
+    assert np.abs(mean(bc)).max() < 1e-13
+    assert np.array_equal(bc[:, 1:], c[:, 1:])
+    bt = co.z_filter(c, "nowhere", "barotropic")
+    assert np.allclose(bt[:, 0], mean(c), rtol=0, atol=1e-13)
+    assert not bt[:, 1:].any()
+
+
+def test_sources_and_penalisation_fields():
+    """Compute_1dCheby_transform of a constant; the default sources; the default
+    penalisation mask's two surfaces at the reference's grid labels."""
+    c = co.source_spectrum(-np.ones(24))
+    assert abs(c[0] + 1.0) < 1e-15 and np.abs(c[1:]).max() < 1e-15
+    g = co.Geometry(8, 8, 16, 2.0, 2.0, 1.0, 0.5)
+    z = g.zgrid()
+    assert abs(co.source_spectrum(z)[1] - 0.5) < 1e-14  # z = 0.5 + T_1 / 2
+    r = co.parse_equations(open(os.path.join(EXAMPLES, "coral.equations.radiative_heating_potentials")).read())
+    s = co.default_sources(r, g)
+    h = 41.66666
+    assert np.allclose(s[1], h * np.exp(-z * h) / (1 - np.exp(-h)) - 1.0, rtol=1e-15)
+    assert np.array_equal(s[2], -np.ones(g.NZAA))
+    m = co.default_penalisation_mask(g)
+    assert m.shape == (g.NYAA, g.NXAA, g.NZAA)
+    pi = float(np.float32(math.pi))
+    x = (np.arange(g.NXAA) + 2) * g.Lx / g.NXAA
+    y = (np.arange(g.NYAA) + 2) * g.Ly / g.NYAA
+    m1 = z[None, None, :] - (float(np.float32(0.9)) + float(np.float32(0.1)) *
+                             np.cos(5 * (x[None, :, None] + y[:, None, None]) * 2 * pi / g.Lx))
+    assert np.all(m >= m1)
+    f = co.penalisation_field(m, 1e3, 1e2)
+    assert f.min() >= 0.0 and f.max() <= 1e3
