@@ -12,7 +12,7 @@ namespace coral {
 constexpr int kMaxGroups = 16;  // monomial groups (i kx)^a (i ky)^b per operator
 constexpr int kMaxStages = 4;   // ARS_443 has 4 implicit stages
 constexpr int kMaxSets = 8;     // coupled systems of one kind
-constexpr int kMaxQuad = 16;    // quadratic variables
+constexpr int kMaxQuad = 32;    // quadratic variables
 constexpr int kMaxFull = 16;    // full variables
 constexpr int kMaxStatic = 4;   // full variables whose physical field is given, not transformed
 constexpr int kMaxFullTerms = 8;

@@ -11,8 +11,8 @@ is stored beside them, with benchmark 02's published mean Nusselt number and
 its standard deviation (velocity-pressure form) and a verbatim copy of that
 benchmark's input files (tests/golden/benchmark02/: both equation forms),
 benchmark 01's (tests/golden/benchmark01/) and the equation files of the
-examples with sources, penalisation and the stratified channel
-(tests/golden/examples/).
+reference's equation examples, the stratified channel, the convective dynamo
+and the baroclinic-turbulence case (tests/golden/examples/).
 
 usage: python tests/golden/extract_published.py <path-to-coral-tree>
 """
@@ -61,10 +61,15 @@ def main(root):
     # the stratified channel (tests/golden/examples/, names kept)
     dst = os.path.join(here, "examples")
     os.makedirs(dst, exist_ok=True)
-    for rel, name in (("etc/coral_equations_examples/coral.equations.RBC_penalised", None),
-                      ("etc/coral_equations_examples/coral.equations.radiative_heating_potentials", None),
+    ex = "etc/coral_equations_examples/coral.equations."
+    for rel, name in ((ex + "RBC_penalised", None), (ex + "radiative_heating_potentials", None),
+                      (ex + "RBC_potentials", None), (ex + "RBC_primitiveVars_Vanilla", None),
+                      (ex + "RBC_primitiveVars_variant1", None), (ex + "RBC_primitiveVars_variant2", None),
                       ("etc/benchmarks/coral.equations.stratifiedChannel.velocityPressure", None),
                       ("etc/benchmarks/coral.equations.stratifiedChannel.toroidalPoloidal", None),
+                      ("etc/benchmarks/03_convective_dynamo/coral.equations", "coral.equations.convective_dynamo"),
+                      ("etc/benchmarks/03_convective_dynamo/coral.equations.toroidalPoloidal",
+                       "coral.equations.convective_dynamo.toroidalPoloidal"),
                       ("etc/baroclinic_turbulence/coral.equations", "coral.equations.baroclinic_turbulence")):
         with open(os.path.join(root, rel), "rb") as f:
             data = f.read()

@@ -254,3 +254,26 @@ def test_bad_arguments_are_refused():
         with pytest.raises(CoralError) as e:
             PlaneLayer(eq, par, args=args)
         assert e.value.code == -1, str(e.value)
+
+
+@pytest.mark.parametrize("name", [
+    "coral.equations.RBC_potentials", "coral.equations.RBC_primitiveVars_Vanilla",
+    "coral.equations.RBC_primitiveVars_variant1", "coral.equations.RBC_primitiveVars_variant2",
+    "coral.equations.stratifiedChannel.toroidalPoloidal", "coral.equations.convective_dynamo"])
+def test_reference_example_recipes_match_oracle(name):
+    """Every other equation file the reference ships, read unmodified: the RBC
+    examples (potentials; primitive variables with up to 11 full and 18
+    quadratic variables), the stratified channel in toroidal-poloidal form and
+    the convective dynamo (three coupled systems, 23 quadratic variables)."""
+    eq = _example(name)
+    par = params(16, 12, 24, dt=1e-5)
+    ref, pl, errs = _run_both(eq, par, 2, 1e-5)
+    pl.close()
+
+
+def test_dynamo_toroidal_poloidal_file_is_refused():
+    """bxFull where the full variable is BxFull: CORAL_EPARSE, as the reference stops."""
+    from coral_b200.solver import CoralError, PlaneLayer
+    with pytest.raises(CoralError) as e:
+        PlaneLayer(_example("coral.equations.convective_dynamo.toroidalPoloidal"), params(16, 12, 24))
+    assert e.value.code == -6 and "bad NL var definition" in str(e.value)

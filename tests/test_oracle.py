@@ -209,3 +209,13 @@ def test_sources_and_penalisation_fields():
     assert np.all(m >= m1)
     f = co.penalisation_field(m, 1e3, 1e2)
     assert f.min() >= 0.0 and f.max() <= 1e3
+
+
+def test_dynamo_toroidal_poloidal_file_is_refused():
+    """The convective-dynamo example's toroidal-poloidal file names bxFull where
+    its full variable is BxFull: the reference's parser stops on it with 'bad NL
+    var definition', and so does the oracle's."""
+    with open(os.path.join(EXAMPLES, "coral.equations.convective_dynamo.toroidalPoloidal")) as f:
+        t = f.read()
+    with pytest.raises(ValueError, match="bad NL var definition"):
+        co.parse_equations(t)
