@@ -529,8 +529,8 @@ void setup(coral_handle* h, const std::string& eqs, const std::string& pars, con
     k.ku = k.ops.ku;
     k.ldab = 2 * k.kl + k.ku + 1;
     k.ldab += k.ldab & 1;  // even column stride: every column starts on a 16-byte boundary
-    if (k.kl > 31 || k.kl + k.ku > 64)
-      throw CoralError(CORAL_EUNSUPPORTED, "band of the coupled system exceeds kl <= 31, kl+ku <= 64");
+    if (k.kl > 63 || k.kl + k.ku > 127)
+      throw CoralError(CORAL_EUNSUPPORTED, "band of the coupled system exceeds kl <= 63, kl+ku <= 127");
     k.M = upload_ell(mem, k.ops.M);
     k.L = upload_ell(mem, k.ops.L);
     k.NL = upload_ell(mem, k.ops.NLop);

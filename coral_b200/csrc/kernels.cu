@@ -1024,6 +1024,9 @@ __device__ __forceinline__ double2 ell_row(const DevEll& op, int t, const double
   return acc;
 }
 
+// WIDE: bands of kl <= 63, kl + ku <= 127 (each lane holds two multipliers and
+// four U entries of a column); otherwise kl <= 31, kl + ku <= 64
+template <bool WIDE>
 __global__ void __launch_bounds__(kWPB * 32) k_solve(SolveArgs a) {
   extern __shared__ double2 sm[];
   __shared__ double2 coefs[kWPB][2][kMaxGroups];
@@ -1062,18 +1065,25 @@ __global__ void __launch_bounds__(kWPB * 32) k_solve(SolveArgs a) {
     const unsigned char* dp = a.dpiv + (size_t)act * ((T + 7) & ~7);
     // ---- forward: apply row interchanges and L (zgbtrs, 'N', kl > 0)
     {
-      double2 lr[kPF];
+      double2 lr[kPF], lr2[WIDE ? kPF : 1];
 #pragma unroll
-      for (int q = 0; q < kPF; ++q)
+      for (int q = 0; q < kPF; ++q) {
         lr[q] = (q < T - 1 && lane < kl) ? ab[(size_t)q * ldab + kv + 1 + lane] : zero2();
+        if constexpr (WIDE) lr2[q] = (q < T - 1 && lane + 32 < kl) ? ab[(size_t)q * ldab + kv + 33 + lane] : zero2();
+      }
       for (int j0 = 0; j0 < T - 1; j0 += kPF) {
 #pragma unroll
         for (int q = 0; q < kPF; ++q) {
           const int j = j0 + q;
           if (j < T - 1) {
             const double2 l = lr[q];
+            double2 l2 = zero2();
             const int jn = j + kPF;
             lr[q] = (jn < T - 1 && lane < kl) ? ab[(size_t)jn * ldab + kv + 1 + lane] : zero2();
+            if constexpr (WIDE) {
+              l2 = lr2[q];
+              lr2[q] = (jn < T - 1 && lane + 32 < kl) ? ab[(size_t)jn * ldab + kv + 33 + lane] : zero2();
+            }
             const int p = j + dp[j];
             if (p != j) {
               if (lane == 0) {
@@ -1086,6 +1096,8 @@ __global__ void __launch_bounds__(kWPB * 32) k_solve(SolveArgs a) {
             const double2 bj = b[j];
             const int lm = min(kl, T - 1 - j);
             if (lane < lm) b[j + 1 + lane] = csub(b[j + 1 + lane], cmul(l, bj));
+            if constexpr (WIDE)
+              if (lane + 32 < lm) b[j + 33 + lane] = csub(b[j + 33 + lane], cmul(l2, bj));
             __syncwarp();
           }
         }
@@ -1093,15 +1105,16 @@ __global__ void __launch_bounds__(kWPB * 32) k_solve(SolveArgs a) {
     }
     // ---- backward: U x = y, U with kl+ku super-diagonals, diagonal stored as its reciprocal
     {
-      double2 u1[kPF], u2[kPF], dg[kPF];
+      constexpr int NU = WIDE ? 4 : 2;  // U entries per lane: offsets 1 + lane + 32 u
+      double2 uu[NU][kPF], dg[kPF];
 #pragma unroll
       for (int q = 0; q < kPF; ++q) {
         const int j = T - 1 - q;
         if (j >= 0) {
           const double2* col = ab + (size_t)j * ldab;
           dg[q] = col[kv];
-          u1[q] = (lane + 1 <= kv) ? col[kv - 1 - lane] : zero2();
-          u2[q] = (lane + 33 <= kv) ? col[kv - 33 - lane] : zero2();
+#pragma unroll
+          for (int u = 0; u < NU; ++u) uu[u][q] = (lane + 1 + 32 * u <= kv) ? col[kv - 1 - 32 * u - lane] : zero2();
         }
       }
       for (int j0 = T - 1; j0 >= 0; j0 -= kPF) {
@@ -1109,19 +1122,25 @@ __global__ void __launch_bounds__(kWPB * 32) k_solve(SolveArgs a) {
         for (int q = 0; q < kPF; ++q) {
           const int j = j0 - q;
           if (j >= 0) {
-            const double2 d = dg[q], c1 = u1[q], c2 = u2[q];
+            const double2 d = dg[q];
+            double2 c[NU];
+#pragma unroll
+            for (int u = 0; u < NU; ++u) c[u] = uu[u][q];
             const int jn = j - kPF;
             if (jn >= 0) {
               const double2* col = ab + (size_t)jn * ldab;
               dg[q] = col[kv];
-              u1[q] = (lane + 1 <= kv) ? col[kv - 1 - lane] : zero2();
-              u2[q] = (lane + 33 <= kv) ? col[kv - 33 - lane] : zero2();
+#pragma unroll
+              for (int u = 0; u < NU; ++u) uu[u][q] = (lane + 1 + 32 * u <= kv) ? col[kv - 1 - 32 * u - lane] : zero2();
             }
             const double2 bj = cmul(b[j], d);
             __syncwarp();
             if (lane == 0) b[j] = bj;
-            if (lane + 1 <= kv && j - lane - 1 >= 0) b[j - lane - 1] = csub(b[j - lane - 1], cmul(c1, bj));
-            if (lane + 33 <= kv && j - lane - 33 >= 0) b[j - lane - 33] = csub(b[j - lane - 33], cmul(c2, bj));
+#pragma unroll
+            for (int u = 0; u < NU; ++u) {
+              const int o = lane + 1 + 32 * u;
+              if (o <= kv && j - o >= 0) b[j - o] = csub(b[j - o], cmul(c[u], bj));
+            }
             __syncwarp();
           }
         }
@@ -1160,6 +1179,8 @@ __device__ __forceinline__ double2 crecip(double2 p) {
   }
 }
 
+// WIDE: kl <= 63 (two pivot candidates per lane); otherwise kl <= 31
+template <bool WIDE>
 __global__ void __launch_bounds__(kWPB * 32) k_factor(FactorArgs a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int sys = blockIdx.x * kWPB + warp;
@@ -1213,6 +1234,13 @@ __global__ void __launch_bounds__(kWPB * 32) k_factor(FactorArgs a) {
       mag = fabs(v.x) + fabs(v.y);
       idx = lane;
     }
+    if constexpr (WIDE) {
+      if (lane + 32 <= km) {  // the later row wins only when strictly larger (first maximum)
+        const double2 v = ab[(size_t)j * ldab + kv + lane + 32];
+        const double m2 = fabs(v.x) + fabs(v.y);
+        if (m2 > mag) { mag = m2; idx = lane + 32; }
+      }
+    }
     for (int o = 16; o > 0; o >>= 1) {
       const double m2 = __shfl_xor_sync(0xffffffffu, mag, o);
       const int i2 = __shfl_xor_sync(0xffffffffu, idx, o);
@@ -1239,10 +1267,11 @@ __global__ void __launch_bounds__(kWPB * 32) k_factor(FactorArgs a) {
     const double2 r = crecip(ab[(size_t)j * ldab + kv]);
     __syncwarp();
     if (km > 0) {
-      if (lane >= 1 && lane <= km) {
-        double2* m = ab + (size_t)j * ldab + kv + lane;
-        *m = cmul(*m, r);
-      }
+      for (int i = lane; i <= km; i += 32)
+        if (i >= 1) {
+          double2* m = ab + (size_t)j * ldab + kv + i;
+          *m = cmul(*m, r);
+        }
       __syncwarp();
       const int nc = ju - j;
       for (int e = lane; e < nc * km; e += 32) {
@@ -3281,12 +3310,18 @@ void launch_nl(const NLArgs& a, cudaStream_t s) {
 void launch_solve(const SolveArgs& a, cudaStream_t s) {
   const int nsys = a.d.NXH * a.d.NYA;
   size_t sm = (size_t)kWPB * a.T * sizeof(double2);
-  set_smem(k_solve, sm);
-  k_solve<<<(nsys + kWPB - 1) / kWPB, kWPB * 32, sm, s>>>(a);
+  if (a.kl > 31 || a.kl + a.ku > 64) {
+    set_smem(k_solve<true>, sm);
+    k_solve<true><<<(nsys + kWPB - 1) / kWPB, kWPB * 32, sm, s>>>(a);
+  } else {
+    set_smem(k_solve<false>, sm);
+    k_solve<false><<<(nsys + kWPB - 1) / kWPB, kWPB * 32, sm, s>>>(a);
+  }
 }
 void launch_factor(const FactorArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;
-  k_factor<<<(a.nact + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
+  if (a.kl > 31) k_factor<true><<<(a.nact + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
+  else k_factor<false><<<(a.nact + kWPB - 1) / kWPB, kWPB * 32, 0, s>>>(a);
 }
 template <int RM, int RN, int G0 = 0, int G1 = 0, int G2 = 0>
 static void launch_rhs_tiles(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {

@@ -116,8 +116,7 @@ def test_user_sources_match_oracle():
     define (the stratified channel's source02 renamed source07, given
     exp(-(1 - z) / 0.5) as the baroclinic-turbulence example's own definitions
     file gives source03): a step fails until coral_set_source gives it, then
-    matches the oracle.  (The baroclinic-turbulence example itself needs a band
-    of kl = 35, ku = 49, beyond the solver's kl <= 31, kl + ku <= 64.)"""
+    matches the oracle."""
     from coral_b200.solver import CoralError, PlaneLayer
     eq = _example("coral.equations.stratifiedChannel.velocityPressure").replace("source02", "source07")
     par = params(16, 12, 24, dt=1e-4)
@@ -136,6 +135,30 @@ def test_user_sources_match_oracle():
 
     ref, pl, errs = _run_both(eq, par, 3, 1e-4, setup=setup)
     pl.close()
+
+
+def test_baroclinic_turbulence_example_matches_oracle():
+    """The baroclinic-turbulence example unmodified: five coupled variables with
+    fourth-order operators (band kl = 35, ku = 49: the wide complex factor and
+    solve), eight mean systems and sources 3-5 of its own definitions file
+    (exp(-(1 - z) / shearL), the same / shearL and / shearL^2, shearL = 0.5)."""
+    eq = _example("coral.equations.baroclinic_turbulence")
+    par = params(16, 16, 24, dt=1e-5)
+
+    def setup(ref, pl):
+        z = ref.g.zgrid()
+        L = 0.5
+        for k, prof in ((3, np.exp(-(1.0 - z) / L)), (4, np.exp(-(1.0 - z) / L) / L),
+                        (5, np.exp(-(1.0 - z) / L) / L ** 2)):
+            ref.set_source(k, prof)
+            pl.set_source(k, prof)
+
+    ref, pl, errs = _run_both(eq, par, 2, 1e-5, setup=setup)
+    try:
+        ref.factorize(1e-5)
+        assert ref.kl_ku[0] == (35, 49)
+    finally:
+        pl.close()
 
 
 SURF = """>>linear_variable_bottom_boundary_value :: pBot <<
