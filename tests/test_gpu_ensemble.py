@@ -81,3 +81,34 @@ def test_seeded_64_member_ensemble_steps():
         assert np.array_equal(p.get_field(0), ens.members[i].get_field(0))
         p.close()
     ens.close()
+
+
+def test_ensemble_of_penalised_sourced_and_filtered_members_bitwise():
+    """Members with a penalisation field, mean-equation sources, and surface
+    values / vertical decompositions (the reference's example files and the
+    feature-test recipe) in one ensemble: bit for bit their single runs."""
+    from coral_b200.ensemble import Ensemble
+    from coral_b200.solver import PlaneLayer
+    from tests.test_gpu_features import _example, _with_surface_vars
+    spec = [(_example("coral.equations.RBC_penalised"), params(16, 16, 16, dt=1e-5)),
+            (_example("coral.equations.radiative_heating_potentials"), params(16, 12, 24, dt=1e-5)),
+            (_example("coral.equations.stratifiedChannel.velocityPressure"), params(24, 16, 24, dt=1e-5)),
+            (_with_surface_vars(equations()), params(16, 12, 24, dt=1e-5))]
+    ens = Ensemble([s[0] for s in spec], [s[1] for s in spec])
+    singles = [PlaneLayer(*s) for s in spec]
+    for i, (m, p) in enumerate(zip(ens.members, singles)):
+        _set_random(m, 70 + i)
+        _set_random(p, 70 + i)
+    ens.march_forward(1e-5, 3)
+    ens.synchronize()
+    for p in singles:
+        p.march_forward(1e-5, 3)
+        p.synchronize()
+    for m, p in zip(ens.members, singles):
+        for s in range(p.n_kxky):
+            assert np.array_equal(m.get_field(s), p.get_field(s))
+        for s in range(p.n_zero):
+            assert np.array_equal(m.get_mean_field(s), p.get_mean_field(s))
+    for p in singles:
+        p.close()
+    ens.close()
