@@ -2412,6 +2412,13 @@ int coral_autotune(coral_handle* h, double dt, int repeats, char* report, int n)
       CK(cudaMemcpy(v.data(), z.dev.field, z.dev.T * sizeof(double), cudaMemcpyDeviceToHost));
       zsaved.push_back(v);
     }
+    // (the Smagorinsky viscosity carries from stage to stage: part of the state)
+    std::vector<double> smago_saved;
+    if (h->smago_prof) {
+      smago_saved.resize(h->d.NZA);
+      CK(cudaStreamSynchronize(h->stream));
+      CK(cudaMemcpy(smago_saved.data(), h->smago_prof, h->d.NZA * sizeof(double), cudaMemcpyDeviceToHost));
+    }
     auto time_phases = [&](std::initializer_list<int> phases) {
       double best = 1e300;
       for (int r = 0; r < repeats + 1; ++r) {  // the first step sets attributes and warms the caches
@@ -2477,6 +2484,8 @@ int coral_autotune(coral_handle* h, double dt, int repeats, char* report, int n)
     for (void* p : saved) cudaFree(p);
     for (size_t i = 0; i < h->zs.size(); ++i)
       CK(cudaMemcpy(h->zs[i].dev.field, zsaved[i].data(), zsaved[i].size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (h->smago_prof)
+      CK(cudaMemcpy(h->smago_prof, smago_saved.data(), h->d.NZA * sizeof(double), cudaMemcpyHostToDevice));
     if (h->graph) {
       cudaGraphExecDestroy(h->graph);
       h->graph = nullptr;
