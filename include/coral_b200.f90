@@ -17,6 +17,10 @@ module coral_b200_c
                                CORAL_ESINGULAR = -4, CORAL_ENONFINITE = -5, CORAL_EPARSE = -6, CORAL_EIO = -7, &
                                CORAL_EUNSUPPORTED = -8, CORAL_ENODEV = -9
 
+  ! the device solver of a plane_layer run built with the replacement include
+  ! PL_IMEX_timestepping_marching_b200.f90 (created by its first march_forward)
+  type(c_ptr), save :: coral_b200_handle = c_null_ptr
+
   interface
     ! ---- creation and queries -------------------------------------------------
     integer(c_int) function coral_create(eqs_text, pars_text, scheme, device, h) bind(C, name="coral_create")

@@ -12,7 +12,8 @@ its standard deviation (velocity-pressure form) and a verbatim copy of that
 benchmark's input files (tests/golden/benchmark02/: both equation forms),
 benchmark 01's (tests/golden/benchmark01/) and the equation files of the
 reference's equation examples, the stratified channel, the convective dynamo
-and the baroclinic-turbulence case (tests/golden/examples/).
+and the baroclinic-turbulence case (tests/golden/examples/), and the names of the procedures of the marching
+include (tests/golden/marching_procedures.txt).
 
 usage: python tests/golden/extract_published.py <path-to-coral-tree>
 """
@@ -75,6 +76,13 @@ def main(root):
             data = f.read()
         with open(os.path.join(dst, name or os.path.basename(rel)), "wb") as f:
             f.write(data)
+    # names of the procedures in the marching include (the ones a replacement
+    # include has to define)
+    with open(os.path.join(root, "src/plane_layer/PL_IMEX_timestepping_marching.f90")) as f:
+        src = f.read()
+    names = re.findall(r"^\s*(?:real\(kind=dp\)\s+)?(?:subroutine|function)\s+(\w+)", src, re.I | re.M)
+    with open(os.path.join(here, "marching_procedures.txt"), "w") as f:
+        f.write("\n".join(names) + "\n")
     # benchmark 01's input files (stress-free Rayleigh-Benard, linear growth)
     dst = os.path.join(here, "benchmark01")
     os.makedirs(dst, exist_ok=True)
