@@ -2899,12 +2899,17 @@ __global__ void k_check_finite(const double2* x, size_t n, unsigned int* flags) 
 
 int grid1d(size_t n, int bs) { return (int)((n + bs - 1) / bs); }
 
-// Raise a kernel's dynamic shared-memory limit when it needs more than the
-// default 48 KB; a refused attribute is reported with the kernel and the size
-// (instead of surfacing later as a generic launch failure).
+// Raise a kernel's dynamic shared-memory limit when its static plus dynamic
+// shared memory exceeds the default 48 KB (a launch above it without the
+// attribute is an invalid argument); a refused attribute is reported with the
+// kernel and the size (instead of surfacing later as a generic launch failure).
 template <typename K>
 void set_smem_named(const char* name, K kernel, size_t bytes) {
-  if (bytes <= 48 * 1024) return;
+  size_t stat = 0;
+  cudaFuncAttributes fa;
+  if (cudaFuncGetAttributes(&fa, kernel) == cudaSuccess) stat = fa.sharedSizeBytes;
+  else cudaGetLastError();
+  if (bytes + stat <= 48 * 1024) return;
   const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();  // the refusal is reported here, not left for the next launch check

@@ -104,3 +104,30 @@ def test_steps_rrbc_cfg1_parameters_match_oracle():
     p = co.read_parameters_text(_cfg("rrbc_stressfree_192x192x96.parameters.in"))
     par = params(24, 24, 96, dt=5e-6, Lx=p["Lx"], Ly=p["Ly"])
     _steps_match(_cfg("rrbc_stressfree_ek1e-4_ra5e7.equations"), par, dt=5e-6, nsteps=3, seed=22, amp=1e-2)
+
+
+@pytest.mark.parametrize("n", [(128, 128, 128), (256, 256, 128)])
+def test_transforms_at_the_closure_grids(n):
+    """The closure's grids: x / y lengths 192 and 384, z length 192 (the
+    instances whose static plus dynamic shared memory crosses 48 KB without
+    either alone doing so)."""
+    from coral_b200.solver import PlaneLayer
+    eq = _cfg("rbc_noslip_ra1e8.equations")
+    par = params(*n, dt=1e-6)
+    p = co.read_parameters_text(par)
+    g = co.Geometry(p["NX"], p["NY"], p["NZ"], p["Lx"], p["Ly"], p["gap"], p["center"])
+    pl = PlaneLayer(eq, par)
+    rng = np.random.default_rng(19)
+    spec = rng.standard_normal((g.NXH, g.NYAA, g.NZ)) + 1j * rng.standard_normal((g.NXH, g.NYAA, g.NZ))
+    p_ref = co.spec_to_phys(spec, g)
+    assert np.abs(pl.spec_to_phys(spec) - p_ref).max() <= 1e-13 * np.abs(p_ref).max()
+    s_ref = co.phys_to_spec(p_ref, g)
+    assert np.abs(pl.phys_to_spec(p_ref) - s_ref).max() <= 1e-13 * np.abs(s_ref).max()
+    pl.close()
+
+
+def test_steps_nz128_match_oracle():
+    """3 ARS_222 steps at 16 x 16 x 128: the fused z kernel at NZAA = 192, as
+    the closure's grids run it (captured in a CUDA graph like every step)."""
+    _steps_match(_cfg("rbc_noslip_ra1e8.equations"), params(16, 16, 128, dt=1e-6), dt=1e-6, nsteps=3, seed=23,
+                 amp=1e-2)
