@@ -35,9 +35,8 @@ def _heat_error(scheme, dt):
     return math.sqrt(np.sum((u2 - u1 * np.exp(-rate * 10 * dt)) ** 2) / np.sum(u1 ** 2))
 
 
-@pytest.mark.parametrize("scheme,key,idx", [
-    ("ARS_222", "err222", 3), ("ARS_222", "err222", 6), ("ARS_111", "err111", 5),
-    ("ARS_443", "err443", 4)])
+@pytest.mark.parametrize("scheme,key,idx", [(s, k, i) for s, k in (("ARS_111", "err111"), ("ARS_222", "err222"),
+                                                                      ("ARS_443", "err443")) for i in range(7)])
 def test_heat_equation_published_errors(scheme, key, idx):
     dt = GOLD["dt"][idx]
     err = _heat_error(scheme, dt)
