@@ -3,6 +3,10 @@
 // stream and a CUDA graph of one timestep.
 #include <algorithm>
 #include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -130,6 +134,150 @@ void set_global_error(const std::string& msg) { g_create_error = msg; }
 // forward x passes per band of y rows, bands round-robin over the streams)
 constexpr int kYStreams = 3;
 
+// Output files written behind the time step (the reference writes them
+// synchronously, PL_IMEX_timestepping_output.f90:489-578): an object formed on
+// the device is copied into a page-locked staging buffer on a copy stream, and a
+// host thread writes the file once that copy has completed, while the next
+// steps run.  At most kOutBufs staging buffers (each grown to the largest
+// object) are in flight; flush() waits for every file and reports the first
+// failed write.
+struct OutputWriter {
+  static constexpr int kOutBufs = 2;
+  struct Job {
+    cudaEvent_t done;
+    int buf;
+    size_t n;
+    std::string dir, path;
+  };
+  int device = 0;
+  cudaStream_t copy = nullptr;
+  double* pin[kOutBufs] = {};
+  size_t cap[kOutBufs] = {};
+  bool busy[kOutBufs] = {};
+  cudaEvent_t last = nullptr;  // the latest copy out of the device buffer
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<Job> q;
+  std::thread th;
+  bool stop = false;
+  int pending = 0;
+  std::string err;
+
+  void start(int dev) {
+    device = dev;
+    if (th.joinable()) return;
+    th = std::thread([this] { run(); });
+  }
+  void run() {
+    cudaSetDevice(device);
+    for (;;) {
+      Job j;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return stop || !q.empty(); });
+        if (q.empty()) return;
+        j = q.front();
+        q.pop_front();
+      }
+      std::string e;
+      if (cudaEventSynchronize(j.done) != cudaSuccess) e = "copy of " + j.path + " failed";
+      if (e.empty() && mkdir_all(j.dir) != 0) e = "cannot create " + j.dir;
+      if (e.empty()) {
+        FILE* fp = std::fopen(j.path.c_str(), "wb");
+        if (!fp) {
+          e = "cannot open " + j.path;
+        } else {
+          if (std::fwrite(pin[j.buf], sizeof(double), j.n, fp) != j.n) e = "short write in " + j.path;
+          std::fclose(fp);
+        }
+      }
+      cudaEventDestroy(j.done);
+      std::lock_guard<std::mutex> lk(mu);
+      if (!e.empty() && err.empty()) err = e;
+      busy[j.buf] = false;
+      --pending;
+      cv.notify_all();
+    }
+  }
+  static int mkdir_all(const std::string& d) {
+    std::string cur;
+    for (size_t i = 0; i <= d.size(); ++i) {
+      if ((i == d.size() || d[i] == '/') && !cur.empty() && mkdir(cur.c_str(), 0755) != 0 && errno != EEXIST)
+        return -1;
+      if (i < d.size()) cur.push_back(d[i]);
+    }
+    return 0;
+  }
+  // copy n doubles of the device buffer src (formed on stream s) out and queue
+  // the file
+  void submit(const double* src, size_t n, cudaStream_t s, const std::string& dir, const std::string& path) {
+    int b = -1;
+    {
+      std::unique_lock<std::mutex> lk(mu);
+      cv.wait(lk, [&] {
+        for (int i = 0; i < kOutBufs; ++i)
+          if (!busy[i]) return true;
+        return false;
+      });
+      for (int i = 0; i < kOutBufs && b < 0; ++i)
+        if (!busy[i]) b = i;
+      busy[b] = true;
+    }
+    if (cap[b] < n) {
+      if (pin[b]) cudaFreeHost(pin[b]);
+      pin[b] = nullptr;
+      cap[b] = 0;
+      if (cudaMallocHost(&pin[b], n * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        std::lock_guard<std::mutex> lk(mu);
+        busy[b] = false;
+        throw CoralError(CORAL_ENOMEM, "page-locked output buffer");
+      }
+      cap[b] = n;
+    }
+    if (!copy) CK(cudaStreamCreateWithFlags(&copy, cudaStreamNonBlocking));
+    if (!last) CK(cudaEventCreateWithFlags(&last, cudaEventDisableTiming));
+    cudaEvent_t formed, done;
+    CK(cudaEventCreateWithFlags(&formed, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    CK(cudaEventRecord(formed, s));
+    CK(cudaStreamWaitEvent(copy, formed, 0));
+    CK(cudaMemcpyAsync(pin[b], src, n * sizeof(double), cudaMemcpyDeviceToHost, copy));
+    CK(cudaEventRecord(done, copy));
+    CK(cudaEventRecord(last, copy));
+    cudaEventDestroy(formed);
+    std::lock_guard<std::mutex> lk(mu);
+    q.push_back(Job{done, b, n, dir, path});
+    ++pending;
+    cv.notify_all();
+  }
+  // stream s waits for the latest copy before it writes the device buffer again
+  void order(cudaStream_t s) {
+    if (last) CK(cudaStreamWaitEvent(s, last, 0));
+  }
+  void flush() {
+    std::unique_lock<std::mutex> lk(mu);
+    cv.wait(lk, [&] { return pending == 0; });
+    if (!err.empty()) {
+      const std::string e = err;
+      err.clear();
+      throw CoralError(CORAL_EIO, e);
+    }
+  }
+  ~OutputWriter() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stop = true;
+      cv.notify_all();
+    }
+    if (th.joinable()) th.join();
+    for (auto& p : pin)
+      if (p) cudaFreeHost(p);
+    if (last) cudaEventDestroy(last);
+    if (copy) cudaStreamDestroy(copy);
+  }
+};
+
 struct coral_handle {
   std::string err;
   int device = 0;
@@ -198,6 +346,7 @@ struct coral_handle {
   std::vector<UsrOut> uo;
   long long time_integer = 1;
   double* uo_buf = nullptr;  // one physical field: an object's file contents before the copy back
+  std::unique_ptr<OutputWriter> writer;
   // z transforms: 0 = FP64 FFT (k_z_fused), 1 = int8-digit contractions on the
   // tensor cores (zsplit.cu); form_last = the form of the last step (KE sums)
   int zform = 0, zform_last = 0;
@@ -1739,6 +1888,11 @@ void write_usr_object(coral_handle* h, const coral_handle::UsrOut& o, long long 
   const char* sub = "Slices";
   size_t n = 0;
   double* out = h->uo_buf;
+  if (!h->writer) {
+    h->writer = std::make_unique<OutputWriter>();
+    h->writer->start(h->device);
+  }
+  h->writer->order(h->stream);  // the previous object's copy out of uo_buf
   switch (o.kind) {
     case 0:
       sub = "Volumes";
@@ -1766,17 +1920,8 @@ void write_usr_object(coral_handle* h, const coral_handle::UsrOut& o, long long 
   }
   ++h->launches;
   CK(cudaGetLastError());
-  std::vector<double> buf(n);
-  CK(cudaMemcpyAsync(buf.data(), out, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
-  CK(cudaStreamSynchronize(h->stream));
   const std::string sdir = dir + "/" + sub;
-  if (mkdir_p(sdir) != 0) throw CoralError(CORAL_EIO, "cannot create " + sdir);
-  const std::string fn = sdir + "/" + name;
-  FILE* fp = std::fopen(fn.c_str(), "wb");
-  if (!fp) throw CoralError(CORAL_EIO, "cannot open " + fn);
-  const size_t w = std::fwrite(buf.data(), sizeof(double), n, fp);
-  std::fclose(fp);
-  if (w != n) throw CoralError(CORAL_EIO, "short write in " + fn);
+  h->writer->submit(out, n, h->stream, sdir, sdir + "/" + name);
 }
 
 // output_slices_volumes_and_profiles (PL_IMEX_timestepping_marching.f90:639-697),
@@ -1846,6 +1991,7 @@ void run_loop(coral_handle* h, int nsteps, const char* outdir) {
   }
   if (outdir) flush_timeseries(h, outdir);
   else h->ts_rows.clear();
+  if (h->writer) h->writer->flush();  // the call's files are on disk when it returns
 }
 
 template <typename F>
@@ -1985,6 +2131,13 @@ void coral_destroy(coral_handle* h) {
   if (!h) return;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->writer) {
+    try {
+      h->writer->flush();
+    } catch (const CoralError&) {
+    }
+    h->writer.reset();
+  }
   if (h->graph) cudaGraphExecDestroy(h->graph);
   h->mem.free_all();
   if (h->h_pin) cudaFreeHost(h->h_pin);
@@ -2306,6 +2459,7 @@ int coral_export_usr_output(coral_handle* h, const char* output_directory, long 
     if (h->uo.empty()) return;
     h->launches += full_vars_to_phys(h, true, false);
     for (auto& o : h->uo) write_usr_object(h, o, time_integer, output_directory);
+    h->writer->flush();
   });
 }
 
