@@ -1950,7 +1950,22 @@ void usr_output_step(coral_handle* h, const char* dir) {
 // objects are recorded every step (time at the start of the step and the
 // values of its first stage) and written to <dir>/Timeseries every 20 steps
 // (buffer_length, PL_IMEX_timestepping.f90:159) and at the end.
+// A call that fails part way still waits for the files it queued, and their
+// errors go with it (the next call starts clean).
+struct DrainWriterOnThrow {
+  coral_handle* h;
+  bool done = false;
+  ~DrainWriterOnThrow() {
+    if (done || !h->writer) return;
+    try {
+      h->writer->flush();
+    } catch (const CoralError&) {
+    }
+  }
+};
+
 void run_loop(coral_handle* h, int nsteps, const char* outdir) {
+  DrainWriterOnThrow drain{h};
   if (nsteps < 0) throw CoralError(CORAL_EBADARG, "coral_run: nsteps must be >= 0");
   if (outdir && !*outdir) outdir = nullptr;  // an empty string (a Fortran c_null_char) means no output
   const Parameters& P = h->P;
@@ -1991,6 +2006,7 @@ void run_loop(coral_handle* h, int nsteps, const char* outdir) {
   }
   if (outdir) flush_timeseries(h, outdir);
   else h->ts_rows.clear();
+  drain.done = true;
   if (h->writer) h->writer->flush();  // the call's files are on disk when it returns
 }
 
@@ -2457,8 +2473,10 @@ int coral_export_usr_output(coral_handle* h, const char* output_directory, long 
   return guarded(h, [&] {
     if (!output_directory || !*output_directory) throw CoralError(CORAL_EBADARG, "null directory");
     if (h->uo.empty()) return;
+    DrainWriterOnThrow drain{h};
     h->launches += full_vars_to_phys(h, true, false);
     for (auto& o : h->uo) write_usr_object(h, o, time_integer, output_directory);
+    drain.done = true;
     h->writer->flush();
   });
 }

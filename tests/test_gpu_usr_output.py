@@ -124,3 +124,24 @@ def test_zsummed_quadratic_variable_is_refused():
         pl.set_usr_output(">>Slab :: uu ;; Period= 3 <<\n>>EOF<<\n")
     assert e.value.code == -6
     pl.close()
+
+
+def test_usr_output_write_failure_is_reported():
+    """The files are written by a host thread behind the step: a directory
+    that cannot be made (a plain file in its path) comes back from coral_run
+    as CORAL_EIO, and the handle keeps working (the next run into a good
+    directory writes its files)."""
+    from coral_b200.solver import CoralError, PlaneLayer
+    eq = equations("rbc_noslip_ra1e8", **{"1.d8": "1.d5"})
+    pl = PlaneLayer(eq, params(16, 12, 48, dt=1e-5))
+    pl.set_usr_output(">>Profile:: tFull ;; Period= 1 <<\n>>Volume :: tFull ;; Period= 1 <<\n>>EOF<<\n")
+    with tempfile.TemporaryDirectory() as d:
+        blocked = os.path.join(d, "blocked")
+        open(blocked, "w").close()
+        with pytest.raises(CoralError) as e:
+            pl.run(2, blocked)
+        assert e.value.code == -7, str(e.value)
+        good = os.path.join(d, "good")
+        pl.run(2, good)
+        assert len(_files(good)) == 4
+    pl.close()
