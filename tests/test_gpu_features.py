@@ -300,3 +300,36 @@ def test_dynamo_toroidal_poloidal_file_is_refused():
     with pytest.raises(CoralError) as e:
         PlaneLayer(_example("coral.equations.convective_dynamo.toroidalPoloidal"), params(16, 12, 24))
     assert e.value.code == -6 and "bad NL var definition" in str(e.value)
+
+
+def test_feature_recipes_under_every_kernel_variant():
+    """The autotuner's kernel variants on recipes with a penalisation field,
+    surface values and vertical decompositions, and the Smagorinsky viscosity, at
+    384 x 384 x 32 (x passes of length 576; the y-chunked pipeline runs its
+    per-band z operations and the fused z pass its given fields): bit for bit
+    the default step where the variant keeps the arithmetic, to 1e-10 (the
+    tolerance of the other feature tests: the penalisation term of strength 1e3
+    amplifies round-off) where it changes an FFT plan, band or tile form."""
+    from coral_b200.solver import PlaneLayer
+    from tests.test_gpu_timeloop import _variants_match
+    cases = [(_example("coral.equations.RBC_penalised"), None),
+             (_with_surface_vars(equations("rbc_noslip_ra1e5")), None),
+             (_with_smagorinsky_vars(equations("rbc_noslip_ra1e5")),
+              "--withHorizontalSmagorinsky --smagorinsky-prefactor 3.d0")]
+    par = params(384, 384, 32, dt=1e-6)
+    for eq, args in cases:
+        rng = np.random.default_rng(41)
+        state = {}
+
+        def make():
+            pl = PlaneLayer(eq, par, args=args)
+            if not state:
+                state["f"] = [1e-3 * (rng.standard_normal((pl.NXH, pl.NYAA, t)) +
+                                      1j * rng.standard_normal((pl.NXH, pl.NYAA, t))) for t in pl.T]
+                state["z"] = [1e-3 * rng.standard_normal(t) for t in pl.Tz]
+            for s, f in enumerate(state["f"]):
+                pl.set_field(s, f)
+            for s, z in enumerate(state["z"]):
+                pl.set_mean_field(s, z)
+            return pl
+        _variants_match(make, 2, 1e-6, tol=1e-10).close()

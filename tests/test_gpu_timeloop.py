@@ -218,7 +218,7 @@ KNOBS = ("z_pass", "inv_x_pass", "inv_y_pass", "band_factor", "y_pipeline", "x_f
 EXACT = ("z_pass", "inv_x_pass", "inv_y_pass", "band_factor", "y_pipeline")
 
 
-def _variants_match(make, steps, dt):
+def _variants_match(make, steps, dt, tol=1e-12):
     ref = make()
     ref.march_forward(dt, steps)
     want = ref.get_field(0)
@@ -230,7 +230,7 @@ def _variants_match(make, steps, dt):
         if knob in EXACT:
             assert np.array_equal(got, want), knob
         else:
-            assert _rel(got, want) < 1e-12, knob
+            assert _rel(got, want) < tol, knob
         pl.close()
     return ref
 
