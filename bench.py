@@ -41,6 +41,16 @@ CONFIGS = {
                           NX=32, NY=32, NZ=192, dt=1e-6, seed=2, Ra=1e8),
     "rrbc_192x192x96": dict(eq="rrbc_stressfree_ek1e-4_ra5e7.equations", par="rrbc_stressfree_192x192x96.parameters.in",
                             NX=192, NY=192, NZ=96, dt=5e-6, seed=1, Ra=5e7),
+    # the benchmark recipe with a penalised velocity (a mask field GAMMA, drag
+    # - GAMMA u) and with the horizontal Smagorinsky viscosity: the cost of those
+    # paths at full size
+    "rbc_penalised_384x384x192": dict(eq="rbc_penalised_ra1e8.equations",
+                                      par="rbc_noslip_ra1e8_384x384x192.parameters.in",
+                                      NX=384, NY=384, NZ=192, dt=1e-6, seed=2, Ra=1e8),
+    "rbc_smagorinsky_384x384x192": dict(eq="rbc_smagorinsky_ra1e8.equations",
+                                        par="rbc_noslip_ra1e8_384x384x192.parameters.in",
+                                        NX=384, NY=384, NZ=192, dt=1e-6, seed=2, Ra=1e8,
+                                        args="--withHorizontalSmagorinsky --smagorinsky-prefactor 0.1"),
 }
 METRIC = "timesteps/s at 384\u00b2\u00d7192 (FP64 vs split-prec TC) at stated err vs FP64 oracle"
 PHASES = ("inv_y", "inv_x", "inv_z", "z_products", "fwd_x", "fwd_y", "nl_assembly", "rhs_nl", "mean_systems",
@@ -319,7 +329,7 @@ def run_ours(args, cfg):
     torch.cuda.set_device(dev)
     eq = open(os.path.join(CONFIG_DIR, cfg["eq"])).read()
     par = open(os.path.join(CONFIG_DIR, cfg["par"])).read()
-    pl = PlaneLayer(eq, par, device=dev)
+    pl = PlaneLayer(eq, par, device=dev, args=cfg.get("args"))
     for v in args.variant:
         knob, val = v.split("=")
         pl.set_variant(knob, int(val))
@@ -571,8 +581,9 @@ class OracleSample:
         g = co.Geometry(p["NX"], p["NY"], p["NZ"], p["Lx"], p["Ly"], p["gap"], p["center"])
         self.g = g
         self.whole = g.NXH * g.NYAA <= 4096
+        smago = "--withHorizontalSmagorinsky" in (cfg.get("args") or "")
         if self.whole:
-            self.solver = co.Solver(eq, par)
+            self.solver = co.Solver(eq, par, smagorinsky=smago)
             self.solver.factorize(cfg["dt"])
             rng = np.random.default_rng(seed)
             for sidx, lay in enumerate(self.solver.lay):
@@ -581,7 +592,7 @@ class OracleSample:
             self.setup_s = time.perf_counter() - t0
             return
         s = co.Solver.__new__(co.Solver)
-        s.recipe = co.parse_equations(eq)
+        s.recipe = co.parse_equations(eq, smago)
         s.params = p
         s.g = g
         s.scheme = p["scheme"]

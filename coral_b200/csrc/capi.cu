@@ -1254,11 +1254,14 @@ int enqueue_stage_pre(coral_handle* h, int i, double dt, PhaseTimer* pt) {
     const bool smago_now = h->smago_var >= 0 && !h->closure;
     if (smago_now) {
       B(3);
-      launch_inv_z(d, h->nF, h->Y2, h->fphys, h->pz, h->dct_tw, h->d_wz, nullptr, h->stream);
+      // only the variables the viscosity is formed from
+      const size_t ystride = (size_t)d.NYA * d.NXA * d.NZ, pstride = (size_t)d.NYA * d.NXA * d.NZA;
+      for (int v : h->smago_src)
+        launch_inv_z(d, 1, h->Y2 + v * ystride, h->fphys + v * pstride, h->pz, h->dct_tw, h->d_wz, nullptr, h->stream);
       launch_smago(d, h->fphys, h->smago_src.data(), (int)h->smago_src.size(), h->smago_prefactor, h->smago_part,
                    h->smago_prof, last ? h->cfl_bits + 3 : nullptr, h->stream);
       E();
-      nl += 3;
+      nl += 2 + (int)h->smago_src.size();
     }
     // z passes fused (inverse DCT, CFL maxima, products, KE, forward DCT); the
     // quadratic variables overwrite Y2 in place, each CTA reading and writing only

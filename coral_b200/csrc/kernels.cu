@@ -3347,8 +3347,12 @@ void launch_rhs_nl(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
     if (!a.generic_tiles && a.NLg.valid && a.NLg.ngroups == 3 && a.Mw.width <= 4) {
       int w[3];
       group_widths(a.NLg, w);
-      // the plane-layer recipes' NL operator: groups i kx, i ky, 1 of widths 3, 3, 2
+      // the plane-layer recipes' NL operator: groups i kx, i ky, 1 of widths 3, 3, 2;
+      // with a penalisation drag (- Iz.Iz.Gu beside - Iz.uw) 3, 3, 5; with a
+      // second flux in each derivative group (an eddy-viscosity term) 6, 6, 2
       if (w[0] == 3 && w[1] == 3 && w[2] == 2) return launch_rhs_tiles<4, 8, 3, 3, 2>(a, n, s);
+      if (w[0] == 3 && w[1] == 3 && w[2] == 5) return launch_rhs_tiles<4, 11, 3, 3, 5>(a, n, s);
+      if (w[0] == 6 && w[1] == 6 && w[2] == 2) return launch_rhs_tiles<4, 14, 6, 6, 2>(a, n, s);
     }
     if (a.Mw.width <= 4 && a.NLw.width <= 8) return launch_rhs_tiles<4, 8>(a, n, s);
     if (a.Mw.width <= 8 && a.NLw.width <= 16) return launch_rhs_tiles<8, 16>(a, n, s);

@@ -333,3 +333,17 @@ def test_feature_recipes_under_every_kernel_variant():
                 pl.set_mean_field(s, z)
             return pl
         _variants_match(make, 2, 1e-6, tol=1e-10).close()
+
+
+@pytest.mark.parametrize("name,args,kw", [
+    ("rbc_penalised_ra1e8", None, {}),
+    ("rbc_smagorinsky_ra1e8", "--withHorizontalSmagorinsky --smagorinsky-prefactor 0.1",
+     dict(smagorinsky=True, smagorinsky_prefactor=0.1))])
+def test_feature_bench_recipes_match_oracle(name, args, kw):
+    """The recipes of the bench's penalised and Smagorinsky configurations
+    (their NL operators take the compiled tile forms of group widths 3, 3, 5
+    and 6, 6, 2) at 16 x 12 x 24: three steps against the oracle."""
+    eq = equations(name)
+    par = params(16, 12, 24, dt=1e-6)
+    ref, pl, errs = _run_both(eq, par, 3, 1e-6, args=args, oracle_kw=kw)
+    pl.close()
