@@ -2143,19 +2143,19 @@ __global__ void __launch_bounds__(kRhsThreads) k_rhs_nl(SolveArgs a, NLArgs n) {
     if (act) {
       // flat index idx = q NZ + nn, advanced without a division per element
       int q = threadIdx.x / NZ, nn = threadIdx.x - q * NZ;
-      for (int idx = threadIdx.x; idx < nqz; idx += kRhsThreads) {
+      for (int idx = threadIdx.x; idx < nqz; idx += blockDim.x) {
         qs[idx] = n.qspec[q * qstride + (size_t)sid * NZ + nn];
-        nn += kRhsThreads;
+        nn += blockDim.x;
         while (nn >= NZ) { nn -= NZ; ++q; }
       }
     }
     const double2* field = a.field + base;
-    for (int t = threadIdx.x; t < T; t += kRhsThreads) fs[t] = field[t];
+    for (int t = threadIdx.x; t < T; t += blockDim.x) fs[t] = field[t];
   }
   __syncthreads();
   const bool zero_out = a.last_stage && !act;
   bool bad = false;
-  for (int t = threadIdx.x; t < T; t += kRhsThreads) {
+  for (int t = threadIdx.x; t < T; t += blockDim.x) {
     double2 kh = zero2();
     if (act) {
       // slots in batches of 4 independent loads; slots are filled in order and
@@ -2242,11 +2242,11 @@ __global__ void __launch_bounds__(kRhsThreads) k_kstd_out(SolveArgs a) {
   const size_t base = (size_t)sid * T;
   {
     const double2* x = in_out ? a.out + base : a.work + (size_t)sid * a.wst;
-    for (int p = threadIdx.x; p < T; p += kRhsThreads) xs[p] = x[p];
+    for (int p = threadIdx.x; p < T; p += blockDim.x) xs[p] = x[p];
   }
   __syncthreads();
   bool bad = false;
-  for (int t = threadIdx.x; t < T; t += kRhsThreads) {
+  for (int t = threadIdx.x; t < T; t += blockDim.x) {
     if (!in_out) {
       const double2 v = xs[t];
       bad |= !(isfinite(v.x) && isfinite(v.y));
@@ -3342,6 +3342,9 @@ static void group_widths(const DevGEll& G, int w[3]) {
   for (int k = 0; k < G.width; ++k)
     if (G.slot_grp[k] < 3) ++w[G.slot_grp[k]];
 }
+// threads of a one-CTA-per-system kernel: one per row up to kRhsThreads (a
+// system of 64 rows takes 2 warps, not 8 of which 6 would idle)
+static int rows_threads(int T) { return std::min(kRhsThreads, std::max(32, (T + 31) / 32 * 32)); }
 void launch_rhs_nl(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
   if (a.work2 && a.rhs_win && a.row_pos) {
     if (!a.generic_tiles && a.NLg.valid && a.NLg.ngroups == 3 && a.Mw.width <= 4) {
@@ -3360,7 +3363,7 @@ void launch_rhs_nl(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
   const int nsys = a.d.NXH * a.d.NYA;
   const size_t sm = ((size_t)n.nq * a.d.NZ + a.T) * sizeof(double2);
   set_smem(k_rhs_nl, sm);
-  k_rhs_nl<<<nsys, kRhsThreads, sm, s>>>(a, n);
+  k_rhs_nl<<<nsys, rows_threads(a.T), sm, s>>>(a, n);
 }
 void launch_subst(const SolveArgs& a, cudaStream_t s) {
   if (a.nact <= 0) return;
@@ -3421,7 +3424,7 @@ void launch_kstd_out(const SolveArgs& a, cudaStream_t s) {
   }
   const size_t smx = (size_t)a.T * sizeof(double2);
   if (smx > 48 * 1024) set_smem(k_kstd_out, smx);
-  k_kstd_out<<<a.nact, kRhsThreads, smx, s>>>(a);
+  k_kstd_out<<<a.nact, rows_threads(a.T), smx, s>>>(a);
 }
 void launch_solve_real(const SolveArgs& a, const NLArgs& n, cudaStream_t s) {
   launch_rhs_nl(a, n, s);
